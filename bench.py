@@ -1,0 +1,493 @@
+#!/usr/bin/env python
+"""Benchmark: images/sec against a 100M-orientation DB on B200, batched vs plain.
+
+Workload (synthetic, seeded; the reference's 100MilOrients.bin and detector
+frames are not available): fcc a=3.52 A, the 1240 fcc-allowed HKLs with
+|h|,|k|,|l|<=8, a 2048x2048 detector of 0.2 mm pixels 500 mm downstream
+normal to the beam, 5-30 keV, MaxNrLaueSpots 30 -> 122-byte records.  The DB
+(100,000,000 Shoemake-uniform orientations, seed 1) is forward-simulated on
+the device by the DB-build kernel.  A step is one DB pass serving a batch of
+64 uint8 frames, each with a grain count drawn from U{1..20} (grains picked
+among DB orientations with >= MinNrSpots spots), Gaussian spots sigma 2 px,
+amplitude U(50,255), Poisson(5) background removed by a fixed threshold.
+
+  value   images/s of the batched pass with DB and images resident in HBM
+          (CUDA events on the engine stream; the 12.2 GB DB is larger than L2)
+  e2e     images/s through the public Python API from pinned host frames:
+          upload + quantise 64 frames, the pass, survivor download
+  plain   the same pass with one image (K=1)
+
+`--impl reference` times the reference's own LaueMatchingCPU (compiled from
+its sources into oracle/_ref/) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "images/sec vs 100M-orient DB, batched vs plain on 1 B200; p50/p99 latency"
+UNIT = "images/s"
+REC_BYTES_PER_ORIENT = 122  # uint16[1 + 2*30]
+
+
+def workload_params(min_intensity=200.0):
+    from lauematching_b200 import params as P, synth
+    txt = synth.params_text(max_nr_spots=30, min_nr_spots=5, min_intensity=min_intensity)
+    return txt, P.parse_params_text(txt)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def scratch_dir(need_bytes):
+    """/dev/shm when it has room (the reference memory-maps files there),
+    else the default temporary directory."""
+    try:
+        st = os.statvfs("/dev/shm")
+        if st.f_bavail * st.f_frsize > 1.5 * need_bytes:
+            return "/dev/shm"
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def make_images(e, p, batch, seed, scan=2_000_000):
+    from lauematching_b200 import synth
+    rng = np.random.default_rng(seed)
+    rec = e.download_db(0, min(scan, e.n_orient))
+    imgs = []
+    for _ in range(batch):
+        g = synth.pick_grains(rec, int(rng.integers(1, 21)), p.min_nr_spots, rng)
+        img = synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng)
+        imgs.append(img.astype(np.uint8))
+    return imgs, rec
+
+
+def dbbuild_parity_sample(e, p, hkls, seed, n_orient, per_block=20000, blocks=5):
+    """Records of the device-built DB against the oracle on sampled ID blocks."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    rng = np.random.default_rng(1234)
+    starts = sorted(set(int(x) for x in rng.integers(0, max(1, n_orient - per_block), blocks)))
+    mism = 0
+    total = 0
+    for s in starts:
+        cnt = min(per_block, n_orient - s)
+        om = e.synth_orientations(seed, s, cnt)
+        ref = O.forward(p, om, hkls)
+        got = e.download_db(s, cnt)
+        mism += int(np.count_nonzero(np.any(ref != got, axis=1)))
+        total += cnt
+    return {"sampled_orientations": total, "records_differing": mism}
+
+
+def cpu_baseline(e, p, txt, hkls, img_u8, seed, n_sample, runs=3):
+    """The reference LaueMatchingCPU (or the oracle port) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lauematching_b200 import formats
+    n_sample = min(n_sample, e.n_orient)
+    cores = os.cpu_count() or 1
+    rec = e.download_db(0, n_sample)
+    img = img_u8.astype(np.float64)
+    if O.have_ref():
+        base = scratch_dir(n_sample * (REC_BYTES_PER_ORIENT + 72))
+        wd = tempfile.mkdtemp(prefix="lmb_cpu_", dir=base)
+        fwd = os.path.join(wd, "fwd.bin")
+        rec.tofile(fwd)
+        om = e.synth_orientations(seed, 0, n_sample)
+        pp = os.path.join(wd, "params.txt")
+        with open(pp, "w") as f:
+            f.write(txt + f"ForwardFile {fwd}\nDoFwd 0\n")
+        op = os.path.join(wd, "orients.bin")
+        formats.write_orientations(op, om)
+        hp = os.path.join(wd, "hkls.csv")
+        formats.write_hkls(hp, hkls)
+        ip = os.path.join(wd, "image.bin")
+        formats.write_image_bin(ip, img)
+        times, walls = [], []
+        for _ in range(runs):
+            r = O.run_reference(pp, op, hp, ip, ncpus=cores)
+            if r.returncode != 0 or r.compare_seconds is None:
+                raise RuntimeError("reference run failed: " + r.stdout[-500:] + r.stderr[-500:])
+            times.append(r.compare_seconds)
+            walls.append(r.wall_seconds)
+        t = statistics.median(times)
+        for fn in os.listdir(wd):
+            os.remove(os.path.join(wd, fn))
+        os.rmdir(wd)
+        per_image = t * (1e8 / n_sample)
+        return {"value": 1.0 / per_image, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"LaueMatchingCPU DoFwd 0 compare stage on {n_sample} of the DB's "
+                          f"records (1 image), median of {runs} runs = {t:.4f} s, scaled x"
+                          f"{1e8 / n_sample:g} to the 1e8-orientation DB; whole-process wall "
+                          f"{statistics.median(walls):.2f} s per run"}
+    t0 = time.perf_counter()
+    for _ in range(runs):
+        O.compare(rec, p.max_nr_spots, img, p.nr_px_x, p.nr_px_y, p.min_nr_spots,
+                  p.min_intensity, nthreads=cores)
+    t = (time.perf_counter() - t0) / runs
+    per_image = t * (1e8 / n_sample)
+    return {"value": 1.0 / per_image, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle compare on {n_sample} records x {runs} runs, scaled to 1e8"}
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "compare_kernel_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+def run_ours(args, rank, world):
+    import torch
+    from lauematching_b200 import synth
+    from lauematching_b200.engine import Engine, PinnedBuffer
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    txt, p = workload_params(args.min_intensity)
+    hkls = synth.hkls_cubic(8)
+    N, K = args.n_orient, args.batch
+    e = Engine(p, device=dev)
+    t0 = time.perf_counter()
+    e.build_db_synthetic(seed=args.seed, n=N, hkls=hkls)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t0
+    log(f"[rank {rank}] DB built on device: {N} orientations in {t_build:.2f} s")
+    imgs, rec_head = make_images(e, p, K, seed=1000 + rank)
+    mean_spots = float(rec_head[:, 0].mean())
+    stream = torch.cuda.ExternalStream(e.stream)
+
+    # ---- resident batched pass ---------------------------------------------
+    for k in range(K):
+        e.load_image(k, imgs[k], want_scale=False)
+    slots = list(range(K))
+
+    def timed(nsteps, slot_list):
+        step_ms, cmp_ms = [], []
+        for _ in range(nsteps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e.match(slot_list, p.min_nr_spots, p.min_intensity)
+            b.record(stream)
+            b.synchronize()
+            step_ms.append(a.elapsed_time(b))
+            cmp_ms.append(e.last_pass_ms()[0])
+        return step_ms, cmp_ms
+
+    timed(args.warmup, slots)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    step_ms, cmp_ms = timed(args.steps, slots)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    clk = clocks.stop()
+    if dist:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        total_ms = float(tt.item())
+    value = world * K * args.steps / (total_ms / 1e3)
+    surv = [int(e.results(k)[0].shape[0]) for k in range(K)]
+
+    # ---- plain pass (one image) --------------------------------------------
+    timed(args.warmup, [0])
+    pstep, pcmp = timed(args.steps, [0])
+    plain_ips = 1e3 / statistics.mean(pstep)
+
+    # ---- end to end through the public API from pinned host frames ----------
+    pins = []
+    for k in range(K):
+        pb = PinnedBuffer((p.nr_px_x * p.nr_px_y,), np.uint8)
+        pb.array[:] = imgs[k]
+        pins.append(pb)
+    d2h = [0]
+
+    def e2e_step():
+        for k in range(K):
+            e.load_image(k, pins[k].array, want_scale=False)
+        e.match(slots, p.min_nr_spots, p.min_intensity)
+        nb = 0
+        for k in range(K):
+            r, _ = e.results(k)
+            nb += r.nbytes
+        d2h[0] = nb + (2 * 64 + 1) * 4
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    lat = []
+    te = time.perf_counter()
+    for _ in range(args.steps):
+        ts = time.perf_counter()
+        e2e_step()
+        lat.append((time.perf_counter() - ts) * 1e3)
+    e2e_s = time.perf_counter() - te
+    e2e_ips = world * K * args.steps / e2e_s
+    # plain e2e: one frame per step
+    platency = []
+    for i in range(args.warmup + args.steps):
+        ts = time.perf_counter()
+        e.load_image(0, pins[i % K].array, want_scale=False)
+        e.match([0], p.min_nr_spots, p.min_intensity)
+        e.results(0)
+        if i >= args.warmup:
+            platency.append((time.perf_counter() - ts) * 1e3)
+
+    # ---- roofline of the compare kernel ----------------------------------------
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    alg_bytes = N * REC_BYTES_PER_ORIENT + K * p.nr_px_x * p.nr_px_y
+    cmp_avg = statistics.mean(cmp_ms)
+    achieved = alg_bytes / (cmp_avg * 1e-3) / 1e9
+    tr = load_traffic()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_src,
+            "kernel": "compare_kernel",
+            "algorithmic_bytes_per_launch": alg_bytes,
+            "avg_launch_ms": round(cmp_avg, 4),
+            "traffic": tr.get("bytes_per_launch_scaled") if tr else None}
+    if tr:
+        roof["traffic_source"] = tr.get("source")
+
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"batched DB pass: {K} uint8 2048x2048 frames (U{{1..20}} fcc "
+                               f"grains each) vs a {N:,}-orientation device-resident DB",
+                   "n_orient": N, "batch": K, "detector": [p.nr_px_x, p.nr_px_y],
+                   "max_nr_spots": p.max_nr_spots, "record_bytes": REC_BYTES_PER_ORIENT,
+                   "hkls": int(len(hkls)), "mean_spots_per_orientation": round(mean_spots, 3),
+                   "min_nr_spots": p.min_nr_spots, "min_intensity": p.min_intensity,
+                   "l2": "inputs larger than L2 (12.2 GB DB streamed every pass)",
+                   "parallelism": f"replicas x{world} (images split, DB replicated)"},
+        "roofline": roof,
+        "e2e": {"value": round(e2e_ips, 2), "unit": UNIT,
+                "h2d_bytes_per_step": K * p.nr_px_x * p.nr_px_y,
+                "d2h_bytes_per_step": d2h[0],
+                "path": "Engine.load_image x64 (pinned uint8) + Engine.match + Engine.results x64"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+        "latency_ms": {"batched_p50": round(float(np.percentile(lat, 50)), 3),
+                       "batched_p99": round(float(np.percentile(lat, 99)), 3),
+                       "plain_p50": round(float(np.percentile(platency, 50)), 3),
+                       "plain_p99": round(float(np.percentile(platency, 99)), 3)},
+        "plain": {"value": round(plain_ips, 2), "unit": UNIT,
+                  "e2e": round(1e3 / statistics.mean(platency), 2),
+                  "compare_ms": round(statistics.mean(pcmp), 4)},
+        "batched_over_plain": round(value / world / plain_ips, 2),
+        "survivors_per_image": {"min": min(surv), "max": max(surv), "mean": statistics.mean(surv)},
+        "dbbuild": {"orientations_per_s": round(N / t_build, 1), "seconds": round(t_build, 3),
+                    "hkl_evals_per_s": round(N * len(hkls) / t_build, 1)},
+    }
+    if rank == 0 and world == 1 and not args.no_parity:
+        out["dbbuild"]["parity"] = dbbuild_parity_sample(e, p, hkls, args.seed, N)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(e, p, txt, hkls, imgs[0], args.seed, args.cpu_sample)
+    for pb in pins:
+        pb.free()
+    e.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU executable on the box's host cores
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lauematching_b200 import formats, synth
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/LaueMatchingCPU was not built (reference sources absent "
+                          "when the repository was built)"}))
+        return
+    txt, p = workload_params(args.min_intensity)
+    hkls = synth.hkls_cubic(8)
+    n_s = args.cpu_sample
+    cores = os.cpu_count() or 1
+    base = scratch_dir(n_s * (REC_BYTES_PER_ORIENT + 72))
+    wd = tempfile.mkdtemp(prefix="lmb_ref_", dir=base)
+    fwd = os.path.join(wd, "fwd.bin")
+    om = synth.shoemake_orientations(n_s, seed=args.seed)
+    op = os.path.join(wd, "orients.bin")
+    formats.write_orientations(op, om)
+    hp = os.path.join(wd, "hkls.csv")
+    formats.write_hkls(hp, hkls)
+    # the reference builds the sample's forward cache itself (DoFwd 1)
+    ip = os.path.join(wd, "image.bin")
+    formats.write_image_bin(ip, np.zeros(p.nr_px_x * p.nr_px_y))
+    pp = os.path.join(wd, "params.txt")
+    with open(pp, "w") as f:
+        f.write(txt + f"ForwardFile {fwd}\nDoFwd 1\n")
+    rb = O.run_reference(pp, op, hp, ip, ncpus=cores)
+    if rb.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": "reference DoFwd 1 run failed: "
+                          + (rb.stderr or rb.stdout)[-200:].replace("\n", " ")}))
+        return
+    rec = np.fromfile(fwd, np.uint16).reshape(n_s, 61)
+    rng = np.random.default_rng(1000)
+    imgs = []
+    for _ in range(max(1, min(args.batch, 8))):
+        g = synth.pick_grains(rec, int(rng.integers(1, 21)), p.min_nr_spots, rng)
+        imgs.append(synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng))
+    with open(pp, "w") as f:
+        f.write(txt + f"ForwardFile {fwd}\nDoFwd 0\n")
+    times, walls = [], []
+    for i in range(args.warmup + args.steps):
+        formats.write_image_bin(ip, imgs[i % len(imgs)])
+        r = O.run_reference(pp, op, hp, ip, ncpus=cores)
+        if r.returncode != 0 or r.compare_seconds is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
+            return
+        if i >= args.warmup:
+            times.append(r.compare_seconds)
+            walls.append(r.wall_seconds)
+    for fn in os.listdir(wd):
+        os.remove(os.path.join(wd, fn))
+    os.rmdir(wd)
+    scale = 1e8 / n_s
+    per_img = statistics.mean(times) * scale
+    value = 1.0 / per_img
+    sample = (f"LaueMatchingCPU (reference source, gcc -O3 -fopenmp, NLopt stand-in) DoFwd 0 "
+              f"compare stage on a {n_s}-orientation sample of the workload, 1 image per run, "
+              f"mean of {args.steps} runs = {statistics.mean(times):.4f} s, scaled x{scale:g} "
+              f"to the 1e8-orientation DB; whole-process wall {statistics.mean(walls):.2f} s per "
+              f"run; sample DB built by the reference (DoFwd 1) in {rb.compare_seconds:.2f} s")
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(per_img * 1e3, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+           "config": {"workload": f"plain single-image compare vs a 100,000,000-orientation DB "
+                                  f"(sampled: {n_s})", "n_orient": 100_000_000,
+                      "max_nr_spots": 30, "hkls": int(len(hkls))},
+           "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores,
+                            "kind": "reference", "sample": sample},
+           "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0},
+           "dbbuild_reference": {"orientations_per_s": round(n_s / rb.compare_seconds, 1),
+                                 "sample": n_s}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n-orient", type=int, default=100_000_000)
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--min-intensity", type=float, default=200.0)
+    ap.add_argument("--cpu-sample", type=int, default=10_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

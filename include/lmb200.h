@@ -1,0 +1,172 @@
+/*
+ * lmb200.h -- C ABI of the B200 orientation-matching library (liblmb200.so).
+ *
+ * The reference LaueMatching has no library interface: its hot path lives
+ * inside three executables (src/LaueMatchingCPU.c, src/LaueMatchingGPU.cu,
+ * src/LaueMatchingGPUStream.cu) that callers drive through argv and files.
+ * Each entry point below replaces one piece of that code path; its comment
+ * names the reference lines it replaces.  A binding for ctypes, cgo or any
+ * other FFI needs only this header: plain C types, opaque handles, int status.
+ *
+ * Conventions
+ *   - Every call returns LMB_OK (0) or a negative LMB_ERR_* code; the message
+ *     of the last failure on the calling thread is in lmb_last_error().
+ *   - The caller owns every host buffer; an engine owns its device buffers.
+ *   - Calls on one engine are not re-entrant: serialise them per engine.
+ *   - Record layout: uint16[1 + 2*S] = {count, x0, y0, x1, y1, ...}, zero
+ *     padded, S = MaxNrLaueSpots (LaueMatchingCPU.c:488-495).
+ *   - Pixel (x, y) of a row-major image is element y*NrPxX + x
+ *     (LaueMatchingCPU.c:676).
+ */
+#ifndef LMB200_H
+#define LMB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LMB_OK 0
+#define LMB_ERR_INVALID (-1)  /* bad argument or state */
+#define LMB_ERR_CUDA (-2)     /* CUDA runtime failure (message has details) */
+#define LMB_ERR_OOM (-3)      /* device or pinned host allocation failed */
+#define LMB_ERR_OVERFLOW (-4) /* a survivor list exceeded its capacity */
+#define LMB_ERR_TIMEOUT (-5)  /* a bounded device wait gave up */
+
+#define LMB_MAX_SLOTS 64 /* images one DB pass can serve */
+
+/* Image pixel types accepted by lmb_image_load. */
+#define LMB_F64 0 /* raw float64, the .bin image of the LaueMatchingGPU CLI */
+#define LMB_F32 1 /* float32, the TCP wire payload of LaueMatchingGPUStream */
+#define LMB_U8 2  /* uint8 frame (values taken as float64, then quantised) */
+
+/* Intensity sources of a compare pass. */
+#define LMB_VALUE_U8 0  /* uint8 image x imScale (LaueMatchingCPU.c:668-682) */
+#define LMB_VALUE_F64 1 /* float64 image (the DoFwd 1 path, :649-653) */
+
+/* Detector / crystal geometry, all FP64, built by lmb_geometry_init. */
+typedef struct lmb_geometry {
+  double recip[9];   /* reciprocal basis, row-major */
+  double rot_t[9];   /* transpose of the detector rotation, row-major */
+  double p[3];       /* P_Array (m) */
+  double px_x, px_y; /* pixel pitch (m) */
+  double elo, ehi;   /* energy band (keV) */
+  int32_t nr_px_x, nr_px_y;
+  int32_t max_nr_spots; /* S */
+  int32_t reserved;
+} lmb_geometry;
+
+/* One matched orientation of one image. */
+typedef struct lmb_survivor {
+  uint64_t id;     /* orientation row number */
+  int32_t n_spots; /* spots landing on a positive pixel */
+  int32_t sum_u8;  /* sum of their uint8 values */
+  double tot_int;  /* FP64 intensity sum in record order (the reference's totInt) */
+  double score;    /* tot_int * sqrt(n_spots) (LaueMatchingCPU.c:688) */
+} lmb_survivor;
+
+typedef struct lmb_engine lmb_engine;
+
+/* Library version and the last error message of the calling thread. */
+const char *lmb_version(void);
+const char *lmb_last_error(void);
+
+/* Detector rotation (Rodrigues of R_Array, LaueMatchingCPU.c:225-239) and the
+ * reciprocal basis (calcRecipArray, LaueMatchingHeaders.h:379-436), FP64 in
+ * the reference's operation order.  R_Array = (0,0,0) gives NaN, as in the
+ * reference. */
+int lmb_geometry_init(const double lattice[6], int32_t space_group,
+                      const double p_array[3], const double r_array[3],
+                      double px_x, double px_y, int32_t nr_px_x,
+                      int32_t nr_px_y, double elo, double ehi,
+                      int32_t max_nr_spots, lmb_geometry *out);
+
+/* Engine: one device, one geometry, one resident DB, LMB_MAX_SLOTS image
+ * slots.  Replaces the device set-up of LaueMatchingGPU.cu:416,665-712 and
+ * LaueMatchingGPUStream.cu:998-1075.  survivor_capacity is the per-image
+ * survivor buffer (0 = default 262144; the reference caps at 100000 and
+ * truncates silently, LaueMatchingGPU.cu:43,754-760). */
+int lmb_engine_create(int32_t device, const lmb_geometry *geo,
+                      uint64_t survivor_capacity, lmb_engine **out);
+int lmb_engine_destroy(lmb_engine *e);
+/* cudaStream_t of the engine's compare pass (for external event timing). */
+void *lmb_engine_stream(lmb_engine *e);
+
+/* Upload a forward cache (n records of 1+2S uint16) into device memory.
+ * Replaces the chunked synchronous H2D of LaueMatchingGPU.cu:619-749 and
+ * the resident upload of LaueMatchingGPUStream.cu:998-1038. */
+int lmb_db_upload(lmb_engine *e, const uint16_t *records, uint64_t n);
+
+/* Forward-simulate the DB on the device from n orientation matrices
+ * (row-major 3x3 FP64 each) and nh HKLs (int32 triplets, file order).
+ * Replaces the OpenMP forward simulation of LaueMatchingCPU.c:595-667
+ * (duplicated at LaueMatchingGPU.cu:478-614, LaueMatchingGPUStream.cu:854-946).
+ * Records are identical to the reference's. */
+int lmb_db_build(lmb_engine *e, const double *orients, uint64_t n,
+                 const int32_t *hkls, int32_t nh);
+
+/* lmb_db_build with flags.  LMB_BUILD_EXACT_FP64 skips the FP32 screen and
+ * evaluates every (orientation, HKL) pair in FP64 (a self-check of the
+ * screen; same records, slower). */
+#define LMB_BUILD_EXACT_FP64 1
+int lmb_db_build_ex(lmb_engine *e, const double *orients, uint64_t n,
+                    const int32_t *hkls, int32_t nh, uint32_t flags);
+
+/* Same, with orientations generated on the device: uniform random rotations
+ * (Shoemake's method) from the counter-based generator keyed by seed, IDs
+ * first..first+n-1.  If orients_out is not NULL the matrices are copied to it
+ * (n*9 doubles).  For synthetic workloads. */
+int lmb_db_build_synthetic(lmb_engine *e, uint64_t seed, uint64_t n,
+                           const int32_t *hkls, int32_t nh, double *orients_out);
+
+/* The orientation matrices IDs first..first+n-1 of the synthetic generator
+ * above (n*9 doubles to out), bitwise the ones lmb_db_build_synthetic used. */
+int lmb_synth_orientations(lmb_engine *e, uint64_t seed, uint64_t first,
+                           uint64_t n, double *out);
+
+/* Copy records [first, first+count) of the resident DB to the host (to write
+ * the ForwardFile, LaueMatchingCPU.c:694-711). */
+int lmb_db_download(lmb_engine *e, uint64_t first, uint64_t count,
+                    uint16_t *out);
+int lmb_db_info(lmb_engine *e, uint64_t *n_orient, int32_t *max_nr_spots);
+
+/* Load one image (NrPxX*NrPxY pixels of dtype LMB_F64 or LMB_F32) into a
+ * slot: host->device copy, uint8 quantisation exactly as
+ * LaueMatchingCPU.c:356-375 (imScale returned), occupancy-bit update.
+ * keep_f64 keeps the float64 copy for LMB_VALUE_F64 passes. */
+int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels,
+                   int32_t dtype, int32_t keep_f64, double *im_scale);
+
+/* One DB pass over every slot in slot_mask: the compare of
+ * LaueMatchingCPU.c:668-690 (replacing the compare kernels
+ * LaueMatchingGPU.cu:45-81 and LaueMatchingGPUStream.cu:69-100), survivor
+ * compaction and ordering by ID (LaueMatchingCPU.c:781-788).  Asynchronous:
+ * results are read with lmb_results. */
+int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots,
+              double min_intensity, int32_t value_mode);
+
+/* Wait for the last pass and copy one slot's survivors (ascending id).
+ * n_survivors receives the full count; n_pass the reference's nrResults
+ * (LaueMatchingCPU.c:686).  Returns LMB_ERR_OVERFLOW when the count exceeded
+ * the engine's survivor capacity (the first capacity survivors by ID are
+ * then not guaranteed: recreate the engine with a larger capacity). */
+int lmb_results(lmb_engine *e, int32_t slot, lmb_survivor *out,
+                uint64_t out_capacity, uint64_t *n_survivors, uint64_t *n_pass);
+
+/* Device time of the last pass in milliseconds (CUDA events on the engine
+ * stream): compare kernel, ordering kernel. */
+int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms);
+
+/* Page-locked host buffers, so image uploads run at full link speed.  No
+ * reference counterpart (the reference pins per-stream buffers internally,
+ * LaueMatchingGPUStream.cu:1041-1075). */
+int lmb_host_alloc(uint64_t bytes, void **out);
+int lmb_host_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LMB200_H */

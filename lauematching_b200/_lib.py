@@ -1,0 +1,110 @@
+"""ctypes binding of liblmb200.so (the C ABI declared in include/lmb200.h).
+
+The library is loaded from this package directory.  There is no CPU
+fallback: if the shared library is missing or no CUDA device is usable, the
+calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblmb200.so")
+
+LMB_OK = 0
+LMB_ERR_INVALID = -1
+LMB_ERR_CUDA = -2
+LMB_ERR_OOM = -3
+LMB_ERR_OVERFLOW = -4
+LMB_ERR_TIMEOUT = -5
+LMB_MAX_SLOTS = 64
+LMB_F64, LMB_F32, LMB_U8 = 0, 1, 2
+LMB_VALUE_U8, LMB_VALUE_F64 = 0, 1
+LMB_BUILD_EXACT_FP64 = 1
+
+# Every function the header declares (checked by the CPU test suite).
+EXPORTS = [
+    "lmb_version", "lmb_last_error", "lmb_geometry_init", "lmb_engine_create",
+    "lmb_engine_destroy", "lmb_engine_stream", "lmb_db_upload", "lmb_db_build",
+    "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
+    "lmb_match", "lmb_results", "lmb_last_pass_ms", "lmb_host_alloc", "lmb_host_free",
+]
+
+
+class LmbGeometry(C.Structure):
+    _fields_ = [
+        ("recip", C.c_double * 9), ("rot_t", C.c_double * 9), ("p", C.c_double * 3),
+        ("px_x", C.c_double), ("px_y", C.c_double), ("elo", C.c_double), ("ehi", C.c_double),
+        ("nr_px_x", C.c_int32), ("nr_px_y", C.c_int32), ("max_nr_spots", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class LmbSurvivor(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("n_spots", C.c_int32), ("sum_u8", C.c_int32),
+                ("tot_int", C.c_double), ("score", C.c_double)]
+
+
+class LmbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"lmb200 error {code}: {msg}")
+        self.code = code
+
+
+class OverflowError_(LmbError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load liblmb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m lauematching_b200.build` "
+            "(the B200 library has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, u64, i32, dbl = C.c_void_p, C.c_uint64, C.c_int32, C.c_double
+    dp = C.POINTER(C.c_double)
+    sig = {
+        "lmb_version": ([], C.c_char_p),
+        "lmb_last_error": ([], C.c_char_p),
+        "lmb_geometry_init": ([dp, i32, dp, dp, dbl, dbl, i32, i32, dbl, dbl, i32,
+                               C.POINTER(LmbGeometry)], C.c_int),
+        "lmb_engine_create": ([i32, C.POINTER(LmbGeometry), u64, C.POINTER(vp)], C.c_int),
+        "lmb_engine_destroy": ([vp], C.c_int),
+        "lmb_engine_stream": ([vp], vp),
+        "lmb_db_upload": ([vp, vp, u64], C.c_int),
+        "lmb_db_build": ([vp, vp, u64, vp, i32], C.c_int),
+        "lmb_db_build_ex": ([vp, vp, u64, vp, i32, C.c_uint32], C.c_int),
+        "lmb_db_build_synthetic": ([vp, u64, u64, vp, i32, vp], C.c_int),
+        "lmb_synth_orientations": ([vp, u64, u64, u64, vp], C.c_int),
+        "lmb_db_download": ([vp, u64, u64, vp], C.c_int),
+        "lmb_db_info": ([vp, C.POINTER(u64), C.POINTER(i32)], C.c_int),
+        "lmb_image_load": ([vp, i32, vp, i32, i32, dp], C.c_int),
+        "lmb_match": ([vp, u64, i32, dbl, i32], C.c_int),
+        "lmb_results": ([vp, i32, vp, u64, C.POINTER(u64), C.POINTER(u64)], C.c_int),
+        "lmb_last_pass_ms": ([vp, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+        "lmb_host_alloc": ([u64, C.POINTER(vp)], C.c_int),
+        "lmb_host_free": ([vp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(rc: int) -> int:
+    if rc != LMB_OK:
+        msg = lib().lmb_last_error().decode(errors="replace")
+        if rc == LMB_ERR_OVERFLOW:
+            raise OverflowError_(rc, msg)
+        raise LmbError(rc, msg)
+    return rc

@@ -1,0 +1,387 @@
+// Compare pass: image quantisation, the batched DB pass, survivor ordering.
+//
+// Quantisation restates LaueMatchingCPU.c:345-375.  The compare restates
+// LaueMatchingCPU.c:668-690 and replaces the reference's compare kernels
+// (LaueMatchingGPU.cu:45-81, LaueMatchingGPUStream.cu:69-100); survivors are
+// delivered in ascending orientation ID like LaueMatchingCPU.c:781-788.
+//
+// Batched pass.  Up to 64 images ("slots") are matched in one pass over the
+// DB.  For every pixel the occupancy word holds bit k set when slot k's
+// uint8 pixel is positive, so one 8-byte gather per spot gives the hit/miss
+// of that spot in every image at once; per-slot spot counts are kept as
+// bit-sliced counters (bit b of all 64 counters in one word).  Only an
+// orientation whose count reaches MinNrSpots in some slot ("candidate") goes
+// back over its spots to sum the intensity of that slot in FP64, in record
+// order, exactly as the reference does; candidates are rare, so the DB
+// stream and the 8-byte gathers are the cost.
+//
+// DB stream.  A persistent grid walks tiles of TILE consecutive records;
+// tile bytes are moved into shared memory by 1-D TMA bulk copies
+// (cp.async.bulk) through a STAGES-deep mbarrier ring, so the stream is
+// coalesced regardless of the 122-byte record stride.  Waits are bounded
+// (2 s of global time) and report through an error word.
+#include <climits>
+
+#include "kernels.cuh"
+
+namespace lmb {
+
+// ----------------------------------------------------------------------------
+// Quantisation: max of the positive pixels, then uint8 + occupancy bit.
+// ----------------------------------------------------------------------------
+template <typename T>
+__global__ void quant_max_kernel(const T *__restrict__ img, size_t npx,
+                                 unsigned long long *__restrict__ max_bits) {
+  double m = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npx;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double v = (double)img[i];
+    if (v > m) m = v;  // NaN never compares greater (LaueMatchingCPU.c:357-359)
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double sm[32];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = (threadIdx.x < (blockDim.x >> 5)) ? sm[threadIdx.x] : 0.0;
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    // non-negative doubles order like their bit patterns
+    if (threadIdx.x == 0 && m > 0.0) atomicMax(max_bits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// u8 = v>=255 ? 255 : v<1 ? 1 : (uint8)v  with v = pixel * (255/max), for
+// positive pixels; 0 otherwise (LaueMatchingCPU.c:367-375).
+template <typename T>
+__global__ void quant_u8_kernel(const T *__restrict__ img, size_t npx,
+                                const unsigned long long *__restrict__ max_bits,
+                                uint8_t *__restrict__ u8, double *__restrict__ f64_keep,
+                                unsigned long long *__restrict__ occ, unsigned long long bit,
+                                double *__restrict__ scale_out) {
+  const double mx = __longlong_as_double((long long)*max_bits);
+  const double inv = (mx > 0) ? ddiv(255.0, mx) : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = (mx > 0) ? ddiv(mx, 255.0) : 1.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npx;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double x = (double)img[i];
+    uint8_t q = 0;
+    if (x > 0) {
+      const double v = dmul(x, inv);
+      // (uint8_t)v of a double: x86 converts via a 32-bit cvttsd2si (NaN -> 0)
+      q = (v >= 255.0) ? 255 : (v < 1.0) ? 1 : (uint8_t)(x86_trunc_i32(v) & 0xFF);
+    }
+    u8[i] = q;
+    if (f64_keep) f64_keep[i] = x;
+    const unsigned long long w = occ[i];
+    occ[i] = q ? (w | bit) : (w & ~bit);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// The DB pass.
+// ----------------------------------------------------------------------------
+
+
+static constexpr uint64_t kWaitNs = 2000000000ull;  // bounded TMA waits: 2 s
+
+// Intensity of slot k over one record, in record order (LaueMatchingCPU.c:671-681
+// for the uint8 image; :649-653 for the float64 image).
+__device__ __noinline__ void candidate(const CmpArgs &a, const uint16_t *rec, int c, uint64_t oid,
+                                       int k) {
+  const uint8_t *img = a.u8 + (size_t)k * a.npx;
+  const double *fim = a.f64 ? a.f64 + (size_t)k * a.npx : nullptr;
+  const double sc = a.scale[k];
+  int ns = 0, su = 0;
+  double tot = 0.0;
+  for (int s = 0; s < c; s++) {
+    const int x = rec[1 + 2 * s], y = rec[2 + 2 * s];
+    if (x >= a.W || y >= a.H) continue;
+    const size_t p = (size_t)y * a.W + x;
+    const uint8_t raw = img[p];
+    if (a.mode == LMB_VALUE_U8) {
+      if (raw > 0) {
+        tot = dadd(tot, dmul((double)raw, sc));
+        ns++;
+        su += raw;
+      }
+    } else {
+      const double v = fim[p];
+      if (v > 0) {
+        tot = dadd(tot, v);
+        ns++;
+        su += raw;
+      }
+    }
+  }
+  if (ns >= a.min_spots && tot >= a.min_int) {
+    atomicAdd(&a.pass_cnt[k], 1u);
+    const double score = dmul(tot, dsqrt((double)ns));
+    if (score != 0.0) {  // collection skips zero scores (LaueMatchingCPU.c:783)
+      const unsigned int pos = atomicAdd(&a.surv_cnt[k], 1u);
+      if (pos < a.cap) {
+        lmb_survivor sv;
+        sv.id = oid;
+        sv.n_spots = ns;
+        sv.sum_u8 = su;
+        sv.tot_int = tot;
+        sv.score = score;
+        a.surv[(size_t)k * a.cap + pos] = sv;
+      }
+    }
+  }
+}
+
+template <int B>
+__device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, uint64_t oid) {
+  int c = rec[0];
+  if (c > a.S) c = a.S;  // clamp like LaueMatchingGPU.cu:54-55
+  unsigned long long cnt[B];
+#pragma unroll
+  for (int b = 0; b < B; b++) cnt[b] = 0ull;
+  // gathers issued four at a time so their L2 latencies overlap
+  for (int s0 = 0; s0 < c; s0 += 4) {
+    unsigned long long m[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      m[j] = 0ull;
+      const int s = s0 + j;
+      if (s < c) {
+        const int x = rec[1 + 2 * s], y = rec[2 + 2 * s];
+        if (x < a.W && y < a.H)  // skip like LaueMatchingGPU.cu:65
+          m[j] = __ldg(a.occ + (size_t)y * a.W + x);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      unsigned long long v = m[j] & a.active;
+      if (v) {
+#pragma unroll
+        for (int b = 0; b < B; b++) {
+          const unsigned long long t = cnt[b] & v;
+          cnt[b] ^= v;
+          v = t;
+        }
+      }
+    }
+  }
+  // count >= min_spots, bit-sliced, from the most significant bit down
+  unsigned long long gt = 0ull, eq = ~0ull;
+#pragma unroll
+  for (int b = B - 1; b >= 0; b--) {
+    if ((a.min_spots >> b) & 1) {
+      eq &= cnt[b];
+    } else {
+      gt |= eq & cnt[b];
+      eq &= ~cnt[b];
+    }
+  }
+  unsigned long long cand = (gt | eq) & a.active;
+  while (cand) {
+    const int k = __ffsll((long long)cand) - 1;
+    cand &= cand - 1;
+    candidate(a, rec, c, oid, k);
+  }
+}
+
+template <int B>
+__global__ void __launch_bounds__(256) compare_kernel(const __grid_constant__ CmpArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  unsigned char *ring = smem + 128;
+  const uint32_t TILE = blockDim.x;
+  const uint64_t G = gridDim.x;
+  const int stages = a.stages;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < stages; s++) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < stages; s++) {
+      const uint64_t tile = blockIdx.x + (uint64_t)s * G;
+      if (tile < a.full_tiles) {
+        mbar_expect_tx(&bars[s], a.tile_bytes);
+        bulk_g2s(ring + (size_t)s * a.tile_bytes,
+                 reinterpret_cast<const unsigned char *>(a.db) + tile * a.tile_bytes,
+                 a.tile_bytes, &bars[s]);
+      }
+    }
+  }
+  uint64_t it = 0;
+  for (uint64_t tile = blockIdx.x; tile < a.ntiles; tile += G, ++it) {
+    const int s = (int)(it % stages);
+    const uint32_t parity = (uint32_t)((it / stages) & 1);
+    const uint64_t oid = tile * TILE + threadIdx.x;
+    if (tile < a.full_tiles) {
+      const bool ok = mbar_wait_bounded(&bars[s], parity, kWaitNs);
+      if (__syncthreads_or(!ok)) {  // block-uniform give-up
+        if (threadIdx.x == 0) {
+          atomicExch(a.err, DEV_TIMEOUT_TMA);
+          // let every copy this block still has in flight land before leaving
+          for (int d = 0; d < stages; d++) {
+            const uint64_t it2 = it + (uint64_t)d;
+            if (blockIdx.x + it2 * G < a.full_tiles)
+              mbar_wait_bounded(&bars[it2 % stages], (uint32_t)((it2 / stages) & 1), kWaitNs);
+          }
+        }
+        return;
+      }
+      const uint16_t *rec = reinterpret_cast<const uint16_t *>(ring + (size_t)s * a.tile_bytes) +
+                            (size_t)threadIdx.x * a.R;
+      process<B>(a, rec, oid);
+    } else if (oid < a.n) {
+      process<B>(a, a.db + oid * a.R, oid);  // partial last tile: direct loads
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint64_t nt = tile + (uint64_t)stages * G;
+      if (nt < a.full_tiles) {
+        mbar_expect_tx(&bars[s], a.tile_bytes);
+        bulk_g2s(ring + (size_t)s * a.tile_bytes,
+                 reinterpret_cast<const unsigned char *>(a.db) + nt * a.tile_bytes, a.tile_bytes,
+                 &bars[s]);
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Ordering: per slot, sort survivors by ID (keys id<<24 | index), bitonic.
+// ----------------------------------------------------------------------------
+
+
+static constexpr uint32_t kSmemSortMax = 8192;
+
+__device__ __forceinline__ void bitonic(unsigned long long *keys, uint32_t P) {
+  for (uint32_t size = 2; size <= P; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      for (uint32_t i = threadIdx.x; i < (P >> 1); i += blockDim.x) {
+        const uint32_t lo = 2 * i - (i & (stride - 1));
+        const uint32_t hi = lo + stride;
+        const bool asc = (lo & size) == 0;
+        const unsigned long long x = keys[lo], y = keys[hi];
+        if ((x > y) == asc) {
+          keys[lo] = y;
+          keys[hi] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) order_kernel(OrderArgs a) {
+  extern __shared__ __align__(16) unsigned long long sk[];  // kSmemSortMax keys
+  const int k = a.slots[blockIdx.x];
+  const uint32_t n = min(a.surv_cnt[k], a.cap);
+  if (n == 0) return;
+  uint32_t P = 1;
+  while (P < n) P <<= 1;
+  unsigned long long *keys = (P <= kSmemSortMax) ? sk : a.scratch + (size_t)k * a.cap2;
+  const lmb_survivor *src = a.surv + (size_t)k * a.cap;
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
+    keys[i] = (i < n) ? ((src[i].id << 24) | i) : ~0ull;
+  __syncthreads();
+  bitonic(keys, P);
+  lmb_survivor *dst = a.out + (size_t)k * a.cap;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[keys[i] & 0xFFFFFFull];
+}
+
+// ----------------------------------------------------------------------------
+// Launchers
+// ----------------------------------------------------------------------------
+int quantize_launch(const void *d_img, int dtype, size_t npx, unsigned long long *d_max_bits,
+                    uint8_t *d_u8, double *d_f64_keep, unsigned long long *d_occ, int slot,
+                    double *d_scale_slot, int num_sms, cudaStream_t st) {
+  LMB_CUDA(cudaMemsetAsync(d_max_bits, 0, sizeof(unsigned long long), st));
+  const unsigned blocks = (unsigned)std::min<size_t>((npx + 255) / 256, (size_t)num_sms * 8);
+  const unsigned long long bit = 1ull << slot;
+  if (dtype == LMB_F64) {
+    const double *p = static_cast<const double *>(d_img);
+    quant_max_kernel<double><<<blocks, 256, 0, st>>>(p, npx, d_max_bits);
+    quant_u8_kernel<double><<<blocks, 256, 0, st>>>(p, npx, d_max_bits, d_u8, d_f64_keep, d_occ,
+                                                     bit, d_scale_slot);
+  } else if (dtype == LMB_F32) {
+    const float *p = static_cast<const float *>(d_img);
+    quant_max_kernel<float><<<blocks, 256, 0, st>>>(p, npx, d_max_bits);
+    quant_u8_kernel<float><<<blocks, 256, 0, st>>>(p, npx, d_max_bits, d_u8, d_f64_keep, d_occ,
+                                                    bit, d_scale_slot);
+  } else {
+    const uint8_t *p = static_cast<const uint8_t *>(d_img);
+    quant_max_kernel<uint8_t><<<blocks, 256, 0, st>>>(p, npx, d_max_bits);
+    quant_u8_kernel<uint8_t><<<blocks, 256, 0, st>>>(p, npx, d_max_bits, d_u8, d_f64_keep, d_occ,
+                                                      bit, d_scale_slot);
+  }
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+static int counter_bits(int S) {
+  int b = 1;
+  while ((1 << b) <= S) b++;
+  return b;
+}
+
+struct CompareConfig {
+  int tile;    // orientations per tile (threads per block)
+  int stages;  // TMA ring depth
+  int blocks_per_sm;
+};
+
+CompareConfig compare_config(int R) {
+  CompareConfig c;
+  c.tile = 256;
+  while (c.tile > 32 && (size_t)c.tile * R * 2 > 48 * 1024) c.tile /= 2;
+  const size_t tb = (size_t)c.tile * R * 2;
+  c.stages = (int)std::min<size_t>(4, std::max<size_t>(2, (96 * 1024) / tb));
+  c.blocks_per_sm = 2;
+  return c;
+}
+
+size_t compare_smem_bytes(int R) {
+  const CompareConfig c = compare_config(R);
+  return 128 + (size_t)c.stages * c.tile * R * 2;
+}
+
+template <int B>
+static int launch_b(const CmpArgs &a, unsigned grid, int tile, size_t smem, cudaStream_t st) {
+  LMB_CUDA(cudaFuncSetAttribute(compare_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+  compare_kernel<B><<<grid, tile, smem, st>>>(a);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+int compare_launch(CmpArgs a, int num_sms, cudaStream_t st) {
+  LMB_REQUIRE((reinterpret_cast<uintptr_t>(a.db) & 15) == 0,
+              "DB device pointer must be 16-byte aligned");
+  const CompareConfig c = compare_config(a.R);
+  a.tile_bytes = (uint32_t)((size_t)c.tile * a.R * 2);  // tile multiple of 8 -> multiple of 16
+  a.full_tiles = a.n / c.tile;
+  a.ntiles = (a.n + c.tile - 1) / c.tile;
+  a.stages = c.stages;
+  if (a.ntiles == 0 || a.active == 0) return LMB_OK;
+  const size_t smem = compare_smem_bytes(a.R);
+  const unsigned grid =
+      (unsigned)std::min<uint64_t>(a.ntiles, (uint64_t)num_sms * c.blocks_per_sm);
+  const int B = counter_bits(a.S);
+  if (B <= 3) return launch_b<3>(a, grid, c.tile, smem, st);
+  if (B <= 5) return launch_b<5>(a, grid, c.tile, smem, st);
+  if (B <= 6) return launch_b<6>(a, grid, c.tile, smem, st);
+  if (B <= 7) return launch_b<7>(a, grid, c.tile, smem, st);
+  if (B <= 9) return launch_b<9>(a, grid, c.tile, smem, st);
+  if (B <= 11) return launch_b<11>(a, grid, c.tile, smem, st);
+  return launch_b<16>(a, grid, c.tile, smem, st);
+}
+
+int order_launch(const OrderArgs &a, int nslots, cudaStream_t st) {
+  if (nslots == 0) return LMB_OK;
+  const int smem = (int)(kSmemSortMax * sizeof(unsigned long long));
+  LMB_CUDA(cudaFuncSetAttribute(order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  order_kernel<<<nslots, 1024, smem, st>>>(a);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+}  // namespace lmb

@@ -1,0 +1,325 @@
+// DB build: forward simulation of the orientation DB on the device.
+//
+// Restates the per-orientation loop of LaueMatchingCPU.c:595-667 (the only
+// implementation in the reference, copied at LaueMatchingGPU.cu:478-614 and
+// LaueMatchingGPUStream.cu:854-946).  One thread owns one orientation and
+// walks the HKL list in file order, appending on-detector, in-band,
+// not-yet-seen pixels until MaxNrLaueSpots are taken.
+//
+// Arithmetic.  Each (orientation, HKL) pair is first screened in FP32 with
+// FMA.  The screen only REJECTS: a pair is dropped when, with an error
+// margin far above the FP32 error of the chain, it is certainly behind the
+// detector, off the detector or outside the energy band.  Every other pair
+// is recomputed in FP64 with the reference's exact operation order and
+// rounding (no FMA; C truncation of the pixel coordinate as x86 performs
+// it), and that result alone decides acceptance and the pixel.  The records
+// are therefore identical to the reference's, byte for byte; a build flag
+// (exact_all) runs the FP64 path for every pair to check the screen.
+//
+// Layout.  Blocks of TB orientations; the HKL list is staged through shared
+// memory in chunks (broadcast reads); accepted pixels live in shared memory
+// as [spot][thread] so the de-duplication scan is bank-conflict free; the
+// block's records (contiguous in the DB) are written with coalesced stores.
+#include <climits>
+#include <cmath>
+
+#include "kernels.cuh"
+
+namespace lmb {
+
+struct BuildGeo {
+  double recip[9], rt[9];
+  double p0, p1, p2, px_x, px_y, cx, cy, elo, ehi;
+  int W, H, S, R;
+  float rtf[9];
+  float p0f, p1f, p2f, inv_pxxf, inv_pyf, cxf, cyf, elof, ehif, hc4pif;
+  float tolx, toly;  // FP32 pixel-error scale: 1e-4 * p2 / |px|
+};
+
+static constexpr double kHcKeVnm = 1.2398419739;              // LaueMatchingHeaders.h:41
+static constexpr double kFourPi = 4.0 * 3.14159265358979323846;  // 4 * M_PI as C folds it
+static constexpr int kHklChunk = 512;
+
+// FP32 screen: false only when the pair is certainly rejected in FP64.
+__device__ __forceinline__ bool screen(const float T[9], const int4 hk, const BuildGeo &g) {
+  const float h = (float)hk.x, k = (float)hk.y, l = (float)hk.z;
+  const float qx = fmaf(T[0], h, fmaf(T[1], k, T[2] * l));
+  const float qy = fmaf(T[3], h, fmaf(T[4], k, T[5] * l));
+  const float qz = fmaf(T[6], h, fmaf(T[7], k, T[8] * l));
+  const float ql2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
+  if (!(ql2 > 1e-30f) || !(ql2 < 1e30f)) return true;  // let FP64 decide
+  const float rq = rsqrtf(ql2);
+  const float hx = qx * rq, hy = qy * rq, hz = qz * rq;
+  const float td = -2.f * hz;
+  const float k0 = td * hx, k1 = td * hy, k2 = fmaf(td, hz, 1.f);
+  const float z = fmaf(g.rtf[6], k0, fmaf(g.rtf[7], k1, g.rtf[8] * k2));
+  if (z < -1e-4f) return false;  // xyz[2] <= 0 for sure
+  if (z <= 1e-4f) return true;   // too close to call
+  const float iz = 1.f / z;
+  const float x = fmaf(g.rtf[0], k0, fmaf(g.rtf[1], k1, g.rtf[2] * k2)) * iz;
+  const float y = fmaf(g.rtf[3], k0, fmaf(g.rtf[4], k1, g.rtf[5] * k2)) * iz;
+  // pixel = (x/z * p2 - p0) / px + (N-1)/2 ; accepted iff trunc in [0, N-1],
+  // i.e. pixel in (-1, N).  |error| <= 3e-6 (1+|x/z|)/z * p2/px (FP32 chain),
+  // the margin below is ~30x that plus 0.05 px.
+  const float pxv = fmaf(fmaf(x, g.p2f, -g.p0f), g.inv_pxxf, g.cxf);
+  const float tx = fmaf(g.tolx * (1.f + fabsf(x)), iz, 0.05f);
+  if (pxv < -1.f - tx || pxv > (float)g.W + tx) return false;
+  const float pyv = fmaf(fmaf(y, g.p2f, -g.p1f), g.inv_pyf, g.cyf);
+  const float ty = fmaf(g.toly * (1.f + fabsf(y)), iz, 0.05f);
+  if (pyv < -1.f - ty || pyv > (float)g.H + ty) return false;
+  const float s = -hz;  // sin(theta)
+  if (fabsf(s) < 1e-5f) return true;
+  const float e = g.hc4pif * (ql2 * rq) / s;
+  const float te = fabsf(e) * (1e-4f / fabsf(s) + 1e-4f);
+  if (e < g.elof - te || e > g.ehif + te) return false;
+  return true;
+}
+
+// FP64 evaluation in the reference's exact order (LaueMatchingCPU.c:605-636,
+// MatrixMultF LaueMatchingHeaders.h:361-369).  Returns acceptance and pixel.
+__device__ __forceinline__ bool exact_spot(const double T[9], const int4 hk, const BuildGeo &g,
+                                           int &ipx, int &ipy) {
+  const double h = (double)hk.x, k = (double)hk.y, l = (double)hk.z;
+  const double q0 = dadd(dadd(dadd(0.0, dmul(T[0], h)), dmul(T[1], k)), dmul(T[2], l));
+  const double q1 = dadd(dadd(dadd(0.0, dmul(T[3], h)), dmul(T[4], k)), dmul(T[5], l));
+  const double q2 = dadd(dadd(dadd(0.0, dmul(T[6], h)), dmul(T[7], k)), dmul(T[8], l));
+  const double ql = dsqrt(dadd(dadd(dmul(q0, q0), dmul(q1, q1)), dmul(q2, q2)));
+  if (ql == 0.0) return false;
+  const double h0 = ddiv(q0, ql), h1 = ddiv(q1, ql), h2 = ddiv(q2, ql);
+  const double td = dmul(2.0, h2);
+  const double k0 = dsub(0.0, dmul(td, h0));
+  const double k1 = dsub(0.0, dmul(td, h1));
+  const double k2 = dsub(1.0, dmul(td, h2));
+  const double x = dadd(dadd(dadd(0.0, dmul(g.rt[0], k0)), dmul(g.rt[1], k1)), dmul(g.rt[2], k2));
+  const double y = dadd(dadd(dadd(0.0, dmul(g.rt[3], k0)), dmul(g.rt[4], k1)), dmul(g.rt[5], k2));
+  const double z = dadd(dadd(dadd(0.0, dmul(g.rt[6], k0)), dmul(g.rt[7], k1)), dmul(g.rt[8], k2));
+  if (z <= 0.0) return false;
+  const double xp = dsub(ddiv(dmul(x, g.p2), z), g.p0);
+  const double yp = dsub(ddiv(dmul(y, g.p2), z), g.p1);
+  const int ix = x86_trunc_i32(dadd(ddiv(xp, g.px_x), g.cx));
+  if (ix < 0 || ix > g.W - 1) return false;
+  const int iy = x86_trunc_i32(dadd(ddiv(yp, g.px_y), g.cy));
+  if (iy < 0 || iy > g.H - 1) return false;
+  const double e = ddiv(dmul(kHcKeVnm, ql), dmul(kFourPi, -h2));
+  if (e < g.elo || e > g.ehi) return false;
+  ipx = ix;
+  ipy = iy;
+  return true;
+}
+
+template <bool kExactAll>
+__global__ void dbbuild_kernel(const double *__restrict__ om, uint64_t n,
+                               const int4 *__restrict__ hkl, int nh, BuildGeo g,
+                               uint16_t *__restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int TB = blockDim.x;
+  int4 *sh_hkl = reinterpret_cast<int4 *>(smem);
+  uint32_t *sh_list = reinterpret_cast<uint32_t *>(smem + kHklChunk * sizeof(int4));
+  int *sh_cnt = reinterpret_cast<int *>(sh_list + (size_t)g.S * TB);
+
+  const int t = threadIdx.x;
+  const uint64_t base = (uint64_t)blockIdx.x * TB;
+  const uint64_t oid = base + t;
+  const bool valid = oid < n;
+
+  double T[9];
+  float Tf[9];
+  if (valid) {
+    double m[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) m[i] = __ldg(om + oid * 9 + i);
+    // thisOrient = OM . recip  (MatrixMultF33, LaueMatchingHeaders.h:349-357)
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        T[r * 3 + c] = dadd(dadd(dmul(m[r * 3 + 0], g.recip[0 * 3 + c]),
+                                 dmul(m[r * 3 + 1], g.recip[1 * 3 + c])),
+                            dmul(m[r * 3 + 2], g.recip[2 * 3 + c]));
+#pragma unroll
+    for (int i = 0; i < 9; i++) Tf[i] = (float)T[i];
+  }
+  int cnt = 0;
+  bool done = !valid || g.S <= 0;
+  for (int c0 = 0; c0 < nh; c0 += kHklChunk) {
+    const int cn = min(kHklChunk, nh - c0);
+    __syncthreads();
+    for (int i = t; i < cn; i += TB) sh_hkl[i] = hkl[c0 + i];
+    __syncthreads();
+    if (!done) {
+      for (int i = 0; i < cn; i++) {
+        const int4 hk = sh_hkl[i];
+        if (!kExactAll && !screen(Tf, hk, g)) continue;
+        int ix, iy;
+        if (!exact_spot(T, hk, g, ix, iy)) continue;
+        const uint32_t key = (uint32_t)(ix & 0xFFFF) | ((uint32_t)(iy & 0xFFFF) << 16);
+        bool dup = false;
+        for (int s = 0; s < cnt; s++)
+          if (sh_list[(size_t)s * TB + t] == key) {
+            dup = true;
+            break;
+          }
+        if (dup) continue;
+        sh_list[(size_t)cnt * TB + t] = key;
+        if (++cnt == g.S) {
+          done = true;
+          break;
+        }
+      }
+    }
+    if (__syncthreads_and(done)) break;
+  }
+  sh_cnt[t] = cnt;
+  __syncthreads();
+  // Coalesced store of this block's records: [count, x0, y0, ...] zero padded.
+  if (base >= n) return;
+  const uint32_t nvalid = (uint32_t)min((uint64_t)TB, n - base);
+  const uint32_t R = (uint32_t)g.R;
+  const uint32_t total = nvalid * R;
+  uint16_t *dst = out + base * R;
+  for (uint32_t w = t; w < total; w += TB) {
+    const uint32_t o = w / R, f = w - o * R;
+    uint16_t v = 0;
+    if (f == 0) {
+      v = (uint16_t)sh_cnt[o];
+    } else {
+      const uint32_t s = (f - 1) >> 1;
+      if ((int)s < sh_cnt[o]) {
+        const uint32_t key = sh_list[(size_t)s * TB + o];
+        v = (f & 1) ? (uint16_t)(key & 0xFFFF) : (uint16_t)(key >> 16);
+      }
+    }
+    dst[w] = v;
+  }
+}
+
+// Synthetic orientations: Shoemake's uniform rotations from a counter-based
+// generator (SplitMix64 finaliser of counter*golden + seed*constant), the
+// same uniforms as lauematching_b200/synth.py.
+__device__ __forceinline__ double u01(uint64_t seed, uint64_t c) {
+  uint64_t z = c * 0x9E3779B97F4A7C15ull + seed * 0xD1B54A32D192ED03ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__global__ void synth_orient_kernel(uint64_t seed, uint64_t first, uint64_t n,
+                                    double *__restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t id = first + i;
+    const double u1 = u01(seed, id * 3 + 0), u2 = u01(seed, id * 3 + 1),
+                 u3 = u01(seed, id * 3 + 2);
+    const double a = sqrt(1.0 - u1), b = sqrt(u1);
+    double s2, c2, s3, c3;
+    sincospi(2.0 * u2, &s2, &c2);
+    sincospi(2.0 * u3, &s3, &c3);
+    const double x = a * s2, y = a * c2, z = b * s3, w = b * c3;
+    double *o = out + i * 9;
+    o[0] = 1.0 - 2.0 * (y * y + z * z);
+    o[1] = 2.0 * (x * y - z * w);
+    o[2] = 2.0 * (x * z + y * w);
+    o[3] = 2.0 * (x * y + z * w);
+    o[4] = 1.0 - 2.0 * (x * x + z * z);
+    o[5] = 2.0 * (y * z - x * w);
+    o[6] = 2.0 * (x * z - y * w);
+    o[7] = 2.0 * (y * z + x * w);
+    o[8] = 1.0 - 2.0 * (x * x + y * y);
+  }
+}
+
+static BuildGeo make_build_geo(const lmb_geometry &geo) {
+  BuildGeo g;
+  for (int i = 0; i < 9; i++) {
+    g.recip[i] = geo.recip[i];
+    g.rt[i] = geo.rot_t[i];
+    g.rtf[i] = (float)geo.rot_t[i];
+  }
+  g.p0 = geo.p[0];
+  g.p1 = geo.p[1];
+  g.p2 = geo.p[2];
+  g.px_x = geo.px_x;
+  g.px_y = geo.px_y;
+  g.cx = 0.5 * (geo.nr_px_x - 1);
+  g.cy = 0.5 * (geo.nr_px_y - 1);
+  g.elo = geo.elo;
+  g.ehi = geo.ehi;
+  g.W = geo.nr_px_x;
+  g.H = geo.nr_px_y;
+  g.S = geo.max_nr_spots;
+  g.R = 1 + 2 * geo.max_nr_spots;
+  g.p0f = (float)g.p0;
+  g.p1f = (float)g.p1;
+  g.p2f = (float)g.p2;
+  g.inv_pxxf = (float)(1.0 / g.px_x);
+  g.inv_pyf = (float)(1.0 / g.px_y);
+  g.cxf = (float)g.cx;
+  g.cyf = (float)g.cy;
+  g.elof = (float)g.elo;
+  g.ehif = (float)g.ehi;
+  g.hc4pif = (float)(kHcKeVnm / kFourPi);
+  g.tolx = (float)(1e-4 * std::fabs(g.p2 / g.px_x));
+  g.toly = (float)(1e-4 * std::fabs(g.p2 / g.px_y));
+  return g;
+}
+
+// The FP32 screen is only sound when every geometry value is finite and
+// within FP32 range; otherwise every pair takes the FP64 path.
+static bool screen_sound(const lmb_geometry &geo) {
+  auto ok = [](double v) { return std::isfinite(v) && std::fabs(v) < 1e30; };
+  for (int i = 0; i < 9; i++)
+    if (!ok(geo.rot_t[i]) || !ok(geo.recip[i])) return false;
+  for (int i = 0; i < 3; i++)
+    if (!ok(geo.p[i])) return false;
+  return ok(geo.px_x) && ok(geo.px_y) && geo.px_x != 0 && geo.px_y != 0 && ok(geo.elo) &&
+         ok(geo.ehi) && std::fabs(geo.p[2] / geo.px_x) < 1e30 && std::fabs(geo.p[2] / geo.px_y) < 1e30;
+}
+
+// Threads per block so that the [S][TB] pixel lists fit in shared memory.
+static int build_block(int S) {
+  int tb = 128;
+  while (tb > 32 && (size_t)S * tb * 4 > 160 * 1024) tb /= 2;
+  return tb;
+}
+
+size_t dbbuild_smem_bytes(int S) {
+  const int tb = build_block(S);
+  return kHklChunk * sizeof(int4) + (size_t)S * tb * 4 + (size_t)tb * 4;
+}
+
+int dbbuild_launch(const double *d_om, uint64_t n, const int4 *d_hkl, int nh,
+                   const lmb_geometry &geo, uint16_t *d_out, cudaStream_t st, bool exact_all) {
+  if (n == 0) return LMB_OK;
+  const int S = geo.max_nr_spots;
+  LMB_REQUIRE(S >= 1 && (size_t)S * 32 * 4 <= 160 * 1024,
+              "MaxNrLaueSpots=%d outside the supported range 1..1280", S);
+  const BuildGeo g = make_build_geo(geo);
+  const bool all = exact_all || !screen_sound(geo);
+  const int tb = build_block(S);
+  const size_t smem = dbbuild_smem_bytes(S);
+  const uint64_t blocks = (n + tb - 1) / tb;
+  LMB_REQUIRE(blocks < (1ull << 31), "too many orientations (%llu)", (unsigned long long)n);
+  if (all) {
+    LMB_CUDA(cudaFuncSetAttribute(dbbuild_kernel<true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dbbuild_kernel<true><<<(unsigned)blocks, tb, smem, st>>>(d_om, n, d_hkl, nh, g, d_out);
+  } else {
+    LMB_CUDA(cudaFuncSetAttribute(dbbuild_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dbbuild_kernel<false><<<(unsigned)blocks, tb, smem, st>>>(d_om, n, d_hkl, nh, g, d_out);
+  }
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+int synth_orient_launch(uint64_t seed, uint64_t first, uint64_t n, double *d_out,
+                        cudaStream_t st) {
+  if (n == 0) return LMB_OK;
+  const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148ull * 32);
+  synth_orient_kernel<<<(unsigned)blocks, 256, 0, st>>>(seed, first, n, d_out);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+}  // namespace lmb

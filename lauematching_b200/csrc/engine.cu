@@ -1,0 +1,485 @@
+// C ABI of liblmb200: engine lifetime, device residency of the DB and the
+// image slots, pass orchestration on one CUDA stream.  See include/lmb200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace lmb {
+
+static thread_local char g_err[2048] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+  set_error("%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  return e == cudaErrorMemoryAllocation ? LMB_ERR_OOM : LMB_ERR_CUDA;
+}
+
+}  // namespace lmb
+
+using namespace lmb;
+
+// Status words copied back after every pass: [0,64) survivor counts,
+// [64,128) pass counts, [128] device error word.
+static constexpr int kStatusWords = 2 * LMB_MAX_SLOTS + 1;
+
+struct lmb_engine {
+  int device = 0;
+  int num_sms = 148;
+  lmb_geometry geo{};
+  size_t npx = 0;
+  int S = 0, R = 0;
+  cudaStream_t st = nullptr;
+  // resident DB
+  uint16_t *d_db = nullptr;
+  uint64_t n = 0;
+  // image slots
+  uint8_t *d_u8 = nullptr;
+  double *d_f64 = nullptr;  // allocated on first keep_f64 load
+  unsigned long long *d_occ = nullptr;
+  double *d_scale = nullptr;
+  unsigned long long *d_max_bits = nullptr;
+  void *d_stage = nullptr;  // one image in its wire dtype
+  uint64_t loaded_mask = 0, f64_mask = 0;
+  // survivors
+  uint32_t cap = 0, cap2 = 0;
+  lmb_survivor *d_surv = nullptr, *d_sorted = nullptr;
+  unsigned long long *d_scratch = nullptr;
+  unsigned int *d_status = nullptr;
+  unsigned int *h_status = nullptr;  // pinned
+  uint64_t last_mask = 0;
+  bool pending = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+int check_engine(lmb_engine *e) {
+  if (!e) {
+    set_error("null engine");
+    return LMB_ERR_INVALID;
+  }
+  LMB_CUDA(cudaSetDevice(e->device));
+  return LMB_OK;
+}
+
+void free_engine(lmb_engine *e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->st) cudaStreamSynchronize(e->st);
+  cudaFree(e->d_db);
+  cudaFree(e->d_u8);
+  cudaFree(e->d_f64);
+  cudaFree(e->d_occ);
+  cudaFree(e->d_scale);
+  cudaFree(e->d_max_bits);
+  cudaFree(e->d_stage);
+  cudaFree(e->d_surv);
+  cudaFree(e->d_sorted);
+  cudaFree(e->d_scratch);
+  cudaFree(e->d_status);
+  cudaFreeHost(e->h_status);
+  for (auto &v : e->ev)
+    if (v) cudaEventDestroy(v);
+  if (e->st) cudaStreamDestroy(e->st);
+  delete e;
+}
+
+size_t dtype_bytes(int dtype) {
+  return dtype == LMB_F64 ? 8 : dtype == LMB_F32 ? 4 : 1;
+}
+
+// Host->device copy of a large pageable buffer through two pinned chunks so
+// the host memcpy of chunk i+1 overlaps the DMA of chunk i.
+int upload_chunked(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+  const size_t kChunk = 64ull << 20;
+  if (bytes <= kChunk) {
+    LMB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    LMB_CUDA(cudaStreamSynchronize(st));
+    return LMB_OK;
+  }
+  void *pin[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  int rc = LMB_OK;
+  for (int i = 0; i < 2 && rc == LMB_OK; i++) {
+    cudaError_t ce = cudaHostAlloc(&pin[i], kChunk, cudaHostAllocDefault);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+    if (ce != cudaSuccess) rc = cuda_fail(ce, "pinned staging", __FILE__, __LINE__);
+  }
+  size_t off = 0;
+  int b = 0;
+  while (rc == LMB_OK && off < bytes) {
+    const size_t len = std::min(kChunk, bytes - off);
+    cudaError_t ce = cudaEventSynchronize(done[b]);  // chunk b free again
+    if (ce == cudaSuccess) {
+      memcpy(pin[b], static_cast<const char *>(src) + off, len);
+      ce = cudaMemcpyAsync(static_cast<char *>(dst) + off, pin[b], len, cudaMemcpyHostToDevice, st);
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(done[b], st);
+    if (ce != cudaSuccess) rc = cuda_fail(ce, "chunked upload", __FILE__, __LINE__);
+    off += len;
+    b ^= 1;
+  }
+  cudaStreamSynchronize(st);
+  for (int i = 0; i < 2; i++) {
+    if (done[i]) cudaEventDestroy(done[i]);
+    if (pin[i]) cudaFreeHost(pin[i]);
+  }
+  return rc;
+}
+
+int alloc_db(lmb_engine *e, uint64_t n) {
+  LMB_REQUIRE(n < (1ull << 40), "at most 2^40 orientations are supported (got %llu)",
+              (unsigned long long)n);
+  cudaFree(e->d_db);
+  e->d_db = nullptr;
+  e->n = 0;
+  const size_t bytes = (size_t)n * e->R * 2;
+  const size_t alloc = ((bytes + 255) / 256) * 256 + 256;
+  LMB_CUDA(cudaMalloc(&e->d_db, alloc));
+  LMB_CUDA(cudaMemsetAsync(e->d_db, 0, alloc, e->st));
+  e->n = n;
+  return LMB_OK;
+}
+
+int upload_hkls(const int32_t *hkls, int nh, int4 **d_out) {
+  std::vector<int4> h((size_t)std::max(nh, 1));
+  for (int i = 0; i < nh; i++) h[i] = make_int4(hkls[3 * i], hkls[3 * i + 1], hkls[3 * i + 2], 0);
+  LMB_CUDA(cudaMalloc(d_out, h.size() * sizeof(int4)));
+  LMB_CUDA(cudaMemcpy(*d_out, h.data(), (size_t)nh * sizeof(int4), cudaMemcpyHostToDevice));
+  return LMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lmb_version(void) { return "lmb200 0.1.0 sm_100a"; }
+const char *lmb_last_error(void) { return g_err; }
+
+int lmb_geometry_init(const double lattice[6], int32_t space_group, const double p_array[3],
+                      const double r_array[3], double px_x, double px_y, int32_t nr_px_x,
+                      int32_t nr_px_y, double elo, double ehi, int32_t max_nr_spots,
+                      lmb_geometry *out);  // geometry.cpp
+
+int lmb_engine_create(int32_t device, const lmb_geometry *geo, uint64_t survivor_capacity,
+                      lmb_engine **out) {
+  LMB_REQUIRE(geo && out, "null argument");
+  LMB_REQUIRE(geo->nr_px_x > 0 && geo->nr_px_y > 0 && geo->nr_px_x <= 65536 &&
+                  geo->nr_px_y <= 65536,
+              "detector size %d x %d outside 1..65536", geo->nr_px_x, geo->nr_px_y);
+  LMB_REQUIRE(geo->max_nr_spots >= 1 && geo->max_nr_spots <= 32767,
+              "MaxNrLaueSpots=%d outside 1..32767", geo->max_nr_spots);
+  if (survivor_capacity == 0) survivor_capacity = 262144;
+  LMB_REQUIRE(survivor_capacity <= (1u << 24), "survivor capacity above 2^24");
+  *out = nullptr;
+  lmb_engine *e = new lmb_engine();
+  e->device = device;
+  e->geo = *geo;
+  e->npx = (size_t)geo->nr_px_x * geo->nr_px_y;
+  e->S = geo->max_nr_spots;
+  e->R = 1 + 2 * e->S;
+  e->cap = (uint32_t)survivor_capacity;
+  e->cap2 = 1;
+  while (e->cap2 < e->cap) e->cap2 <<= 1;
+  auto fail = [&](int rc) {
+    free_engine(e);
+    return rc;
+  };
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) return fail(cuda_fail(ce, "cudaSetDevice", __FILE__, __LINE__));
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  e->num_sms = sms > 0 ? sms : 148;
+#define TRY(call)                                                              \
+  do {                                                                         \
+    cudaError_t _e = (call);                                                   \
+    if (_e != cudaSuccess) return fail(cuda_fail(_e, #call, __FILE__, __LINE__)); \
+  } while (0)
+  TRY(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+  for (auto &v : e->ev) TRY(cudaEventCreate(&v));
+  TRY(cudaMalloc(&e->d_u8, e->npx * LMB_MAX_SLOTS));
+  TRY(cudaMalloc(&e->d_occ, e->npx * sizeof(unsigned long long)));
+  TRY(cudaMemset(e->d_occ, 0, e->npx * sizeof(unsigned long long)));
+  TRY(cudaMalloc(&e->d_scale, LMB_MAX_SLOTS * sizeof(double)));
+  TRY(cudaMemset(e->d_scale, 0, LMB_MAX_SLOTS * sizeof(double)));
+  TRY(cudaMalloc(&e->d_max_bits, sizeof(unsigned long long)));
+  TRY(cudaMalloc(&e->d_stage, e->npx * sizeof(double)));
+  TRY(cudaMalloc(&e->d_surv, (size_t)LMB_MAX_SLOTS * e->cap * sizeof(lmb_survivor)));
+  TRY(cudaMalloc(&e->d_sorted, (size_t)LMB_MAX_SLOTS * e->cap * sizeof(lmb_survivor)));
+  TRY(cudaMalloc(&e->d_scratch, (size_t)LMB_MAX_SLOTS * e->cap2 * sizeof(unsigned long long)));
+  TRY(cudaMalloc(&e->d_status, kStatusWords * sizeof(unsigned int)));
+  TRY(cudaMemset(e->d_status, 0, kStatusWords * sizeof(unsigned int)));
+  TRY(cudaHostAlloc(&e->h_status, kStatusWords * sizeof(unsigned int), cudaHostAllocDefault));
+  memset(e->h_status, 0, kStatusWords * sizeof(unsigned int));
+#undef TRY
+  *out = e;
+  return LMB_OK;
+}
+
+int lmb_engine_destroy(lmb_engine *e) {
+  if (!e) return LMB_OK;
+  free_engine(e);
+  return LMB_OK;
+}
+
+void *lmb_engine_stream(lmb_engine *e) { return e ? (void *)e->st : nullptr; }
+
+int lmb_db_upload(lmb_engine *e, const uint16_t *records, uint64_t n) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(records || n == 0, "null records");
+  LMB_CUDA(cudaStreamSynchronize(e->st));
+  rc = alloc_db(e, n);
+  if (rc) return rc;
+  LMB_CUDA(cudaStreamSynchronize(e->st));
+  return upload_chunked(e->d_db, records, (size_t)n * e->R * 2, e->st);
+}
+
+static int db_build_common(lmb_engine *e, const double *orients, uint64_t seed, bool synthetic,
+                           uint64_t n, const int32_t *hkls, int32_t nh, double *orients_out,
+                           uint32_t flags) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(nh >= 0 && (hkls || nh == 0), "bad HKL list");
+  LMB_REQUIRE(synthetic || orients || n == 0, "null orientations");
+  LMB_CUDA(cudaStreamSynchronize(e->st));
+  rc = alloc_db(e, n);
+  if (rc) return rc;
+  int4 *d_hkl = nullptr;
+  rc = upload_hkls(hkls, nh, &d_hkl);
+  if (rc) return rc;
+  const uint64_t kChunk = 4ull << 20;  // orientations per chunk (288 MB of matrices)
+  double *d_om = nullptr;
+  cudaError_t ce = cudaMalloc(&d_om, std::min(kChunk, std::max<uint64_t>(n, 1)) * 72);
+  if (ce != cudaSuccess) {
+    cudaFree(d_hkl);
+    return cuda_fail(ce, "cudaMalloc(orientation chunk)", __FILE__, __LINE__);
+  }
+  for (uint64_t off = 0; off < n && rc == LMB_OK; off += kChunk) {
+    const uint64_t len = std::min(kChunk, n - off);
+    if (synthetic) {
+      rc = synth_orient_launch(seed, off, len, d_om, e->st);
+    } else {
+      rc = upload_chunked(d_om, orients + off * 9, len * 72, e->st);
+    }
+    if (rc == LMB_OK)
+      rc = dbbuild_launch(d_om, len, d_hkl, nh, e->geo, e->d_db + off * e->R, e->st,
+                          (flags & LMB_BUILD_EXACT_FP64) != 0);
+    if (rc == LMB_OK && synthetic && orients_out) {
+      ce = cudaMemcpyAsync(orients_out + off * 9, d_om, len * 72, cudaMemcpyDeviceToHost, e->st);
+      if (ce != cudaSuccess) rc = cuda_fail(ce, "orientation download", __FILE__, __LINE__);
+    }
+    ce = cudaStreamSynchronize(e->st);
+    if (ce != cudaSuccess && rc == LMB_OK) rc = cuda_fail(ce, "DB build", __FILE__, __LINE__);
+  }
+  cudaFree(d_om);
+  cudaFree(d_hkl);
+  return rc;
+}
+
+int lmb_db_build(lmb_engine *e, const double *orients, uint64_t n, const int32_t *hkls,
+                 int32_t nh) {
+  return db_build_common(e, orients, 0, false, n, hkls, nh, nullptr, 0);
+}
+
+int lmb_db_build_ex(lmb_engine *e, const double *orients, uint64_t n, const int32_t *hkls,
+                    int32_t nh, uint32_t flags) {
+  return db_build_common(e, orients, 0, false, n, hkls, nh, nullptr, flags);
+}
+
+int lmb_db_build_synthetic(lmb_engine *e, uint64_t seed, uint64_t n, const int32_t *hkls,
+                           int32_t nh, double *orients_out) {
+  return db_build_common(e, nullptr, seed, true, n, hkls, nh, orients_out, 0);
+}
+
+int lmb_synth_orientations(lmb_engine *e, uint64_t seed, uint64_t first, uint64_t n,
+                           double *out) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(out || n == 0, "null output");
+  if (n == 0) return LMB_OK;
+  double *d = nullptr;
+  LMB_CUDA(cudaMalloc(&d, n * 72));
+  rc = synth_orient_launch(seed, first, n, d, e->st);
+  cudaError_t ce = cudaSuccess;
+  if (rc == LMB_OK) ce = cudaMemcpyAsync(out, d, n * 72, cudaMemcpyDeviceToHost, e->st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
+  cudaFree(d);
+  if (ce != cudaSuccess) return cuda_fail(ce, "synthetic orientations", __FILE__, __LINE__);
+  return rc;
+}
+
+int lmb_db_download(lmb_engine *e, uint64_t first, uint64_t count, uint16_t *out) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(first <= e->n && count <= e->n - first, "record range outside the DB");
+  LMB_REQUIRE(out || count == 0, "null output");
+  LMB_CUDA(cudaStreamSynchronize(e->st));
+  LMB_CUDA(cudaMemcpy(out, e->d_db + first * e->R, (size_t)count * e->R * 2,
+                      cudaMemcpyDeviceToHost));
+  return LMB_OK;
+}
+
+int lmb_db_info(lmb_engine *e, uint64_t *n_orient, int32_t *max_nr_spots) {
+  LMB_REQUIRE(e, "null engine");
+  if (n_orient) *n_orient = e->n;
+  if (max_nr_spots) *max_nr_spots = e->S;
+  return LMB_OK;
+}
+
+int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtype,
+                   int32_t keep_f64, double *im_scale) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(slot >= 0 && slot < LMB_MAX_SLOTS, "slot %d outside 0..%d", slot,
+              LMB_MAX_SLOTS - 1);
+  LMB_REQUIRE(pixels, "null pixels");
+  LMB_REQUIRE(dtype == LMB_F64 || dtype == LMB_F32 || dtype == 2, "unknown dtype %d", dtype);
+  if (keep_f64 && !e->d_f64)
+    LMB_CUDA(cudaMalloc(&e->d_f64, e->npx * sizeof(double) * LMB_MAX_SLOTS));
+  LMB_CUDA(cudaMemcpyAsync(e->d_stage, pixels, e->npx * dtype_bytes(dtype),
+                           cudaMemcpyHostToDevice, e->st));
+  rc = quantize_launch(e->d_stage, dtype, e->npx, e->d_max_bits, e->d_u8 + (size_t)slot * e->npx,
+                       keep_f64 ? e->d_f64 + (size_t)slot * e->npx : nullptr, e->d_occ, slot,
+                       e->d_scale + slot, e->num_sms, e->st);
+  if (rc) return rc;
+  e->loaded_mask |= 1ull << slot;
+  if (keep_f64)
+    e->f64_mask |= 1ull << slot;
+  else
+    e->f64_mask &= ~(1ull << slot);
+  if (im_scale) {
+    LMB_CUDA(cudaMemcpyAsync(im_scale, e->d_scale + slot, sizeof(double), cudaMemcpyDeviceToHost,
+                             e->st));
+    LMB_CUDA(cudaStreamSynchronize(e->st));
+  }
+  return LMB_OK;
+}
+
+int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double min_intensity,
+              int32_t value_mode) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(e->d_db || e->n == 0, "no DB loaded");
+  LMB_REQUIRE((slot_mask & ~e->loaded_mask) == 0, "slot mask names slots with no image");
+  LMB_REQUIRE(value_mode == LMB_VALUE_U8 || value_mode == LMB_VALUE_F64, "unknown value mode");
+  LMB_REQUIRE(value_mode == LMB_VALUE_U8 || (slot_mask & ~e->f64_mask) == 0,
+              "float64 pass needs images loaded with keep_f64");
+  LMB_CUDA(cudaMemsetAsync(e->d_status, 0, kStatusWords * sizeof(unsigned int), e->st));
+  LMB_CUDA(cudaEventRecord(e->ev[0], e->st));
+  CmpArgs a{};
+  a.db = e->d_db;
+  a.n = e->n;
+  a.R = e->R;
+  a.S = e->S;
+  a.W = e->geo.nr_px_x;
+  a.H = e->geo.nr_px_y;
+  a.occ = e->d_occ;
+  a.active = slot_mask;
+  a.u8 = e->d_u8;
+  a.f64 = value_mode == LMB_VALUE_F64 ? e->d_f64 : nullptr;
+  a.npx = e->npx;
+  a.scale = e->d_scale;
+  a.mode = value_mode;
+  // count >= MinNrSpots can only hold for MinNrSpots <= S; <= 0 always holds
+  a.min_spots = min_nr_spots < 0 ? 0 : min_nr_spots;
+  a.min_int = min_intensity;
+  a.surv = e->d_surv;
+  a.cap = e->cap;
+  a.surv_cnt = e->d_status;
+  a.pass_cnt = e->d_status + LMB_MAX_SLOTS;
+  a.err = reinterpret_cast<int *>(e->d_status + 2 * LMB_MAX_SLOTS);
+  if (min_nr_spots <= e->S && !std::isnan(min_intensity)) {
+    rc = compare_launch(a, e->num_sms, e->st);
+    if (rc) return rc;
+  }
+  LMB_CUDA(cudaEventRecord(e->ev[1], e->st));
+  OrderArgs o{};
+  o.surv = e->d_surv;
+  o.out = e->d_sorted;
+  o.surv_cnt = e->d_status;
+  o.cap = e->cap;
+  o.scratch = e->d_scratch;
+  o.cap2 = e->cap2;
+  int ns = 0;
+  for (int k = 0; k < LMB_MAX_SLOTS; k++)
+    if (slot_mask >> k & 1) o.slots[ns++] = k;
+  rc = order_launch(o, ns, e->st);
+  if (rc) return rc;
+  LMB_CUDA(cudaEventRecord(e->ev[2], e->st));
+  LMB_CUDA(cudaMemcpyAsync(e->h_status, e->d_status, kStatusWords * sizeof(unsigned int),
+                           cudaMemcpyDeviceToHost, e->st));
+  e->last_mask = slot_mask;
+  e->pending = true;
+  return LMB_OK;
+}
+
+int lmb_results(lmb_engine *e, int32_t slot, lmb_survivor *out, uint64_t out_capacity,
+                uint64_t *n_survivors, uint64_t *n_pass) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(e->pending, "no pass has been run");
+  LMB_REQUIRE(slot >= 0 && slot < LMB_MAX_SLOTS && (e->last_mask >> slot & 1),
+              "slot %d was not part of the last pass", slot);
+  LMB_CUDA(cudaStreamSynchronize(e->st));
+  const int derr = (int)e->h_status[2 * LMB_MAX_SLOTS];
+  if (derr != DEV_OK) {
+    set_error("device wait gave up in the compare pass (code %d)", derr);
+    return LMB_ERR_TIMEOUT;
+  }
+  const uint64_t cnt = e->h_status[slot];
+  if (n_survivors) *n_survivors = cnt;
+  if (n_pass) *n_pass = e->h_status[LMB_MAX_SLOTS + slot];
+  if (cnt > e->cap) {
+    set_error("slot %d: %llu survivors exceed the engine capacity %u", slot,
+              (unsigned long long)cnt, e->cap);
+    return LMB_ERR_OVERFLOW;
+  }
+  if (!out) return LMB_OK;
+  if (out_capacity < cnt) {
+    set_error("slot %d: %llu survivors exceed the output capacity %llu", slot,
+              (unsigned long long)cnt, (unsigned long long)out_capacity);
+    return LMB_ERR_OVERFLOW;
+  }
+  if (cnt)
+    LMB_CUDA(cudaMemcpy(out, e->d_sorted + (size_t)slot * e->cap, cnt * sizeof(lmb_survivor),
+                        cudaMemcpyDeviceToHost));
+  return LMB_OK;
+}
+
+int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(e->pending, "no pass has been run");
+  LMB_CUDA(cudaEventSynchronize(e->ev[2]));
+  float a = 0, b = 0;
+  LMB_CUDA(cudaEventElapsedTime(&a, e->ev[0], e->ev[1]));
+  LMB_CUDA(cudaEventElapsedTime(&b, e->ev[1], e->ev[2]));
+  if (compare_ms) *compare_ms = a;
+  if (order_ms) *order_ms = b;
+  return LMB_OK;
+}
+
+int lmb_host_alloc(uint64_t bytes, void **out) {
+  LMB_REQUIRE(out, "null output");
+  *out = nullptr;
+  LMB_CUDA(cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault));
+  return LMB_OK;
+}
+
+int lmb_host_free(void *p) {
+  if (p) LMB_CUDA(cudaFreeHost(p));
+  return LMB_OK;
+}
+
+}  // extern "C"

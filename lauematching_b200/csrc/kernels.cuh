@@ -1,0 +1,55 @@
+// Kernel argument blocks and launchers shared by the translation units of
+// liblmb200 (dbbuild.cu, compare.cu, engine.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace lmb {
+
+// One batched DB pass (compare.cu).
+struct CmpArgs {
+  const uint16_t *db;  // n records of R uint16, 16-byte aligned
+  uint64_t n;
+  int R, S, W, H;
+  const unsigned long long *occ;  // per pixel: bit k = slot k's uint8 pixel > 0
+  unsigned long long active;      // slots of this pass
+  const uint8_t *u8;              // slot k image at u8 + k*npx
+  const double *f64;              // slot k float64 image at f64 + k*npx (value mode F64)
+  size_t npx;
+  const double *scale;  // imScale per slot
+  int mode;             // LMB_VALUE_U8 / LMB_VALUE_F64
+  int min_spots;        // MinNrSpots clamped to >= 0
+  double min_int;       // MinIntensity
+  lmb_survivor *surv;   // slot k list at surv + k*cap, unordered
+  uint32_t cap;
+  unsigned int *surv_cnt;  // [64] survivors (score != 0)
+  unsigned int *pass_cnt;  // [64] orientations passing both thresholds
+  int *err;                // device error word
+  // filled by compare_launch
+  uint64_t full_tiles, ntiles;
+  uint32_t tile_bytes;
+  int stages;
+};
+
+// Ordering of the survivor lists of a pass by orientation ID (compare.cu).
+struct OrderArgs {
+  const lmb_survivor *surv;
+  lmb_survivor *out;
+  const unsigned int *surv_cnt;
+  uint32_t cap;
+  unsigned long long *scratch;  // [64][cap2] keys for lists above the shared-memory size
+  uint32_t cap2;                // power of two >= cap
+  int slots[LMB_MAX_SLOTS];
+};
+
+int dbbuild_launch(const double *d_om, uint64_t n, const int4 *d_hkl, int nh,
+                   const lmb_geometry &geo, uint16_t *d_out, cudaStream_t st, bool exact_all);
+int synth_orient_launch(uint64_t seed, uint64_t first, uint64_t n, double *d_out,
+                        cudaStream_t st);
+int quantize_launch(const void *d_img, int dtype, size_t npx, unsigned long long *d_max_bits,
+                    uint8_t *d_u8, double *d_f64_keep, unsigned long long *d_occ, int slot,
+                    double *d_scale_slot, int num_sms, cudaStream_t st);
+int compare_launch(CmpArgs a, int num_sms, cudaStream_t st);
+int order_launch(const OrderArgs &a, int nslots, cudaStream_t st);
+
+}  // namespace lmb

@@ -1,0 +1,175 @@
+"""Python host API over the C ABI: one engine per (device, detector geometry).
+
+An :class:`Engine` keeps the forward-simulated DB resident in HBM together
+with up to 64 image slots; :meth:`Engine.match` runs one DB pass for any set
+of loaded slots and :meth:`Engine.results` returns each slot's survivors in
+ascending orientation ID, with the reference's integer and FP64 values.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .params import LaueParams
+
+__all__ = ["SURVIVOR_DTYPE", "geometry_from_params", "Engine", "PinnedBuffer"]
+
+SURVIVOR_DTYPE = np.dtype([("id", "<u8"), ("n_spots", "<i4"), ("sum_u8", "<i4"),
+                           ("tot_int", "<f8"), ("score", "<f8")])
+assert SURVIVOR_DTYPE.itemsize == C.sizeof(_lib.LmbSurvivor)
+
+_DTYPES = {np.dtype(np.float64): _lib.LMB_F64, np.dtype(np.float32): _lib.LMB_F32,
+           np.dtype(np.uint8): _lib.LMB_U8}
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def geometry_from_params(p: LaueParams) -> _lib.LmbGeometry:
+    g = _lib.LmbGeometry()
+    lat = np.asarray(p.lattice, np.float64)
+    pa = np.asarray(p.p_array, np.float64)
+    ra = np.asarray(p.r_array, np.float64)
+    check(lib().lmb_geometry_init(_dptr(lat), int(p.space_group), _dptr(pa), _dptr(ra),
+                                  float(p.px_x), float(p.px_y), int(p.nr_px_x), int(p.nr_px_y),
+                                  float(p.elo), float(p.ehi), int(p.max_nr_spots), C.byref(g)))
+    return g
+
+
+class PinnedBuffer:
+    """Page-locked host memory viewed as a numpy array."""
+
+    def __init__(self, shape, dtype):
+        self.dtype = np.dtype(dtype)
+        n = int(np.prod(shape)) * self.dtype.itemsize
+        p = C.c_void_p()
+        check(lib().lmb_host_alloc(n, C.byref(p)))
+        self._p = p
+        buf = (C.c_byte * max(n, 1)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def free(self):
+        if self._p is not None:
+            self.array = None
+            lib().lmb_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:  # interpreter shutdown
+            pass
+
+
+class Engine:
+    def __init__(self, params: LaueParams, device: int = 0, survivor_capacity: int = 0):
+        self.params = params
+        self.geometry = geometry_from_params(params)
+        self.S = int(params.max_nr_spots)
+        self.R = 1 + 2 * self.S
+        self.npx = int(params.nr_px_x) * int(params.nr_px_y)
+        h = C.c_void_p()
+        check(lib().lmb_engine_create(int(device), C.byref(self.geometry),
+                                      int(survivor_capacity), C.byref(h)))
+        self._h = h
+        self.n_orient = 0
+
+    # ---- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().lmb_engine_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(lib().lmb_engine_stream(self._h) or 0)
+
+    # ---- DB -------------------------------------------------------------------
+    def upload_db(self, records: np.ndarray) -> None:
+        rec = np.ascontiguousarray(records, dtype=np.uint16).reshape(-1, self.R)
+        check(lib().lmb_db_upload(self._h, rec.ctypes.data, rec.shape[0]))
+        self.n_orient = rec.shape[0]
+
+    def build_db(self, orients: np.ndarray, hkls: np.ndarray, exact_fp64: bool = False) -> None:
+        om = np.ascontiguousarray(orients, dtype=np.float64).reshape(-1, 9)
+        hk = np.ascontiguousarray(hkls, dtype=np.int32).reshape(-1, 3)
+        flags = _lib.LMB_BUILD_EXACT_FP64 if exact_fp64 else 0
+        check(lib().lmb_db_build_ex(self._h, om.ctypes.data, om.shape[0], hk.ctypes.data,
+                                    hk.shape[0], flags))
+        self.n_orient = om.shape[0]
+
+    def build_db_synthetic(self, seed: int, n: int, hkls: np.ndarray,
+                           return_orients: bool = False):
+        hk = np.ascontiguousarray(hkls, dtype=np.int32).reshape(-1, 3)
+        out = np.empty((n, 9), np.float64) if return_orients else None
+        check(lib().lmb_db_build_synthetic(self._h, int(seed), int(n), hk.ctypes.data,
+                                           hk.shape[0], out.ctypes.data if out is not None else None))
+        self.n_orient = n
+        return out
+
+    def synth_orientations(self, seed: int, first: int, n: int) -> np.ndarray:
+        out = np.empty((n, 9), np.float64)
+        check(lib().lmb_synth_orientations(self._h, int(seed), int(first), int(n), out.ctypes.data))
+        return out
+
+    def download_db(self, first: int = 0, count: int | None = None) -> np.ndarray:
+        if count is None:
+            count = self.n_orient - first
+        out = np.empty((count, self.R), np.uint16)
+        check(lib().lmb_db_download(self._h, first, count, out.ctypes.data))
+        return out
+
+    # ---- images ---------------------------------------------------------------
+    def load_image(self, slot: int, pixels: np.ndarray, keep_f64: bool = False,
+                   want_scale: bool = True):
+        px = np.ascontiguousarray(pixels).ravel()
+        if px.size != self.npx:
+            raise ValueError(f"image has {px.size} pixels, detector has {self.npx}")
+        dt = _DTYPES.get(px.dtype)
+        if dt is None:
+            px = px.astype(np.float64)
+            dt = _lib.LMB_F64
+        sc = C.c_double(0.0)
+        check(lib().lmb_image_load(self._h, int(slot), px.ctypes.data, dt, int(bool(keep_f64)),
+                                   C.byref(sc) if want_scale else None))
+        return sc.value if want_scale else None
+
+    # ---- passes ---------------------------------------------------------------
+    def match(self, slots, min_nr_spots: int, min_intensity: float, value_mode: int = 0) -> None:
+        mask = 0
+        for s in slots:
+            mask |= 1 << int(s)
+        check(lib().lmb_match(self._h, mask, int(min_nr_spots), float(min_intensity),
+                              int(value_mode)))
+
+    def results(self, slot: int):
+        """(survivors structured array sorted by id, n_pass)."""
+        n = C.c_uint64(0)
+        npass = C.c_uint64(0)
+        check(lib().lmb_results(self._h, int(slot), None, 0, C.byref(n), C.byref(npass)))
+        out = np.empty(n.value, SURVIVOR_DTYPE)
+        if n.value:
+            check(lib().lmb_results(self._h, int(slot), out.ctypes.data, n.value, C.byref(n),
+                                    C.byref(npass)))
+        return out, int(npass.value)
+
+    def last_pass_ms(self):
+        a, b = C.c_float(0), C.c_float(0)
+        check(lib().lmb_last_pass_ms(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value

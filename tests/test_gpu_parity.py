@@ -1,0 +1,167 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the
+oracle and the reference's golden outputs.
+
+Bar: bit-exact.  Records byte for byte; survivors' IDs, spot counts and uint8
+sums equal; the FP64 intensity sums and scores equal to the last bit (the
+kernels reproduce the reference's operation order and rounding).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden_case, golden_names
+from lauematching_b200 import synth, params as P
+from lauematching_b200._lib import OverflowError_, LmbError
+
+pytestmark = pytest.mark.gpu
+
+
+def engine_for(p, cap=0):
+    from lauematching_b200.engine import Engine
+    return Engine(p, device=0, survivor_capacity=cap)
+
+
+def assert_same_survivors(got, ref):
+    assert got.shape[0] == ref.ids.shape[0]
+    assert np.array_equal(got["id"], ref.ids.astype(np.uint64))
+    assert np.array_equal(got["n_spots"], ref.n_spots)
+    assert np.array_equal(got["sum_u8"], ref.sum_u8)
+    assert np.array_equal(got["tot_int"].view(np.uint64), ref.tot_int.view(np.uint64))
+    assert np.array_equal(got["score"].view(np.uint64), ref.score.view(np.uint64))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_db_build_matches_reference_cache(name):
+    c = golden_case(name)
+    with engine_for(c.params) as e:
+        e.build_db(c.orients, c.hkls)
+        assert np.array_equal(e.download_db(), c.records)
+
+
+@pytest.mark.parametrize("name", ["tilted_fcc", "tilted_hex", "beamnormal_fcc"])
+def test_db_build_fp32_screen_equals_all_fp64(name):
+    c = golden_case(name)
+    om = synth.shoemake_orientations(200000, seed=123)
+    with engine_for(c.params) as e:
+        e.build_db(om, c.hkls, exact_fp64=True)
+        full = e.download_db()
+        e.build_db(om, c.hkls)
+        assert np.array_equal(e.download_db(), full)
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("mode", [0, 1])
+def test_compare_matches_oracle(name, mode):
+    c = golden_case(name)
+    p = c.params
+    ref = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                    p.min_nr_spots, p.min_intensity, mode=mode)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        e.load_image(5, c.image, keep_f64=(mode == 1))
+        e.match([5], p.min_nr_spots, p.min_intensity, value_mode=mode)
+        got, npass = e.results(5)
+    assert npass == ref.n_pass
+    assert npass == c.meta["cmp_initial" if mode == 0 else "fwd_initial"]
+    assert_same_survivors(got, ref)
+
+
+def _batch_case(n=300000, k=12, seed=9, S=30, min_spots=5, min_int=150.0):
+    txt = synth.params_text(p=(0.028745, 0.002788, 0.513115),
+                            r=(-1.20131258, -1.21399082, -1.21881158), max_nr_spots=S,
+                            min_nr_spots=min_spots, min_intensity=min_int)
+    p = P.parse_params_text(txt)
+    hk = synth.hkls_cubic(8)
+    return p, hk
+
+
+def test_batched_pass_equals_single_passes_and_oracle():
+    """K images of uneven grain counts in one DB pass == K separate passes
+    == the oracle, each image alone."""
+    p, hk = _batch_case()
+    rng = np.random.default_rng(3)
+    with engine_for(p) as e:
+        om = e.build_db_synthetic(seed=77, n=300000, hkls=hk, return_orients=True)
+        rec = e.download_db()
+        imgs = []
+        for k in range(12):
+            g = synth.pick_grains(rec, int(rng.integers(1, 21)), 8, rng)
+            img = synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng,
+                                     threshold=None if k == 3 else 20.0)
+            if k == 7:
+                img = img * 2.71
+            imgs.append(img)
+            e.load_image(k, img)
+        e.match(range(12), p.min_nr_spots, p.min_intensity)
+        batched = [e.results(k) for k in range(12)]
+        for k in range(12):
+            e.match([k], p.min_nr_spots, p.min_intensity)
+            single = e.results(k)
+            assert single[1] == batched[k][1]
+            assert np.array_equal(single[0], batched[k][0])
+    assert np.array_equal(O.forward(p, om[:20000], hk), rec[:20000])
+    for k in (0, 3, 7, 11):
+        ref = O.compare(rec, p.max_nr_spots, imgs[k], p.nr_px_x, p.nr_px_y,
+                        p.min_nr_spots, p.min_intensity)
+        assert batched[k][1] == ref.n_pass
+        assert_same_survivors(batched[k][0], ref)
+
+
+def test_input_dtypes_f32_u8_match_f64():
+    c = golden_case("tilted_fcc")
+    p = c.params
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        e.load_image(0, c.image)
+        e.load_image(1, c.image.astype(np.float32))
+        e.load_image(2, c.img_u8)
+        e.match([0, 1, 2], p.min_nr_spots, p.min_intensity)
+        r = [e.results(k) for k in range(3)]
+    for k in (1, 2):
+        assert np.array_equal(r[0][0], r[k][0]) and r[0][1] == r[k][1]
+
+
+def test_edge_records_partial_tiles_and_thresholds():
+    """Counts above S (clamped), pixels off the detector (skipped), DB sizes
+    that are not a multiple of the tile, MinNrSpots <= 0 and > S."""
+    rng = np.random.default_rng(1)
+    txt = synth.params_text(nr_px=(300, 200), max_nr_spots=7, min_nr_spots=2,
+                            min_intensity=3.0)
+    p = P.parse_params_text(txt)
+    for n in (0, 1, 7, 255, 256, 257, 1000, 4099):
+        rec = np.zeros((n, 15), np.uint16)
+        if n:
+            rec[:, 0] = rng.integers(0, 12, n)       # some counts exceed S=7
+            rec[:, 1::2] = rng.integers(0, 330, (n, 7))  # some x >= 300
+            rec[:, 2::2] = rng.integers(0, 220, (n, 7))  # some y >= 200
+        img = np.where(rng.random(300 * 200) < 0.3, rng.integers(1, 256, 300 * 200), 0)
+        img = img.astype(np.float64) * 0.77
+        with engine_for(p) as e:
+            e.upload_db(rec)
+            e.load_image(0, img)
+            for ms, mi in ((2, 3.0), (0, 0.0), (-3, -1.0), (8, 0.0), (1, 1e9)):
+                e.match([0], ms, mi)
+                got, npass = e.results(0)
+                ref = O.compare(rec, 7, img, 300, 200, ms, mi)
+                assert npass == ref.n_pass, (n, ms, mi)
+                assert_same_survivors(got, ref)
+
+
+def test_survivor_overflow_is_reported():
+    c = golden_case("tilted_dense")
+    p = c.params
+    with engine_for(p, cap=64) as e:
+        e.upload_db(c.records)
+        e.load_image(0, c.image)
+        e.match([0], p.min_nr_spots, p.min_intensity)
+        with pytest.raises(OverflowError_):
+            e.results(0)
+
+
+def test_errors_are_reported_not_silent():
+    c = golden_case("tilted_fcc")
+    with engine_for(c.params) as e:
+        with pytest.raises(LmbError):
+            e.match([3], 5, 1.0)  # slot 3 holds no image
+        with pytest.raises(LmbError):
+            e.load_image(64, c.image)
