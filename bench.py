@@ -85,6 +85,10 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5:  # first sample before timing
+                time.sleep(0.02)
+            self.lines.clear()
         except Exception:
             self.proc = None
 
@@ -400,7 +404,7 @@ def run_reference(args, rank, world):
         return
     txt, p = workload_params(args.min_intensity)
     hkls = synth.hkls_cubic(8)
-    n_s = args.cpu_sample
+    n_s = args.ref_sample
     cores = os.cpu_count() or 1
     base = scratch_dir(n_s * (REC_BYTES_PER_ORIENT + 72))
     wd = tempfile.mkdtemp(prefix="lmb_ref_", dir=base)
@@ -469,14 +473,17 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n-orient", type=int, default=100_000_000)
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--min-intensity", type=float, default=200.0)
-    ap.add_argument("--cpu-sample", type=int, default=10_000_000)
+    ap.add_argument("--cpu-sample", type=int, default=10_000_000,
+                    help="orientations in the CPU-baseline sample of our arm")
+    ap.add_argument("--ref-sample", type=int, default=2_000_000,
+                    help="orientations per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
     args = ap.parse_args()

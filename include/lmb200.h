@@ -94,6 +94,15 @@ int lmb_engine_destroy(lmb_engine *e);
 /* cudaStream_t of the engine's compare pass (for external event timing). */
 void *lmb_engine_stream(lmb_engine *e);
 
+/* Launch shape of the compare pass: fields = {variant (0 block-barrier ring,
+ * 1 warp-specialised), tile_sub (32-orientation sub-tiles per tile), stages,
+ * consumer warps, blocks per SM, grid multiplier}; 0 = default.  Written by
+ * the autotuner; get returns the shape actually used for this DB.  No
+ * reference counterpart (the reference launches <<<ceil(n/1024),1024>>>,
+ * LaueMatchingGPU.cu:739-743). */
+int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields);
+int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields);
+
 /* Upload a forward cache (n records of 1+2S uint16) into device memory.
  * Replaces the chunked synchronous H2D of LaueMatchingGPU.cu:619-749 and
  * the resident upload of LaueMatchingGPUStream.cu:998-1038. */
@@ -158,6 +167,44 @@ int lmb_results(lmb_engine *e, int32_t slot, lmb_survivor *out,
 /* Device time of the last pass in milliseconds (CUDA events on the engine
  * stream): compare kernel, ordering kernel. */
 int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms);
+
+/* ---- host post-stage ------------------------------------------------------
+ * Duplicate merge (mergeDuplicateOrientations, LaueMatchingHeaders.h:969-1065)
+ * and refinement + output text (fitAndWriteOrientations, :1072-1153) for the
+ * survivors of one image, as LaueMatchingCPU.c:735-809 and
+ * LaueMatchingGPUStream.cu:436-533 call them.  The refinement optimiser
+ * evaluates the objective once at the coarse orientation (NLopt is not
+ * available here; the reference built with an evaluate-once NLopt writes the
+ * same text).  Grains are written in grain order. */
+typedef struct lmb_post_params {
+  double lattice[6];     /* LatticeParameter (nm, degrees) */
+  int32_t space_group;   /* SpaceGroup */
+  int32_t max_nr_spots;  /* unused: the fit uses 3*geometry max_nr_spots */
+  double tol_latc[6];    /* tol_LatC */
+  double tol_c_over_a;   /* tol_c_over_a (non-zero zeroes tol_latc) */
+  double max_angle;      /* MaxAngle (degrees) */
+  int32_t min_nr_spots;  /* MinNrSpots (CLI) or MinGoodSpots (daemon) */
+  int32_t image_num;     /* > 0: prepend the ImageNr column (daemon format) */
+  int32_t num_threads;   /* host threads */
+  int32_t optimizer;     /* 0 = evaluate once */
+} lmb_post_params;
+
+typedef struct lmb_post_output {
+  char *solutions; /* solutions.txt lines (no header), NUL terminated */
+  uint64_t solutions_len;
+  char *spots; /* spots.txt lines (no header) */
+  uint64_t spots_len;
+  int32_t n_unique; /* clusters after the merge ("Unique Orientations") */
+} lmb_post_output;
+
+/* ids/scores: the image's survivors in ascending id (the CPU collection
+ * order); orients: all n_orients matrices; image: the float image. */
+int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *pp,
+                     const double *orients, uint64_t n_orients,
+                     const uint64_t *ids, const double *scores,
+                     int64_t n_results, const float *image,
+                     const int32_t *hkls, int32_t nh, lmb_post_output *out);
+void lmb_post_free(lmb_post_output *out);
 
 /* Page-locked host buffers, so image uploads run at full link speed.  No
  * reference counterpart (the reference pins per-stream buffers internally,

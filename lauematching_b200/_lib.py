@@ -26,9 +26,11 @@ LMB_BUILD_EXACT_FP64 = 1
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = [
     "lmb_version", "lmb_last_error", "lmb_geometry_init", "lmb_engine_create",
-    "lmb_engine_destroy", "lmb_engine_stream", "lmb_db_upload", "lmb_db_build",
+    "lmb_engine_destroy", "lmb_engine_stream", "lmb_engine_set_tuning",
+    "lmb_engine_get_tuning", "lmb_db_upload", "lmb_db_build",
     "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
-    "lmb_match", "lmb_results", "lmb_last_pass_ms", "lmb_host_alloc", "lmb_host_free",
+    "lmb_match", "lmb_results", "lmb_last_pass_ms", "lmb_post_process", "lmb_post_free",
+    "lmb_host_alloc", "lmb_host_free",
 ]
 
 
@@ -44,6 +46,19 @@ class LmbGeometry(C.Structure):
 class LmbSurvivor(C.Structure):
     _fields_ = [("id", C.c_uint64), ("n_spots", C.c_int32), ("sum_u8", C.c_int32),
                 ("tot_int", C.c_double), ("score", C.c_double)]
+
+
+class LmbPostParams(C.Structure):
+    _fields_ = [("lattice", C.c_double * 6), ("space_group", C.c_int32),
+                ("max_nr_spots", C.c_int32), ("tol_latc", C.c_double * 6),
+                ("tol_c_over_a", C.c_double), ("max_angle", C.c_double),
+                ("min_nr_spots", C.c_int32), ("image_num", C.c_int32),
+                ("num_threads", C.c_int32), ("optimizer", C.c_int32)]
+
+
+class LmbPostOutput(C.Structure):
+    _fields_ = [("solutions", C.c_void_p), ("solutions_len", C.c_uint64),
+                ("spots", C.c_void_p), ("spots_len", C.c_uint64), ("n_unique", C.c_int32)]
 
 
 class LmbError(RuntimeError):
@@ -79,6 +94,8 @@ def lib():
         "lmb_engine_create": ([i32, C.POINTER(LmbGeometry), u64, C.POINTER(vp)], C.c_int),
         "lmb_engine_destroy": ([vp], C.c_int),
         "lmb_engine_stream": ([vp], vp),
+        "lmb_engine_set_tuning": ([vp, C.POINTER(i32), i32], C.c_int),
+        "lmb_engine_get_tuning": ([vp, C.POINTER(i32), i32], C.c_int),
         "lmb_db_upload": ([vp, vp, u64], C.c_int),
         "lmb_db_build": ([vp, vp, u64, vp, i32], C.c_int),
         "lmb_db_build_ex": ([vp, vp, u64, vp, i32, C.c_uint32], C.c_int),
@@ -90,6 +107,9 @@ def lib():
         "lmb_match": ([vp, u64, i32, dbl, i32], C.c_int),
         "lmb_results": ([vp, i32, vp, u64, C.POINTER(u64), C.POINTER(u64)], C.c_int),
         "lmb_last_pass_ms": ([vp, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+        "lmb_post_process": ([C.POINTER(LmbGeometry), C.POINTER(LmbPostParams), vp, u64, vp, vp,
+                              C.c_int64, vp, vp, i32, C.POINTER(LmbPostOutput)], C.c_int),
+        "lmb_post_free": ([C.POINTER(LmbPostOutput)], None),
         "lmb_host_alloc": ([u64, C.POINTER(vp)], C.c_int),
         "lmb_host_free": ([vp], C.c_int),
     }

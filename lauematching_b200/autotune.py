@@ -1,0 +1,136 @@
+"""Autotuner of the compare pass launch shape.
+
+Sweeps kernel variant (block-barrier ring / warp-specialised), tile size,
+ring depth, consumer warps and grid size on the device for a DB of the given
+record size and batch width, checks that every shape returns the same
+survivors, and writes the fastest shape per (record words, batch bucket) to
+``tuning.json`` next to this file.  Engines load that table at creation.
+
+    python -m lauematching_b200.autotune --n-orient 100000000 --batch 64
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import os
+import statistics
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE = os.path.join(HERE, "tuning.json")
+BATCH_BUCKETS = (1, 4, 16, 64)
+
+
+def batch_bucket(k: int) -> int:
+    for b in BATCH_BUCKETS:
+        if k <= b:
+            return b
+    return BATCH_BUCKETS[-1]
+
+
+def load_table() -> dict:
+    if os.path.exists(TABLE):
+        with open(TABLE) as f:
+            return json.load(f)
+    return {}
+
+
+def lookup(R: int, k: int) -> dict | None:
+    """Best shape for records of R uint16 words and a pass of k images."""
+    t = load_table().get("entries", {})
+    key = f"R{R}_K{batch_bucket(k)}"
+    if key in t:
+        return t[key]["shape"]
+    # nearest record size with the same batch bucket
+    cands = [(abs(int(kk.split("_")[0][1:]) - R), v) for kk, v in t.items()
+             if kk.endswith(f"_K{batch_bucket(k)}")]
+    return min(cands, key=lambda x: x[0])[1]["shape"] if cands else None
+
+
+def candidate_shapes():
+    for ts, st, cons in itertools.product((4, 8), (4, 6, 8, 12), (8, 12, 16)):
+        yield dict(variant=1, tile_sub=ts, stages=st, consumers=cons)
+    for ts, st, bps in itertools.product((4, 8), (2, 3, 4), (1, 2, 3)):
+        yield dict(variant=0, tile_sub=ts, stages=st, blocks_per_sm=bps)
+
+
+def time_shape(e, slots, p, reps=5, warm=2):
+    for _ in range(warm):
+        e.match(slots, p.min_nr_spots, p.min_intensity)
+        e.last_pass_ms()
+    ms = []
+    for _ in range(reps):
+        e.match(slots, p.min_nr_spots, p.min_intensity)
+        ms.append(e.last_pass_ms()[0])
+    return statistics.median(ms)
+
+
+def main():
+    sys.path.insert(0, os.path.dirname(HERE))
+    from lauematching_b200 import synth, params as P
+    from lauematching_b200.engine import Engine
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n-orient", type=int, default=100_000_000)
+    ap.add_argument("--batches", type=str, default="1,64")
+    ap.add_argument("--max-nr-spots", type=int, default=30)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--write", action="store_true", help="update tuning.json")
+    args = ap.parse_args()
+    txt = synth.params_text(max_nr_spots=args.max_nr_spots, min_nr_spots=5, min_intensity=200.0)
+    p = P.parse_params_text(txt)
+    hk = synth.hkls_cubic(8)
+    e = Engine(p)
+    t0 = time.time()
+    e.build_db_synthetic(args.seed, args.n_orient, hk)
+    print(f"DB of {args.n_orient} built in {time.time() - t0:.1f} s", file=sys.stderr)
+    rec = e.download_db(0, min(2_000_000, args.n_orient))
+    rng = np.random.default_rng(7)
+    kmax = max(int(b) for b in args.batches.split(","))
+    for k in range(kmax):
+        g = synth.pick_grains(rec, int(rng.integers(1, 21)), p.min_nr_spots, rng)
+        e.load_image(k, synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng).astype(np.uint8),
+                     want_scale=False)
+    table = load_table()
+    entries = table.setdefault("entries", {})
+    R = 1 + 2 * args.max_nr_spots
+    for kb in (int(b) for b in args.batches.split(",")):
+        slots = list(range(kb))
+        ref = None
+        results = []
+        for shape in candidate_shapes():
+            e.set_tuning(**shape)
+            try:
+                ms = time_shape(e, slots, p)
+            except Exception as exc:  # a shape that does not fit is skipped
+                print(f"skip {shape}: {exc}", file=sys.stderr)
+                continue
+            got = [e.results(k)[0] for k in slots]
+            if ref is None:
+                ref = got
+            same = all(np.array_equal(a, b) for a, b in zip(ref, got))
+            used = e.get_tuning()
+            results.append((ms, used, same))
+            print(f"K={kb} {used} {ms:.4f} ms identical={same}", file=sys.stderr)
+        ok = [r for r in results if r[2]]
+        best = min(ok, key=lambda r: r[0])
+        bytes_pass = args.n_orient * R * 2 + kb * p.nr_px_x * p.nr_px_y
+        entries[f"R{R}_K{batch_bucket(kb)}"] = {
+            "shape": best[1], "compare_ms": round(best[0], 4),
+            "gbs": round(bytes_pass / (best[0] * 1e-3) / 1e9, 1), "n_orient": args.n_orient,
+            "swept": len(results),
+            "all": [{"shape": r[1], "ms": round(r[0], 4)} for r in sorted(results, key=lambda r: r[0])],
+        }
+        print(json.dumps({"K": kb, "best": best[1], "ms": best[0]}))
+    table["device"] = "NVIDIA B200"
+    if args.write:
+        with open(TABLE, "w") as f:
+            json.dump(table, f, indent=1)
+    e.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "liblmb200.so")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2,-fopenmp",
     "--expt-relaxed-constexpr",
 ]
 
@@ -65,7 +65,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
         objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
-           "-o", tmp, *objs, "-cudart", "static"]
+           "-o", tmp, *objs, "-cudart", "static", "-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -132,7 +132,8 @@ __device__ __noinline__ void candidate(const CmpArgs &a, const uint16_t *rec, in
 }
 
 template <int B>
-__device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, uint64_t oid) {
+__device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, uint64_t oid,
+                                        uint64_t pol) {
   int c = rec[0];
   if (c > a.S) c = a.S;  // clamp like LaueMatchingGPU.cu:54-55
   unsigned long long cnt[B];
@@ -148,7 +149,7 @@ __device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, u
       if (s < c) {
         const int x = rec[1 + 2 * s], y = rec[2 + 2 * s];
         if (x < a.W && y < a.H)  // skip like LaueMatchingGPU.cu:65
-          m[j] = __ldg(a.occ + (size_t)y * a.W + x);
+          m[j] = ld_nc_hint(a.occ + (size_t)y * a.W + x, pol);
       }
     }
 #pragma unroll
@@ -183,14 +184,17 @@ __device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, u
   }
 }
 
+// Variant 0: every thread consumes; thread 0 refills the ring after a block
+// barrier.  One orientation per thread per tile.
 template <int B>
-__global__ void __launch_bounds__(256) compare_kernel(const __grid_constant__ CmpArgs a) {
+__global__ void __launch_bounds__(256) compare_ring_kernel(const __grid_constant__ CmpArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-  unsigned char *ring = smem + 128;
-  const uint32_t TILE = blockDim.x;
+  unsigned char *ring = smem + 256;
+  const uint32_t TILE = a.tile;
   const uint64_t G = gridDim.x;
   const int stages = a.stages;
+  const uint64_t pol_db = l2_evict_first(), pol_occ = l2_evict_last();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < stages; s++) mbar_init(&bars[s], 1);
@@ -202,9 +206,9 @@ __global__ void __launch_bounds__(256) compare_kernel(const __grid_constant__ Cm
       const uint64_t tile = blockIdx.x + (uint64_t)s * G;
       if (tile < a.full_tiles) {
         mbar_expect_tx(&bars[s], a.tile_bytes);
-        bulk_g2s(ring + (size_t)s * a.tile_bytes,
-                 reinterpret_cast<const unsigned char *>(a.db) + tile * a.tile_bytes,
-                 a.tile_bytes, &bars[s]);
+        bulk_g2s_hint(ring + (size_t)s * a.tile_bytes,
+                      reinterpret_cast<const unsigned char *>(a.db) + tile * a.tile_bytes,
+                      a.tile_bytes, &bars[s], pol_db);
       }
     }
   }
@@ -229,19 +233,96 @@ __global__ void __launch_bounds__(256) compare_kernel(const __grid_constant__ Cm
       }
       const uint16_t *rec = reinterpret_cast<const uint16_t *>(ring + (size_t)s * a.tile_bytes) +
                             (size_t)threadIdx.x * a.R;
-      process<B>(a, rec, oid);
+      process<B>(a, rec, oid, pol_occ);
     } else if (oid < a.n) {
-      process<B>(a, a.db + oid * a.R, oid);  // partial last tile: direct loads
+      process<B>(a, a.db + oid * a.R, oid, pol_occ);  // partial last tile: direct loads
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       const uint64_t nt = tile + (uint64_t)stages * G;
       if (nt < a.full_tiles) {
         mbar_expect_tx(&bars[s], a.tile_bytes);
-        bulk_g2s(ring + (size_t)s * a.tile_bytes,
-                 reinterpret_cast<const unsigned char *>(a.db) + nt * a.tile_bytes, a.tile_bytes,
-                 &bars[s]);
+        bulk_g2s_hint(ring + (size_t)s * a.tile_bytes,
+                      reinterpret_cast<const unsigned char *>(a.db) + nt * a.tile_bytes,
+                      a.tile_bytes, &bars[s], pol_db);
       }
+    }
+  }
+}
+
+// Variant 1: warp-specialised.  Warp 0 (one lane) is the producer: it
+// refills a stage as soon as the consumers release it (empty barrier), so
+// there is no block barrier on the stream.  Consumer warps are grouped: a
+// group of tile_sub warps takes one tile (each warp 32 orientations), the
+// groups take successive tiles of this block in turn.  Tiles that share a
+// stage belong to the same group (stages % groups == 0), so no waiter is ever
+// more than one barrier phase ahead.
+template <int B>
+__global__ void __launch_bounds__(576, 1) compare_ws_kernel(const __grid_constant__ CmpArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int ST = a.stages;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *empty = full + 16;
+  unsigned char *ring = smem + 256;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int TS = a.tile_sub;
+  const int NG = a.consumers / TS;
+  const uint64_t G = gridDim.x;
+  const uint64_t my_tiles = (a.ntiles > blockIdx.x) ? (a.ntiles - 1 - blockIdx.x) / G + 1 : 0;
+  const uint64_t my_full =
+      (a.full_tiles > blockIdx.x) ? (a.full_tiles - 1 - blockIdx.x) / G + 1 : 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], TS);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    if (lane != 0) return;
+    const uint64_t pol_db = l2_evict_first();
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < my_full; i++) {
+      const int s = (int)(i % ST);
+      if (i >= (uint64_t)ST &&
+          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+        atomicExch(a.err, DEV_TIMEOUT_TMA);
+        break;
+      }
+      mbar_expect_tx(&full[s], a.tile_bytes);
+      bulk_g2s_hint(ring + (size_t)s * a.tile_bytes,
+                    reinterpret_cast<const unsigned char *>(a.db) +
+                        (blockIdx.x + i * G) * (uint64_t)a.tile_bytes,
+                    a.tile_bytes, &full[s], pol_db);
+      issued = i + 1;
+    }
+    // stay until the last copies have landed (bounded)
+    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
+      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    return;
+  }
+  const int cw = warp - 1;
+  const int g = cw / TS, sub = cw % TS;
+  if (g >= NG) return;
+  const uint64_t pol_occ = l2_evict_last();
+  for (uint64_t i = g; i < my_tiles; i += NG) {
+    const uint64_t tile = blockIdx.x + i * G;
+    const uint64_t oid = tile * a.tile + (uint64_t)sub * 32 + lane;
+    if (i < my_full) {
+      const int s = (int)(i % ST);
+      const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
+        return;
+      }
+      const uint16_t *rec = reinterpret_cast<const uint16_t *>(ring + (size_t)s * a.tile_bytes) +
+                            (size_t)(sub * 32 + lane) * a.R;
+      process<B>(a, rec, oid, pol_occ);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    } else if (oid < a.n) {
+      process<B>(a, a.db + oid * a.R, oid, pol_occ);  // partial last tile: direct loads
     }
   }
 }
@@ -323,56 +404,76 @@ static int counter_bits(int S) {
   return b;
 }
 
-struct CompareConfig {
-  int tile;    // orientations per tile (threads per block)
-  int stages;  // TMA ring depth
-  int blocks_per_sm;
-};
-
-CompareConfig compare_config(int R) {
-  CompareConfig c;
-  c.tile = 256;
-  while (c.tile > 32 && (size_t)c.tile * R * 2 > 48 * 1024) c.tile /= 2;
-  const size_t tb = (size_t)c.tile * R * 2;
-  c.stages = (int)std::min<size_t>(4, std::max<size_t>(2, (96 * 1024) / tb));
-  c.blocks_per_sm = 2;
+// Launch shape for records of R uint16: the fields set in `req` (from the
+// tuning table), defaults for the rest, clamped to what fits.
+CompareTuning compare_config(int R, const CompareTuning &req) {
+  CompareTuning c = req;
+  const size_t rb = (size_t)R * 2;
+  if (c.variant == 1) {
+    if (c.tile_sub <= 0) c.tile_sub = 8;
+    while (c.tile_sub > 1 && (size_t)c.tile_sub * 32 * rb * 3 > 200 * 1024) c.tile_sub /= 2;
+    if (c.stages <= 0) c.stages = (int)std::min<size_t>(12, (200 * 1024) / ((size_t)c.tile_sub * 32 * rb));
+    if (c.consumers <= 0) c.consumers = 16;
+    c.consumers = std::min(c.consumers, 17);  // 18 warps per block at most
+    int groups = std::max(1, c.consumers / c.tile_sub);
+    while (groups > 1 && c.stages % groups) groups--;
+    c.consumers = groups * c.tile_sub;
+    c.blocks_per_sm = 1;
+  } else {
+    c.variant = 0;
+    if (c.tile_sub <= 0 || c.tile_sub > 8) c.tile_sub = 8;  // one thread per orientation, <= 256
+    while (c.tile_sub > 1 && (size_t)c.tile_sub * 32 * rb > 48 * 1024) c.tile_sub /= 2;
+    const size_t tb = (size_t)c.tile_sub * 32 * rb;
+    if (c.stages <= 0) c.stages = (int)std::min<size_t>(4, std::max<size_t>(2, (96 * 1024) / tb));
+    if (c.blocks_per_sm <= 0) c.blocks_per_sm = 2;
+    c.consumers = c.tile_sub;
+  }
+  if (c.stages > 16) c.stages = 16;
+  if (c.stages < 2) c.stages = 2;
   return c;
 }
 
-size_t compare_smem_bytes(int R) {
-  const CompareConfig c = compare_config(R);
-  return 128 + (size_t)c.stages * c.tile * R * 2;
-}
-
 template <int B>
-static int launch_b(const CmpArgs &a, unsigned grid, int tile, size_t smem, cudaStream_t st) {
-  LMB_CUDA(cudaFuncSetAttribute(compare_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
-  compare_kernel<B><<<grid, tile, smem, st>>>(a);
+static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, size_t smem,
+                    cudaStream_t st) {
+  if (c.variant == 1) {
+    LMB_CUDA(cudaFuncSetAttribute(compare_ws_kernel<B>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    compare_ws_kernel<B><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
+  } else {
+    LMB_CUDA(cudaFuncSetAttribute(compare_ring_kernel<B>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    compare_ring_kernel<B><<<grid, a.tile, smem, st>>>(a);
+  }
   LMB_CUDA(cudaGetLastError());
   return LMB_OK;
 }
 
-int compare_launch(CmpArgs a, int num_sms, cudaStream_t st) {
+int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_t st) {
   LMB_REQUIRE((reinterpret_cast<uintptr_t>(a.db) & 15) == 0,
               "DB device pointer must be 16-byte aligned");
-  const CompareConfig c = compare_config(a.R);
-  a.tile_bytes = (uint32_t)((size_t)c.tile * a.R * 2);  // tile multiple of 8 -> multiple of 16
-  a.full_tiles = a.n / c.tile;
-  a.ntiles = (a.n + c.tile - 1) / c.tile;
+  const CompareTuning c = compare_config(a.R, req);
+  a.tile_sub = c.tile_sub;
+  a.consumers = c.consumers;
+  a.tile = (uint32_t)c.tile_sub * 32;
+  a.tile_bytes = (uint32_t)((size_t)a.tile * a.R * 2);  // tile multiple of 8 -> multiple of 16
+  a.full_tiles = a.n / a.tile;
+  a.ntiles = (a.n + a.tile - 1) / a.tile;
   a.stages = c.stages;
   if (a.ntiles == 0 || a.active == 0) return LMB_OK;
-  const size_t smem = compare_smem_bytes(a.R);
-  const unsigned grid =
-      (unsigned)std::min<uint64_t>(a.ntiles, (uint64_t)num_sms * c.blocks_per_sm);
+  const size_t smem = 256 + (size_t)c.stages * a.tile_bytes;
+  LMB_REQUIRE(smem <= 227 * 1024, "compare ring of %zu bytes exceeds shared memory", smem);
+  const int mult = c.grid_mult > 0 ? c.grid_mult : 1;
+  const unsigned grid = (unsigned)std::min<uint64_t>(
+      a.ntiles, (uint64_t)num_sms * c.blocks_per_sm * (uint64_t)mult);
   const int B = counter_bits(a.S);
-  if (B <= 3) return launch_b<3>(a, grid, c.tile, smem, st);
-  if (B <= 5) return launch_b<5>(a, grid, c.tile, smem, st);
-  if (B <= 6) return launch_b<6>(a, grid, c.tile, smem, st);
-  if (B <= 7) return launch_b<7>(a, grid, c.tile, smem, st);
-  if (B <= 9) return launch_b<9>(a, grid, c.tile, smem, st);
-  if (B <= 11) return launch_b<11>(a, grid, c.tile, smem, st);
-  return launch_b<16>(a, grid, c.tile, smem, st);
+  if (B <= 3) return launch_b<3>(a, c, grid, smem, st);
+  if (B <= 5) return launch_b<5>(a, c, grid, smem, st);
+  if (B <= 6) return launch_b<6>(a, c, grid, smem, st);
+  if (B <= 7) return launch_b<7>(a, c, grid, smem, st);
+  if (B <= 9) return launch_b<9>(a, c, grid, smem, st);
+  if (B <= 11) return launch_b<11>(a, c, grid, smem, st);
+  return launch_b<16>(a, c, grid, smem, st);
 }
 
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st) {

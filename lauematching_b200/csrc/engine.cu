@@ -59,6 +59,7 @@ struct lmb_engine {
   uint64_t last_mask = 0;
   bool pending = false;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  CompareTuning tuning{1, 0, 0, 0, 0, 0};  // warp-specialised, default shape
 };
 
 namespace {
@@ -400,7 +401,7 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   a.pass_cnt = e->d_status + LMB_MAX_SLOTS;
   a.err = reinterpret_cast<int *>(e->d_status + 2 * LMB_MAX_SLOTS);
   if (min_nr_spots <= e->S && !std::isnan(min_intensity)) {
-    rc = compare_launch(a, e->num_sms, e->st);
+    rc = compare_launch(a, e->tuning, e->num_sms, e->st);
     if (rc) return rc;
   }
   LMB_CUDA(cudaEventRecord(e->ev[1], e->st));
@@ -467,6 +468,26 @@ int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms) {
   LMB_CUDA(cudaEventElapsedTime(&b, e->ev[1], e->ev[2]));
   if (compare_ms) *compare_ms = a;
   if (order_ms) *order_ms = b;
+  return LMB_OK;
+}
+
+int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields) {
+  LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
+  CompareTuning t{1, 0, 0, 0, 0, 0};
+  int32_t *dst[6] = {&t.variant, &t.tile_sub, &t.stages, &t.consumers, &t.blocks_per_sm,
+                     &t.grid_mult};
+  for (int i = 0; i < n_fields && i < 6; i++) *dst[i] = fields[i];
+  LMB_REQUIRE(t.variant == 0 || t.variant == 1, "unknown compare variant %d", t.variant);
+  e->tuning = t;
+  return LMB_OK;
+}
+
+int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields) {
+  LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
+  const CompareTuning c = compare_config(e->R, e->tuning);
+  const int32_t src[6] = {c.variant, c.tile_sub, c.stages, c.consumers, c.blocks_per_sm,
+                          c.grid_mult};
+  for (int i = 0; i < n_fields && i < 6; i++) fields[i] = src[i];
   return LMB_OK;
 }
 

@@ -28,8 +28,22 @@ struct CmpArgs {
   // filled by compare_launch
   uint64_t full_tiles, ntiles;
   uint32_t tile_bytes;
-  int stages;
+  uint32_t tile;  // orientations per tile (tile_sub * 32)
+  int stages;     // TMA ring depth
+  int tile_sub;   // 32-orientation sub-tiles per tile
+  int consumers;  // consumer warps (warp-specialised variant)
 };
+
+// Launch shape of the compare pass (autotuned; zero fields = defaults).
+struct CompareTuning {
+  int variant;        // 0 = block-barrier ring, 1 = warp-specialised
+  int tile_sub;       // 32-orientation sub-tiles per tile
+  int stages;         // ring depth
+  int consumers;      // consumer warps (variant 1)
+  int blocks_per_sm;  // resident blocks per SM (variant 0)
+  int grid_mult;      // grid = SMs * blocks_per_sm * grid_mult
+};
+CompareTuning compare_config(int R, const CompareTuning &req);
 
 // Ordering of the survivor lists of a pass by orientation ID (compare.cu).
 struct OrderArgs {
@@ -49,7 +63,7 @@ int synth_orient_launch(uint64_t seed, uint64_t first, uint64_t n, double *d_out
 int quantize_launch(const void *d_img, int dtype, size_t npx, unsigned long long *d_max_bits,
                     uint8_t *d_u8, double *d_f64_keep, unsigned long long *d_occ, int slot,
                     double *d_scale_slot, int num_sms, cudaStream_t st);
-int compare_launch(CmpArgs a, int num_sms, cudaStream_t st);
+int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_t st);
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st);
 
 }  // namespace lmb

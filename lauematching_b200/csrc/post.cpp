@@ -1,0 +1,664 @@
+// Host post-stage after the compare pass: duplicate merge, orientation
+// refinement objective, solutions/spots text.
+//
+// Restates, in the reference's operation order (FP64, glibc libm, printf):
+//   mergeDuplicateOrientations  LaueMatchingHeaders.h:969-1065
+//   fitAndWriteOrientations     LaueMatchingHeaders.h:1072-1153
+//   (prefilterHKLs :513-561, calcOverlapFiltered :564-636, problem_function
+//    :640-694, FitOrientation :696-801, writeCalcOverlap :805-947, and the
+//    quaternion / Euler / symmetry utilities :147-347).
+// The symmetry quaternion tables must hold the reference's values (5-decimal
+// roundings) in the reference's order, because the fundamental-region
+// reduction keeps the first maximum; they are data, listed below.
+//
+// Refinement.  The reference refines each grain with NLopt (BOBYQA or
+// Nelder-Mead, 200 evaluations).  NLopt is not available here, so the
+// optimiser of this stage evaluates the objective once at the start point and
+// returns it unchanged; the reference built against the same evaluate-once
+// NLopt stand-in writes byte-identical files.
+//
+// Output order.  The reference writes grains from an OpenMP loop inside a
+// critical section, so its line order depends on thread timing; here grains
+// are evaluated in parallel and written in grain order (the reference's order
+// with one thread).
+#include <omp.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lmb200.h"
+
+namespace lmb {
+void set_error(const char *fmt, ...);
+}
+
+namespace {
+
+constexpr double kDeg2Rad = 0.0174532925199433;  // LaueMatchingHeaders.h:32
+constexpr double kRad2Deg = 57.2957795130823;    // :33
+constexpr double kEps = 1E-12;                    // :42
+constexpr double kHc = 1.2398419739;              // :41
+constexpr int kMergeMax = 50000;                  // :953
+
+// Symmetry quaternions (w, x, y, z) per crystal system, LaueMatchingHeaders.h:83-145.
+const double kTric[1][4] = {{1, 0, 0, 0}};
+const double kMono[2][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}};
+const double kOrth[4][4] = {{1, 0, 0, 0}, {1, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+const double kTetr[8][4] = {{1, 0, 0, 0},          {0.70711, 0, 0, 0.70711}, {0, 0, 0, 1},
+                            {0.70711, -0.0, -0.0, -0.70711}, {0, 1, 0, 0},   {0, 0, 1, 0},
+                            {0, 0.70711, 0.70711, 0},        {0, -0.70711, 0.70711, 0}};
+const double kTrig[6][4] = {{1, 0, 0, 0},          {0, 0.86603, -0.5, 0}, {0.5, 0, 0, 0.86603},
+                            {0, 0, 1, 0},          {0.5, -0.0, -0.0, -0.86603},
+                            {0, 0.86603, 0.5, 0}};
+const double kHexa[12][4] = {{1, 0, 0, 0},           {0.86603, 0, 0, 0.5},
+                             {0.5, 0, 0, 0.86603},   {0, 0, 0, 1},
+                             {0.5, -0.0, -0.0, -0.86603}, {0.86603, -0.0, -0.0, -0.5},
+                             {0, 1, 0, 0},           {0, 0.86603, 0.5, 0},
+                             {0, 0.5, 0.86603, 0},   {0, 0, 1, 0},
+                             {0, -0.5, 0.86603, 0},  {0, -0.86603, 0.5, 0}};
+const double kCubi[24][4] = {
+    {1, 0, 0, 0},          {0.70711, 0.70711, 0, 0},  {0, 1, 0, 0},
+    {0.70711, -0.70711, 0, 0}, {0.70711, 0, 0.70711, 0}, {0, 0, 1, 0},
+    {0.70711, 0, -0.70711, 0}, {0.70711, 0, 0, 0.70711}, {0, 0, 0, 1},
+    {0.70711, 0, 0, -0.70711}, {0.5, 0.5, 0.5, 0.5},      {0.5, -0.5, -0.5, -0.5},
+    {0.5, -0.5, 0.5, 0.5},     {0.5, 0.5, -0.5, -0.5},    {0.5, 0.5, -0.5, 0.5},
+    {0.5, -0.5, 0.5, -0.5},    {0.5, -0.5, -0.5, 0.5},    {0.5, 0.5, 0.5, -0.5},
+    {0, 0.70711, 0.70711, 0},  {0, -0.70711, 0.70711, 0}, {0, 0.70711, 0, 0.70711},
+    {0, 0.70711, 0, -0.70711}, {0, 0, 0.70711, 0.70711}, {0, 0, 0.70711, -0.70711}};
+
+struct Sym {
+  int n = 1;
+  double q[24][4];
+};
+
+Sym make_sym(int sg) {  // MakeSymmetries, :180-219
+  Sym s;
+  const double(*t)[4];
+  if (sg <= 2) {
+    s.n = 1, t = kTric;
+  } else if (sg <= 15) {
+    s.n = 2, t = kMono;
+  } else if (sg <= 74) {
+    s.n = 4, t = kOrth;
+  } else if (sg <= 142) {
+    s.n = 8, t = kTetr;
+  } else if (sg <= 167) {
+    s.n = 6, t = kTrig;
+  } else if (sg <= 194) {
+    s.n = 12, t = kHexa;
+  } else {
+    s.n = 24, t = kCubi;
+  }
+  for (int i = 0; i < s.n; i++)
+    for (int j = 0; j < 4; j++) s.q[i][j] = t[i][j];
+  return s;
+}
+
+inline double length3(double x, double y, double z) { return std::sqrt(x * x + y * y + z * z); }
+inline double zero_out(double v) { return (std::fabs(v) < kEps) ? 0 : v; }
+
+void normalize4(double q[4]) {
+  const double n = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  q[0] /= n;
+  q[1] /= n;
+  q[2] /= n;
+  q[3] /= n;
+}
+
+// Quaternion product as LaueMatchingHeaders.h:166-178 (w>=0 hemisphere, normalised).
+void qmul(const double q[4], const double r[4], double Q[4]) {
+  Q[0] = r[0] * q[0] - r[1] * q[1] - r[2] * q[2] - r[3] * q[3];
+  Q[1] = r[1] * q[0] + r[0] * q[1] + r[3] * q[2] - r[2] * q[3];
+  Q[2] = r[2] * q[0] + r[0] * q[2] + r[1] * q[3] - r[3] * q[1];
+  Q[3] = r[3] * q[0] + r[0] * q[3] + r[2] * q[1] - r[1] * q[2];
+  if (Q[0] < 0) {
+    Q[0] = -Q[0];
+    Q[1] = -Q[1];
+    Q[2] = -Q[2];
+    Q[3] = -Q[3];
+  }
+  normalize4(Q);
+}
+
+void to_fundamental(const Sym &S, const double in[4], double out[4]) {  // :221-245
+  int best = 0;
+  double best_w = -10000, cand[24][4];
+  for (int i = 0; i < S.n; i++) {
+    qmul(in, S.q[i], cand[i]);
+    if (best_w < cand[i][0]) {
+      best_w = cand[i][0];
+      best = i;
+    }
+  }
+  for (int j = 0; j < 4; j++) out[j] = cand[best][j];
+  normalize4(out);
+}
+
+double misorientation_deg(const Sym &S, const double a[4], const double b[4]) {  // :247-260
+  double af[4], bf[4], ai[4], p[4], m[4];
+  to_fundamental(S, a, af);
+  to_fundamental(S, b, bf);
+  ai[0] = -af[0];
+  ai[1] = af[1];
+  ai[2] = af[2];
+  ai[3] = af[3];
+  qmul(ai, bf, p);
+  to_fundamental(S, p, m);
+  if (m[0] > 1) m[0] = 1;
+  return 2 * (std::acos(m[0])) * kRad2Deg;
+}
+
+void om_to_quat(const double m[9], double q[4]) {  // OrientMat2Quat, :262-302
+  const double tr = m[0] + m[4] + m[8];
+  if (tr > 0) {
+    const double s = 0.5 / std::sqrt(tr + 1.0);
+    q[0] = 0.25 / s;
+    q[1] = (m[7] - m[5]) * s;
+    q[2] = (m[2] - m[6]) * s;
+    q[3] = (m[3] - m[1]) * s;
+  } else if (m[0] > m[4] && m[0] > m[8]) {
+    const double s = 2.0 * std::sqrt(1.0 + m[0] - m[4] - m[8]);
+    q[0] = (m[7] - m[5]) / s;
+    q[1] = 0.25 * s;
+    q[2] = (m[1] + m[3]) / s;
+    q[3] = (m[2] + m[6]) / s;
+  } else if (m[4] > m[8]) {
+    const double s = 2.0 * std::sqrt(1.0 + m[4] - m[0] - m[8]);
+    q[0] = (m[2] - m[6]) / s;
+    q[1] = (m[1] + m[3]) / s;
+    q[2] = 0.25 * s;
+    q[3] = (m[5] + m[7]) / s;
+  } else {
+    const double s = 2.0 * std::sqrt(1.0 + m[8] - m[0] - m[4]);
+    q[0] = (m[3] - m[1]) / s;
+    q[1] = (m[2] + m[6]) / s;
+    q[2] = (m[5] + m[7]) / s;
+    q[3] = 0.25 * s;
+  }
+  if (q[0] < 0) {
+    q[0] = -q[0];
+    q[1] = -q[1];
+    q[2] = -q[2];
+    q[3] = -q[3];
+  }
+  normalize4(q);
+}
+
+inline double angle_from_sc(double s, double c) {  // sin_cos_to_angle, :149-151
+  return (s >= 0.0) ? std::acos(c) : 2.0 * M_PI - std::acos(c);
+}
+
+void om_to_euler(const double m[3][3], double e[3]) {  // OrientMat2Euler, :313-332
+  double psi, phi, theta;
+  if (std::fabs(m[2][2] - 1.0) < kEps)
+    phi = 0;
+  else
+    phi = std::acos(m[2][2]);
+  const double sph = std::sin(phi);
+  if (std::fabs(sph) < kEps) {
+    psi = 0.0;
+    theta = (std::fabs(m[2][2] - 1.0) < kEps) ? angle_from_sc(m[1][0], m[0][0])
+                                               : angle_from_sc(-m[1][0], m[0][0]);
+  } else {
+    psi = (std::fabs(-m[1][2] / sph) <= 1.0) ? angle_from_sc(m[0][2] / sph, -m[1][2] / sph)
+                                             : angle_from_sc(m[0][2] / sph, 1);
+    theta = (std::fabs(m[2][1] / sph) <= 1.0) ? angle_from_sc(m[2][0] / sph, m[2][1] / sph)
+                                              : angle_from_sc(m[2][0] / sph, 1);
+  }
+  e[0] = psi;
+  e[1] = phi;
+  e[2] = theta;
+}
+
+void euler_to_om(const double e[3], double m[3][3]) {  // Euler2OrientMat, :334-347
+  const double psi = e[0], phi = e[1], theta = e[2];
+  const double cps = std::cos(psi), cph = std::cos(phi), cth = std::cos(theta);
+  const double sps = std::sin(psi), sph = std::sin(phi), sth = std::sin(theta);
+  m[0][0] = cth * cps - sth * cph * sps;
+  m[0][1] = -cth * cph * sps - sth * cps;
+  m[0][2] = sph * sps;
+  m[1][0] = cth * sps + sth * cph * cps;
+  m[1][1] = cth * cph * cps - sth * sps;
+  m[1][2] = -sph * cps;
+  m[2][0] = sth * sph;
+  m[2][1] = cth * sph;
+  m[2][2] = cph;
+}
+
+void mat33(const double m[3][3], const double n[3][3], double r[3][3]) {  // :349-357
+  for (int i = 0; i < 3; i++) {
+    r[i][0] = m[i][0] * n[0][0] + m[i][1] * n[1][0] + m[i][2] * n[2][0];
+    r[i][1] = m[i][0] * n[0][1] + m[i][1] * n[1][1] + m[i][2] * n[2][1];
+    r[i][2] = m[i][0] * n[0][2] + m[i][1] * n[1][2] + m[i][2] * n[2][2];
+  }
+}
+
+void matvec(const double m[3][3], const double v[3], double r[3]) {  // :361-369
+  r[0] = 0;
+  r[1] = 0;
+  r[2] = 0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) r[i] += m[i][j] * v[j];
+}
+
+void recip_of(const double lat[6], int sg, double recip[3][3]) {  // calcRecipArray, :379-436
+  const double a = lat[0], b = lat[1], c = lat[2];
+  const bool rh = sg == 146 || sg == 148 || sg == 155 || sg == 160 || sg == 161 || sg == 166 ||
+                  sg == 167;
+  const double ca = std::cos(lat[3] * kDeg2Rad), cb = std::cos(lat[4] * kDeg2Rad);
+  const double cg = std::cos(lat[5] * kDeg2Rad), sgm = std::sin(lat[5] * kDeg2Rad);
+  const double phi = std::sqrt(1.0 - ca * ca - cb * cb - cg * cg + 2 * ca * cb * cg);
+  const double pv = (2 * M_PI) / (a * b * c * phi);
+  double a0, a1, a2, b0, b1, b2, c0, c1, c2;
+  if (!rh) {
+    a0 = zero_out(a), a1 = zero_out(0.0), a2 = zero_out(0.0);
+    b0 = b * cg, b1 = zero_out(b * sgm), b2 = zero_out(0.0);
+    c0 = c * cb, c1 = c * (ca - cb * cg) / sgm, c2 = zero_out(c * phi / sgm);
+  } else {
+    const double p = std::sqrt(1.0 + 2 * ca), q = std::sqrt(1.0 - ca);
+    const double pmq = (a / 3.0) * (p - q), p2q = (a / 3.0) * (p + 2 * q);
+    a0 = p2q, a1 = pmq, a2 = pmq, b0 = pmq, b1 = p2q, b2 = pmq, c0 = pmq, c1 = pmq, c2 = p2q;
+  }
+  recip[0][0] = zero_out((b1 * c2 - b2 * c1) * pv);
+  recip[1][0] = zero_out((b2 * c0 - b0 * c2) * pv);
+  recip[2][0] = zero_out((b0 * c1 - b1 * c0) * pv);
+  recip[0][1] = zero_out((c1 * a2 - c2 * a1) * pv);
+  recip[1][1] = zero_out((c2 * a0 - c0 * a2) * pv);
+  recip[2][1] = zero_out((c0 * a1 - c1 * a0) * pv);
+  recip[0][2] = zero_out((a1 * b2 - a2 * b1) * pv);
+  recip[1][2] = zero_out((a2 * b0 - a0 * b2) * pv);
+  recip[2][2] = zero_out((a0 * b1 - a1 * b0) * pv);
+}
+
+struct Detector {
+  double rt[3][3];
+  double p[3];
+  double px_x, px_y, elo, ehi;
+  int W, H;
+};
+
+// One reflection through the detector model (steps shared by prefilterHKLs,
+// calcOverlapFiltered and writeCalcOverlap).  Returns false when rejected;
+// px/py are the unrounded pixel coordinates.
+inline bool project(const double OM[3][3], const int *hkl, const Detector &d, double qhat[3],
+                    double &px, double &py, double &qlen) {
+  const double h[3] = {(double)hkl[0], (double)hkl[1], (double)hkl[2]};
+  double q[3];
+  matvec(OM, h, q);
+  qlen = length3(q[0], q[1], q[2]);
+  if (qlen == 0) return false;
+  qhat[0] = q[0] / qlen;
+  qhat[1] = q[1] / qlen;
+  qhat[2] = q[2] / qlen;
+  const double dot = qhat[2];
+  const double kf[3] = {0 - 2 * dot * qhat[0], 0 - 2 * dot * qhat[1], 1.0 - 2 * dot * qhat[2]};
+  double xyz[3];
+  matvec(d.rt, kf, xyz);
+  if (xyz[2] <= 0) return false;
+  const double x = xyz[0] * d.p[2] / xyz[2];
+  const double y = xyz[1] * d.p[2] / xyz[2];
+  const double xp = x - d.p[0], yp = y - d.p[1];
+  px = (xp / d.px_x) + (0.5 * (d.W - 1));
+  if (px < 0 || px > (d.W - 1)) return false;
+  py = (yp / d.px_y) + (0.5 * (d.H - 1));
+  if (py < 0 || py > (d.H - 1)) return false;
+  const double sin_th = -qhat[2];
+  const double e = kHc * qlen / (4 * M_PI * sin_th);
+  if (e < d.elo || e > d.ehi) return false;
+  return true;
+}
+
+// de-duplication of refinement spots by scattering direction (:487-495)
+inline bool seen_qhat(const std::vector<double> &acc, int n, const double qh[3]) {
+  for (int i = 0; i < n; i++)
+    if ((std::fabs(qh[0] - acc[3 * i + 0]) * 100000 < 0.1) &&
+        (std::fabs(qh[1] - acc[3 * i + 1]) * 100000 < 0.1) &&
+        (std::fabs(qh[2] - acc[3 * i + 2]) * 100000 < 0.1))
+      return true;
+  return false;
+}
+
+struct Crystal {
+  double lat[6];
+  int sg;
+  double tol_latc[6];
+  double tol_c_over_a;
+  double c_over_a_orig;
+  double cell_vol, phi_vol;  // calcV of the params lattice, :371-377
+};
+
+// Objective of the refinement at x (problem_function, :640-694 with
+// calcOverlapFiltered :564-636).
+double objective(unsigned n, const double *x, const Crystal &cr, const double recip0[3][3],
+                 const Detector &d, const float *img, const int32_t *hkls, const int *valid,
+                 int nvalid, int max_spots, std::vector<double> &acc) {
+  double recip[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) recip[i][j] = recip0[i][j];
+  if (n > 3) {
+    double lat[6];
+    int c = 0;
+    for (int i = 0; i < 6; i++) {
+      if (cr.tol_latc[i] != 0)
+        lat[i] = x[3 + c++];
+      else
+        lat[i] = cr.lat[i];
+    }
+    if (cr.tol_c_over_a != 0) {
+      const double a_new = std::cbrt(cr.cell_vol / (x[3] * cr.phi_vol));
+      lat[0] = a_new;
+      lat[1] = a_new;
+      lat[2] = x[3] * a_new;
+    }
+    recip_of(lat, cr.sg, recip);
+  }
+  const double eul[3] = {x[0], x[1], x[2]};
+  double OMt[3][3], OM[3][3];
+  euler_to_om(eul, OMt);
+  mat33(OMt, recip, OM);
+  double result = 0;
+  int nspot = 0, npos = 0;
+  for (int vi = 0; vi < nvalid; vi++) {
+    double qh[3], px, py, ql;
+    if (!project(OM, hkls + 3 * valid[vi], d, qh, px, py, ql)) continue;
+    if (seen_qhat(acc, nspot, qh)) continue;
+    acc[3 * nspot + 0] = qh[0];
+    acc[3 * nspot + 1] = qh[1];
+    acc[3 * nspot + 2] = qh[2];
+    const float v = img[(size_t)((size_t)py * d.W + (size_t)px)];
+    if (v > 0) {
+      result += v;
+      npos++;
+    }
+    if (++nspot == max_spots) break;
+  }
+  return -(npos * std::sqrt(result));
+}
+
+struct GrainOut {
+  bool keep = false;
+  std::string sol, spots;
+};
+
+// Append printf-formatted text.
+void appendf(std::string &s, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+void appendf(std::string &s, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  const int n = vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (n < (int)sizeof(buf)) {
+    s.append(buf, n > 0 ? n : 0);
+  } else {
+    std::vector<char> big(n + 1);
+    va_start(ap, fmt);
+    vsnprintf(big.data(), big.size(), fmt, ap);
+    va_end(ap);
+    s.append(big.data(), n);
+  }
+}
+
+}  // namespace
+
+extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *pp,
+                                const double *orients, uint64_t n_orients, const uint64_t *ids,
+                                const double *scores, int64_t n_results, const float *image,
+                                const int32_t *hkls, int32_t nh, lmb_post_output *out) {
+  if (!geo || !pp || !out || (!orients && n_orients) || (n_results > 0 && (!ids || !scores)) ||
+      !image || (!hkls && nh)) {
+    lmb::set_error("null argument");
+    return LMB_ERR_INVALID;
+  }
+  for (int64_t i = 0; i < n_results; i++)
+    if (ids[i] >= n_orients) {
+      lmb::set_error("survivor id %llu outside the %llu orientations",
+                     (unsigned long long)ids[i], (unsigned long long)n_orients);
+      return LMB_ERR_INVALID;
+    }
+  const int nthreads = pp->num_threads > 0 ? pp->num_threads : 1;
+  const Sym S = make_sym(pp->space_group);
+  Crystal cr;
+  for (int i = 0; i < 6; i++) {
+    cr.lat[i] = pp->lattice[i];
+    cr.tol_latc[i] = pp->tol_c_over_a != 0 ? 0.0 : pp->tol_latc[i];
+  }
+  cr.sg = pp->space_group;
+  cr.tol_c_over_a = pp->tol_c_over_a;
+  cr.c_over_a_orig = cr.lat[2] / cr.lat[0];
+  {
+    const double ca = std::cos(cr.lat[3] * kDeg2Rad), cb = std::cos(cr.lat[4] * kDeg2Rad);
+    const double cg = std::cos(cr.lat[5] * kDeg2Rad);
+    cr.phi_vol = std::sqrt(1.0 - ca * ca - cb * cb - cg * cg + 2 * ca * cb * cg);
+    cr.cell_vol = cr.lat[0] * cr.lat[1] * cr.lat[2] * cr.phi_vol;
+  }
+  double recip[3][3];
+  Detector d;
+  for (int i = 0; i < 3; i++) {
+    d.p[i] = geo->p[i];
+    for (int j = 0; j < 3; j++) {
+      recip[i][j] = geo->recip[i * 3 + j];
+      d.rt[i][j] = geo->rot_t[i * 3 + j];
+    }
+  }
+  d.px_x = geo->px_x;
+  d.px_y = geo->px_y;
+  d.elo = geo->elo;
+  d.ehi = geo->ehi;
+  d.W = geo->nr_px_x;
+  d.H = geo->nr_px_y;
+  const int max_spots = 3 * geo->max_nr_spots;  // LaueMatchingCPU.c:740
+  const double tol = 3 * kDeg2Rad;                // :739
+
+  // ---- duplicate merge (:969-1065) ---------------------------------------------
+  int64_t nr = n_results;
+  std::vector<uint64_t> rows(ids, ids + nr);
+  std::vector<double> sc(scores, scores + nr);
+  if (nr > kMergeMax) {
+    fprintf(stderr,
+            "WARNING: %lld coarse matches exceed merge cap %d; keeping the top-scored before "
+            "clustering.\n",
+            (long long)nr, kMergeMax);
+    struct SR {
+      double score;
+      size_t row;
+    };
+    std::vector<SR> sr(nr);
+    for (int64_t i = 0; i < nr; i++) sr[i] = {sc[i], (size_t)rows[i]};
+    qsort(sr.data(), (size_t)nr, sizeof(SR), [](const void *a, const void *b) {
+      const double x = ((const SR *)a)->score, y = ((const SR *)b)->score;
+      return (x < y) - (x > y);
+    });
+    for (int i = 0; i < kMergeMax; i++) {
+      sc[i] = sr[i].score;
+      rows[i] = sr[i].row;
+    }
+    nr = kMergeMax;
+  }
+  std::vector<double> quat((size_t)nr * 4);
+#pragma omp parallel for num_threads(nthreads)
+  for (int64_t i = 0; i < nr; i++) om_to_quat(orients + rows[i] * 9, &quat[i * 4]);
+  std::vector<float> miso((size_t)nr * (nr > 0 ? nr - 1 : 0) / 2);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic)
+  for (int64_t i = 1; i < nr; i++)
+    for (int64_t j = 0; j < i; j++)
+      miso[(size_t)i * (i - 1) / 2 + j] = (float)misorientation_deg(S, &quat[i * 4], &quat[j * 4]);
+  std::vector<int> done(nr, 0), dcount, best_row;
+  std::vector<double> best_score;
+  for (int64_t g = 0; g < nr; g++) {
+    if (done[g]) continue;
+    done[g] = 1;
+    int bs = (int)rows[g];
+    double bsc = sc[g];
+    for (int64_t l = g + 1; l < nr; l++) {
+      if (done[l] > 0) continue;
+      if (miso[(size_t)l * (l - 1) / 2 + g] <= pp->max_angle) {
+        done[l] = 1;
+        done[g]++;
+        if (sc[l] > bsc) {
+          bsc = sc[l];
+          bs = (int)rows[l];
+        }
+      }
+    }
+    dcount.push_back(done[g]);
+    best_row.push_back(bs);
+    best_score.push_back(bsc);
+  }
+  const int nsol = (int)dcount.size();
+
+  // ---- refine + write (:1072-1153) ---------------------------------------------
+  std::vector<GrainOut> go(nsol);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic)
+  for (int it = 0; it < nsol; it++) {
+    double ob[3][3], eb[3], ef[3], of[3][3], q1[4], q2[4];
+    const double *m = orients + (size_t)best_row[it] * 9;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) ob[i][j] = m[i * 3 + j];
+    om_to_euler(ob, eb);
+    // HKLs that project onto the detector at the coarse orientation (:513-561)
+    std::vector<int> valid;
+    {
+      double OMt[3][3], OM[3][3];
+      euler_to_om(eb, OMt);
+      mat33(OMt, recip, OM);
+      for (int h = 0; h < nh; h++) {
+        double qh[3], px, py, ql;
+        if (project(OM, hkls + 3 * h, d, qh, px, py, ql)) valid.push_back(h);
+      }
+    }
+    // FitOrientation (:696-801) with the evaluate-once optimiser
+    unsigned n = 3;
+    {
+      int nz = 0;
+      for (int i = 0; i < 6; i++)
+        if (cr.tol_latc[i] != 0) nz++;
+      n = 3 + nz;
+      if (cr.tol_c_over_a != 0) n = 4;
+    }
+    std::vector<double> x(n);
+    x[0] = eb[0];
+    x[1] = eb[1];
+    x[2] = eb[2];
+    {
+      int c = 3;
+      for (int i = 0; i < 6; i++)
+        if (cr.tol_latc[i] != 0) x[c++] = cr.lat[i];
+      if (cr.tol_c_over_a != 0) x[3] = cr.c_over_a_orig;
+    }
+    (void)tol;  // bounds of the search box; unused by the evaluate-once optimiser
+    std::vector<double> acc((size_t)3 * max_spots, 0.0);
+    const double minf = objective(n, x.data(), cr, recip, d, image, hkls, valid.data(),
+                                  (int)valid.size(), max_spots, acc);
+    const double mv = -minf;
+    for (int i = 0; i < 3; i++) ef[i] = x[i];
+    double latf[6];
+    {
+      int c = 0;
+      for (int i = 0; i < 6; i++) latf[i] = (cr.tol_latc[i] != 0) ? x[3 + c++] : cr.lat[i];
+      if (cr.tol_c_over_a != 0) {
+        const double a_new = std::cbrt(cr.cell_vol / (x[3] * cr.phi_vol));
+        latf[0] = a_new;
+        latf[1] = a_new;
+        latf[2] = x[3] * a_new;
+      }
+    }
+    euler_to_om(ef, of);
+    double qb[9], qf[9];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        qb[i * 3 + j] = ob[i][j];
+        qf[i * 3 + j] = of[i][j];
+      }
+    om_to_quat(qb, q1);
+    om_to_quat(qf, q2);
+    double recf[3][3];
+    recip_of(latf, cr.sg, recf);
+    // writeCalcOverlap (:805-947): spots of the refined grain on positive pixels
+    std::fill(acc.begin(), acc.end(), 0.0);
+    double OMt[3][3], OM[3][3];
+    euler_to_om(ef, OMt);
+    mat33(OMt, recf, OM);
+    const int grain_nr = it + 1;
+    int nspot = 0, npos = 0;
+    std::string spots;
+    for (int h = 0; h < nh; h++) {
+      double qh[3], px, py, ql;
+      if (!project(OM, hkls + 3 * h, d, qh, px, py, ql)) continue;
+      if (seen_qhat(acc, nspot, qh)) continue;
+      acc[3 * nspot + 0] = qh[0];
+      acc[3 * nspot + 1] = qh[1];
+      acc[3 * nspot + 2] = qh[2];
+      const float v = image[(size_t)((size_t)py * d.W + (size_t)px)];
+      if (v > 0) {
+        const int *hk = hkls + 3 * h;
+        if (pp->image_num > 0)
+          appendf(spots, "%d\t%d\t%d\t%d\t%d\t%d\t%5d\t%5d\t%lf\t%lf\t%lf\t%lf\n", pp->image_num,
+                  grain_nr, nspot, hk[0], hk[1], hk[2], (int)px, (int)py, qh[0], qh[1], qh[2],
+                  (double)v);
+        else
+          appendf(spots, "%d\t%d\t%d\t%d\t%d\t%5d\t%5d\t%lf\t%lf\t%lf\t%lf\n", grain_nr, nspot,
+                  hk[0], hk[1], hk[2], (int)px, (int)py, qh[0], qh[1], qh[2], (double)v);
+        npos++;
+      }
+      if (++nspot == max_spots) break;
+    }
+    // the reference's spot buffer holds max_spots*256 bytes (snprintf-truncated)
+    const size_t cap = (size_t)max_spots * 256;
+    if (spots.size() > cap - 1) spots.resize(cap - 1);
+    go[it].spots = spots;
+    if (npos >= pp->min_nr_spots) {
+      const double mis = misorientation_deg(S, q1, q2);
+      double OF[3][3];
+      mat33(of, recf, OF);
+      std::string &s = go[it].sol;
+      if (pp->image_num > 0) appendf(s, "%d\t", pp->image_num);
+      appendf(s, "%d\t%d\t", it + 1, dcount[it]);
+      appendf(s, "%-13.4lf\t", (mv / npos) * (mv / npos));
+      appendf(s, "%-13.4lf\t", npos * (mv / npos) * (mv / npos));
+      appendf(s, "%-13.4lf\t", mv);
+      appendf(s, "%d\t", npos);
+      appendf(s, "%d\t", nspot);
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) appendf(s, "%-13.7lf\t\t", OF[k][l]);
+      for (int k = 0; k < 6; k++) appendf(s, "%-13.7lf\t\t", latf[k]);
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) appendf(s, "%-13.7lf\t\t", of[k][l]);
+      appendf(s, "%-13.4lf\t%-13.7lf\t%d\n", best_score[it], mis, best_row[it]);
+      go[it].keep = true;
+    }
+  }
+  std::string sol, spt;
+  for (int it = 0; it < nsol; it++) {
+    spt += go[it].spots;
+    if (go[it].keep) sol += go[it].sol;
+  }
+  out->n_unique = nsol;
+  out->solutions = (char *)malloc(sol.size() + 1);
+  out->spots = (char *)malloc(spt.size() + 1);
+  if (!out->solutions || !out->spots) {
+    free(out->solutions);
+    free(out->spots);
+    out->solutions = out->spots = nullptr;
+    lmb::set_error("out of host memory for the solution text");
+    return LMB_ERR_OOM;
+  }
+  memcpy(out->solutions, sol.c_str(), sol.size() + 1);
+  memcpy(out->spots, spt.c_str(), spt.size() + 1);
+  out->solutions_len = sol.size();
+  out->spots_len = spt.size();
+  return LMB_OK;
+}
+
+extern "C" void lmb_post_free(lmb_post_output *out) {
+  if (!out) return;
+  free(out->solutions);
+  free(out->spots);
+  out->solutions = out->spots = nullptr;
+  out->solutions_len = out->spots_len = 0;
+}

@@ -77,6 +77,8 @@ class Engine:
                                       int(survivor_capacity), C.byref(h)))
         self._h = h
         self.n_orient = 0
+        self._pinned_shape = False
+        self._shape_bucket = None
 
     # ---- lifetime -------------------------------------------------------------
     def close(self):
@@ -99,6 +101,20 @@ class Engine:
     @property
     def stream(self) -> int:
         return int(lib().lmb_engine_stream(self._h) or 0)
+
+    TUNING_FIELDS = ("variant", "tile_sub", "stages", "consumers", "blocks_per_sm", "grid_mult")
+
+    def set_tuning(self, **kw) -> None:
+        vals = (C.c_int32 * 6)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS])
+        if "variant" not in kw:
+            vals[0] = 1
+        check(lib().lmb_engine_set_tuning(self._h, vals, 6))
+        self._pinned_shape = True
+
+    def get_tuning(self) -> dict:
+        vals = (C.c_int32 * 6)()
+        check(lib().lmb_engine_get_tuning(self._h, vals, 6))
+        return dict(zip(self.TUNING_FIELDS, list(vals)))
 
     # ---- DB -------------------------------------------------------------------
     def upload_db(self, records: np.ndarray) -> None:
@@ -151,10 +167,27 @@ class Engine:
         return sc.value if want_scale else None
 
     # ---- passes ---------------------------------------------------------------
+    def _apply_table_shape(self, k: int) -> None:
+        """Use the autotuned launch shape for passes of k images, unless the
+        caller fixed one with set_tuning."""
+        if self._pinned_shape:
+            return
+        from .autotune import batch_bucket, lookup
+        b = batch_bucket(k)
+        if b != self._shape_bucket:
+            shape = lookup(self.R, b)
+            if shape:
+                vals = (C.c_int32 * 6)(*[int(shape.get(f, 0)) for f in self.TUNING_FIELDS])
+                check(lib().lmb_engine_set_tuning(self._h, vals, 6))
+            self._shape_bucket = b
+
     def match(self, slots, min_nr_spots: int, min_intensity: float, value_mode: int = 0) -> None:
         mask = 0
+        n = 0
         for s in slots:
             mask |= 1 << int(s)
+            n += 1
+        self._apply_table_shape(n)
         check(lib().lmb_match(self._h, mask, int(min_nr_spots), float(min_intensity),
                               int(value_mode)))
 

@@ -1,0 +1,62 @@
+"""The drop-in ``bin/LaueMatchingGPU`` executable, end to end on the GPU,
+against the reference's own output files for the same inputs.
+
+DoFwd 0: the golden forward cache is read, compared on the uint8 image.
+DoFwd 1: the DB is simulated on the device and written as ForwardFile (must
+equal the reference's cache), then compared on the float64 image.
+Both runs must write solutions.txt / spots.txt identical to the reference's.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_case
+from lauematching_b200 import formats
+
+pytestmark = pytest.mark.gpu
+EXE = os.path.join(ROOT, "bin", "LaueMatchingGPU")
+
+
+def _case_files(c, tmp_path, do_fwd):
+    fwd = str(tmp_path / "fwd.bin")
+    txt = c.params_text
+    lines = [ln for ln in txt.splitlines() if not ln.startswith(("ForwardFile", "DoFwd"))]
+    lines += [f"ForwardFile {fwd}", f"DoFwd {do_fwd}"]
+    pp = str(tmp_path / "params.txt")
+    with open(pp, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    op = str(tmp_path / "orients.bin")
+    formats.write_orientations(op, c.orients)
+    hp = str(tmp_path / "hkls.csv")
+    formats.write_hkls(hp, c.hkls)
+    ip = str(tmp_path / "image.bin")
+    formats.write_image_bin(ip, c.image)
+    if do_fwd == 0:
+        c.records.tofile(fwd)
+    return pp, op, hp, ip, fwd
+
+
+@pytest.mark.parametrize("name", ["tilted_fcc", "tilted_dense", "tilted_scaled", "tilted_hex"])
+@pytest.mark.parametrize("do_fwd", [0, 1])
+def test_cli_writes_reference_files(name, do_fwd, tmp_path):
+    c = golden_case(name)
+    pp, op, hp, ip, fwd = _case_files(c, tmp_path, do_fwd)
+    r = subprocess.run([sys.executable, EXE, pp, op, hp, ip, "4"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    key = "cmp" if do_fwd == 0 else "fwd"
+    assert f"Initial solutions: {c.meta[key + '_initial']} " in r.stdout
+    assert open(ip + ".solutions.txt").read() == (c.cmp_solutions if do_fwd == 0 else c.fwd_solutions)
+    assert open(ip + ".spots.txt").read() == (c.cmp_spots if do_fwd == 0 else c.fwd_spots)
+    if do_fwd == 1:
+        assert np.array_equal(np.fromfile(fwd, np.uint16).reshape(c.records.shape), c.records)
+
+
+def test_cli_usage_and_fatal_errors(tmp_path):
+    r = subprocess.run([sys.executable, EXE, "a", "b"], capture_output=True, text=True)
+    assert r.returncode == 0 and "Arguments" in r.stdout
+    r = subprocess.run([sys.executable, EXE, str(tmp_path / "nope.txt"), "o", "h", "i", "1"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "Could not open parameter file" in r.stdout

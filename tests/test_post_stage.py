@@ -1,0 +1,50 @@
+"""Host post-stage (merge + evaluate-once refinement + output text) against the
+reference's own solutions.txt / spots.txt.
+
+The golden text was written by the reference LaueMatchingCPU (one thread,
+NLopt replaced by an evaluate-once stand-in).  Feeding the oracle's
+survivors of the same case to lmb_post_process must give the same bytes.
+Host code only: runs without a GPU.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden_case, golden_names
+from lauematching_b200 import post
+from lauematching_b200.engine import geometry_from_params
+
+
+def _strip_header(txt):
+    return "".join(txt.splitlines(keepends=True)[1:])
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("mode", [0, 1])
+def test_post_stage_text_matches_reference(name, mode):
+    c = golden_case(name)
+    p = c.params
+    s = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                  p.min_nr_spots, p.min_intensity, mode=mode)
+    surv = np.zeros(len(s.ids), [("id", "<u8"), ("score", "<f8")])
+    surv["id"] = s.ids
+    surv["score"] = s.score
+    ids, sc = post.collected_matches(surv, s.n_pass)
+    sol, spt, nu = post.post_process(p, geometry_from_params(p), c.orients, ids, sc,
+                                     c.image.astype(np.float32), c.hkls, num_threads=4)
+    ref_sol = c.cmp_solutions if mode == 0 else c.fwd_solutions
+    ref_spt = c.cmp_spots if mode == 0 else c.fwd_spots
+    assert ref_sol.splitlines(keepends=True)[0] == post.SOLUTIONS_HEADER
+    assert ref_spt.splitlines(keepends=True)[0] == post.SPOTS_HEADER
+    assert sol == _strip_header(ref_sol)
+    assert spt == _strip_header(ref_spt)
+    assert nu == c.meta["cmp_unique" if mode == 0 else "fwd_unique"]
+
+
+def test_post_stage_tolerates_no_survivors():
+    c = golden_case("tilted_fcc")
+    p = c.params
+    sol, spt, nu = post.post_process(p, geometry_from_params(p), c.orients,
+                                     np.zeros(0, np.uint64), np.zeros(0),
+                                     c.image.astype(np.float32), c.hkls)
+    assert (sol, spt, nu) == ("", "", 0)
