@@ -206,6 +206,25 @@ int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *pp,
                      const int32_t *hkls, int32_t nh, lmb_post_output *out);
 void lmb_post_free(lmb_post_output *out);
 
+/* ---- survivor ordering that allocates nothing ------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory themselves (code running inside another framework's memory pool, or
+ * on a thread that must not take cudaMalloc's implicit device
+ * synchronisation) but hold device buffers: sorts d_in[0..n) (unsorted
+ * survivors, ids < 2^40) by orientation id into d_out (no aliasing), with the
+ * same order as lmb_results delivers, on `stream` (a cudaStream_t; NULL =
+ * legacy default stream).  Makes no cudaMalloc/cudaFree call: lists above 8192
+ * entries use a fixed 8 MiB device array inside the library as key scratch,
+ * which every GPU that loads the library holds until the process exits.
+ * n above LMB_NOALLOC_ORDER_MAX is rejected with LMB_ERR_INVALID.  The first
+ * call on a device resolves that array's address (cudaGetSymbolAddress) and
+ * sets the kernel's shared-memory limit; make it before any stream capture.
+ * All calls share the one scratch array, so calls that overlap on the GPU
+ * (other streams, other threads) race: serialise them. */
+#define LMB_NOALLOC_ORDER_MAX (1u << 20)
+int lmb_order_survivors_noalloc(const lmb_survivor *d_in, uint64_t n,
+                                lmb_survivor *d_out, void *stream);
+
 /* Page-locked host buffers, so image uploads run at full link speed.  No
  * reference counterpart (the reference pins per-stream buffers internally,
  * LaueMatchingGPUStream.cu:1041-1075). */

@@ -22,6 +22,7 @@ LMB_MAX_SLOTS = 64
 LMB_F64, LMB_F32, LMB_U8 = 0, 1, 2
 LMB_VALUE_U8, LMB_VALUE_F64 = 0, 1
 LMB_BUILD_EXACT_FP64 = 1
+LMB_NOALLOC_ORDER_MAX = 1 << 20
 
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = [
@@ -30,6 +31,7 @@ EXPORTS = [
     "lmb_engine_get_tuning", "lmb_db_upload", "lmb_db_build",
     "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
     "lmb_match", "lmb_results", "lmb_last_pass_ms", "lmb_post_process", "lmb_post_free",
+    "lmb_order_survivors_noalloc",
     "lmb_host_alloc", "lmb_host_free",
 ]
 
@@ -110,6 +112,7 @@ def lib():
         "lmb_post_process": ([C.POINTER(LmbGeometry), C.POINTER(LmbPostParams), vp, u64, vp, vp,
                               C.c_int64, vp, vp, i32, C.POINTER(LmbPostOutput)], C.c_int),
         "lmb_post_free": ([C.POINTER(LmbPostOutput)], None),
+        "lmb_order_survivors_noalloc": ([vp, u64, vp, vp], C.c_int),
         "lmb_host_alloc": ([u64, C.POINTER(vp)], C.c_int),
         "lmb_host_free": ([vp], C.c_int),
     }
