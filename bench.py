@@ -302,17 +302,61 @@ def run_ours(args, rank, world):
             nb += r.nbytes
         d2h[0] = nb + (2 * 64 + 1) * 4
 
+    # sequential: upload 64 frames, one pass, download
     for _ in range(args.warmup):
         e2e_step()
     torch.cuda.synchronize()
-    lat = []
+    seq_lat = []
     te = time.perf_counter()
     for _ in range(args.steps):
         ts = time.perf_counter()
         e2e_step()
-        lat.append((time.perf_counter() - ts) * 1e3)
+        seq_lat.append((time.perf_counter() - ts) * 1e3)
+    seq_ips = world * K * args.steps / (time.perf_counter() - te)
+
+    # pipelined: two halves of 32 slots; the frames of one half upload (load
+    # stream) while the pass over the other half runs
+    halves = [slots[: K // 2], slots[K // 2:]] if K >= 2 else [slots, slots]
+    fidx = [0]
+
+    def load_half(h):
+        for k in halves[h]:
+            e.load_image(k, pins[fidx[0] % K].array, want_scale=False)
+            fidx[0] += 1
+
+    def collect(h):
+        nb = 0
+        for k in halves[h]:
+            r, _ = e.results(k)
+            nb += r.nbytes
+        return nb
+
+    def pipelined(npasses, lat=None):
+        load_half(0)
+        e.match(halves[0], p.min_nr_spots, p.min_intensity)
+        t_prev = time.perf_counter()
+        nb = 0
+        for i in range(npasses):
+            h = i % 2
+            if i + 1 < npasses:
+                load_half(1 - h)
+            nb += collect(h)
+            if i + 1 < npasses:
+                e.match(halves[1 - h], p.min_nr_spots, p.min_intensity)
+            if lat is not None:
+                t = time.perf_counter()
+                lat.append((t - t_prev) * 1e3)
+                t_prev = t
+        return nb
+
+    pipelined(2 * args.warmup)
+    torch.cuda.synchronize()
+    lat = []
+    te = time.perf_counter()
+    nb = pipelined(2 * args.steps, lat)
     e2e_s = time.perf_counter() - te
-    e2e_ips = world * K * args.steps / e2e_s
+    e2e_ips = world * len(halves[0]) * 2 * args.steps / e2e_s
+    d2h[0] = nb // args.steps + 2 * (2 * 64 + 1) * 4
     # plain e2e: one frame per step
     platency = []
     for i in range(args.warmup + args.steps):
@@ -360,11 +404,16 @@ def run_ours(args, rank, world):
         "e2e": {"value": round(e2e_ips, 2), "unit": UNIT,
                 "h2d_bytes_per_step": K * p.nr_px_x * p.nr_px_y,
                 "d2h_bytes_per_step": d2h[0],
-                "path": "Engine.load_image x64 (pinned uint8) + Engine.match + Engine.results x64"},
+                "path": "public Engine API from pinned uint8 frames: per step 64 frames in two "
+                        "passes of 32, the upload of one half overlapping the pass of the other "
+                        "(load_image x32, match, results x32, twice)",
+                "sequential": round(seq_ips, 2)},
         "gpu_launches": 2 * args.steps,
         "clocks": clk,
-        "latency_ms": {"batched_p50": round(float(np.percentile(lat, 50)), 3),
-                       "batched_p99": round(float(np.percentile(lat, 99)), 3),
+        "latency_ms": {"batched_p50": round(float(np.percentile(seq_lat, 50)), 3),
+                       "batched_p99": round(float(np.percentile(seq_lat, 99)), 3),
+                       "pipelined_pass_p50": round(float(np.percentile(lat, 50)), 3),
+                       "pipelined_pass_p99": round(float(np.percentile(lat, 99)), 3),
                        "plain_p50": round(float(np.percentile(platency, 50)), 3),
                        "plain_p99": round(float(np.percentile(platency, 99)), 3)},
         "plain": {"value": round(plain_ips, 2), "unit": UNIT,
@@ -470,6 +519,85 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# serving: Poisson arrivals of mixed 1024^2 / 2048^2 frames through the daemon
+# ---------------------------------------------------------------------------
+def run_serve(args):
+    import socket
+    import struct
+    import threading as th
+    from lauematching_b200 import synth, params as P
+    from lauematching_b200.engine import Engine
+    from lauematching_b200.stream import StreamServer
+    txt2, p2 = workload_params(args.min_intensity)
+    p2 = P.parse_params_text(txt2 + "MinGoodSpots 5\n", binary="stream")
+    txt1 = txt2.replace("NrPxX 2048", "NrPxX 1024").replace("NrPxY 2048", "NrPxY 1024")
+    txt1 = txt1.replace("PxX 0.0002", "PxX 0.0004").replace("PxY 0.0002", "PxY 0.0004")
+    p1 = P.parse_params_text(txt1 + "MinGoodSpots 5\n", binary="stream")
+    hkls = synth.hkls_cubic(8)
+    N = args.n_orient
+    e2 = Engine(p2)
+    om = e2.build_db_synthetic(args.seed, N, hkls, return_orients=True)
+    e1 = Engine(p1)
+    e1.build_db_synthetic(args.seed, N, hkls)
+    rng = np.random.default_rng(11)
+    pool = {}
+    for e, p in ((e2, p2), (e1, p1)):
+        rec = e.download_db(0, min(2_000_000, N))
+        frames = []
+        for _ in range(16):
+            g = synth.pick_grains(rec, int(rng.integers(1, 31)), p.min_nr_spots, rng)
+            frames.append(synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng).astype(np.uint8))
+        pool[(p.nr_px_x, p.nr_px_y)] = frames
+    keys = list(pool)
+    results = []
+    port0 = 45000 + (os.getpid() % 200) * 10
+    for mode, mb in (("batched", 64), ("plain", 1)):
+        for rate in [float(r) for r in args.serve_rates.split(",")]:
+            port0 += 2
+            srv = StreamServer([p2, p1], om, hkls, ncpus=os.cpu_count() or 1, max_batch=mb,
+                               result_dir=tempfile.mkdtemp(prefix="lmb_serve_"), port=port0,
+                               ext_port=port0 + 1, host="127.0.0.1", log=lambda *a: None,
+                               engines=[e2, e1], max_queue=256).start()
+            time.sleep(0.3)
+            n_total = int(min(args.serve_images, max(50, rate * args.serve_seconds)))
+            nsend = 4
+            def sender(j):
+                r2 = np.random.default_rng(100 + j)
+                s = socket.create_connection(("127.0.0.1", port0 + 1))
+                t = time.perf_counter()
+                for i in range(j, n_total, nsend):
+                    t += r2.exponential(nsend / rate)
+                    dt = t - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                    key = keys[int(r2.integers(0, 2))]
+                    fr = pool[key][int(r2.integers(0, 16))]
+                    s.sendall(struct.pack("<4sHHHBB", b"LMB2", (i % 65535) + 1, key[0], key[1], 1, 0))
+                    s.sendall(fr.tobytes())
+                s.close()
+            ts = [th.Thread(target=sender, args=(j,)) for j in range(nsend)]
+            t0 = time.perf_counter()
+            for t in ts:
+                t.start()
+            for t in ts:
+                t.join()
+            deadline = time.time() + 300
+            while srv.images_done < n_total and time.time() < deadline:
+                time.sleep(0.02)
+            wall = time.perf_counter() - t0
+            st = srv.stop(close_engines=False)
+            st.update({"mode": mode, "offered_rate": rate, "sent": n_total,
+                       "throughput": round(srv.images_done / wall, 1)})
+            results.append(st)
+            log(json.dumps(st))
+    e1.close()
+    e2.close()
+    print(json.dumps({"metric": "serving: p50/p99 image latency under Poisson arrivals, "
+                                "mixed 1024^2/2048^2 uint8 frames, 100M-orientation DB each",
+                      "n_orient": N, "serving": results}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -486,12 +614,18 @@ def main():
                     help="orientations per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--serve", action="store_true", help="serving benchmark (Poisson arrivals)")
+    ap.add_argument("--serve-rates", type=str, default="50,200,500,1000,2000")
+    ap.add_argument("--serve-seconds", type=float, default=4.0)
+    ap.add_argument("--serve-images", type=int, default=4000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.serve:
+        run_serve(args)
     else:
         run_ours(args, rank, world)
 

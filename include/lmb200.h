@@ -73,6 +73,12 @@ typedef struct lmb_engine lmb_engine;
 const char *lmb_version(void);
 const char *lmb_last_error(void);
 
+/* Free/total device memory, L2 size and SM count of a device: the budget a
+ * server admits image slots against.  No reference counterpart (the
+ * reference sizes its DB chunks from cudaMemGetInfo, LaueMatchingGPU.cu:665-687). */
+int lmb_device_info(int32_t device, uint64_t *free_bytes, uint64_t *total_bytes,
+                    int32_t *l2_bytes, int32_t *sm_count);
+
 /* Detector rotation (Rodrigues of R_Array, LaueMatchingCPU.c:225-239) and the
  * reciprocal basis (calcRecipArray, LaueMatchingHeaders.h:379-436), FP64 in
  * the reference's operation order.  R_Array = (0,0,0) gives NaN, as in the

@@ -26,7 +26,7 @@ LMB_NOALLOC_ORDER_MAX = 1 << 20
 
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = [
-    "lmb_version", "lmb_last_error", "lmb_geometry_init", "lmb_engine_create",
+    "lmb_version", "lmb_last_error", "lmb_device_info", "lmb_geometry_init", "lmb_engine_create",
     "lmb_engine_destroy", "lmb_engine_stream", "lmb_engine_set_tuning",
     "lmb_engine_get_tuning", "lmb_db_upload", "lmb_db_build",
     "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
@@ -91,6 +91,8 @@ def lib():
     sig = {
         "lmb_version": ([], C.c_char_p),
         "lmb_last_error": ([], C.c_char_p),
+        "lmb_device_info": ([i32, C.POINTER(u64), C.POINTER(u64), C.POINTER(i32),
+                             C.POINTER(i32)], C.c_int),
         "lmb_geometry_init": ([dp, i32, dp, dp, dbl, dbl, i32, i32, dbl, dbl, i32,
                                C.POINTER(LmbGeometry)], C.c_int),
         "lmb_engine_create": ([i32, C.POINTER(LmbGeometry), u64, C.POINTER(vp)], C.c_int),
@@ -122,6 +124,13 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+def device_info(device: int = 0) -> dict:
+    fr, tot = C.c_uint64(), C.c_uint64()
+    l2, sms = C.c_int32(), C.c_int32()
+    check(lib().lmb_device_info(int(device), C.byref(fr), C.byref(tot), C.byref(l2), C.byref(sms)))
+    return {"free": fr.value, "total": tot.value, "l2": l2.value, "sms": sms.value}
 
 
 def check(rc: int) -> int:

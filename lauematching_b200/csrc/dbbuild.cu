@@ -41,21 +41,37 @@ static constexpr double kFourPi = 4.0 * 3.14159265358979323846;  // 4 * M_PI as 
 static constexpr int kHklChunk = 512;
 
 // FP32 screen: false only when the pair is certainly rejected in FP64.
-__device__ __forceinline__ bool screen(const float T[9], const int4 hk, const BuildGeo &g) {
-  const float h = (float)hk.x, k = (float)hk.y, l = (float)hk.z;
-  const float qx = fmaf(T[0], h, fmaf(T[1], k, T[2] * l));
-  const float qy = fmaf(T[3], h, fmaf(T[4], k, T[5] * l));
-  const float qz = fmaf(T[6], h, fmaf(T[7], k, T[8] * l));
+// Ordered cheapest-first: the energy band needs only q (E = c*|q|^2/(-q_z),
+// c = hc/4pi, tested by multiplication), which rejects most pairs before the
+// detector projection is computed.  Margins: the FP32 chain has relative
+// error ~1e-6 in |q|^2 and absolute ~2e-6*|q| in q_z, ~3e-6 in the unit
+// vectors; every test below leaves >= 30x that.
+__device__ __forceinline__ bool screen(const float T[9], const float4 hf, const BuildGeo &g) {
+  const float qx = fmaf(T[0], hf.x, fmaf(T[1], hf.y, T[2] * hf.z));
+  const float qy = fmaf(T[3], hf.x, fmaf(T[4], hf.y, T[5] * hf.z));
+  const float qz = fmaf(T[6], hf.x, fmaf(T[7], hf.y, T[8] * hf.z));
   const float ql2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
   if (!(ql2 > 1e-30f) || !(ql2 < 1e30f)) return true;  // let FP64 decide
   const float rq = rsqrtf(ql2);
+  const float ql = ql2 * rq;
+  const float nq = -qz;   // |q| sin(theta)
+  const float s = nq * rq;  // sin(theta)
+  if (fabsf(s) >= 1e-5f) {
+    const float cq = g.hc4pif * ql2;  // E * (-q_z)
+    if (s < 0.f) {
+      if (g.elof > 0.f) return false;  // E < 0 < Elo
+    } else {
+      if (g.ehif > 0.f && cq > g.ehif * fmaf(nq, 1e-4f, nq) + g.ehif * 1e-4f * ql) return false;
+      if (g.elof > 0.f && cq < g.elof * fmaf(nq, -1e-4f, nq) - g.elof * 1e-4f * ql) return false;
+    }
+  }
   const float hx = qx * rq, hy = qy * rq, hz = qz * rq;
   const float td = -2.f * hz;
   const float k0 = td * hx, k1 = td * hy, k2 = fmaf(td, hz, 1.f);
   const float z = fmaf(g.rtf[6], k0, fmaf(g.rtf[7], k1, g.rtf[8] * k2));
   if (z < -1e-4f) return false;  // xyz[2] <= 0 for sure
   if (z <= 1e-4f) return true;   // too close to call
-  const float iz = 1.f / z;
+  const float iz = __fdividef(1.f, z);
   const float x = fmaf(g.rtf[0], k0, fmaf(g.rtf[1], k1, g.rtf[2] * k2)) * iz;
   const float y = fmaf(g.rtf[3], k0, fmaf(g.rtf[4], k1, g.rtf[5] * k2)) * iz;
   // pixel = (x/z * p2 - p0) / px + (N-1)/2 ; accepted iff trunc in [0, N-1],
@@ -67,11 +83,6 @@ __device__ __forceinline__ bool screen(const float T[9], const int4 hk, const Bu
   const float pyv = fmaf(fmaf(y, g.p2f, -g.p1f), g.inv_pyf, g.cyf);
   const float ty = fmaf(g.toly * (1.f + fabsf(y)), iz, 0.05f);
   if (pyv < -1.f - ty || pyv > (float)g.H + ty) return false;
-  const float s = -hz;  // sin(theta)
-  if (fabsf(s) < 1e-5f) return true;
-  const float e = g.hc4pif * (ql2 * rq) / s;
-  const float te = fabsf(e) * (1e-4f / fabsf(s) + 1e-4f);
-  if (e < g.elof - te || e > g.ehif + te) return false;
   return true;
 }
 
@@ -114,7 +125,8 @@ __global__ void dbbuild_kernel(const double *__restrict__ om, uint64_t n,
   extern __shared__ __align__(16) unsigned char smem[];
   const int TB = blockDim.x;
   int4 *sh_hkl = reinterpret_cast<int4 *>(smem);
-  uint32_t *sh_list = reinterpret_cast<uint32_t *>(smem + kHklChunk * sizeof(int4));
+  float4 *sh_hklf = reinterpret_cast<float4 *>(smem + kHklChunk * sizeof(int4));
+  uint32_t *sh_list = reinterpret_cast<uint32_t *>(smem + kHklChunk * 2 * sizeof(int4));
   int *sh_cnt = reinterpret_cast<int *>(sh_list + (size_t)g.S * TB);
 
   const int t = threadIdx.x;
@@ -144,28 +156,30 @@ __global__ void dbbuild_kernel(const double *__restrict__ om, uint64_t n,
   for (int c0 = 0; c0 < nh; c0 += kHklChunk) {
     const int cn = min(kHklChunk, nh - c0);
     __syncthreads();
-    for (int i = t; i < cn; i += TB) sh_hkl[i] = hkl[c0 + i];
+    for (int i = t; i < cn; i += TB) {
+      const int4 v = hkl[c0 + i];
+      sh_hkl[i] = v;
+      sh_hklf[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+    }
     __syncthreads();
-    if (!done) {
-      for (int i = 0; i < cn; i++) {
-        const int4 hk = sh_hkl[i];
-        if (!kExactAll && !screen(Tf, hk, g)) continue;
-        int ix, iy;
-        if (!exact_spot(T, hk, g, ix, iy)) continue;
-        const uint32_t key = (uint32_t)(ix & 0xFFFF) | ((uint32_t)(iy & 0xFFFF) << 16);
-        bool dup = false;
-        for (int s = 0; s < cnt; s++)
-          if (sh_list[(size_t)s * TB + t] == key) {
-            dup = true;
-            break;
+    // Warp-uniform loop: no break/continue, so lanes that took the (rare)
+    // FP64 path reconverge with the others at the end of every HKL.
+    for (int i = 0; i < cn; i++) {
+      bool go = !done;
+      if (!kExactAll && go) go = screen(Tf, sh_hklf[i], g);
+      if (go) {
+        int ix = 0, iy = 0;
+        if (exact_spot(T, sh_hkl[i], g, ix, iy)) {
+          const uint32_t key = (uint32_t)(ix & 0xFFFF) | ((uint32_t)(iy & 0xFFFF) << 16);
+          bool dup = false;
+          for (int s = 0; s < cnt; s++) dup |= (sh_list[(size_t)s * TB + t] == key);
+          if (!dup) {
+            sh_list[(size_t)cnt * TB + t] = key;
+            done = (++cnt == g.S);
           }
-        if (dup) continue;
-        sh_list[(size_t)cnt * TB + t] = key;
-        if (++cnt == g.S) {
-          done = true;
-          break;
         }
       }
+      __syncwarp();
     }
     if (__syncthreads_and(done)) break;
   }
@@ -285,7 +299,7 @@ static int build_block(int S) {
 
 size_t dbbuild_smem_bytes(int S) {
   const int tb = build_block(S);
-  return kHklChunk * sizeof(int4) + (size_t)S * tb * 4 + (size_t)tb * 4;
+  return kHklChunk * 2 * sizeof(int4) + (size_t)S * tb * 4 + (size_t)tb * 4;
 }
 
 int dbbuild_launch(const double *d_om, uint64_t n, const int4 *d_hkl, int nh,

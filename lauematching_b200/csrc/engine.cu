@@ -59,6 +59,12 @@ struct lmb_engine {
   uint64_t last_mask = 0;
   bool pending = false;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  // image uploads run on their own stream so they overlap a running pass:
+  // a pass waits for its slots' uploads, an upload waits until the last pass
+  // that read its slot has finished.
+  cudaStream_t ld = nullptr;
+  cudaEvent_t ev_loaded[LMB_MAX_SLOTS] = {};
+  cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
   CompareTuning tuning{1, 0, 0, 0, 0, 0};  // warp-specialised, default shape
 };
 
@@ -77,6 +83,7 @@ void free_engine(lmb_engine *e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->st) cudaStreamSynchronize(e->st);
+  if (e->ld) cudaStreamSynchronize(e->ld);
   cudaFree(e->d_db);
   cudaFree(e->d_u8);
   cudaFree(e->d_f64);
@@ -91,7 +98,12 @@ void free_engine(lmb_engine *e) {
   cudaFreeHost(e->h_status);
   for (auto &v : e->ev)
     if (v) cudaEventDestroy(v);
+  for (int k = 0; k < LMB_MAX_SLOTS; k++) {
+    if (e->ev_loaded[k]) cudaEventDestroy(e->ev_loaded[k]);
+    if (e->ev_released[k]) cudaEventDestroy(e->ev_released[k]);
+  }
   if (e->st) cudaStreamDestroy(e->st);
+  if (e->ld) cudaStreamDestroy(e->ld);
   delete e;
 }
 
@@ -165,6 +177,21 @@ int upload_hkls(const int32_t *hkls, int nh, int4 **d_out) {
 extern "C" {
 
 const char *lmb_version(void) { return "lmb200 0.1.0 sm_100a"; }
+
+int lmb_device_info(int32_t device, uint64_t *free_bytes, uint64_t *total_bytes,
+                    int32_t *l2_bytes, int32_t *sm_count) {
+  LMB_CUDA(cudaSetDevice(device));
+  size_t fr = 0, tot = 0;
+  LMB_CUDA(cudaMemGetInfo(&fr, &tot));
+  int l2 = 0, sms = 0;
+  LMB_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
+  LMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  if (free_bytes) *free_bytes = fr;
+  if (total_bytes) *total_bytes = tot;
+  if (l2_bytes) *l2_bytes = l2;
+  if (sm_count) *sm_count = sms;
+  return LMB_OK;
+}
 const char *lmb_last_error(void) { return g_err; }
 
 int lmb_geometry_init(const double lattice[6], int32_t space_group, const double p_array[3],
@@ -207,7 +234,12 @@ int lmb_engine_create(int32_t device, const lmb_geometry *geo, uint64_t survivor
     if (_e != cudaSuccess) return fail(cuda_fail(_e, #call, __FILE__, __LINE__)); \
   } while (0)
   TRY(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+  TRY(cudaStreamCreateWithFlags(&e->ld, cudaStreamNonBlocking));
   for (auto &v : e->ev) TRY(cudaEventCreate(&v));
+  for (int k = 0; k < LMB_MAX_SLOTS; k++) {
+    TRY(cudaEventCreateWithFlags(&e->ev_loaded[k], cudaEventDisableTiming));
+    TRY(cudaEventCreateWithFlags(&e->ev_released[k], cudaEventDisableTiming));
+  }
   TRY(cudaMalloc(&e->d_u8, e->npx * LMB_MAX_SLOTS));
   TRY(cudaMalloc(&e->d_occ, e->npx * sizeof(unsigned long long)));
   TRY(cudaMemset(e->d_occ, 0, e->npx * sizeof(unsigned long long)));
@@ -348,12 +380,14 @@ int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtyp
   LMB_REQUIRE(dtype == LMB_F64 || dtype == LMB_F32 || dtype == 2, "unknown dtype %d", dtype);
   if (keep_f64 && !e->d_f64)
     LMB_CUDA(cudaMalloc(&e->d_f64, e->npx * sizeof(double) * LMB_MAX_SLOTS));
+  LMB_CUDA(cudaStreamWaitEvent(e->ld, e->ev_released[slot], 0));
   LMB_CUDA(cudaMemcpyAsync(e->d_stage, pixels, e->npx * dtype_bytes(dtype),
-                           cudaMemcpyHostToDevice, e->st));
+                           cudaMemcpyHostToDevice, e->ld));
   rc = quantize_launch(e->d_stage, dtype, e->npx, e->d_max_bits, e->d_u8 + (size_t)slot * e->npx,
                        keep_f64 ? e->d_f64 + (size_t)slot * e->npx : nullptr, e->d_occ, slot,
-                       e->d_scale + slot, e->num_sms, e->st);
+                       e->d_scale + slot, e->num_sms, e->ld);
   if (rc) return rc;
+  LMB_CUDA(cudaEventRecord(e->ev_loaded[slot], e->ld));
   e->loaded_mask |= 1ull << slot;
   if (keep_f64)
     e->f64_mask |= 1ull << slot;
@@ -361,8 +395,8 @@ int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtyp
     e->f64_mask &= ~(1ull << slot);
   if (im_scale) {
     LMB_CUDA(cudaMemcpyAsync(im_scale, e->d_scale + slot, sizeof(double), cudaMemcpyDeviceToHost,
-                             e->st));
-    LMB_CUDA(cudaStreamSynchronize(e->st));
+                             e->ld));
+    LMB_CUDA(cudaStreamSynchronize(e->ld));
   }
   return LMB_OK;
 }
@@ -376,6 +410,8 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   LMB_REQUIRE(value_mode == LMB_VALUE_U8 || value_mode == LMB_VALUE_F64, "unknown value mode");
   LMB_REQUIRE(value_mode == LMB_VALUE_U8 || (slot_mask & ~e->f64_mask) == 0,
               "float64 pass needs images loaded with keep_f64");
+  for (int k = 0; k < LMB_MAX_SLOTS; k++)
+    if (slot_mask >> k & 1) LMB_CUDA(cudaStreamWaitEvent(e->st, e->ev_loaded[k], 0));
   LMB_CUDA(cudaMemsetAsync(e->d_status, 0, kStatusWords * sizeof(unsigned int), e->st));
   LMB_CUDA(cudaEventRecord(e->ev[0], e->st));
   CmpArgs a{};
@@ -418,6 +454,8 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   rc = order_launch(o, ns, e->st);
   if (rc) return rc;
   LMB_CUDA(cudaEventRecord(e->ev[2], e->st));
+  for (int k = 0; k < LMB_MAX_SLOTS; k++)
+    if (slot_mask >> k & 1) LMB_CUDA(cudaEventRecord(e->ev_released[k], e->st));
   LMB_CUDA(cudaMemcpyAsync(e->h_status, e->d_status, kStatusWords * sizeof(unsigned int),
                            cudaMemcpyDeviceToHost, e->st));
   e->last_mask = slot_mask;

@@ -1,0 +1,443 @@
+"""``LaueMatchingGPUStream`` daemon, drop-in for the reference executable.
+
+    LaueMatchingGPUStream <params.txt> <orientations.bin> <hkls.csv> <nCPUs>
+        [--extra-params other_detector.txt ...] [--max-batch 64] [--device 0]
+
+Wire protocol of the reference (LaueMatchingGPUStream.cu:42-46,295-383;
+client scripts/laue_stream_utils.py:553-565): TCP port 60517, each message a
+2-byte host-endian image number followed by NrPxX*NrPxY float32 pixels, many
+messages per connection, no reply.  Results are appended, one image at a
+time and flushed, to ``<cwd>/<ResultDir>/solutions.txt`` and ``spots.txt``
+with the ImageNr column (LaueMatchingGPUStream.cu:1079-1104); the written
+grains are gated by MinGoodSpots (:1173).  SIGINT/SIGTERM: stop accepting,
+finish every received image, exit 0.
+
+What changes (the serving side of the B200 design):
+
+* continuous batching -- the reference runs one full DB pass per image with
+  kernels serialised (gpu_gate, :1160-1165, :1196, :1248).  Here every image
+  that arrives while a pass is running is uploaded into a free slot (the
+  upload overlaps the pass on its own stream) and joins the next pass; one
+  pass serves up to 64 images;
+* admission by memory budget -- slots per geometry are limited by the free
+  HBM after the DB is resident, and the per-pixel occupancy word keeps the
+  L2-resident working set at 8 bytes per pixel whatever the batch;
+* mixed detector sizes -- ``--extra-params`` adds further detector
+  geometries, each with its own resident DB; frames for them arrive on port
+  60518 with an extended header (``b"LMB2"``, uint16 image number, uint16
+  width, uint16 height, uint8 dtype 0=float32/1=uint8, one pad byte);
+* the post-stage (merge, refinement, text) runs on a writer thread, off the
+  GPU loop; per-image latency (arrival -> lines written) is recorded and
+  p50/p99 reported.
+"""
+from __future__ import annotations
+
+import argparse
+import collections
+import os
+import queue
+import signal
+import socket
+import struct
+import sys
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PORT = 60517
+EXT_PORT = 60518
+MAX_CONNECTIONS = 10
+MAX_QUEUE = 32
+EXT_MAGIC = b"LMB2"
+EXT_HEADER = struct.Struct("<4sHHHBB")
+
+
+@dataclass
+class Request:
+    image_num: int
+    key: tuple  # (NrPxX, NrPxY)
+    pixels: np.ndarray
+    t_arrival: float
+
+
+@dataclass
+class Done:
+    req: Request
+    survivors: np.ndarray
+    n_pass: int
+    t_gpu_done: float
+
+
+@dataclass
+class Geometry:
+    params: object
+    engine: object
+    free: list = field(default_factory=list)
+    loaded: list = field(default_factory=list)  # (slot, Request) uploaded, waiting for a pass
+    inflight: list = field(default_factory=list)  # (slot, Request) in the running pass
+
+
+def _recv_exact(sock, buf, running):
+    view = memoryview(buf)
+    got = 0
+    while got < len(buf):
+        try:
+            n = sock.recv_into(view[got:])
+        except socket.timeout:
+            if not running():
+                return False
+            continue
+        except InterruptedError:
+            continue
+        except OSError:
+            return False
+        if n == 0:
+            return False
+        got += n
+    return True
+
+
+class StreamServer:
+    """The daemon, usable in-process (tests, benchmarks) or from the CLI."""
+
+    def __init__(self, params_list, orients, hkls, ncpus=1, max_batch=64, device=0,
+                 result_dir=None, port=PORT, ext_port=EXT_PORT, host="0.0.0.0",
+                 log=print, max_queue=MAX_QUEUE, engines=None):
+        from . import _lib, formats
+        from .engine import Engine
+        self.log = log
+        self.ncpus = max(1, int(ncpus))
+        # images are post-processed concurrently, each on few threads
+        self.n_writers = max(1, min(8, self.ncpus))
+        self.post_threads = max(1, self.ncpus // self.n_writers)
+        self._out_lock = threading.Lock()
+        self.orients = orients
+        self.hkls = hkls
+        self.primary = params_list[0]
+        self.result_dir = result_dir if result_dir is not None else self.primary.result_dir
+        self.geoms: dict = {}
+        for i, p in enumerate(params_list):
+            key = (int(p.nr_px_x), int(p.nr_px_y))
+            if key in self.geoms:
+                raise ValueError(f"two parameter files describe a {key} detector")
+            if engines is not None:  # DBs already resident (in-process use)
+                self.geoms[key] = Geometry(p, engines[i])
+                continue
+            e = Engine(p, device=device)
+            fwd = p.forward_file
+            if p.do_fwd == 0 and fwd and os.path.exists(fwd):
+                e.upload_db(formats.read_forward_cache(fwd, orients.shape[0], p.max_nr_spots))
+                log(f"{fwd} file was found. Will not do forward simulation.")
+            else:
+                t0 = time.perf_counter()
+                e.build_db(orients, hkls)
+                log(f"Forward simulation on the device: {orients.shape[0]} orientations in "
+                    f"{time.perf_counter() - t0:.2f} s")
+                if fwd:
+                    from .cli import _write_cache
+                    try:
+                        _write_cache(e, fwd, orients.shape[0])
+                    except OSError as exc:
+                        log(f"Could not write the forward simulation to {fwd}: {exc}")
+            self.geoms[key] = Geometry(p, e)
+        # admission: slots per geometry within the free HBM after the DBs
+        info = _lib.device_info(device)
+        per_slot = max(int(k[0]) * int(k[1]) * 5 for k in self.geoms)  # u8 frame + wire staging
+        budget = max(1, int(0.5 * info["free"] // per_slot))
+        self.max_batch = int(min(max_batch, 64, budget))
+        for g in self.geoms.values():
+            g.free = list(range(self.max_batch))[::-1]
+        self.queue: queue.Queue = queue.Queue(maxsize=max_queue)
+        self._backlog = collections.deque()
+        self.done_q: queue.Queue = queue.Queue()
+        self.running = False
+        self.latencies_ms: list = []
+        self.gpu_latencies_ms: list = []
+        self.passes = 0
+        self.images_done = 0
+        self.batch_sizes: list = []
+        self._threads: list = []
+        self._socks: list = []
+        self.port, self.ext_port, self.host = port, ext_port, host
+        self.t_first = None
+        self.t_last = None
+        os.makedirs(self.result_dir, exist_ok=True)
+        from .post import STREAM_SOLUTIONS_HEADER, STREAM_SPOTS_HEADER
+        self.sol_f = open(os.path.join(self.result_dir, "solutions.txt"), "w")
+        self.spt_f = open(os.path.join(self.result_dir, "spots.txt"), "w")
+        self.spt_f.write(STREAM_SPOTS_HEADER)
+        self.sol_f.write(STREAM_SOLUTIONS_HEADER)
+        self.sol_f.flush()
+        self.spt_f.flush()
+
+    # ---- network --------------------------------------------------------------
+    def _listen(self, port):
+        s = socket.socket(socket.AF_INET, socket.SOCK_STREAM)
+        s.setsockopt(socket.SOL_SOCKET, socket.SO_REUSEADDR, 1)
+        s.bind((self.host, port))
+        s.listen(MAX_CONNECTIONS)
+        s.settimeout(0.5)
+        self._socks.append(s)
+        return s
+
+    def _accept_loop(self, srv, extended):
+        try:
+            while self.running:
+                try:
+                    c, _ = srv.accept()
+                except socket.timeout:
+                    continue
+                except OSError:
+                    break
+                t = threading.Thread(target=self._client, args=(c, extended), daemon=True)
+                t.start()
+                self._threads.append(t)
+        finally:
+            srv.close()
+
+    def _client(self, c, extended):
+        c.settimeout(0.5)  # bounded recv so shutdown is seen (reference: 5 s SO_RCVTIMEO)
+        run = lambda: self.running  # noqa: E731
+        W, H = int(self.primary.nr_px_x), int(self.primary.nr_px_y)
+        try:
+            while self.running:
+                if extended:
+                    hb = bytearray(EXT_HEADER.size)
+                    if not _recv_exact(c, hb, run):
+                        break
+                    magic, num, w, h, dt, _ = EXT_HEADER.unpack(hb)
+                    if magic != EXT_MAGIC or dt not in (0, 1):
+                        self.log("bad extended header; closing connection")
+                        break
+                    key = (w, h)
+                    dtype = np.float32 if dt == 0 else np.uint8
+                else:
+                    hb = bytearray(2)
+                    if not _recv_exact(c, hb, run):
+                        break
+                    num = int.from_bytes(hb, sys.byteorder)  # host-endian, as memcpy
+                    key, dtype = (W, H), np.float32
+                    w, h = W, H
+                payload = np.empty(w * h, dtype)
+                if not _recv_exact(c, payload.view(np.uint8), run):
+                    break
+                t = time.perf_counter()
+                if key not in self.geoms:
+                    self.log(f"image {num}: no DB for a {w}x{h} detector; dropped")
+                    continue
+                # blocks while MAX_QUEUE images wait (back-pressure, as queue_push)
+                while self.running:
+                    try:
+                        self.queue.put(Request(num, key, payload, t), timeout=0.5)
+                        break
+                    except queue.Full:
+                        continue
+        finally:
+            c.close()
+
+    # ---- GPU loop -------------------------------------------------------------
+    def _gpu_loop(self):
+        while True:
+            idle = not any(g.loaded or g.inflight for g in self.geoms.values())
+            if not self.running and idle and self.queue.empty() and not self._backlog:
+                break
+            # admit arrivals into free slots (uploads overlap the running pass)
+            admitted = self._admit(block=idle)
+            # start a pass on every geometry with uploaded images and none running
+            for g in self.geoms.values():
+                if g.loaded and not g.inflight:
+                    g.inflight, g.loaded = g.loaded, []
+                    p = g.params
+                    g.engine.match([s for s, _ in g.inflight], p.min_nr_spots, p.min_intensity)
+                    self.passes += 1
+                    self.batch_sizes.append(len(g.inflight))
+            if not admitted:
+                self._admit(block=False)
+            # collect the passes (sync), free their slots
+            for g in self.geoms.values():
+                if not g.inflight:
+                    continue
+                t = None
+                for s, r in g.inflight:
+                    surv, npass = g.engine.results(s)
+                    t = t or time.perf_counter()
+                    self.done_q.put(Done(r, surv, npass, t))
+                    g.free.append(s)
+                g.inflight = []
+        self.done_q.put(None)
+
+    def _admit(self, block):
+        """Upload waiting images into free slots; images whose geometry has no
+        free slot stay in the backlog (in arrival order) until a pass ends."""
+        n = 0
+        while len(self._backlog) < 4 * self.max_batch:
+            try:
+                r = self.queue.get(timeout=0.05) if (block and not self._backlog and n == 0) \
+                    else self.queue.get_nowait()
+            except queue.Empty:
+                break
+            self._backlog.append(r)
+            block = False
+        keep = collections.deque()
+        while self._backlog:
+            r = self._backlog.popleft()
+            g = self.geoms[r.key]
+            if not g.free:
+                keep.append(r)
+                continue
+            s = g.free.pop()
+            g.engine.load_image(s, r.pixels, want_scale=False)
+            g.loaded.append((s, r))
+            n += 1
+        self._backlog = keep
+        return n
+
+    # ---- post-stage + output ----------------------------------------------------
+    def _writer(self):
+        """One of the writer threads: post-stage of finished images (the C
+        post-stage releases the GIL), then an atomic append of the image's
+        lines to both files."""
+        from .post import collected_matches, post_process
+        while True:
+            d = self.done_q.get()
+            if d is None:
+                break
+            g = self.geoms[d.req.key]
+            p = g.params
+            img = d.req.pixels.astype(np.float32, copy=False)
+            sol = spt = ""
+            if d.survivors.shape[0] or d.n_pass:
+                ids, sc = collected_matches(d.survivors, d.n_pass)
+                sol, spt, nu = post_process(p, g.engine.geometry, self.orients, ids, sc, img,
+                                            self.hkls, min_nr_spots=p.min_good_spots,
+                                            image_num=d.req.image_num,
+                                            num_threads=self.post_threads)
+            with self._out_lock:
+                if sol or spt:
+                    self.sol_f.write(sol)
+                    self.spt_f.write(spt)
+                    self.sol_f.flush()
+                    self.spt_f.flush()
+                t = time.perf_counter()
+                self.latencies_ms.append((t - d.req.t_arrival) * 1e3)
+                self.gpu_latencies_ms.append((d.t_gpu_done - d.req.t_arrival) * 1e3)
+                self.images_done += 1
+                self.t_first = self.t_first or d.req.t_arrival
+                self.t_last = t
+
+    # ---- lifecycle --------------------------------------------------------------
+    def start(self, listen=True):
+        self.running = True
+        if listen:
+            self._accept_threads = [
+                threading.Thread(target=self._accept_loop, args=(self._listen(self.port), False),
+                                 daemon=True)]
+            if len(self.geoms) > 1 or self.ext_port:
+                self._accept_threads.append(threading.Thread(
+                    target=self._accept_loop, args=(self._listen(self.ext_port), True),
+                    daemon=True))
+            for t in self._accept_threads:
+                t.start()
+        self._gpu = threading.Thread(target=self._gpu_loop, daemon=True)
+        self._wr = [threading.Thread(target=self._writer, daemon=True)
+                    for _ in range(self.n_writers)]
+        self._gpu.start()
+        for t in self._wr:
+            t.start()
+        return self
+
+    def submit(self, image_num, pixels, key=None):
+        """In-process submission (same path as a received message)."""
+        key = key or (int(self.primary.nr_px_x), int(self.primary.nr_px_y))
+        self.queue.put(Request(int(image_num), key, pixels, time.perf_counter()))
+
+    def stop(self, drain_timeout=600.0, close_engines=True):
+        """Stop accepting, finish every received image, close the files."""
+        self.running = False
+        for t in getattr(self, "_accept_threads", []):
+            t.join(timeout=5.0)  # each closes its listening socket
+        for t in self._threads:
+            t.join(timeout=5.0)
+        self._gpu.join(timeout=drain_timeout)
+        for _ in range(len(self._wr) - 1):  # the GPU loop queued one end marker
+            self.done_q.put(None)
+        for t in self._wr:
+            t.join(timeout=drain_timeout)
+        self.sol_f.close()
+        self.spt_f.close()
+        if close_engines:
+            for g in self.geoms.values():
+                g.engine.close()
+        return self.stats()
+
+    def stats(self):
+        lat = np.asarray(self.latencies_ms) if self.latencies_ms else np.zeros(1)
+        glat = np.asarray(self.gpu_latencies_ms) if self.gpu_latencies_ms else np.zeros(1)
+        span = (self.t_last - self.t_first) if self.t_first and self.t_last else 0.0
+        return {"images": self.images_done, "passes": self.passes,
+                "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "gpu_p50_ms": float(np.percentile(glat, 50)),
+                "gpu_p99_ms": float(np.percentile(glat, 99)),
+                "images_per_s": self.images_done / span if span > 0 else 0.0,
+                "max_batch": self.max_batch}
+
+
+def main(argv=None) -> int:
+    argv = sys.argv if argv is None else argv
+    if len(argv) < 5:
+        print("LaueMatchingGPUStream -- persistent GPU daemon (B200)\n\n"
+              f"Usage: {argv[0] if argv else 'LaueMatchingGPUStream'} parameterFile "
+              "orientationFile hklFile nCPUs\n\n"
+              f"Listens on TCP port {PORT} for binary images.\n"
+              "Wire protocol: uint16_t image_num + float[NrPxX*NrPxY]")
+        return 0
+    ap = argparse.ArgumentParser(add_help=False)
+    ap.add_argument("--extra-params", action="append", default=[])
+    ap.add_argument("--max-batch", type=int, default=64)
+    ap.add_argument("--device", type=int, default=int(os.environ.get("LMB_DEVICE", "0")))
+    ap.add_argument("--port", type=int, default=PORT)
+    ap.add_argument("--ext-port", type=int, default=EXT_PORT)
+    opts, rest = ap.parse_known_args(argv[5:])
+    from . import formats
+    from .params import ParamsError, read_params
+    param_fn, orient_fn, hkl_fn, ncpu_s = argv[1:5]
+    print("Reading parameter file", flush=True)
+    try:
+        plist = [read_params(param_fn, binary="stream")]
+        plist += [read_params(x, binary="stream") for x in opts.extra_params]
+    except (OSError, ParamsError) as exc:
+        print(f"Could not open parameter file {param_fn}: {exc}")
+        return 1
+    print("Parameters read", flush=True)
+    orients = formats.read_orientations(orient_fn)
+    hkls = formats.read_hkls(hkl_fn)
+    print(f"{orients.shape[0]} orientations, {len(hkls)} hkls", flush=True)
+    srv = StreamServer(plist, orients, hkls, ncpus=int(ncpu_s), max_batch=opts.max_batch,
+                       device=opts.device, port=opts.port, ext_port=opts.ext_port,
+                       log=lambda *a: print(*a, flush=True))
+    stop = threading.Event()
+
+    def on_signal(signum, frame):
+        if stop.is_set():
+            os._exit(1)  # second signal: hard exit, as the reference
+        stop.set()
+
+    signal.signal(signal.SIGINT, on_signal)
+    signal.signal(signal.SIGTERM, on_signal)
+    srv.start()
+    print(f"Listening on port {opts.port} (extended header on {opts.ext_port}); "
+          f"up to {srv.max_batch} images per DB pass", flush=True)
+    while not stop.wait(0.5):
+        pass
+    st = srv.stop()
+    print(f"Processed {st['images']} images in {st['passes']} DB passes "
+          f"(mean batch {st['mean_batch']:.1f}); latency p50 {st['p50_ms']:.1f} ms, "
+          f"p99 {st['p99_ms']:.1f} ms", flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

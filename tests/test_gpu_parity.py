@@ -38,7 +38,7 @@ def test_db_build_matches_reference_cache(name):
         assert np.array_equal(e.download_db(), c.records)
 
 
-@pytest.mark.parametrize("name", ["tilted_fcc", "tilted_hex", "beamnormal_fcc"])
+@pytest.mark.parametrize("name", ["tilted_fcc", "tilted_hex", "beamnormal_fcc", "tilted_rhomb", "tilted_cap5"])
 def test_db_build_fp32_screen_equals_all_fp64(name):
     c = golden_case(name)
     om = synth.shoemake_orientations(200000, seed=123)
