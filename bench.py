@@ -455,11 +455,14 @@ def run_reference(args, rank, world):
     hkls = synth.hkls_cubic(8)
     n_s = args.ref_sample
     cores = os.cpu_count() or 1
-    base = scratch_dir(n_s * (REC_BYTES_PER_ORIENT + 72))
+    base = scratch_dir(n_s * REC_BYTES_PER_ORIENT)
     wd = tempfile.mkdtemp(prefix="lmb_ref_", dir=base)
+    # the orientation file stays off /dev/shm: with DoFwd 1 the reference
+    # free()s a memory-mapped orientation file at exit (LaueMatchingCPU.c:825-830)
+    wd_o = tempfile.mkdtemp(prefix="lmb_ref_o_")
     fwd = os.path.join(wd, "fwd.bin")
     om = synth.shoemake_orientations(n_s, seed=args.seed)
-    op = os.path.join(wd, "orients.bin")
+    op = os.path.join(wd_o, "orients.bin")
     formats.write_orientations(op, om)
     hp = os.path.join(wd, "hkls.csv")
     formats.write_hkls(hp, hkls)
@@ -492,9 +495,10 @@ def run_reference(args, rank, world):
         if i >= args.warmup:
             times.append(r.compare_seconds)
             walls.append(r.wall_seconds)
-    for fn in os.listdir(wd):
-        os.remove(os.path.join(wd, fn))
-    os.rmdir(wd)
+    for d in (wd, wd_o):
+        for fn in os.listdir(d):
+            os.remove(os.path.join(d, fn))
+        os.rmdir(d)
     scale = 1e8 / n_s
     per_img = statistics.mean(times) * scale
     value = 1.0 / per_img

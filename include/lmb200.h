@@ -193,6 +193,9 @@ typedef struct lmb_post_params {
   int32_t image_num;     /* > 0: prepend the ImageNr column (daemon format) */
   int32_t num_threads;   /* host threads */
   int32_t optimizer;     /* 0 = evaluate once */
+  int32_t max_results;   /* candidates kept for the merge, top by score;
+                            0 = the reference's cap MERGE_MAX_RESULTS 50000 */
+  int32_t reserved;
 } lmb_post_params;
 
 typedef struct lmb_post_output {

@@ -55,7 +55,8 @@ class LmbPostParams(C.Structure):
                 ("max_nr_spots", C.c_int32), ("tol_latc", C.c_double * 6),
                 ("tol_c_over_a", C.c_double), ("max_angle", C.c_double),
                 ("min_nr_spots", C.c_int32), ("image_num", C.c_int32),
-                ("num_threads", C.c_int32), ("optimizer", C.c_int32)]
+                ("num_threads", C.c_int32), ("optimizer", C.c_int32),
+                ("max_results", C.c_int32), ("reserved", C.c_int32)]
 
 
 class LmbPostOutput(C.Structure):

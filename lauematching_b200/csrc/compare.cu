@@ -21,10 +21,32 @@
 // coalesced regardless of the 122-byte record stride.  Waits are bounded
 // (2 s of global time) and report through an error word.
 #include <climits>
+#include <mutex>
+#include <vector>
 
 #include "kernels.cuh"
 
 namespace lmb {
+
+// cudaFuncSetAttribute once per (device, kernel, size): later launches, and
+// launches captured into a CUDA graph, need no attribute call.
+static int ensure_smem(const void *fn, int bytes) {
+  static std::mutex mu;
+  struct Done {
+    int dev;
+    const void *fn;
+    int bytes;
+  };
+  static std::vector<Done> done;
+  int dev = 0;
+  LMB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto &d : done)
+    if (d.dev == dev && d.fn == fn && d.bytes >= bytes) return LMB_OK;
+  LMB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.push_back({dev, fn, bytes});
+  return LMB_OK;
+}
 
 // ----------------------------------------------------------------------------
 // Quantisation: max of the positive pixels, then uint8 + occupancy bit.
@@ -85,9 +107,10 @@ __global__ void quant_u8_kernel(const T *__restrict__ img, size_t npx,
 static constexpr uint64_t kWaitNs = 2000000000ull;  // bounded TMA waits: 2 s
 
 // Intensity of slot k over one record, in record order (LaueMatchingCPU.c:671-681
-// for the uint8 image; :649-653 for the float64 image).
-__device__ __noinline__ void candidate(const CmpArgs &a, const uint16_t *rec, int c, uint64_t oid,
-                                       int k) {
+// for the uint8 image; :649-653 for the float64 image).  Returns the spot
+// count; tot/su receive the FP64 sum and the uint8 sum.
+__device__ __noinline__ int slot_sum(const CmpArgs &a, const uint16_t *rec, int c, int k,
+                                     double &tot_out, int &su_out) {
   const uint8_t *img = a.u8 + (size_t)k * a.npx;
   const double *fim = a.f64 ? a.f64 + (size_t)k * a.npx : nullptr;
   const double sc = a.scale[k];
@@ -113,28 +136,16 @@ __device__ __noinline__ void candidate(const CmpArgs &a, const uint16_t *rec, in
       }
     }
   }
-  if (ns >= a.min_spots && tot >= a.min_int) {
-    atomicAdd(&a.pass_cnt[k], 1u);
-    const double score = dmul(tot, dsqrt((double)ns));
-    if (score != 0.0) {  // collection skips zero scores (LaueMatchingCPU.c:783)
-      const unsigned int pos = atomicAdd(&a.surv_cnt[k], 1u);
-      if (pos < a.cap) {
-        lmb_survivor sv;
-        sv.id = oid;
-        sv.n_spots = ns;
-        sv.sum_u8 = su;
-        sv.tot_int = tot;
-        sv.score = score;
-        a.surv[(size_t)k * a.cap + pos] = sv;
-      }
-    }
-  }
+  tot_out = tot;
+  su_out = su;
+  return ns;
 }
 
+// Called by all 32 lanes of a warp (lanes without a record pass valid=false).
 template <int B>
 __device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, uint64_t oid,
-                                        uint64_t pol) {
-  int c = rec[0];
+                                        uint64_t pol, bool valid) {
+  int c = valid ? rec[0] : 0;
   if (c > a.S) c = a.S;  // clamp like LaueMatchingGPU.cu:54-55
   unsigned long long cnt[B];
 #pragma unroll
@@ -176,11 +187,48 @@ __device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, u
       eq &= ~cnt[b];
     }
   }
-  unsigned long long cand = (gt | eq) & a.active;
-  while (cand) {
-    const int k = __ffsll((long long)cand) - 1;
-    cand &= cand - 1;
-    candidate(a, rec, c, oid, k);
+  const unsigned long long cand = valid ? ((gt | eq) & a.active) : 0ull;
+  // Candidates, slot by slot, warp-uniformly: the lanes whose orientation is
+  // a candidate for slot k sum it; one leader reserves the warp's survivor
+  // positions with a single atomic (warp-aggregated compaction).
+  unsigned long long wc = ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(cand >> 32))
+                           << 32) |
+                          __reduce_or_sync(0xffffffffu, (unsigned)cand);
+  const int lane = threadIdx.x & 31;
+  while (wc) {
+    const int k = __ffsll((long long)wc) - 1;
+    wc &= wc - 1;
+    bool pass = false, surv = false;
+    double tot = 0.0, score = 0.0;
+    int ns = 0, su = 0;
+    if ((cand >> k) & 1) {
+      ns = slot_sum(a, rec, c, k, tot, su);
+      pass = ns >= a.min_spots && tot >= a.min_int;
+      if (pass) {
+        score = dmul(tot, dsqrt((double)ns));
+        surv = score != 0.0;  // collection skips zero scores (LaueMatchingCPU.c:783)
+      }
+    }
+    const unsigned pm = __ballot_sync(0xffffffffu, pass);
+    const unsigned sm = __ballot_sync(0xffffffffu, surv);
+    unsigned base = 0;
+    if (lane == 0) {
+      if (pm) atomicAdd(&a.pass_cnt[k], (unsigned)__popc(pm));
+      if (sm) base = atomicAdd(&a.surv_cnt[k], (unsigned)__popc(sm));
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (surv) {
+      const unsigned pos = base + __popc(sm & ((1u << lane) - 1u));
+      if (pos < a.cap) {
+        lmb_survivor sv;
+        sv.id = oid;
+        sv.n_spots = ns;
+        sv.sum_u8 = su;
+        sv.tot_int = tot;
+        sv.score = score;
+        a.surv[(size_t)k * a.cap + pos] = sv;
+      }
+    }
   }
 }
 
@@ -233,9 +281,10 @@ __global__ void __launch_bounds__(256) compare_ring_kernel(const __grid_constant
       }
       const uint16_t *rec = reinterpret_cast<const uint16_t *>(ring + (size_t)s * a.tile_bytes) +
                             (size_t)threadIdx.x * a.R;
-      process<B>(a, rec, oid, pol_occ);
-    } else if (oid < a.n) {
-      process<B>(a, a.db + oid * a.R, oid, pol_occ);  // partial last tile: direct loads
+      process<B>(a, rec, oid, pol_occ, true);
+    } else {
+      const bool v = oid < a.n;  // partial last tile: direct loads, whole warps
+      process<B>(a, v ? a.db + oid * a.R : a.db, oid, pol_occ, v);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -318,11 +367,12 @@ __global__ void __launch_bounds__(576, 1) compare_ws_kernel(const __grid_constan
       }
       const uint16_t *rec = reinterpret_cast<const uint16_t *>(ring + (size_t)s * a.tile_bytes) +
                             (size_t)(sub * 32 + lane) * a.R;
-      process<B>(a, rec, oid, pol_occ);
+      process<B>(a, rec, oid, pol_occ, true);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
-    } else if (oid < a.n) {
-      process<B>(a, a.db + oid * a.R, oid, pol_occ);  // partial last tile: direct loads
+    } else {
+      const bool v = oid < a.n;  // partial last tile: direct loads, whole warps
+      process<B>(a, v ? a.db + oid * a.R : a.db, oid, pol_occ, v);
     }
   }
 }
@@ -437,12 +487,12 @@ template <int B>
 static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, size_t smem,
                     cudaStream_t st) {
   if (c.variant == 1) {
-    LMB_CUDA(cudaFuncSetAttribute(compare_ws_kernel<B>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int rc = ensure_smem((const void *)compare_ws_kernel<B>, (int)smem);
+    if (rc) return rc;
     compare_ws_kernel<B><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
   } else {
-    LMB_CUDA(cudaFuncSetAttribute(compare_ring_kernel<B>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int rc = ensure_smem((const void *)compare_ring_kernel<B>, (int)smem);
+    if (rc) return rc;
     compare_ring_kernel<B><<<grid, a.tile, smem, st>>>(a);
   }
   LMB_CUDA(cudaGetLastError());
@@ -479,7 +529,8 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st) {
   if (nslots == 0) return LMB_OK;
   const int smem = (int)(kSmemSortMax * sizeof(unsigned long long));
-  LMB_CUDA(cudaFuncSetAttribute(order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int rc = ensure_smem((const void *)order_kernel, smem);
+  if (rc) return rc;
   order_kernel<<<nslots, 1024, smem, st>>>(a);
   LMB_CUDA(cudaGetLastError());
   return LMB_OK;

@@ -32,6 +32,25 @@ using namespace lmb;
 // [64,128) pass counts, [128] device error word.
 static constexpr int kStatusWords = 2 * LMB_MAX_SLOTS + 1;
 
+// Configuration of one pass; a captured graph is reusable for an equal key.
+struct PassKey {
+  uint64_t mask = 0;
+  int min_spots = 0;
+  double min_int = 0;
+  int mode = 0;
+  CompareTuning tuning{};
+  bool operator==(const PassKey &o) const {
+    return mask == o.mask && min_spots == o.min_spots &&
+           memcmp(&min_int, &o.min_int, sizeof(double)) == 0 && mode == o.mode &&
+           memcmp(&tuning, &o.tuning, sizeof(CompareTuning)) == 0;
+  }
+};
+
+struct PassGraph {
+  PassKey key;
+  cudaGraphExec_t exec;
+};
+
 struct lmb_engine {
   int device = 0;
   int num_sms = 148;
@@ -66,6 +85,10 @@ struct lmb_engine {
   cudaEvent_t ev_loaded[LMB_MAX_SLOTS] = {};
   cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
   CompareTuning tuning{1, 0, 0, 0, 0, 0};  // warp-specialised, default shape
+  std::vector<PassGraph> graphs;  // captured passes, most recent last
+  bool use_graphs = true;
+  void *h_stage[2] = {nullptr, nullptr};   // pinned upload staging (lazy)
+  cudaEvent_t ev_stage[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -96,6 +119,12 @@ void free_engine(lmb_engine *e) {
   cudaFree(e->d_scratch);
   cudaFree(e->d_status);
   cudaFreeHost(e->h_status);
+  for (auto &g : e->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  for (int i = 0; i < 2; i++) {
+    if (e->h_stage[i]) cudaFreeHost(e->h_stage[i]);
+    if (e->ev_stage[i]) cudaEventDestroy(e->ev_stage[i]);
+  }
   for (auto &v : e->ev)
     if (v) cudaEventDestroy(v);
   for (int k = 0; k < LMB_MAX_SLOTS; k++) {
@@ -111,48 +140,50 @@ size_t dtype_bytes(int dtype) {
   return dtype == LMB_F64 ? 8 : dtype == LMB_F32 ? 4 : 1;
 }
 
-// Host->device copy of a large pageable buffer through two pinned chunks so
-// the host memcpy of chunk i+1 overlaps the DMA of chunk i.
-int upload_chunked(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+// Host->device copy of a large pageable buffer (a memory-mapped cache or
+// orientation file) through the engine's two pinned 64 MiB staging chunks:
+// the host copy into chunk b (split over OpenMP threads) overlaps the DMA of
+// chunk b^1.
+int upload_chunked(lmb_engine *e, void *dst, const void *src, size_t bytes, cudaStream_t st) {
   const size_t kChunk = 64ull << 20;
-  if (bytes <= kChunk) {
+  if (bytes <= (4ull << 20)) {
     LMB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
     LMB_CUDA(cudaStreamSynchronize(st));
     return LMB_OK;
   }
-  void *pin[2] = {nullptr, nullptr};
-  cudaEvent_t done[2] = {nullptr, nullptr};
-  int rc = LMB_OK;
-  for (int i = 0; i < 2 && rc == LMB_OK; i++) {
-    cudaError_t ce = cudaHostAlloc(&pin[i], kChunk, cudaHostAllocDefault);
-    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
-    if (ce != cudaSuccess) rc = cuda_fail(ce, "pinned staging", __FILE__, __LINE__);
+  for (int i = 0; i < 2; i++) {
+    if (!e->h_stage[i]) LMB_CUDA(cudaHostAlloc(&e->h_stage[i], kChunk, cudaHostAllocDefault));
+    if (!e->ev_stage[i]) LMB_CUDA(cudaEventCreateWithFlags(&e->ev_stage[i], cudaEventDisableTiming));
   }
   size_t off = 0;
   int b = 0;
-  while (rc == LMB_OK && off < bytes) {
+  while (off < bytes) {
     const size_t len = std::min(kChunk, bytes - off);
-    cudaError_t ce = cudaEventSynchronize(done[b]);  // chunk b free again
-    if (ce == cudaSuccess) {
-      memcpy(pin[b], static_cast<const char *>(src) + off, len);
-      ce = cudaMemcpyAsync(static_cast<char *>(dst) + off, pin[b], len, cudaMemcpyHostToDevice, st);
+    LMB_CUDA(cudaEventSynchronize(e->ev_stage[b]));  // chunk b free again
+    char *dstp = static_cast<char *>(e->h_stage[b]);
+    const char *srcp = static_cast<const char *>(src) + off;
+    const size_t piece = 4ull << 20;
+    const long np = (long)((len + piece - 1) / piece);
+#pragma omp parallel for schedule(static) num_threads(8)
+    for (long i = 0; i < np; i++) {
+      const size_t o = (size_t)i * piece;
+      memcpy(dstp + o, srcp + o, std::min(piece, len - o));
     }
-    if (ce == cudaSuccess) ce = cudaEventRecord(done[b], st);
-    if (ce != cudaSuccess) rc = cuda_fail(ce, "chunked upload", __FILE__, __LINE__);
+    LMB_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + off, dstp, len, cudaMemcpyHostToDevice, st));
+    LMB_CUDA(cudaEventRecord(e->ev_stage[b], st));
     off += len;
     b ^= 1;
   }
-  cudaStreamSynchronize(st);
-  for (int i = 0; i < 2; i++) {
-    if (done[i]) cudaEventDestroy(done[i]);
-    if (pin[i]) cudaFreeHost(pin[i]);
-  }
-  return rc;
+  LMB_CUDA(cudaStreamSynchronize(st));
+  return LMB_OK;
 }
 
 int alloc_db(lmb_engine *e, uint64_t n) {
   LMB_REQUIRE(n < (1ull << 40), "at most 2^40 orientations are supported (got %llu)",
               (unsigned long long)n);
+  for (auto &g : e->graphs)  // captured passes name the old DB
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  e->graphs.clear();
   cudaFree(e->d_db);
   e->d_db = nullptr;
   e->n = 0;
@@ -169,6 +200,59 @@ int upload_hkls(const int32_t *hkls, int nh, int4 **d_out) {
   for (int i = 0; i < nh; i++) h[i] = make_int4(hkls[3 * i], hkls[3 * i + 1], hkls[3 * i + 2], 0);
   LMB_CUDA(cudaMalloc(d_out, h.size() * sizeof(int4)));
   LMB_CUDA(cudaMemcpy(*d_out, h.data(), (size_t)nh * sizeof(int4), cudaMemcpyHostToDevice));
+  return LMB_OK;
+}
+
+
+// One pass: status reset, compare, ordering, status copy-back, on e->st.
+int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
+  // timing events recorded inside a captured graph must be external to be
+  // observable (and timed) after each replay
+  const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  LMB_CUDA(cudaMemsetAsync(e->d_status, 0, kStatusWords * sizeof(unsigned int), e->st));
+  LMB_CUDA(cudaEventRecordWithFlags(e->ev[0], e->st, evf));
+  CmpArgs a{};
+  a.db = e->d_db;
+  a.n = e->n;
+  a.R = e->R;
+  a.S = e->S;
+  a.W = e->geo.nr_px_x;
+  a.H = e->geo.nr_px_y;
+  a.occ = e->d_occ;
+  a.active = k.mask;
+  a.u8 = e->d_u8;
+  a.f64 = k.mode == LMB_VALUE_F64 ? e->d_f64 : nullptr;
+  a.npx = e->npx;
+  a.scale = e->d_scale;
+  a.mode = k.mode;
+  // count >= MinNrSpots can only hold for MinNrSpots <= S; <= 0 always holds
+  a.min_spots = k.min_spots < 0 ? 0 : k.min_spots;
+  a.min_int = k.min_int;
+  a.surv = e->d_surv;
+  a.cap = e->cap;
+  a.surv_cnt = e->d_status;
+  a.pass_cnt = e->d_status + LMB_MAX_SLOTS;
+  a.err = reinterpret_cast<int *>(e->d_status + 2 * LMB_MAX_SLOTS);
+  if (k.min_spots <= e->S && !std::isnan(k.min_int)) {
+    const int rc = compare_launch(a, k.tuning, e->num_sms, e->st);
+    if (rc) return rc;
+  }
+  LMB_CUDA(cudaEventRecordWithFlags(e->ev[1], e->st, evf));
+  OrderArgs o{};
+  o.surv = e->d_surv;
+  o.out = e->d_sorted;
+  o.surv_cnt = e->d_status;
+  o.cap = e->cap;
+  o.scratch = e->d_scratch;
+  o.cap2 = e->cap2;
+  int ns = 0;
+  for (int i = 0; i < LMB_MAX_SLOTS; i++)
+    if (k.mask >> i & 1) o.slots[ns++] = i;
+  const int rc = order_launch(o, ns, e->st);
+  if (rc) return rc;
+  LMB_CUDA(cudaEventRecordWithFlags(e->ev[2], e->st, evf));
+  LMB_CUDA(cudaMemcpyAsync(e->h_status, e->d_status, kStatusWords * sizeof(unsigned int),
+                           cudaMemcpyDeviceToHost, e->st));
   return LMB_OK;
 }
 
@@ -275,7 +359,7 @@ int lmb_db_upload(lmb_engine *e, const uint16_t *records, uint64_t n) {
   rc = alloc_db(e, n);
   if (rc) return rc;
   LMB_CUDA(cudaStreamSynchronize(e->st));
-  return upload_chunked(e->d_db, records, (size_t)n * e->R * 2, e->st);
+  return upload_chunked(e, e->d_db, records, (size_t)n * e->R * 2, e->st);
 }
 
 static int db_build_common(lmb_engine *e, const double *orients, uint64_t seed, bool synthetic,
@@ -303,7 +387,7 @@ static int db_build_common(lmb_engine *e, const double *orients, uint64_t seed, 
     if (synthetic) {
       rc = synth_orient_launch(seed, off, len, d_om, e->st);
     } else {
-      rc = upload_chunked(d_om, orients + off * 9, len * 72, e->st);
+      rc = upload_chunked(e, d_om, orients + off * 9, len * 72, e->st);
     }
     if (rc == LMB_OK)
       rc = dbbuild_launch(d_om, len, d_hkl, nh, e->geo, e->d_db + off * e->R, e->st,
@@ -412,52 +496,47 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
               "float64 pass needs images loaded with keep_f64");
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
     if (slot_mask >> k & 1) LMB_CUDA(cudaStreamWaitEvent(e->st, e->ev_loaded[k], 0));
-  LMB_CUDA(cudaMemsetAsync(e->d_status, 0, kStatusWords * sizeof(unsigned int), e->st));
-  LMB_CUDA(cudaEventRecord(e->ev[0], e->st));
-  CmpArgs a{};
-  a.db = e->d_db;
-  a.n = e->n;
-  a.R = e->R;
-  a.S = e->S;
-  a.W = e->geo.nr_px_x;
-  a.H = e->geo.nr_px_y;
-  a.occ = e->d_occ;
-  a.active = slot_mask;
-  a.u8 = e->d_u8;
-  a.f64 = value_mode == LMB_VALUE_F64 ? e->d_f64 : nullptr;
-  a.npx = e->npx;
-  a.scale = e->d_scale;
-  a.mode = value_mode;
-  // count >= MinNrSpots can only hold for MinNrSpots <= S; <= 0 always holds
-  a.min_spots = min_nr_spots < 0 ? 0 : min_nr_spots;
-  a.min_int = min_intensity;
-  a.surv = e->d_surv;
-  a.cap = e->cap;
-  a.surv_cnt = e->d_status;
-  a.pass_cnt = e->d_status + LMB_MAX_SLOTS;
-  a.err = reinterpret_cast<int *>(e->d_status + 2 * LMB_MAX_SLOTS);
-  if (min_nr_spots <= e->S && !std::isnan(min_intensity)) {
-    rc = compare_launch(a, e->tuning, e->num_sms, e->st);
+  // The pass (status reset, compare, ordering, status copy-back) replays from
+  // a CUDA graph once a configuration has been seen before; the first pass of
+  // a configuration runs eagerly (it also sets the kernels' attributes).
+  PassKey key;
+  key.mask = slot_mask;
+  key.min_spots = min_nr_spots;
+  key.min_int = min_intensity;
+  key.mode = value_mode;
+  key.tuning = e->tuning;
+  PassGraph *pg = nullptr;
+  for (auto &g : e->graphs)
+    if (g.key == key) pg = &g;
+  if (pg && pg->exec) {
+    LMB_CUDA(cudaGraphLaunch(pg->exec, e->st));
+  } else if (pg && e->use_graphs) {
+    cudaGraph_t graph = nullptr;
+    LMB_CUDA(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_pass(e, key, true);
+    const cudaError_t ce = cudaStreamEndCapture(e->st, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    LMB_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&pg->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    LMB_CUDA(ie);
+    LMB_CUDA(cudaGraphLaunch(pg->exec, e->st));
+  } else {
+    if (!pg) {
+      if (e->graphs.size() >= 8) {  // keep the 8 most recent configurations
+        if (e->graphs.front().exec) cudaGraphExecDestroy(e->graphs.front().exec);
+        e->graphs.erase(e->graphs.begin());
+      }
+      e->graphs.push_back(PassGraph{key, nullptr});
+    }
+    rc = enqueue_pass(e, key, false);
     if (rc) return rc;
   }
-  LMB_CUDA(cudaEventRecord(e->ev[1], e->st));
-  OrderArgs o{};
-  o.surv = e->d_surv;
-  o.out = e->d_sorted;
-  o.surv_cnt = e->d_status;
-  o.cap = e->cap;
-  o.scratch = e->d_scratch;
-  o.cap2 = e->cap2;
-  int ns = 0;
-  for (int k = 0; k < LMB_MAX_SLOTS; k++)
-    if (slot_mask >> k & 1) o.slots[ns++] = k;
-  rc = order_launch(o, ns, e->st);
-  if (rc) return rc;
-  LMB_CUDA(cudaEventRecord(e->ev[2], e->st));
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
     if (slot_mask >> k & 1) LMB_CUDA(cudaEventRecord(e->ev_released[k], e->st));
-  LMB_CUDA(cudaMemcpyAsync(e->h_status, e->d_status, kStatusWords * sizeof(unsigned int),
-                           cudaMemcpyDeviceToHost, e->st));
   e->last_mask = slot_mask;
   e->pending = true;
   return LMB_OK;

@@ -459,11 +459,12 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
   int64_t nr = n_results;
   std::vector<uint64_t> rows(ids, ids + nr);
   std::vector<double> sc(scores, scores + nr);
-  if (nr > kMergeMax) {
+  const int64_t cap = pp->max_results > 0 ? pp->max_results : kMergeMax;
+  if (nr > cap) {
     fprintf(stderr,
-            "WARNING: %lld coarse matches exceed merge cap %d; keeping the top-scored before "
+            "WARNING: %lld coarse matches exceed merge cap %lld; keeping the top-scored before "
             "clustering.\n",
-            (long long)nr, kMergeMax);
+            (long long)nr, (long long)cap);
     struct SR {
       double score;
       size_t row;
@@ -474,11 +475,11 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
       const double x = ((const SR *)a)->score, y = ((const SR *)b)->score;
       return (x < y) - (x > y);
     });
-    for (int i = 0; i < kMergeMax; i++) {
+    for (int64_t i = 0; i < cap; i++) {
       sc[i] = sr[i].score;
       rows[i] = sr[i].row;
     }
-    nr = kMergeMax;
+    nr = cap;
   }
   std::vector<double> quat((size_t)nr * 4);
 #pragma omp parallel for num_threads(nthreads)

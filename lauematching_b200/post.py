@@ -32,11 +32,13 @@ STREAM_SPOTS_HEADER = "%ImageNr\t" + SPOTS_HEADER[1:]
 def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndarray,
                  scores: np.ndarray, image_f32: np.ndarray, hkls: np.ndarray,
                  min_nr_spots: int | None = None, image_num: int = 0,
-                 num_threads: int | None = None):
+                 num_threads: int | None = None, max_results: int = 0):
     """Return (solutions_text, spots_text, n_unique) for one image.
 
     ``ids``/``scores`` are the image's collected matches in the reference's
-    collection order (ascending orientation ID)."""
+    collection order (ascending orientation ID).  ``max_results`` > 0 keeps
+    only that many top-scored candidates for the merge (the reference's own
+    cap path, LaueMatchingHeaders.h:976-997, with its cap of 50000 lowered)."""
     pp = _lib.LmbPostParams()
     for i in range(6):
         pp.lattice[i] = params.lattice[i]
@@ -49,6 +51,7 @@ def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndar
     pp.image_num = int(image_num)
     pp.num_threads = int(num_threads or os.cpu_count() or 1)
     pp.optimizer = 0
+    pp.max_results = int(max_results)  # 0: the reference's 50000
     om = np.ascontiguousarray(orients, dtype=np.float64).reshape(-1, 9)
     idv = np.ascontiguousarray(ids, dtype=np.uint64)
     scv = np.ascontiguousarray(scores, dtype=np.float64)

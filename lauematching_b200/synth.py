@@ -75,6 +75,55 @@ def shoemake_orientations(n: int, seed: int, start: int = 0) -> np.ndarray:
     return om
 
 
+_HEX_SYM = np.array([[1, 0, 0, 0], [0.86603, 0, 0, 0.5], [0.5, 0, 0, 0.86603], [0, 0, 0, 1],
+                     [0.5, 0, 0, -0.86603], [0.86603, 0, 0, -0.5], [0, 1, 0, 0],
+                     [0, 0.86603, 0.5, 0], [0, 0.5, 0.86603, 0], [0, 0, 1, 0],
+                     [0, -0.5, 0.86603, 0], [0, -0.86603, 0.5, 0]])
+
+
+def _om_to_quat(om: np.ndarray) -> np.ndarray:
+    """Unit quaternions (w >= 0) of row-major rotation matrices (n, 9)."""
+    m = om.reshape(-1, 3, 3)
+    w = 0.5 * np.sqrt(np.maximum(0.0, 1.0 + m[:, 0, 0] + m[:, 1, 1] + m[:, 2, 2]))
+    x = 0.5 * np.sqrt(np.maximum(0.0, 1.0 + m[:, 0, 0] - m[:, 1, 1] - m[:, 2, 2]))
+    y = 0.5 * np.sqrt(np.maximum(0.0, 1.0 - m[:, 0, 0] + m[:, 1, 1] - m[:, 2, 2]))
+    z = 0.5 * np.sqrt(np.maximum(0.0, 1.0 - m[:, 0, 0] - m[:, 1, 1] + m[:, 2, 2]))
+    x = np.copysign(x, m[:, 2, 1] - m[:, 1, 2])
+    y = np.copysign(y, m[:, 0, 2] - m[:, 2, 0])
+    z = np.copysign(z, m[:, 1, 0] - m[:, 0, 1])
+    q = np.stack([w, x, y, z], 1)
+    return q / np.linalg.norm(q, axis=1, keepdims=True)
+
+
+def _quat_to_om(q: np.ndarray) -> np.ndarray:
+    w, x, y, z = q.T
+    return np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w),
+                     2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                     2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], 1)
+
+
+def hexagonal_fundamental_zone(om: np.ndarray) -> np.ndarray:
+    """Reduce rotations to the hexagonal (622) fundamental zone: of the 12
+    symmetry-equivalent quaternions q*s (the operator order and product of
+    LaueMatchingHeaders.h:111-122,166-178) keep the one with the largest
+    scalar part.  Uniform rotations map to uniform rotations in the zone."""
+    q = _om_to_quat(np.asarray(om, np.float64))
+    s = _HEX_SYM / np.linalg.norm(_HEX_SYM, axis=1, keepdims=True)
+    # product Q = q (x) r with the reference's component formula
+    w = s[None, :, 0] * q[:, None, 0] - s[None, :, 1] * q[:, None, 1] \
+        - s[None, :, 2] * q[:, None, 2] - s[None, :, 3] * q[:, None, 3]
+    best = np.argmax(np.abs(w), axis=1)
+    r = s[best]
+    Q = np.stack([
+        r[:, 0] * q[:, 0] - r[:, 1] * q[:, 1] - r[:, 2] * q[:, 2] - r[:, 3] * q[:, 3],
+        r[:, 1] * q[:, 0] + r[:, 0] * q[:, 1] + r[:, 3] * q[:, 2] - r[:, 2] * q[:, 3],
+        r[:, 2] * q[:, 0] + r[:, 0] * q[:, 2] + r[:, 1] * q[:, 3] - r[:, 3] * q[:, 1],
+        r[:, 3] * q[:, 0] + r[:, 0] * q[:, 3] + r[:, 2] * q[:, 1] - r[:, 1] * q[:, 2]], 1)
+    Q *= np.where(Q[:, :1] < 0, -1.0, 1.0)
+    Q /= np.linalg.norm(Q, axis=1, keepdims=True)
+    return _quat_to_om(Q)
+
+
 def _sorted_hkls(mask_fn, m: int) -> np.ndarray:
     r = np.arange(-m, m + 1)
     h, k, l = np.meshgrid(r, r, r, indexing="ij")

@@ -158,6 +158,33 @@ def test_survivor_overflow_is_reported():
             e.results(0)
 
 
+def test_repeated_pass_replays_graph_with_same_results():
+    """The first pass of a configuration runs eagerly, the second is captured
+    into a CUDA graph, later ones replay it: results and timings stay valid."""
+    c = golden_case("tilted_dense")
+    p = c.params
+    ref = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                    p.min_nr_spots, p.min_intensity)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        e.load_image(2, c.image)
+        e.load_image(9, c.image * 0.5)
+        for it in range(5):
+            e.match([2, 9], p.min_nr_spots, p.min_intensity)
+            got, npass = e.results(2)
+            assert npass == ref.n_pass
+            assert_same_survivors(got, ref)
+            cmp_ms, ord_ms = e.last_pass_ms()
+            assert cmp_ms > 0 and ord_ms >= 0
+        e.load_image(2, c.image * 0.25)  # new frame, same configuration: graph replays
+        e.match([2, 9], p.min_nr_spots, p.min_intensity)
+        got, npass = e.results(2)
+        ref2 = O.compare(c.records, p.max_nr_spots, c.image * 0.25, p.nr_px_x, p.nr_px_y,
+                         p.min_nr_spots, p.min_intensity)
+        assert npass == ref2.n_pass
+        assert_same_survivors(got, ref2)
+
+
 def test_errors_are_reported_not_silent():
     c = golden_case("tilted_fcc")
     with engine_for(c.params) as e:
