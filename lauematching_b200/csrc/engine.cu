@@ -286,9 +286,9 @@ int lmb_geometry_init(const double lattice[6], int32_t space_group, const double
 int lmb_engine_create(int32_t device, const lmb_geometry *geo, uint64_t survivor_capacity,
                       lmb_engine **out) {
   LMB_REQUIRE(geo && out, "null argument");
-  LMB_REQUIRE(geo->nr_px_x > 0 && geo->nr_px_y > 0 && geo->nr_px_x <= 65536 &&
-                  geo->nr_px_y <= 65536,
-              "detector size %d x %d outside 1..65536", geo->nr_px_x, geo->nr_px_y);
+  LMB_REQUIRE(geo->nr_px_x > 0 && geo->nr_px_y > 0 && geo->nr_px_x <= 65535 &&
+                  geo->nr_px_y <= 65535,
+              "detector size %d x %d outside 1..65535", geo->nr_px_x, geo->nr_px_y);
   LMB_REQUIRE(geo->max_nr_spots >= 1 && geo->max_nr_spots <= 32767,
               "MaxNrLaueSpots=%d outside 1..32767", geo->max_nr_spots);
   if (survivor_capacity == 0) survivor_capacity = 262144;
