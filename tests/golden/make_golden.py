@@ -59,6 +59,12 @@ CASES = {
     "tilted_rhomb": dict(n=3000, seed=7, hkl=("cubic", 6, "P"), geom=TILTED, S=30, grains=2,
                          min_spots=5, min_int=200.0, grain_min=6,
                          lattice=(0.45, 0.45, 0.45, 58, 58, 58), sg=166),
+    # hexagonal with c/a refinement (tol_c_over_a): the lattice of the refined
+    # grains comes from the c/a path of FitOrientation (cbrt of the cell volume)
+    "tilted_hex_ca": dict(n=3000, seed=8, hkl=("hex", 8), geom=TILTED, S=30, grains=3,
+                          min_spots=5, min_int=200.0, grain_min=8,
+                          lattice=(0.295, 0.295, 0.468, 90, 90, 120), sg=194,
+                          tol_c_over_a=0.01, max_angle=5.0),
 }
 
 
@@ -69,7 +75,8 @@ def make_case(name, c, workdir):
     txt = synth.params_text(lattice=lattice, space_group=sg, max_nr_spots=c["S"],
                             min_nr_spots=c["min_spots"], min_intensity=c["min_int"],
                             forward_file=fwd, do_fwd=1, nr_px=c.get("nr_px", (2048, 2048)),
-                            px=c.get("px", 0.0002), **c["geom"])
+                            px=c.get("px", 0.0002), tol_c_over_a=c.get("tol_c_over_a", 0.0),
+                            max_angle=c.get("max_angle", 2.0), **c["geom"])
     p = P.parse_params_text(txt)
     om = synth.shoemake_orientations(c["n"], seed=c["seed"])
     kind = c["hkl"][0]
