@@ -296,10 +296,7 @@ def run_ours(args, rank, world):
         for k in range(K):
             e.load_image(k, pins[k].array, want_scale=False)
         e.match(slots, p.min_nr_spots, p.min_intensity)
-        nb = 0
-        for k in range(K):
-            r, _ = e.results(k)
-            nb += r.nbytes
+        nb = sum(r.nbytes for r, _ in e.results_batch(slots).values())
         d2h[0] = nb + (2 * 64 + 1) * 4
 
     # sequential: upload 64 frames, one pass, download
@@ -325,11 +322,7 @@ def run_ours(args, rank, world):
             fidx[0] += 1
 
     def collect(h):
-        nb = 0
-        for k in halves[h]:
-            r, _ = e.results(k)
-            nb += r.nbytes
-        return nb
+        return sum(r.nbytes for r, _ in e.results_batch(halves[h]).values())
 
     def pipelined(npasses, lat=None):
         load_half(0)

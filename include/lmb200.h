@@ -109,6 +109,13 @@ void *lmb_engine_stream(lmb_engine *e);
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields);
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields);
 
+/* lmb_image_load sends a frame whose positive pixels are few (their
+ * (uint32 index, value) pairs smaller than half the dense frame) as those
+ * pairs, found by a multi-threaded host scan, instead of the whole frame
+ * (default on; results are identical either way).  No reference counterpart
+ * (the reference copies the dense float frame, LaueMatchingGPUStream.cu:1204). */
+int lmb_engine_set_sparse_uploads(lmb_engine *e, int32_t enable);
+
 /* Upload a forward cache (n records of 1+2S uint16) into device memory.
  * Replaces the chunked synchronous H2D of LaueMatchingGPU.cu:619-749 and
  * the resident upload of LaueMatchingGPUStream.cu:998-1038. */
@@ -169,6 +176,14 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots,
  * then not guaranteed: recreate the engine with a larger capacity). */
 int lmb_results(lmb_engine *e, int32_t slot, lmb_survivor *out,
                 uint64_t out_capacity, uint64_t *n_survivors, uint64_t *n_pass);
+
+/* lmb_results for several slots at once: survivors of slots[0..nslots) are
+ * written back to back into out (slot order as given, each ascending id);
+ * counts[i] / n_pass[i] receive each slot's survivor and pass counts.
+ * Returns LMB_ERR_OVERFLOW (counts filled, nothing copied) when out_capacity
+ * is too small or a slot overflowed the engine capacity. */
+int lmb_results_batch(lmb_engine *e, const int32_t *slots, int32_t nslots, lmb_survivor *out,
+                      uint64_t out_capacity, uint64_t *counts, uint64_t *n_pass);
 
 /* Device time of the last pass in milliseconds (CUDA events on the engine
  * stream): compare kernel, ordering kernel. */

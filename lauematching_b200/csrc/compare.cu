@@ -99,6 +99,73 @@ __global__ void quant_u8_kernel(const T *__restrict__ img, size_t npx,
   }
 }
 
+// Sparse frame upload.  slot_clear: zero the slot's previous positive pixels
+// (found through its uint8 image) and their occupancy bits.  sparse_scatter:
+// quantise the positive pixels of the new frame (index, value) with the scale
+// of its maximum `mx` (computed by the host over the same values) exactly as
+// quant_u8_kernel does, and set their occupancy bits.
+__global__ void slot_clear_kernel(uint8_t *__restrict__ u8, unsigned long long *__restrict__ occ,
+                                  unsigned long long bit, size_t npx) {
+  // 16-pixel vector path only when the slot starts on a 16-byte boundary
+  const size_t n16 = (reinterpret_cast<uintptr_t>(u8) & 15) ? 0 : npx / 16;
+  uint4 *u = reinterpret_cast<uint4 *>(u8);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint4 v = u[i];
+    if ((v.x | v.y | v.z | v.w) == 0u) continue;
+    const uint8_t *b = reinterpret_cast<const uint8_t *>(&v);
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+      if (b[j]) occ[i * 16 + j] &= ~bit;
+    u[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  for (size_t i = n16 * 16 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npx;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (u8[i]) {
+      occ[i] &= ~bit;
+      u8[i] = 0;
+    }
+  }
+}
+
+template <typename T>
+__global__ void sparse_scatter_kernel(const uint32_t *__restrict__ idx, const T *__restrict__ val,
+                                      size_t nnz, double mx, uint8_t *__restrict__ u8,
+                                      unsigned long long *__restrict__ occ, unsigned long long bit,
+                                      double *__restrict__ scale_out) {
+  const double inv = (mx > 0) ? ddiv(255.0, mx) : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = (mx > 0) ? ddiv(mx, 255.0) : 1.0;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < nnz;
+       j += (size_t)gridDim.x * blockDim.x) {
+    const double x = (double)val[j];  // > 0 by construction
+    const double v = dmul(x, inv);
+    const uint8_t q = (v >= 255.0) ? 255 : (v < 1.0) ? 1 : (uint8_t)(x86_trunc_i32(v) & 0xFF);
+    const uint32_t p = idx[j];
+    u8[p] = q;
+    occ[p] |= bit;
+  }
+}
+
+int sparse_load_launch(const uint32_t *d_idx, const void *d_val, int dtype, size_t nnz, double mx,
+                       uint8_t *d_u8, unsigned long long *d_occ, int slot, double *d_scale_slot,
+                       size_t npx, int num_sms, cudaStream_t st) {
+  const unsigned long long bit = 1ull << slot;
+  const unsigned cb = (unsigned)std::min<size_t>((npx / 16 + 255) / 256 + 1, (size_t)num_sms * 8);
+  slot_clear_kernel<<<cb, 256, 0, st>>>(d_u8, d_occ, bit, npx);
+  const unsigned sb = (unsigned)std::max<size_t>(1, std::min<size_t>((nnz + 255) / 256, (size_t)num_sms * 8));
+  if (dtype == LMB_F64)
+    sparse_scatter_kernel<double><<<sb, 256, 0, st>>>(d_idx, static_cast<const double *>(d_val),
+                                                      nnz, mx, d_u8, d_occ, bit, d_scale_slot);
+  else if (dtype == LMB_F32)
+    sparse_scatter_kernel<float><<<sb, 256, 0, st>>>(d_idx, static_cast<const float *>(d_val), nnz,
+                                                     mx, d_u8, d_occ, bit, d_scale_slot);
+  else
+    sparse_scatter_kernel<uint8_t><<<sb, 256, 0, st>>>(
+        d_idx, static_cast<const uint8_t *>(d_val), nnz, mx, d_u8, d_occ, bit, d_scale_slot);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
 // ----------------------------------------------------------------------------
 // The DB pass.
 // ----------------------------------------------------------------------------

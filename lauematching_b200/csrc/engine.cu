@@ -6,6 +6,8 @@
 #include <cstring>
 #include <vector>
 
+#include <omp.h>
+
 #include "kernels.cuh"
 
 namespace lmb {
@@ -31,6 +33,8 @@ using namespace lmb;
 // Status words copied back after every pass: [0,64) survivor counts,
 // [64,128) pass counts, [128] device error word.
 static constexpr int kStatusWords = 2 * LMB_MAX_SLOTS + 1;
+
+static constexpr int kSparseRing = 4;  // pinned staging buffers for sparse frames
 
 // Configuration of one pass; a captured graph is reusable for an equal key.
 struct PassKey {
@@ -87,6 +91,11 @@ struct lmb_engine {
   CompareTuning tuning{1, 0, 0, 0, 0, 0};  // warp-specialised, default shape
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
+  bool sparse_uploads = true;               // frames cross the link as pairs when sparse
+  void *sp_host[kSparseRing] = {};          // pinned (index, value) staging ring (lazy)
+  cudaEvent_t sp_ev[kSparseRing] = {};
+  int sp_next = 0;
+  uint64_t sparse_loads = 0;
   void *h_stage[2] = {nullptr, nullptr};   // pinned upload staging (lazy)
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
 };
@@ -121,6 +130,10 @@ void free_engine(lmb_engine *e) {
   cudaFreeHost(e->h_status);
   for (auto &g : e->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
+  for (int i = 0; i < kSparseRing; i++) {
+    if (e->sp_host[i]) cudaFreeHost(e->sp_host[i]);
+    if (e->sp_ev[i]) cudaEventDestroy(e->sp_ev[i]);
+  }
   for (int i = 0; i < 2; i++) {
     if (e->h_stage[i]) cudaFreeHost(e->h_stage[i]);
     if (e->ev_stage[i]) cudaEventDestroy(e->ev_stage[i]);
@@ -203,6 +216,109 @@ int upload_hkls(const int32_t *hkls, int nh, int4 **d_out) {
   return LMB_OK;
 }
 
+
+// Host scan of a frame: if its positive pixels, as (uint32 index, value)
+// pairs, take less than half the dense bytes, upload the pairs (through a
+// ring of pinned staging buffers) and scatter them on the load stream;
+// otherwise leave *sparse false for the dense path.  The maximum is taken over
+// the same positive values the device would see (NaN and non-positive
+// pixels quantise to 0 and are not listed).
+// Positive (and not NaN) pixel test on the bits: uint8 != 0; IEEE floats
+// with the sign bit clear, not zero, and at most +infinity.
+inline bool positive(uint8_t v) { return v != 0; }
+inline bool positive(float v) {
+  uint32_t b;
+  memcpy(&b, &v, 4);
+  return b - 1u < 0x7F800000u;
+}
+inline bool positive(double v) {
+  uint64_t b;
+  memcpy(&b, &v, 8);
+  return b - 1ull < 0x7FF0000000000000ull;
+}
+
+// Visit the positive pixels of px[lo, hi) in order, skipping all-zero 64-byte
+// blocks (a thresholded frame is mostly zero bytes).
+template <typename T, typename F>
+inline void for_positive(const T *px, size_t lo, size_t hi, F &&f) {
+  constexpr size_t kPer = 64 / sizeof(T);
+  size_t i = lo;
+  while (i < hi && (i % kPer)) {
+    if (positive(px[i])) f(i, px[i]);
+    i++;
+  }
+  for (; i + kPer <= hi; i += kPer) {
+    uint64_t w[8];
+    memcpy(w, px + i, 64);
+    if ((w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) == 0) continue;
+    for (size_t j = 0; j < kPer; j++)
+      if (positive(px[i + j])) f(i + j, px[i + j]);
+  }
+  for (; i < hi; i++)
+    if (positive(px[i])) f(i, px[i]);
+}
+
+template <typename T>
+int try_sparse(lmb_engine *e, const T *px, int slot, int dtype, bool *sparse) {
+  *sparse = false;
+  const size_t npx = e->npx;
+  const size_t vb = sizeof(T);
+  const size_t limit = npx * vb / (2 * (4 + vb));
+  const int nt = (int)std::max<size_t>(
+      1, std::min<size_t>(std::min(16, omp_get_num_procs()), npx / (1 << 16) + 1));
+  std::vector<size_t> cnt((size_t)nt + 1, 0);
+  std::vector<double> mxs((size_t)nt, 0.0);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num();
+    const size_t lo = npx * t / nt, hi = npx * (t + 1) / nt;
+    size_t c = 0;
+    double m = 0.0;
+    for_positive(px, lo, hi, [&](size_t, T v) {
+      c++;
+      if ((double)v > m) m = (double)v;
+    });
+    cnt[t + 1] = c;
+    mxs[t] = m;
+  }
+  for (int t = 0; t < nt; t++) cnt[t + 1] += cnt[t];
+  const size_t nnz = cnt[nt];
+  if (nnz > limit) return LMB_OK;
+  double mx = 0.0;
+  for (int t = 0; t < nt; t++)
+    if (mxs[t] > mx) mx = mxs[t];
+  const int r = e->sp_next;
+  e->sp_next = (r + 1) % kSparseRing;
+  const size_t cap = npx * 4 + 64;
+  if (!e->sp_host[r]) LMB_CUDA(cudaHostAlloc(&e->sp_host[r], cap, cudaHostAllocDefault));
+  if (!e->sp_ev[r]) LMB_CUDA(cudaEventCreateWithFlags(&e->sp_ev[r], cudaEventDisableTiming));
+  LMB_CUDA(cudaEventSynchronize(e->sp_ev[r]));  // ring entry free again
+  uint32_t *hidx = static_cast<uint32_t *>(e->sp_host[r]);
+  const size_t voff = ((nnz * 4 + 15) / 16) * 16;
+  T *hval = reinterpret_cast<T *>(static_cast<char *>(e->sp_host[r]) + voff);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num();
+    const size_t lo = npx * t / nt, hi = npx * (t + 1) / nt;
+    size_t o = cnt[t];
+    for_positive(px, lo, hi, [&](size_t i, T v) {
+      hidx[o] = (uint32_t)i;
+      hval[o] = v;
+      o++;
+    });
+  }
+  const size_t bytes = voff + nnz * vb;
+  LMB_CUDA(cudaMemcpyAsync(e->d_stage, e->sp_host[r], bytes, cudaMemcpyHostToDevice, e->ld));
+  LMB_CUDA(cudaEventRecord(e->sp_ev[r], e->ld));
+  const int rc = sparse_load_launch(
+      static_cast<const uint32_t *>(e->d_stage), static_cast<const char *>(e->d_stage) + voff,
+      dtype, nnz, mx, e->d_u8 + (size_t)slot * npx, e->d_occ, slot, e->d_scale + slot, npx,
+      e->num_sms, e->ld);
+  if (rc) return rc;
+  e->sparse_loads++;
+  *sparse = true;
+  return LMB_OK;
+}
 
 // One pass: status reset, compare, ordering, status copy-back, on e->st.
 int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
@@ -325,6 +441,7 @@ int lmb_engine_create(int32_t device, const lmb_geometry *geo, uint64_t survivor
     TRY(cudaEventCreateWithFlags(&e->ev_released[k], cudaEventDisableTiming));
   }
   TRY(cudaMalloc(&e->d_u8, e->npx * LMB_MAX_SLOTS));
+  TRY(cudaMemset(e->d_u8, 0, e->npx * LMB_MAX_SLOTS));
   TRY(cudaMalloc(&e->d_occ, e->npx * sizeof(unsigned long long)));
   TRY(cudaMemset(e->d_occ, 0, e->npx * sizeof(unsigned long long)));
   TRY(cudaMalloc(&e->d_scale, LMB_MAX_SLOTS * sizeof(double)));
@@ -465,12 +582,24 @@ int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtyp
   if (keep_f64 && !e->d_f64)
     LMB_CUDA(cudaMalloc(&e->d_f64, e->npx * sizeof(double) * LMB_MAX_SLOTS));
   LMB_CUDA(cudaStreamWaitEvent(e->ld, e->ev_released[slot], 0));
-  LMB_CUDA(cudaMemcpyAsync(e->d_stage, pixels, e->npx * dtype_bytes(dtype),
-                           cudaMemcpyHostToDevice, e->ld));
-  rc = quantize_launch(e->d_stage, dtype, e->npx, e->d_max_bits, e->d_u8 + (size_t)slot * e->npx,
-                       keep_f64 ? e->d_f64 + (size_t)slot * e->npx : nullptr, e->d_occ, slot,
-                       e->d_scale + slot, e->num_sms, e->ld);
-  if (rc) return rc;
+  // A sparse frame (the usual thresholded Laue image) crosses the host link
+  // as (index, value) pairs of its positive pixels; a dense one as is.
+  bool sparse = false;
+  if (!keep_f64 && e->sparse_uploads) {
+    rc = dtype == LMB_F64   ? try_sparse(e, static_cast<const double *>(pixels), slot, dtype, &sparse)
+         : dtype == LMB_F32 ? try_sparse(e, static_cast<const float *>(pixels), slot, dtype, &sparse)
+                            : try_sparse(e, static_cast<const uint8_t *>(pixels), slot, dtype, &sparse);
+    if (rc) return rc;
+  }
+  if (!sparse) {
+    LMB_CUDA(cudaMemcpyAsync(e->d_stage, pixels, e->npx * dtype_bytes(dtype),
+                             cudaMemcpyHostToDevice, e->ld));
+    rc = quantize_launch(e->d_stage, dtype, e->npx, e->d_max_bits,
+                         e->d_u8 + (size_t)slot * e->npx,
+                         keep_f64 ? e->d_f64 + (size_t)slot * e->npx : nullptr, e->d_occ, slot,
+                         e->d_scale + slot, e->num_sms, e->ld);
+    if (rc) return rc;
+  }
   LMB_CUDA(cudaEventRecord(e->ev_loaded[slot], e->ld));
   e->loaded_mask |= 1ull << slot;
   if (keep_f64)
@@ -575,6 +704,49 @@ int lmb_results(lmb_engine *e, int32_t slot, lmb_survivor *out, uint64_t out_cap
   return LMB_OK;
 }
 
+int lmb_results_batch(lmb_engine *e, const int32_t *slots, int32_t nslots, lmb_survivor *out,
+                      uint64_t out_capacity, uint64_t *counts, uint64_t *n_pass) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(e->pending, "no pass has been run");
+  LMB_REQUIRE(nslots >= 0 && (slots || nslots == 0) && counts, "bad slot list");
+  LMB_CUDA(cudaStreamSynchronize(e->st));
+  const int derr = (int)e->h_status[2 * LMB_MAX_SLOTS];
+  if (derr != DEV_OK) {
+    set_error("device wait gave up in the compare pass (code %d)", derr);
+    return LMB_ERR_TIMEOUT;
+  }
+  uint64_t total = 0;
+  bool over = false;
+  for (int i = 0; i < nslots; i++) {
+    const int k = slots[i];
+    LMB_REQUIRE(k >= 0 && k < LMB_MAX_SLOTS && (e->last_mask >> k & 1),
+                "slot %d was not part of the last pass", k);
+    counts[i] = e->h_status[k];
+    if (n_pass) n_pass[i] = e->h_status[LMB_MAX_SLOTS + k];
+    over |= counts[i] > e->cap;
+    total += counts[i];
+  }
+  if (over) {
+    set_error("a slot's survivors exceed the engine capacity %u", e->cap);
+    return LMB_ERR_OVERFLOW;
+  }
+  if (total > out_capacity || (!out && total)) {
+    set_error("%llu survivors exceed the output capacity %llu", (unsigned long long)total,
+              (unsigned long long)out_capacity);
+    return LMB_ERR_OVERFLOW;
+  }
+  uint64_t off = 0;
+  for (int i = 0; i < nslots; i++) {
+    if (counts[i])
+      LMB_CUDA(cudaMemcpyAsync(out + off, e->d_sorted + (size_t)slots[i] * e->cap,
+                               counts[i] * sizeof(lmb_survivor), cudaMemcpyDeviceToHost, e->st));
+    off += counts[i];
+  }
+  LMB_CUDA(cudaStreamSynchronize(e->st));
+  return LMB_OK;
+}
+
 int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms) {
   int rc = check_engine(e);
   if (rc) return rc;
@@ -596,6 +768,12 @@ int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields
   for (int i = 0; i < n_fields && i < 6; i++) *dst[i] = fields[i];
   LMB_REQUIRE(t.variant == 0 || t.variant == 1, "unknown compare variant %d", t.variant);
   e->tuning = t;
+  return LMB_OK;
+}
+
+int lmb_engine_set_sparse_uploads(lmb_engine *e, int32_t enable) {
+  LMB_REQUIRE(e, "null engine");
+  e->sparse_uploads = enable != 0;
   return LMB_OK;
 }
 

@@ -63,6 +63,9 @@ int synth_orient_launch(uint64_t seed, uint64_t first, uint64_t n, double *d_out
 int quantize_launch(const void *d_img, int dtype, size_t npx, unsigned long long *d_max_bits,
                     uint8_t *d_u8, double *d_f64_keep, unsigned long long *d_occ, int slot,
                     double *d_scale_slot, int num_sms, cudaStream_t st);
+int sparse_load_launch(const uint32_t *d_idx, const void *d_val, int dtype, size_t nnz, double mx,
+                       uint8_t *d_u8, unsigned long long *d_occ, int slot, double *d_scale_slot,
+                       size_t npx, int num_sms, cudaStream_t st);
 int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_t st);
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st);
 

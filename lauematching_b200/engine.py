@@ -111,6 +111,9 @@ class Engine:
         check(lib().lmb_engine_set_tuning(self._h, vals, 6))
         self._pinned_shape = True
 
+    def set_sparse_uploads(self, enable: bool) -> None:
+        check(lib().lmb_engine_set_sparse_uploads(self._h, int(bool(enable))))
+
     def get_tuning(self) -> dict:
         vals = (C.c_int32 * 6)()
         check(lib().lmb_engine_get_tuning(self._h, vals, 6))
@@ -201,6 +204,32 @@ class Engine:
             check(lib().lmb_results(self._h, int(slot), out.ctypes.data, n.value, C.byref(n),
                                     C.byref(npass)))
         return out, int(npass.value)
+
+    def results_batch(self, slots):
+        """{slot: (survivors, n_pass)} for several slots with one library call
+        per pass (a second one only when the survivors outgrow the buffer)."""
+        sl = np.ascontiguousarray(list(slots), dtype=np.int32)
+        n = sl.shape[0]
+        counts = np.zeros(n, np.uint64)
+        npass = np.zeros(n, np.uint64)
+        cap = max(getattr(self, "_rb_cap", 4096), 1)
+        while True:
+            out = np.empty(cap, SURVIVOR_DTYPE)
+            rc = lib().lmb_results_batch(self._h, sl.ctypes.data, n, out.ctypes.data, cap,
+                                         counts.ctypes.data, npass.ctypes.data)
+            total = int(counts.sum())
+            if rc == _lib.LMB_ERR_OVERFLOW and total > cap:
+                cap = total
+                self._rb_cap = total
+                continue
+            check(rc)
+            break
+        res, off = {}, 0
+        for i, s in enumerate(sl.tolist()):
+            c = int(counts[i])
+            res[s] = (out[off:off + c].copy(), int(npass[i]))
+            off += c
+        return res
 
     def last_pass_ms(self):
         a, b = C.c_float(0), C.c_float(0)

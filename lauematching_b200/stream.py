@@ -259,10 +259,10 @@ class StreamServer:
             for g in self.geoms.values():
                 if not g.inflight:
                     continue
-                t = None
+                res = g.engine.results_batch([s for s, _ in g.inflight])
+                t = time.perf_counter()
                 for s, r in g.inflight:
-                    surv, npass = g.engine.results(s)
-                    t = t or time.perf_counter()
+                    surv, npass = res[s]
                     self.done_q.put(Done(r, surv, npass, t))
                     g.free.append(s)
                 g.inflight = []

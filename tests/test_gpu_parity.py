@@ -107,6 +107,21 @@ def test_batched_pass_equals_single_passes_and_oracle():
         assert_same_survivors(batched[k][0], ref)
 
 
+def test_results_batch_equals_per_slot_results():
+    c = golden_case("tilted_dense")
+    p = c.params
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        for k, s in enumerate((0.5, 1.0, 2.0)):
+            e.load_image(k * 7, c.image * s)
+        e.match([0, 7, 14], p.min_nr_spots, p.min_intensity)
+        per = {k: e.results(k) for k in (14, 0, 7)}
+        e.match([0, 7, 14], p.min_nr_spots, p.min_intensity)
+        bat = e.results_batch([14, 0, 7])
+    for k in (0, 7, 14):
+        assert bat[k][1] == per[k][1] and np.array_equal(bat[k][0], per[k][0])
+
+
 def test_input_dtypes_f32_u8_match_f64():
     c = golden_case("tilted_fcc")
     p = c.params
@@ -156,6 +171,46 @@ def test_survivor_overflow_is_reported():
         e.match([0], p.min_nr_spots, p.min_intensity)
         with pytest.raises(OverflowError_):
             e.results(0)
+
+
+def test_sparse_and_dense_uploads_agree_and_slots_reuse_cleanly():
+    """Frames sent as (index, value) pairs give the same survivors as dense
+    frames, for every dtype, and a slot reloaded many times (sparse after
+    dense after sparse) holds only its latest frame."""
+    c = golden_case("tilted_fcc")
+    p = c.params
+    rng = np.random.default_rng(4)
+    frames = [c.image, c.image * 0.37, c.image.astype(np.float32), c.img_u8]
+    other = synth.render_image(c.records[rng.choice(np.nonzero(c.records[:, 0] >= 8)[0], 3)],
+                               p.nr_px_x, p.nr_px_y, rng)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        e.set_sparse_uploads(False)
+        refs = []
+        for f in frames:
+            e.load_image(0, f)
+            e.match([0], p.min_nr_spots, p.min_intensity)
+            refs.append(e.results(0))
+        e.set_sparse_uploads(True)
+        for k, f in enumerate(frames):
+            e.load_image(3, other)  # previous content of the slot
+            e.load_image(3, f)
+            e.match([3], p.min_nr_spots, p.min_intensity)
+            got = e.results(3)
+            assert got[1] == refs[k][1] and np.array_equal(got[0], refs[k][0])
+        # dense frame into a slot last used by a sparse one, and back
+        dense = c.image + 3.0  # every pixel positive: sent dense
+        e.load_image(3, dense)
+        e.set_sparse_uploads(False)
+        e.load_image(4, dense)
+        e.set_sparse_uploads(True)
+        e.match([3, 4], p.min_nr_spots, p.min_intensity)
+        a, b = e.results(3), e.results(4)
+        assert a[1] == b[1] and np.array_equal(a[0], b[0])
+        e.load_image(3, c.image)
+        e.match([3], p.min_nr_spots, p.min_intensity)
+        got = e.results(3)
+        assert got[1] == refs[0][1] and np.array_equal(got[0], refs[0][0])
 
 
 def test_repeated_pass_replays_graph_with_same_results():
