@@ -19,6 +19,9 @@ amplitude U(50,255), Poisson(5) background removed by a fixed threshold.
 
 `--impl reference` times the reference's own LaueMatchingCPU (compiled from
 its sources into oracle/_ref/) on a bounded sample of the same workload.
+`--impl reference-gpu` times the reference's plain single-image GPU executable
+(LaueMatchingGPU.cu compiled for sm_100a into oracle/_ref/) on one 8-grain
+frame against the full DB: one process and one DB stream per image.
 """
 from __future__ import annotations
 
@@ -345,11 +348,16 @@ def run_ours(args, rank, world):
     pipelined(2 * args.warmup)
     torch.cuda.synchronize()
     lat = []
+    moved0 = e.bytes_moved()
     te = time.perf_counter()
     nb = pipelined(2 * args.steps, lat)
     e2e_s = time.perf_counter() - te
+    moved1 = e.bytes_moved()
     e2e_ips = world * len(halves[0]) * 2 * args.steps / e2e_s
-    d2h[0] = nb // args.steps + 2 * (2 * 64 + 1) * 4
+    # bytes that crossed the host link per step of 64 frames, as counted by
+    # the engine (sparse frames travel as (index, value) pairs)
+    h2d_step = (moved1[0] - moved0[0]) // args.steps
+    d2h[0] = (moved1[1] - moved0[1]) // args.steps
     # plain e2e: one frame per step
     platency = []
     for i in range(args.warmup + args.steps):
@@ -395,7 +403,8 @@ def run_ours(args, rank, world):
                    "parallelism": f"replicas x{world} (images split, DB replicated)"},
         "roofline": roof,
         "e2e": {"value": round(e2e_ips, 2), "unit": UNIT,
-                "h2d_bytes_per_step": K * p.nr_px_x * p.nr_px_y,
+                "h2d_bytes_per_step": h2d_step,
+                "h2d_dense_frame_bytes_per_step": K * p.nr_px_x * p.nr_px_y,
                 "d2h_bytes_per_step": d2h[0],
                 "path": "public Engine API from pinned uint8 frames: per step 64 frames in two "
                         "passes of 32, the upload of one half overlapping the pass of the other "
@@ -516,6 +525,112 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def _ref_gpu_sample_size(n_want):
+    """Largest DB (<= n_want) whose files fit the host: the forward cache
+    (122 B) and orientations (72 B) per orientation, held twice (page cache and
+    the reference's own read buffer), within half the available RAM and the
+    temporary directory's free space."""
+    import psutil
+    per = 2 * (REC_BYTES_PER_ORIENT + 72)
+    ram = psutil.virtual_memory().available // 2
+    st = os.statvfs(tempfile.gettempdir())
+    disk = int(st.f_bavail * st.f_frsize * 0.8) // (REC_BYTES_PER_ORIENT + 72)
+    return max(0, min(n_want, ram // per, disk))
+
+
+def run_reference_gpu(args, rank, world):
+    """The reference's plain single-image GPU path (LaueMatchingGPU.cu built
+    for sm_100a): one process per image, each streaming the forward cache to
+    the device in <= 4 GB chunks (LaueMatchingGPU.cu:660-749) and running its
+    one-thread-per-orientation kernel (:45-81) on each chunk.  The device DB
+    build writes the input cache (byte-identical to the reference's own
+    DoFwd 1 cache); nothing of ours runs inside the reference process."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lauematching_b200 import formats, synth
+    from lauematching_b200.engine import Engine
+    if not O.have_ref_gpu():
+        print(json.dumps({"impl": "reference-gpu", "unavailable":
+                          "oracle/_ref/LaueMatchingGPU was not built (reference sources or nvcc "
+                          "absent when the repository was built)"}))
+        return
+    txt, p = workload_params(args.min_intensity)
+    hkls = synth.hkls_cubic(8)
+    n = _ref_gpu_sample_size(args.n_orient)
+    if n < 1_000_000:
+        print(json.dumps({"impl": "reference-gpu", "unavailable":
+                          f"host RAM/disk too small for the reference's input files ({n})"}))
+        return
+    e = Engine(p)
+    e.build_db_synthetic(seed=args.seed, n=n, hkls=hkls)
+    wd = tempfile.mkdtemp(prefix="lmb_refgpu_")
+    fwd, op = os.path.join(wd, "fwd.bin"), os.path.join(wd, "orients.bin")
+    step = 4_000_000
+    with open(fwd, "wb") as ff, open(op, "wb") as fo:
+        for s in range(0, n, step):
+            c = min(step, n - s)
+            e.download_db(s, c).tofile(ff)
+            e.synth_orientations(args.seed, s, c).tofile(fo)
+    hp, ip, pp = (os.path.join(wd, x) for x in ("hkls.csv", "image.bin", "params.txt"))
+    formats.write_hkls(hp, hkls)
+    rng = np.random.default_rng(2000)
+    rec = e.download_db(0, min(2_000_000, n))
+    img = synth.render_image(rec[synth.pick_grains(rec, 8, p.min_nr_spots, rng)],
+                             p.nr_px_x, p.nr_px_y, rng)
+    formats.write_image_bin(ip, img)
+    with open(pp, "w") as f:
+        f.write(txt + f"ForwardFile {fwd}\nDoFwd 0\n")
+    e.load_image(0, img)
+    e.match([0], p.min_nr_spots, p.min_intensity)
+    n_pass_ours = e.results(0)[1]
+    e.close()
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+    warm, runs = min(args.warmup, 1), max(1, min(args.steps, 3))
+    kern, match, walls, reads, chunks, nm = [], [], [], [], None, None
+    for i in range(warm + runs):
+        r = O.run_reference_gpu(pp, op, hp, ip, ncpus=cores, env=env)
+        if r.returncode != 0 or not r.chunks:
+            print(json.dumps({"impl": "reference-gpu", "unavailable": "reference GPU run failed: "
+                              + (r.stderr or r.stdout)[-200:].replace("\n", " ")}))
+            return
+        if i >= warm:
+            kern.append(sum(k for _, k in r.chunks))
+            match.append(r.match_seconds)
+            walls.append(r.wall_seconds)
+            reads.append(r.read_seconds)
+            chunks, nm = r.chunks, r.n_matches
+    for fn in os.listdir(wd):
+        os.remove(os.path.join(wd, fn))
+    os.rmdir(wd)
+    scale = 1e8 / n
+    k_img = statistics.median(kern) * scale
+    m_img = statistics.median(match) * scale
+    out = {"impl": "reference-gpu", "metric": METRIC, "value": round(1.0 / k_img, 3),
+           "unit": UNIT, "n_gpus": 1, "steps": runs, "warmup": warm,
+           "ms_per_step": round(k_img * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "plain single-image compare (reference LaueMatchingGPU, sm_100a "
+                                  "build) vs a 100,000,000-orientation DB"
+                                  + ("" if n == 100_000_000 else f" (sampled: {n})"),
+                      "n_orient": n, "max_nr_spots": 30, "hkls": int(len(hkls)), "grains": 8},
+           "e2e": {"value": round(1.0 / m_img, 4), "unit": UNIT,
+                   "h2d_bytes_per_step": int(n * REC_BYTES_PER_ORIENT + p.nr_px_x * p.nr_px_y * 4),
+                   "d2h_bytes_per_step": int((nm or 0) * 12 + 4)},
+           "reference_gpu": {
+               "build": "nvcc -O3 -w -rdc=true -gencode arch=compute_100a,code=sm_100a "
+                        "-Xcompiler=-fopenmp (reference CMake flags, sm_100a target)",
+               "kernel_s_per_image": round(k_img, 5),
+               "match_stage_s_per_image": round(m_img, 4),
+               "chunks_h2d_kernel_s": chunks, "forward_read_s": statistics.median(reads),
+               "process_wall_s": round(statistics.median(walls), 2),
+               "module_loading": "EAGER", "cores": cores,
+               "nr_matches": nm, "n_pass_ours": n_pass_ours}}
+    print(json.dumps(out), flush=True)
+
+
 # ---------------------------------------------------------------------------
 # serving: Poisson arrivals of mixed 1024^2 / 2048^2 frames through the daemon
 # ---------------------------------------------------------------------------
@@ -600,7 +715,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours",
+                    help="reference: the reference's CPU path; reference-gpu: its plain "
+                         "single-image GPU executable built for sm_100a")
     ap.add_argument("--n-orient", type=int, default=100_000_000)
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--seed", type=int, default=1)
@@ -621,6 +738,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.impl == "reference-gpu":
+        run_reference_gpu(args, rank, world)
     elif args.serve:
         run_serve(args)
     else:

@@ -189,6 +189,13 @@ int lmb_results_batch(lmb_engine *e, const int32_t *slots, int32_t nslots, lmb_s
  * stream): compare kernel, ordering kernel. */
 int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms);
 
+/* Bytes the engine has moved host->device and device->host since it was
+ * created (DB and orientation uploads, frames as sent -- sparse or dense --,
+ * status words, survivors, downloads).  The reference prints its transfer
+ * sizes and times per chunk (LaueMatchingGPU.cu:683-717,747); these counters
+ * are the engine's equivalent for a caller's end-to-end accounting. */
+int lmb_engine_bytes(lmb_engine *e, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
+
 /* ---- host post-stage ------------------------------------------------------
  * Duplicate merge (mergeDuplicateOrientations, LaueMatchingHeaders.h:969-1065)
  * and refinement + output text (fitAndWriteOrientations, :1072-1153) for the

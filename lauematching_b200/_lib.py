@@ -30,7 +30,8 @@ EXPORTS = [
     "lmb_engine_destroy", "lmb_engine_stream", "lmb_engine_set_tuning",
     "lmb_engine_get_tuning", "lmb_engine_set_sparse_uploads", "lmb_db_upload", "lmb_db_build",
     "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
-    "lmb_match", "lmb_results", "lmb_results_batch", "lmb_last_pass_ms", "lmb_post_process", "lmb_post_free",
+    "lmb_match", "lmb_results", "lmb_results_batch", "lmb_last_pass_ms", "lmb_engine_bytes",
+    "lmb_post_process", "lmb_post_free",
     "lmb_order_survivors_noalloc",
     "lmb_host_alloc", "lmb_host_free",
 ]
@@ -114,6 +115,7 @@ def lib():
         "lmb_results": ([vp, i32, vp, u64, C.POINTER(u64), C.POINTER(u64)], C.c_int),
         "lmb_results_batch": ([vp, vp, i32, vp, u64, vp, vp], C.c_int),
         "lmb_last_pass_ms": ([vp, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+        "lmb_engine_bytes": ([vp, C.POINTER(u64), C.POINTER(u64)], C.c_int),
         "lmb_post_process": ([C.POINTER(LmbGeometry), C.POINTER(LmbPostParams), vp, u64, vp, vp,
                               C.c_int64, vp, vp, i32, C.POINTER(LmbPostOutput)], C.c_int),
         "lmb_post_free": ([C.POINTER(LmbPostOutput)], None),

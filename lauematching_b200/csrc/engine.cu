@@ -98,6 +98,7 @@ struct lmb_engine {
   uint64_t sparse_loads = 0;
   void *h_stage[2] = {nullptr, nullptr};   // pinned upload staging (lazy)
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
+  uint64_t bytes_h2d = 0, bytes_d2h = 0;   // host<->device bytes moved so far
 };
 
 namespace {
@@ -159,6 +160,7 @@ size_t dtype_bytes(int dtype) {
 // chunk b^1.
 int upload_chunked(lmb_engine *e, void *dst, const void *src, size_t bytes, cudaStream_t st) {
   const size_t kChunk = 64ull << 20;
+  e->bytes_h2d += bytes;
   if (bytes <= (4ull << 20)) {
     LMB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
     LMB_CUDA(cudaStreamSynchronize(st));
@@ -310,6 +312,7 @@ int try_sparse(lmb_engine *e, const T *px, int slot, int dtype, bool *sparse) {
   const size_t bytes = voff + nnz * vb;
   LMB_CUDA(cudaMemcpyAsync(e->d_stage, e->sp_host[r], bytes, cudaMemcpyHostToDevice, e->ld));
   LMB_CUDA(cudaEventRecord(e->sp_ev[r], e->ld));
+  e->bytes_h2d += bytes;
   const int rc = sparse_load_launch(
       static_cast<const uint32_t *>(e->d_stage), static_cast<const char *>(e->d_stage) + voff,
       dtype, nnz, mx, e->d_u8 + (size_t)slot * npx, e->d_occ, slot, e->d_scale + slot, npx,
@@ -511,6 +514,7 @@ static int db_build_common(lmb_engine *e, const double *orients, uint64_t seed, 
                           (flags & LMB_BUILD_EXACT_FP64) != 0);
     if (rc == LMB_OK && synthetic && orients_out) {
       ce = cudaMemcpyAsync(orients_out + off * 9, d_om, len * 72, cudaMemcpyDeviceToHost, e->st);
+      e->bytes_d2h += len * 72;
       if (ce != cudaSuccess) rc = cuda_fail(ce, "orientation download", __FILE__, __LINE__);
     }
     ce = cudaStreamSynchronize(e->st);
@@ -548,6 +552,7 @@ int lmb_synth_orientations(lmb_engine *e, uint64_t seed, uint64_t first, uint64_
   cudaError_t ce = cudaSuccess;
   if (rc == LMB_OK) ce = cudaMemcpyAsync(out, d, n * 72, cudaMemcpyDeviceToHost, e->st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
+  e->bytes_d2h += n * 72;
   cudaFree(d);
   if (ce != cudaSuccess) return cuda_fail(ce, "synthetic orientations", __FILE__, __LINE__);
   return rc;
@@ -561,6 +566,7 @@ int lmb_db_download(lmb_engine *e, uint64_t first, uint64_t count, uint16_t *out
   LMB_CUDA(cudaStreamSynchronize(e->st));
   LMB_CUDA(cudaMemcpy(out, e->d_db + first * e->R, (size_t)count * e->R * 2,
                       cudaMemcpyDeviceToHost));
+  e->bytes_d2h += (size_t)count * e->R * 2;
   return LMB_OK;
 }
 
@@ -594,6 +600,7 @@ int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtyp
   if (!sparse) {
     LMB_CUDA(cudaMemcpyAsync(e->d_stage, pixels, e->npx * dtype_bytes(dtype),
                              cudaMemcpyHostToDevice, e->ld));
+    e->bytes_h2d += e->npx * dtype_bytes(dtype);
     rc = quantize_launch(e->d_stage, dtype, e->npx, e->d_max_bits,
                          e->d_u8 + (size_t)slot * e->npx,
                          keep_f64 ? e->d_f64 + (size_t)slot * e->npx : nullptr, e->d_occ, slot,
@@ -609,6 +616,7 @@ int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtyp
   if (im_scale) {
     LMB_CUDA(cudaMemcpyAsync(im_scale, e->d_scale + slot, sizeof(double), cudaMemcpyDeviceToHost,
                              e->ld));
+    e->bytes_d2h += sizeof(double);
     LMB_CUDA(cudaStreamSynchronize(e->ld));
   }
   return LMB_OK;
@@ -666,6 +674,7 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   }
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
     if (slot_mask >> k & 1) LMB_CUDA(cudaEventRecord(e->ev_released[k], e->st));
+  e->bytes_d2h += kStatusWords * sizeof(unsigned int);
   e->last_mask = slot_mask;
   e->pending = true;
   return LMB_OK;
@@ -701,6 +710,7 @@ int lmb_results(lmb_engine *e, int32_t slot, lmb_survivor *out, uint64_t out_cap
   if (cnt)
     LMB_CUDA(cudaMemcpy(out, e->d_sorted + (size_t)slot * e->cap, cnt * sizeof(lmb_survivor),
                         cudaMemcpyDeviceToHost));
+  e->bytes_d2h += cnt * sizeof(lmb_survivor);
   return LMB_OK;
 }
 
@@ -744,6 +754,14 @@ int lmb_results_batch(lmb_engine *e, const int32_t *slots, int32_t nslots, lmb_s
     off += counts[i];
   }
   LMB_CUDA(cudaStreamSynchronize(e->st));
+  e->bytes_d2h += total * sizeof(lmb_survivor);
+  return LMB_OK;
+}
+
+int lmb_engine_bytes(lmb_engine *e, uint64_t *h2d, uint64_t *d2h) {
+  LMB_REQUIRE(e, "null engine");
+  if (h2d) *h2d = e->bytes_h2d;
+  if (d2h) *d2h = e->bytes_d2h;
   return LMB_OK;
 }
 

@@ -235,3 +235,9 @@ class Engine:
         a, b = C.c_float(0), C.c_float(0)
         check(lib().lmb_last_pass_ms(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def bytes_moved(self):
+        """(host->device, device->host) bytes since the engine was created."""
+        a, b = C.c_uint64(0), C.c_uint64(0)
+        check(lib().lmb_engine_bytes(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)

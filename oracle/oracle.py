@@ -4,10 +4,14 @@
   (lm_oracle.c), loaded with ctypes;
 * ``_ref/LaueMatchingCPU`` -- the reference's own CPU executable compiled from
   its sources by oracle/Makefile (NLopt replaced by an evaluate-once
-  stand-in), driven through its 5-argument command line.
+  stand-in), driven through its 5-argument command line;
+* ``_ref/LaueMatchingGPU`` -- the reference's single-image GPU executable
+  compiled from its sources for sm_100a, the plain one-pass-per-image GPU
+  baseline (same command line).
 
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
-module; the product never imports it.
+Only tests/, __graft_entry__.smoke() and bench.py's baseline legs (the CPU
+baseline and the reference arms) use this module; the product never imports
+it.
 """
 from __future__ import annotations
 
@@ -24,6 +28,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblmoracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "LaueMatchingCPU")
+REF_GPU_BIN = os.path.join(HERE, "_ref", "LaueMatchingGPU")
 
 _lib = None
 
@@ -155,6 +160,47 @@ def run_reference(params_path, orient_path, hkl_path, image_path, ncpus=1,
     return RefRun(pr.returncode, pr.stdout, pr.stderr, sol, spt,
                   int(m.group(1)) if m else None, int(m.group(2)) if m else None,
                   float(mc.group(1)) if mc else None, wall)
+
+
+@dataclass
+class RefGpuRun:
+    returncode: int
+    stdout: str
+    stderr: str
+    n_matches: int | None
+    chunks: list            # [(h2d_seconds, kernel_seconds)] per DB chunk
+    read_seconds: float | None
+    match_seconds: float | None
+    compare_seconds: float | None
+    wall_seconds: float
+
+
+def have_ref_gpu() -> bool:
+    return os.path.exists(REF_GPU_BIN)
+
+
+def run_reference_gpu(params_path, orient_path, hkl_path, image_path, ncpus=1,
+                      timeout=900, env=None) -> RefGpuRun:
+    """Run the reference LaueMatchingGPU on files and parse its timing report:
+    per-chunk H2D and kernel seconds (LaueMatchingGPU.cu:747), the match
+    stage (:777), the forward-file read (:658) and NrMatches (:791)."""
+    t0 = time.perf_counter()
+    pr = subprocess.run([REF_GPU_BIN, params_path, orient_path, hkl_path, image_path,
+                         str(ncpus)], capture_output=True, text=True, timeout=timeout,
+                        env=env)
+    wall = time.perf_counter() - t0
+    num = r"([0-9.eE+-]+)"
+    chunks = [(float(a), float(b)) for a, b in
+              re.findall(r"chunk \d+/\d+: H2D=" + num + r"s\s+kernel=" + num + "s", pr.stdout)]
+
+    def grab(pat, cast=float):
+        m = re.search(pat, pr.stdout)
+        return cast(m.group(1)) if m else None
+    return RefGpuRun(pr.returncode, pr.stdout, pr.stderr, grab(r"NrMatches: (\d+)", int), chunks,
+                     grab(r"Time elapsed to read the forward simulation: " + num),
+                     grab(r"Time elapsed to match on the GPU: " + num),
+                     grab(r"Finished comparing, time elapsed after comparing with forward "
+                          r"simulation: " + num), wall)
 
 
 def reference_case(workdir, params_text, orients, hkls, image, ncpus=1):

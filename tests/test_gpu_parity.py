@@ -213,6 +213,33 @@ def test_sparse_and_dense_uploads_agree_and_slots_reuse_cleanly():
         assert got[1] == refs[0][1] and np.array_equal(got[0], refs[0][0])
 
 
+def test_byte_counters_follow_the_copies():
+    """lmb_engine_bytes: a dense frame adds its size, a sparse one its
+    (index, value) pairs, a pass its status words, results their survivors."""
+    c = golden_case("tilted_fcc")
+    p = c.params
+    npx = p.nr_px_x * p.nr_px_y
+    nnz = int(np.count_nonzero(c.img_u8))
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        h0, d0 = e.bytes_moved()
+        assert h0 == c.records.nbytes
+        e.set_sparse_uploads(False)
+        e.load_image(0, c.img_u8, want_scale=False)
+        h1, _ = e.bytes_moved()
+        assert h1 - h0 == npx
+        e.set_sparse_uploads(True)
+        e.load_image(1, c.img_u8, want_scale=False)
+        h2, _ = e.bytes_moved()
+        assert 0 < h2 - h1 < npx and h2 - h1 >= 5 * nnz
+        e.match([0, 1], p.min_nr_spots, p.min_intensity)
+        _, d1 = e.bytes_moved()
+        assert d1 - d0 == (2 * 64 + 1) * 4
+        got = e.results_batch([0, 1])
+        _, d2 = e.bytes_moved()
+        assert d2 - d1 == sum(r.nbytes for r, _ in got.values())
+
+
 def test_repeated_pass_replays_graph_with_same_results():
     """The first pass of a configuration runs eagerly, the second is captured
     into a CUDA graph, later ones replay it: results and timings stay valid."""
