@@ -161,15 +161,28 @@ int lmb_db_info(lmb_engine *e, uint64_t *n_orient, int32_t *max_nr_spots);
 int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels,
                    int32_t dtype, int32_t keep_f64, double *im_scale);
 
+/* Load n frames (n <= 64, distinct slots, one dtype) in one call; each slot
+ * ends exactly as after lmb_image_load(e, slots[i], frames[i], dtype, 0, ...)
+ * and im_scales[i] (optional) receives its imScale.  With sparse uploads on,
+ * every frame is read once by a parallel host scan and the pairs of all
+ * sparse frames cross the link in one copy, followed by two kernels for the
+ * whole batch.  Replaces the per-image H2D of the reference's stream loop
+ * (LaueMatchingGPUStream.cu:1201-1205) for a batch of admitted images. */
+int lmb_image_load_batch(lmb_engine *e, const int32_t *slots, const void *const *frames,
+                         int32_t n, int32_t dtype, double *im_scales);
+
 /* One DB pass over every slot in slot_mask: the compare of
  * LaueMatchingCPU.c:668-690 (replacing the compare kernels
  * LaueMatchingGPU.cu:45-81 and LaueMatchingGPUStream.cu:69-100), survivor
  * compaction and ordering by ID (LaueMatchingCPU.c:781-788).  Asynchronous:
- * results are read with lmb_results. */
+ * results are read with lmb_results.  Passes queue on the engine stream: a
+ * pass over other slots may be started before the previous pass's results
+ * have been read (they stay valid until a later pass includes the slot). */
 int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots,
               double min_intensity, int32_t value_mode);
 
-/* Wait for the last pass and copy one slot's survivors (ascending id).
+/* Wait for the last pass that included the slot and copy its survivors
+ * (ascending id).
  * n_survivors receives the full count; n_pass the reference's nrResults
  * (LaueMatchingCPU.c:686).  Returns LMB_ERR_OVERFLOW when the count exceeded
  * the engine's survivor capacity (the first capacity survivors by ID are

@@ -30,6 +30,7 @@ EXPORTS = [
     "lmb_engine_destroy", "lmb_engine_stream", "lmb_engine_set_tuning",
     "lmb_engine_get_tuning", "lmb_engine_set_sparse_uploads", "lmb_db_upload", "lmb_db_build",
     "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
+    "lmb_image_load_batch",
     "lmb_match", "lmb_results", "lmb_results_batch", "lmb_last_pass_ms", "lmb_engine_bytes",
     "lmb_post_process", "lmb_post_free",
     "lmb_order_survivors_noalloc",
@@ -111,6 +112,7 @@ def lib():
         "lmb_db_download": ([vp, u64, u64, vp], C.c_int),
         "lmb_db_info": ([vp, C.POINTER(u64), C.POINTER(i32)], C.c_int),
         "lmb_image_load": ([vp, i32, vp, i32, i32, dp], C.c_int),
+        "lmb_image_load_batch": ([vp, vp, vp, i32, i32, dp], C.c_int),
         "lmb_match": ([vp, u64, i32, dbl, i32], C.c_int),
         "lmb_results": ([vp, i32, vp, u64, C.POINTER(u64), C.POINTER(u64)], C.c_int),
         "lmb_results_batch": ([vp, vp, i32, vp, u64, vp, vp], C.c_int),

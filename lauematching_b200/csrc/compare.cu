@@ -166,6 +166,83 @@ int sparse_load_launch(const uint32_t *d_idx, const void *d_val, int dtype, size
   return LMB_OK;
 }
 
+// Batched sparse upload: blockIdx.y selects the frame.  The arithmetic per
+// pixel is that of sparse_scatter_kernel / quant_u8_kernel; the occupancy
+// updates are atomic because several slots' bits live in one word.
+__global__ void batch_clear_kernel(const SparseFrameDesc *__restrict__ desc,
+                                   uint8_t *__restrict__ u8_base,
+                                   unsigned long long *__restrict__ occ, size_t npx) {
+  const int slot = desc[blockIdx.y].slot;
+  uint8_t *u8 = u8_base + (size_t)slot * npx;
+  const unsigned long long keep = ~(1ull << slot);
+  const size_t n16 = (reinterpret_cast<uintptr_t>(u8) & 15) ? 0 : npx / 16;
+  uint4 *u = reinterpret_cast<uint4 *>(u8);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint4 v = u[i];
+    if ((v.x | v.y | v.z | v.w) == 0u) continue;
+    const uint8_t *b = reinterpret_cast<const uint8_t *>(&v);
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+      if (b[j]) atomicAnd(&occ[i * 16 + j], keep);
+    u[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  for (size_t i = n16 * 16 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npx;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (u8[i]) {
+      atomicAnd(&occ[i], keep);
+      u8[i] = 0;
+    }
+  }
+}
+
+template <typename T>
+__global__ void batch_scatter_kernel(const SparseFrameDesc *__restrict__ desc,
+                                     const uint32_t *__restrict__ idx, const T *__restrict__ val,
+                                     uint8_t *__restrict__ u8_base,
+                                     unsigned long long *__restrict__ occ,
+                                     double *__restrict__ scale, size_t npx) {
+  const SparseFrameDesc d = desc[blockIdx.y];
+  const double inv = (d.mx > 0) ? ddiv(255.0, d.mx) : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) scale[d.slot] = (d.mx > 0) ? ddiv(d.mx, 255.0) : 1.0;
+  uint8_t *u8 = u8_base + (size_t)d.slot * npx;
+  const unsigned long long bit = 1ull << d.slot;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < d.nnz;
+       j += (size_t)gridDim.x * blockDim.x) {
+    const double x = (double)val[d.off + j];  // > 0 by construction
+    const double v = dmul(x, inv);
+    const uint8_t q = (v >= 255.0) ? 255 : (v < 1.0) ? 1 : (uint8_t)(x86_trunc_i32(v) & 0xFF);
+    const uint32_t p = idx[d.off + j];
+    u8[p] = q;
+    atomicOr(&occ[p], bit);
+  }
+}
+
+int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_t max_nnz,
+                             const uint32_t *d_idx, const void *d_val, int dtype, uint8_t *d_u8,
+                             unsigned long long *d_occ, double *d_scale, size_t npx, int num_sms,
+                             cudaStream_t st) {
+  if (nframes <= 0) return LMB_OK;
+  LMB_REQUIRE(nframes <= LMB_MAX_SLOTS, "batch of %d frames", nframes);
+  const size_t budget = std::max<size_t>(1, (size_t)num_sms * 8 / nframes);
+  const unsigned cb = (unsigned)std::min<size_t>((npx / 16 + 255) / 256 + 1, budget);
+  batch_clear_kernel<<<dim3(cb, nframes), 256, 0, st>>>(d_desc, d_u8, d_occ, npx);
+  const unsigned sb =
+      (unsigned)std::max<size_t>(1, std::min<size_t>(((size_t)max_nnz + 255) / 256, budget));
+  const dim3 g(sb, nframes);
+  if (dtype == LMB_F64)
+    batch_scatter_kernel<double><<<g, 256, 0, st>>>(
+        d_desc, d_idx, static_cast<const double *>(d_val), d_u8, d_occ, d_scale, npx);
+  else if (dtype == LMB_F32)
+    batch_scatter_kernel<float><<<g, 256, 0, st>>>(
+        d_desc, d_idx, static_cast<const float *>(d_val), d_u8, d_occ, d_scale, npx);
+  else
+    batch_scatter_kernel<uint8_t><<<g, 256, 0, st>>>(
+        d_desc, d_idx, static_cast<const uint8_t *>(d_val), d_u8, d_occ, d_scale, npx);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
 // ----------------------------------------------------------------------------
 // The DB pass.
 // ----------------------------------------------------------------------------
@@ -591,6 +668,23 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   if (B <= 9) return launch_b<9>(a, c, grid, smem, st);
   if (B <= 11) return launch_b<11>(a, c, grid, smem, st);
   return launch_b<16>(a, c, grid, smem, st);
+}
+
+// Zero the survivor and pass counters of the pass's slots only: the counters
+// of other slots keep the results of their own last pass, so a pass can be
+// queued before the previous one has been collected.
+__global__ void status_reset_kernel(unsigned int *__restrict__ status, unsigned long long mask) {
+  const int k = threadIdx.x;
+  if (k < LMB_MAX_SLOTS && ((mask >> k) & 1ull)) {
+    status[k] = 0u;
+    status[LMB_MAX_SLOTS + k] = 0u;
+  }
+}
+
+int status_reset_launch(unsigned int *d_status, uint64_t mask, cudaStream_t st) {
+  status_reset_kernel<<<1, LMB_MAX_SLOTS, 0, st>>>(d_status, (unsigned long long)mask);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
 }
 
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st) {

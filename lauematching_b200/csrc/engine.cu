@@ -31,8 +31,12 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
 using namespace lmb;
 
 // Status words copied back after every pass: [0,64) survivor counts,
-// [64,128) pass counts, [128] device error word.
+// [64,128) pass counts, [128] device error word (sticky).  A pass resets only
+// its own slots' counters and copies all words into the next entry of a
+// small pinned ring, so several passes can be in flight and each slot's
+// results are read from the entry of the last pass that included it.
 static constexpr int kStatusWords = 2 * LMB_MAX_SLOTS + 1;
+static constexpr int kStatusRing = 4;
 
 static constexpr int kSparseRing = 4;  // pinned staging buffers for sparse frames
 
@@ -78,9 +82,12 @@ struct lmb_engine {
   lmb_survivor *d_surv = nullptr, *d_sorted = nullptr;
   unsigned long long *d_scratch = nullptr;
   unsigned int *d_status = nullptr;
-  unsigned int *h_status = nullptr;  // pinned
-  uint64_t last_mask = 0;
-  bool pending = false;
+  unsigned int *h_status = nullptr;  // pinned, kStatusRing x kStatusWords
+  cudaEvent_t ev_done[kStatusRing] = {};  // a pass and its status copy finished
+  uint64_t pass_seq = 0;                  // passes enqueued so far
+  int slot_ring[LMB_MAX_SLOTS] = {};      // status entry of each slot's last pass
+  uint64_t done_mask = 0;                 // slots that have been in a pass
+  cudaStream_t dl = nullptr;              // survivor downloads
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   // image uploads run on their own stream so they overlap a running pass:
   // a pass waits for its slots' uploads, an upload waits until the last pass
@@ -99,6 +106,16 @@ struct lmb_engine {
   void *h_stage[2] = {nullptr, nullptr};   // pinned upload staging (lazy)
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
   uint64_t bytes_h2d = 0, bytes_d2h = 0;   // host<->device bytes moved so far
+  // batched sparse uploads: per-task scan output (pageable), a two-deep ring
+  // of pinned packed staging buffers, the device copy of the packed batch
+  std::vector<uint32_t> bt_idx;
+  std::vector<unsigned char> bt_val;
+  void *bt_host[2] = {nullptr, nullptr};
+  size_t bt_host_cap[2] = {0, 0};
+  cudaEvent_t bt_ev[2] = {nullptr, nullptr};
+  int bt_next = 0;
+  void *d_batch = nullptr;
+  size_t d_batch_cap = 0;
 };
 
 namespace {
@@ -129,6 +146,12 @@ void free_engine(lmb_engine *e) {
   cudaFree(e->d_scratch);
   cudaFree(e->d_status);
   cudaFreeHost(e->h_status);
+  for (auto &v : e->ev_done)
+    if (v) cudaEventDestroy(v);
+  if (e->dl) {
+    cudaStreamSynchronize(e->dl);
+    cudaStreamDestroy(e->dl);
+  }
   for (auto &g : e->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (int i = 0; i < kSparseRing; i++) {
@@ -138,7 +161,10 @@ void free_engine(lmb_engine *e) {
   for (int i = 0; i < 2; i++) {
     if (e->h_stage[i]) cudaFreeHost(e->h_stage[i]);
     if (e->ev_stage[i]) cudaEventDestroy(e->ev_stage[i]);
+    if (e->bt_host[i]) cudaFreeHost(e->bt_host[i]);
+    if (e->bt_ev[i]) cudaEventDestroy(e->bt_ev[i]);
   }
+  cudaFree(e->d_batch);
   for (auto &v : e->ev)
     if (v) cudaEventDestroy(v);
   for (int k = 0; k < LMB_MAX_SLOTS; k++) {
@@ -328,7 +354,10 @@ int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   // timing events recorded inside a captured graph must be external to be
   // observable (and timed) after each replay
   const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
-  LMB_CUDA(cudaMemsetAsync(e->d_status, 0, kStatusWords * sizeof(unsigned int), e->st));
+  {
+    const int rc = status_reset_launch(e->d_status, k.mask, e->st);
+    if (rc) return rc;
+  }
   LMB_CUDA(cudaEventRecordWithFlags(e->ev[0], e->st, evf));
   CmpArgs a{};
   a.db = e->d_db;
@@ -370,8 +399,6 @@ int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   const int rc = order_launch(o, ns, e->st);
   if (rc) return rc;
   LMB_CUDA(cudaEventRecordWithFlags(e->ev[2], e->st, evf));
-  LMB_CUDA(cudaMemcpyAsync(e->h_status, e->d_status, kStatusWords * sizeof(unsigned int),
-                           cudaMemcpyDeviceToHost, e->st));
   return LMB_OK;
 }
 
@@ -438,6 +465,8 @@ int lmb_engine_create(int32_t device, const lmb_geometry *geo, uint64_t survivor
   } while (0)
   TRY(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
   TRY(cudaStreamCreateWithFlags(&e->ld, cudaStreamNonBlocking));
+  TRY(cudaStreamCreateWithFlags(&e->dl, cudaStreamNonBlocking));
+  for (auto &v : e->ev_done) TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
   for (auto &v : e->ev) TRY(cudaEventCreate(&v));
   for (int k = 0; k < LMB_MAX_SLOTS; k++) {
     TRY(cudaEventCreateWithFlags(&e->ev_loaded[k], cudaEventDisableTiming));
@@ -456,8 +485,9 @@ int lmb_engine_create(int32_t device, const lmb_geometry *geo, uint64_t survivor
   TRY(cudaMalloc(&e->d_scratch, (size_t)LMB_MAX_SLOTS * e->cap2 * sizeof(unsigned long long)));
   TRY(cudaMalloc(&e->d_status, kStatusWords * sizeof(unsigned int)));
   TRY(cudaMemset(e->d_status, 0, kStatusWords * sizeof(unsigned int)));
-  TRY(cudaHostAlloc(&e->h_status, kStatusWords * sizeof(unsigned int), cudaHostAllocDefault));
-  memset(e->h_status, 0, kStatusWords * sizeof(unsigned int));
+  TRY(cudaHostAlloc(&e->h_status, kStatusRing * kStatusWords * sizeof(unsigned int),
+                    cudaHostAllocDefault));
+  memset(e->h_status, 0, kStatusRing * kStatusWords * sizeof(unsigned int));
 #undef TRY
   *out = e;
   return LMB_OK;
@@ -622,6 +652,187 @@ int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtyp
   return LMB_OK;
 }
 
+// Batched sparse upload of n frames of type T (slots already validated).
+// One host pass over each frame's memory: tasks of (frame, segment) scan in
+// parallel, each writing its positive pixels' (index, value) pairs into its
+// own scratch area (capacity capf pairs, the per-frame sparse limit of a
+// batch).  Frames whose pairs fit are packed back to back behind a
+// descriptor table in a pinned buffer and cross the link in ONE copy; two
+// kernels clear their slots and scatter them.  Frames that do not fit go the
+// dense way, one frame at a time.
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+int load_batch_sparse(lmb_engine *e, const int32_t *slots, const void *const *frames,
+                             int n, int dtype) {
+  const size_t npx = e->npx, vb = sizeof(T);
+  const size_t limit = npx * vb / (2 * (4 + vb));
+  const size_t capf = std::max<size_t>(1, std::min(limit, npx / 64 + 1));
+  const int nt = std::max(1, std::min(16, omp_get_num_procs()));
+  const int nseg = std::max(1, std::min((nt + n - 1) / n, (int)(npx / 4096) + 1));
+  const int ntask = n * nseg;
+  if (e->bt_idx.size() < (size_t)ntask * capf) e->bt_idx.resize((size_t)ntask * capf);
+  if (e->bt_val.size() < (size_t)ntask * capf * vb) e->bt_val.resize((size_t)ntask * capf * vb);
+  uint32_t *sidx = e->bt_idx.data();
+  T *sval = reinterpret_cast<T *>(e->bt_val.data());
+  std::vector<size_t> tcnt((size_t)ntask, 0);
+  std::vector<double> tmax((size_t)ntask, 0.0);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+  for (int t = 0; t < ntask; t++) {
+    const int f = t / nseg, sg = t % nseg;
+    const T *px = static_cast<const T *>(frames[f]);
+    const size_t lo = npx * sg / nseg, hi = npx * (sg + 1) / nseg;
+    uint32_t *ix = sidx + (size_t)t * capf;
+    T *vx = sval + (size_t)t * capf;
+    size_t o = 0;
+    double m = 0.0;
+    for_positive(px, lo, hi, [&](size_t i, T v) {
+      if (o < capf) {
+        ix[o] = (uint32_t)i;
+        vx[o] = v;
+      }
+      o++;
+      if ((double)v > m) m = (double)v;
+    });
+    tcnt[t] = o;
+    tmax[t] = m;
+  }
+  // frames that fit, their descriptors and packed offsets
+  std::vector<SparseFrameDesc> desc;
+  std::vector<int> dense;
+  std::vector<size_t> toff((size_t)ntask, 0);
+  size_t total = 0;
+  uint32_t max_nnz = 0;
+  for (int f = 0; f < n; f++) {
+    size_t nnz = 0;
+    double mx = 0.0;
+    for (int sg = 0; sg < nseg; sg++) {
+      nnz += tcnt[(size_t)f * nseg + sg];
+      mx = std::max(mx, tmax[(size_t)f * nseg + sg]);
+    }
+    if (nnz > capf) {
+      dense.push_back(f);
+      continue;
+    }
+    SparseFrameDesc d{};
+    d.off = total;
+    d.nnz = (uint32_t)nnz;
+    d.slot = slots[f];
+    d.mx = mx;
+    for (int sg = 0; sg < nseg; sg++) {
+      toff[(size_t)f * nseg + sg] = total;
+      total += tcnt[(size_t)f * nseg + sg];
+    }
+    max_nnz = std::max(max_nnz, d.nnz);
+    desc.push_back(d);
+  }
+  const int ns = (int)desc.size();
+  if (ns) {
+    const size_t hdr = (size_t)ns * sizeof(SparseFrameDesc);
+    const size_t ioff = ((hdr + 15) / 16) * 16;
+    const size_t voff = ioff + ((total * 4 + 15) / 16) * 16;
+    const size_t bytes = voff + total * vb;
+    const int r = e->bt_next;
+    e->bt_next ^= 1;
+    if (!e->bt_ev[r]) LMB_CUDA(cudaEventCreateWithFlags(&e->bt_ev[r], cudaEventDisableTiming));
+    LMB_CUDA(cudaEventSynchronize(e->bt_ev[r]));  // ring entry free again
+    if (e->bt_host_cap[r] < bytes) {
+      if (e->bt_host[r]) LMB_CUDA(cudaFreeHost(e->bt_host[r]));
+      e->bt_host[r] = nullptr;
+      e->bt_host_cap[r] = 0;
+      const size_t want = std::max(bytes + bytes / 4, (size_t)1 << 20);
+      LMB_CUDA(cudaHostAlloc(&e->bt_host[r], want, cudaHostAllocDefault));
+      e->bt_host_cap[r] = want;
+    }
+    if (e->d_batch_cap < bytes) {
+      LMB_CUDA(cudaStreamSynchronize(e->ld));  // the old buffer may still be read
+      cudaFree(e->d_batch);
+      e->d_batch = nullptr;
+      e->d_batch_cap = 0;
+      const size_t want = std::max(bytes + bytes / 4, (size_t)1 << 20);
+      LMB_CUDA(cudaMalloc(&e->d_batch, want));
+      e->d_batch_cap = want;
+    }
+    char *h = static_cast<char *>(e->bt_host[r]);
+    memcpy(h, desc.data(), hdr);
+    uint32_t *pidx = reinterpret_cast<uint32_t *>(h + ioff);
+    T *pval = reinterpret_cast<T *>(h + voff);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int t = 0; t < ntask; t++) {
+      const int f = t / nseg;
+      const size_t c = tcnt[t];
+      size_t ff = 0;  // is frame f packed?  (dense frames have nnz > capf)
+      for (int sg = 0; sg < nseg; sg++) ff += tcnt[(size_t)f * nseg + sg];
+      if (ff > capf || c == 0) continue;
+      memcpy(pidx + toff[t], sidx + (size_t)t * capf, c * 4);
+      memcpy(pval + toff[t], sval + (size_t)t * capf, c * vb);
+    }
+    for (int i = 0; i < ns; i++)
+      LMB_CUDA(cudaStreamWaitEvent(e->ld, e->ev_released[desc[i].slot], 0));
+    LMB_CUDA(cudaMemcpyAsync(e->d_batch, h, bytes, cudaMemcpyHostToDevice, e->ld));
+    LMB_CUDA(cudaEventRecord(e->bt_ev[r], e->ld));
+    e->bytes_h2d += bytes;
+    char *d = static_cast<char *>(e->d_batch);
+    const int rc = batch_sparse_load_launch(
+        reinterpret_cast<const SparseFrameDesc *>(d), ns, max_nnz,
+        reinterpret_cast<const uint32_t *>(d + ioff), d + voff, dtype, e->d_u8, e->d_occ,
+        e->d_scale, npx, e->num_sms, e->ld);
+    if (rc) return rc;
+    e->sparse_loads += ns;
+    for (int i = 0; i < ns; i++) {
+      const int s = desc[i].slot;
+      LMB_CUDA(cudaEventRecord(e->ev_loaded[s], e->ld));
+      e->loaded_mask |= 1ull << s;
+      e->f64_mask &= ~(1ull << s);
+    }
+  }
+  for (int f : dense) {
+    const int rc = lmb_image_load(e, slots[f], frames[f], dtype, 0, nullptr);
+    if (rc) return rc;
+  }
+  return LMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lmb_image_load_batch(lmb_engine *e, const int32_t *slots, const void *const *frames,
+                         int32_t n, int32_t dtype, double *im_scales) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(n >= 0 && n <= LMB_MAX_SLOTS, "batch of %d frames (at most %d)", n, LMB_MAX_SLOTS);
+  LMB_REQUIRE(n == 0 || (slots && frames), "null slot or frame list");
+  LMB_REQUIRE(dtype == LMB_F64 || dtype == LMB_F32 || dtype == LMB_U8, "unknown dtype %d", dtype);
+  uint64_t seen = 0;
+  for (int i = 0; i < n; i++) {
+    LMB_REQUIRE(slots[i] >= 0 && slots[i] < LMB_MAX_SLOTS, "slot %d outside 0..%d", slots[i],
+                LMB_MAX_SLOTS - 1);
+    LMB_REQUIRE(!(seen >> slots[i] & 1), "slot %d appears twice in the batch", slots[i]);
+    LMB_REQUIRE(frames[i], "null frame %d", i);
+    seen |= 1ull << slots[i];
+  }
+  if (!e->sparse_uploads) {
+    for (int i = 0; i < n && rc == LMB_OK; i++)
+      rc = lmb_image_load(e, slots[i], frames[i], dtype, 0, nullptr);
+  } else if (n) {
+    rc = dtype == LMB_F64   ? load_batch_sparse<double>(e, slots, frames, n, dtype)
+         : dtype == LMB_F32 ? load_batch_sparse<float>(e, slots, frames, n, dtype)
+                            : load_batch_sparse<uint8_t>(e, slots, frames, n, dtype);
+  }
+  if (rc) return rc;
+  if (im_scales && n) {
+    double sc[LMB_MAX_SLOTS];
+    LMB_CUDA(cudaMemcpyAsync(sc, e->d_scale, sizeof(sc), cudaMemcpyDeviceToHost, e->ld));
+    LMB_CUDA(cudaStreamSynchronize(e->ld));
+    e->bytes_d2h += sizeof(sc);
+    for (int i = 0; i < n; i++) im_scales[i] = sc[slots[i]];
+  }
+  return LMB_OK;
+}
+
 int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double min_intensity,
               int32_t value_mode) {
   int rc = check_engine(e);
@@ -674,28 +885,52 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   }
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
     if (slot_mask >> k & 1) LMB_CUDA(cudaEventRecord(e->ev_released[k], e->st));
+  // the pass's status words into the next ring entry
+  const int r = (int)(e->pass_seq % kStatusRing);
+  LMB_CUDA(cudaMemcpyAsync(e->h_status + (size_t)r * kStatusWords, e->d_status,
+                           kStatusWords * sizeof(unsigned int), cudaMemcpyDeviceToHost, e->st));
+  LMB_CUDA(cudaEventRecord(e->ev_done[r], e->st));
   e->bytes_d2h += kStatusWords * sizeof(unsigned int);
-  e->last_mask = slot_mask;
-  e->pending = true;
+  for (int k = 0; k < LMB_MAX_SLOTS; k++)
+    if (slot_mask >> k & 1) e->slot_ring[k] = r;
+  e->done_mask |= slot_mask;
+  e->pass_seq++;
   return LMB_OK;
 }
+
+}  // extern "C"
+
+namespace {
+
+// Wait for the last pass that included `slot`; its status words.
+int slot_status(lmb_engine *e, int slot, const unsigned int **st) {
+  LMB_REQUIRE(slot >= 0 && slot < LMB_MAX_SLOTS && (e->done_mask >> slot & 1),
+              "slot %d has not been part of a pass", slot);
+  const int r = e->slot_ring[slot];
+  LMB_CUDA(cudaEventSynchronize(e->ev_done[r]));
+  *st = e->h_status + (size_t)r * kStatusWords;
+  const int derr = (int)(*st)[2 * LMB_MAX_SLOTS];
+  if (derr != DEV_OK) {
+    set_error("device wait gave up in the compare pass (code %d)", derr);
+    return LMB_ERR_TIMEOUT;
+  }
+  return LMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 int lmb_results(lmb_engine *e, int32_t slot, lmb_survivor *out, uint64_t out_capacity,
                 uint64_t *n_survivors, uint64_t *n_pass) {
   int rc = check_engine(e);
   if (rc) return rc;
-  LMB_REQUIRE(e->pending, "no pass has been run");
-  LMB_REQUIRE(slot >= 0 && slot < LMB_MAX_SLOTS && (e->last_mask >> slot & 1),
-              "slot %d was not part of the last pass", slot);
-  LMB_CUDA(cudaStreamSynchronize(e->st));
-  const int derr = (int)e->h_status[2 * LMB_MAX_SLOTS];
-  if (derr != DEV_OK) {
-    set_error("device wait gave up in the compare pass (code %d)", derr);
-    return LMB_ERR_TIMEOUT;
-  }
-  const uint64_t cnt = e->h_status[slot];
+  const unsigned int *sw = nullptr;
+  rc = slot_status(e, slot, &sw);
+  if (rc) return rc;
+  const uint64_t cnt = sw[slot];
   if (n_survivors) *n_survivors = cnt;
-  if (n_pass) *n_pass = e->h_status[LMB_MAX_SLOTS + slot];
+  if (n_pass) *n_pass = sw[LMB_MAX_SLOTS + slot];
   if (cnt > e->cap) {
     set_error("slot %d: %llu survivors exceed the engine capacity %u", slot,
               (unsigned long long)cnt, e->cap);
@@ -718,22 +953,16 @@ int lmb_results_batch(lmb_engine *e, const int32_t *slots, int32_t nslots, lmb_s
                       uint64_t out_capacity, uint64_t *counts, uint64_t *n_pass) {
   int rc = check_engine(e);
   if (rc) return rc;
-  LMB_REQUIRE(e->pending, "no pass has been run");
   LMB_REQUIRE(nslots >= 0 && (slots || nslots == 0) && counts, "bad slot list");
-  LMB_CUDA(cudaStreamSynchronize(e->st));
-  const int derr = (int)e->h_status[2 * LMB_MAX_SLOTS];
-  if (derr != DEV_OK) {
-    set_error("device wait gave up in the compare pass (code %d)", derr);
-    return LMB_ERR_TIMEOUT;
-  }
   uint64_t total = 0;
   bool over = false;
   for (int i = 0; i < nslots; i++) {
     const int k = slots[i];
-    LMB_REQUIRE(k >= 0 && k < LMB_MAX_SLOTS && (e->last_mask >> k & 1),
-                "slot %d was not part of the last pass", k);
-    counts[i] = e->h_status[k];
-    if (n_pass) n_pass[i] = e->h_status[LMB_MAX_SLOTS + k];
+    const unsigned int *sw = nullptr;
+    rc = slot_status(e, k, &sw);
+    if (rc) return rc;
+    counts[i] = sw[k];
+    if (n_pass) n_pass[i] = sw[LMB_MAX_SLOTS + k];
     over |= counts[i] > e->cap;
     total += counts[i];
   }
@@ -746,14 +975,16 @@ int lmb_results_batch(lmb_engine *e, const int32_t *slots, int32_t nslots, lmb_s
               (unsigned long long)out_capacity);
     return LMB_ERR_OVERFLOW;
   }
+  // the survivor lists are final (their passes' events have completed); copy
+  // them on the download stream so a pass queued meanwhile keeps running
   uint64_t off = 0;
   for (int i = 0; i < nslots; i++) {
     if (counts[i])
       LMB_CUDA(cudaMemcpyAsync(out + off, e->d_sorted + (size_t)slots[i] * e->cap,
-                               counts[i] * sizeof(lmb_survivor), cudaMemcpyDeviceToHost, e->st));
+                               counts[i] * sizeof(lmb_survivor), cudaMemcpyDeviceToHost, e->dl));
     off += counts[i];
   }
-  LMB_CUDA(cudaStreamSynchronize(e->st));
+  LMB_CUDA(cudaStreamSynchronize(e->dl));
   e->bytes_d2h += total * sizeof(lmb_survivor);
   return LMB_OK;
 }
@@ -768,7 +999,7 @@ int lmb_engine_bytes(lmb_engine *e, uint64_t *h2d, uint64_t *d2h) {
 int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms) {
   int rc = check_engine(e);
   if (rc) return rc;
-  LMB_REQUIRE(e->pending, "no pass has been run");
+  LMB_REQUIRE(e->pass_seq > 0, "no pass has been run");
   LMB_CUDA(cudaEventSynchronize(e->ev[2]));
   float a = 0, b = 0;
   LMB_CUDA(cudaEventElapsedTime(&a, e->ev[0], e->ev[1]));

@@ -66,7 +66,28 @@ int quantize_launch(const void *d_img, int dtype, size_t npx, unsigned long long
 int sparse_load_launch(const uint32_t *d_idx, const void *d_val, int dtype, size_t nnz, double mx,
                        uint8_t *d_u8, unsigned long long *d_occ, int slot, double *d_scale_slot,
                        size_t npx, int num_sms, cudaStream_t st);
+
+// One frame of a batched sparse upload: its (pixel index, value) pairs are
+// entries [off, off + nnz) of the packed index and value arrays; mx is the
+// largest of its values (0 when it has none).
+struct SparseFrameDesc {
+  uint64_t off;
+  uint32_t nnz;
+  int32_t slot;
+  double mx;
+  double reserved;
+};
+static_assert(sizeof(SparseFrameDesc) == 32, "descriptor layout");
+
+// Clear the frames' slots, then quantise and scatter all frames' pairs: two
+// launches for the whole batch (occupancy bits of different slots share a
+// word, so both kernels update it atomically).
+int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_t max_nnz,
+                             const uint32_t *d_idx, const void *d_val, int dtype, uint8_t *d_u8,
+                             unsigned long long *d_occ, double *d_scale, size_t npx, int num_sms,
+                             cudaStream_t st);
 int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_t st);
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st);
+int status_reset_launch(unsigned int *d_status, uint64_t mask, cudaStream_t st);
 
 }  // namespace lmb

@@ -169,6 +169,34 @@ class Engine:
                                    C.byref(sc) if want_scale else None))
         return sc.value if want_scale else None
 
+    def load_images(self, slots, frames, want_scales: bool = False):
+        """Load several frames (one dtype) into distinct slots with one
+        library call: each slot ends as after ``load_image(slot, frame)``.
+        Returns the imScale of each frame when ``want_scales``."""
+        sl = np.ascontiguousarray(list(slots), dtype=np.int32)
+        n = sl.shape[0]
+        if len(frames) != n:
+            raise ValueError(f"{n} slots for {len(frames)} frames")
+        pxs = []
+        dt = None
+        for f in frames:
+            px = np.ascontiguousarray(f).ravel()
+            if px.size != self.npx:
+                raise ValueError(f"image has {px.size} pixels, detector has {self.npx}")
+            if px.dtype not in _DTYPES:
+                px = px.astype(np.float64)
+            if dt is None:
+                dt = px.dtype
+            elif px.dtype != dt:
+                raise ValueError("frames of one batch share a dtype")
+            pxs.append(px)
+        ptrs = (C.c_void_p * max(n, 1))(*[p.ctypes.data for p in pxs])
+        sc = np.zeros(max(n, 1), np.float64)
+        check(lib().lmb_image_load_batch(self._h, sl.ctypes.data, ptrs, n,
+                                         _DTYPES[dt] if n else _lib.LMB_U8,
+                                         _dptr(sc) if want_scales else None))
+        return sc[:n].tolist() if want_scales else None
+
     # ---- passes ---------------------------------------------------------------
     def _apply_table_shape(self, k: int) -> None:
         """Use the autotuned launch shape for passes of k images, unless the

@@ -281,16 +281,24 @@ class StreamServer:
             self._backlog.append(r)
             block = False
         keep = collections.deque()
+        admitted = {}
         while self._backlog:
             r = self._backlog.popleft()
             g = self.geoms[r.key]
             if not g.free:
                 keep.append(r)
                 continue
-            s = g.free.pop()
-            g.engine.load_image(s, r.pixels, want_scale=False)
-            g.loaded.append((s, r))
+            admitted.setdefault(r.key, []).append((g.free.pop(), r))
             n += 1
+        # one batched upload per geometry and pixel type
+        for key, items in admitted.items():
+            g = self.geoms[key]
+            by_type = collections.defaultdict(list)
+            for s, r in items:
+                by_type[r.pixels.dtype].append((s, r))
+            for its in by_type.values():
+                g.engine.load_images([s for s, _ in its], [r.pixels for _, r in its])
+            g.loaded.extend(items)
         self._backlog = keep
         return n
 
@@ -351,7 +359,7 @@ class StreamServer:
     def submit(self, image_num, pixels, key=None):
         """In-process submission (same path as a received message)."""
         key = key or (int(self.primary.nr_px_x), int(self.primary.nr_px_y))
-        self.queue.put(Request(int(image_num), key, pixels, time.perf_counter()))
+        self.queue.put(Request(int(image_num), key, np.asarray(pixels), time.perf_counter()))
 
     def stop(self, drain_timeout=600.0, close_engines=True):
         """Stop accepting, finish every received image, close the files."""

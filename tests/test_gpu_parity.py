@@ -213,6 +213,80 @@ def test_sparse_and_dense_uploads_agree_and_slots_reuse_cleanly():
         assert got[1] == refs[0][1] and np.array_equal(got[0], refs[0][0])
 
 
+@pytest.mark.parametrize("dtype", [np.uint8, np.float32, np.float64])
+def test_batched_frame_loads_equal_single_loads(dtype):
+    """load_images (one host scan per frame, one copy, two kernels per batch)
+    leaves every slot as load_image does: same survivors, same imScale, for
+    sparse frames, a dense frame in the same batch, batches of 1..3 frames
+    (several scan segments per frame) and slots that held other frames."""
+    c = golden_case("tilted_fcc")
+    p = c.params
+    rng = np.random.default_rng(8)
+    base = [c.image, c.image * 0.37, c.image * 3.0 + 0.0]
+    other = synth.render_image(c.records[rng.choice(np.nonzero(c.records[:, 0] >= 8)[0], 4)],
+                               p.nr_px_x, p.nr_px_y, rng)
+    frames = [f.astype(dtype) if dtype != np.uint8 else np.clip(f, 0, 255).astype(np.uint8)
+              for f in base + [other]]
+    dense = np.clip(frames[0].astype(np.float64) + 2.0, 0, 255).astype(dtype)  # all positive
+    frames.append(dense)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        singles, scales = [], []
+        for f in frames:
+            scales.append(e.load_image(0, f))
+            e.match([0], p.min_nr_spots, p.min_intensity)
+            singles.append(e.results(0))
+        # previous content in every target slot
+        for s in (1, 2, 5, 40, 63):
+            e.load_image(s, other.astype(dtype) if dtype != np.uint8 else
+                         np.clip(other, 0, 255).astype(np.uint8))
+        got_sc = e.load_images([63, 1, 40, 2, 5], frames, want_scales=True)
+        assert got_sc == scales
+        e.match([1, 2, 5, 40, 63], p.min_nr_spots, p.min_intensity)
+        res = e.results_batch([63, 1, 40, 2, 5])
+        for i, s in enumerate([63, 1, 40, 2, 5]):
+            assert res[s][1] == singles[i][1] and np.array_equal(res[s][0], singles[i][0])
+        for k in (1, 2, 3):  # small batches: a frame split over scan segments
+            e.load_images(list(range(10, 10 + k)), frames[:k])
+            e.match(range(10, 10 + k), p.min_nr_spots, p.min_intensity)
+            for i in range(k):
+                r = e.results(10 + i)
+                assert r[1] == singles[i][1] and np.array_equal(r[0], singles[i][0])
+        with pytest.raises(LmbError):
+            e.load_images([3, 3], frames[:2])
+
+
+def test_queued_passes_keep_each_slots_results():
+    """A pass over other slots queued before the previous pass's results are
+    read leaves those results intact; a slot's results are those of the last
+    pass that included it; a slot never matched has none."""
+    c = golden_case("tilted_dense")
+    p = c.params
+    scales = (1.0, 0.5, 2.0, 0.25)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        for k, s in enumerate(scales):
+            e.load_image(k, c.image * s)
+        alone = {}
+        for k in range(4):
+            e.match([k], p.min_nr_spots, p.min_intensity)
+            alone[k] = e.results(k)
+        for _ in range(3):  # more passes in flight than status entries are kept
+            e.match([0, 1], p.min_nr_spots, p.min_intensity)
+            e.match([2], p.min_nr_spots, p.min_intensity)
+            e.match([3], p.min_nr_spots, p.min_intensity)
+        got = e.results_batch([3, 0, 2, 1])
+        for k in range(4):
+            assert got[k][1] == alone[k][1] and np.array_equal(got[k][0], alone[k][0])
+        e.match([2], p.min_nr_spots, 1e12)  # slot 2 again: nothing passes
+        assert e.results(2)[1] == 0
+        r0 = e.results(0)
+        assert r0[1] == alone[0][1] and np.array_equal(r0[0], alone[0][0])
+        e.load_image(9, c.image)
+        with pytest.raises(LmbError):
+            e.results(9)
+
+
 def test_byte_counters_follow_the_copies():
     """lmb_engine_bytes: a dense frame adds its size, a sparse one its
     (index, value) pairs, a pass its status words, results their survivors."""
