@@ -210,12 +210,13 @@ def cpu_baseline(e, p, txt, hkls, img_u8, seed, n_sample, runs=3):
             "sample": f"oracle compare on {n_sample} records x {runs} runs, scaled to 1e8"}
 
 
-def load_traffic():
-    path = os.path.join(ROOT, "profiles", "compare_kernel_traffic.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            return json.load(f)
-    return None
+# DRAM bytes (read + write) per orientation of one compare launch, from ncu
+# captures of smaller DBs of this workload (the figures and commands are in
+# profiles/compare_*.md); traffic grows with the DB, so roofline.traffic
+# scales them to N.
+TRAFFIC_BYTES_PER_ORIENT = {
+    "reference": 271.1e6 / 2_000_000,  # compare_ws_kernel, 2M orientations, K=16
+}
 
 
 def run_ours(args, rank, world):
@@ -233,6 +234,8 @@ def run_ours(args, rank, world):
     hkls = synth.hkls_cubic(8)
     N, K = args.n_orient, args.batch
     e = Engine(p, device=dev)
+    if args.variant is not None:  # pin the compare variant (else: the autotuned table)
+        e.set_tuning(variant=args.variant)
     t0 = time.perf_counter()
     e.build_db_synthetic(seed=args.seed, n=N, hkls=hkls)
     torch.cuda.synchronize()
@@ -281,6 +284,7 @@ def run_ours(args, rank, world):
         total_ms = float(tt.item())
     value = world * K * args.steps / (total_ms / 1e3)
     surv = [int(e.results(k)[0].shape[0]) for k in range(K)]
+    shape_main, lay_main = e.get_tuning(), e.layout_info()  # the timed pass's shape
 
     # ---- plain pass (one image) --------------------------------------------
     timed(args.warmup, [0])
@@ -296,11 +300,20 @@ def run_ours(args, rank, world):
     d2h = [0]
 
     frames_all = [pb.array for pb in pins]
+    phase = {"seq_load": [], "seq_match": [], "seq_collect": [], "pipe_load": [],
+             "pipe_match": [], "pipe_collect": []}
 
     def e2e_step():
+        t0 = time.perf_counter()
         e.load_images(slots, frames_all)
+        t1 = time.perf_counter()
         e.match(slots, p.min_nr_spots, p.min_intensity)
+        t2 = time.perf_counter()
         nb = sum(r.nbytes for r, _ in e.results_batch(slots).values())
+        t3 = time.perf_counter()
+        phase["seq_load"].append(t1 - t0)
+        phase["seq_match"].append(t2 - t1)
+        phase["seq_collect"].append(t3 - t2)
         d2h[0] = nb + (2 * 64 + 1) * 4
 
     # sequential: upload 64 frames, one pass, download
@@ -334,13 +347,20 @@ def run_ours(args, rank, world):
         nb = 0
         for i in range(npasses):
             h = i % 2
+            t0 = time.perf_counter()
             if i + 1 < npasses:
                 # next half: host scan while pass h runs, then its pass queued
                 # behind pass h so the device never waits for the host
                 load_half(1 - h)
+            t1 = time.perf_counter()
+            if i + 1 < npasses:
                 e.match(halves[1 - h], p.min_nr_spots, p.min_intensity)
+            t2 = time.perf_counter()
             nb += collect(h)
             if lat is not None:
+                phase["pipe_load"].append(t1 - t0)
+                phase["pipe_match"].append(t2 - t1)
+                phase["pipe_collect"].append(time.perf_counter() - t2)
                 t = time.perf_counter()
                 lat.append((t - t_prev) * 1e3)
                 t_prev = t
@@ -369,6 +389,19 @@ def run_ours(args, rank, world):
         if i >= args.warmup:
             platency.append((time.perf_counter() - ts) * 1e3)
 
+    # ---- the same batched pass gathering every spot ----------------------------
+    # (records with fewer spots than MinNrSpots are otherwise not gathered:
+    # they cannot pass; the survivors are identical either way)
+    e.set_tuning(**dict(shape_main, full_gather=1))
+    for k in range(K):
+        e.load_image(k, imgs[k], want_scale=False)
+    timed(args.warmup, slots)
+    fg_step, fg_cmp = timed(max(10, args.steps // 4), slots)
+    fg_surv = [int(e.results(k)[0].shape[0]) for k in range(K)]
+    full_gather = {"value": round(K / (statistics.mean(fg_step) * 1e-3), 2), "unit": UNIT,
+                   "compare_ms": round(statistics.mean(fg_cmp), 4),
+                   "same_survivor_counts": fg_surv == surv}
+
     # ---- roofline of the compare kernel ----------------------------------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
@@ -376,18 +409,31 @@ def run_ours(args, rank, world):
         peak_src = "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
-    alg_bytes = N * REC_BYTES_PER_ORIENT + K * p.nr_px_x * p.nr_px_y
+    # Algorithmic bytes of one pass: the reference records (122 B per
+    # orientation) plus the K uint8 frames; with the compact layout, the bytes
+    # that layout streams (1 B per orientation + 4 B per on-detector spot +
+    # tile headers) plus the occupancy words the gathers read (8 B per pixel).
+    lay, shape = lay_main, shape_main
+    compact = shape["variant"] == 2 and lay["compact"] == 1
+    ref_bytes = N * REC_BYTES_PER_ORIENT + K * p.nr_px_x * p.nr_px_y
+    alg_bytes = lay["bytes"] + p.nr_px_x * p.nr_px_y * 8 if compact else ref_bytes
     cmp_avg = statistics.mean(cmp_ms)
     achieved = alg_bytes / (cmp_avg * 1e-3) / 1e9
-    tr = load_traffic()
+    tpo = TRAFFIC_BYTES_PER_ORIENT.get("compact" if compact else "reference")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_src,
-            "kernel": "compare_kernel",
+            "kernel": "compare_clist_kernel" if compact else "compare_ws_kernel",
+            "layout": "compact" if compact else "reference",
             "algorithmic_bytes_per_launch": alg_bytes,
             "avg_launch_ms": round(cmp_avg, 4),
-            "traffic": tr.get("bytes_per_launch_scaled") if tr else None}
-    if tr:
-        roof["traffic_source"] = tr.get("source")
+            "traffic": round(tpo * N) if tpo else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per orientation "
+                              "of a smaller capture, scaled to N (see profiles/)" if tpo else None,
+            "reference_layout_bytes_per_launch": ref_bytes,
+            "reference_layout_equivalent_gbs": round(ref_bytes / (cmp_avg * 1e-3) / 1e9, 1),
+            "tuning": shape}
+    if compact:
+        roof["compact_layout"] = lay
 
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
@@ -411,7 +457,11 @@ def run_ours(args, rank, world):
                         "passes of 32, the upload of one half overlapping the pass of the other "
                         "and its pass queued before the other's results are read (load_images "
                         "of 32 frames, match, results_batch of the previous 32, twice)",
-                "sequential": round(seq_ips, 2)},
+                "sequential": round(seq_ips, 2),
+                # host wall time per call, median: load_images (host scan + copy
+                # enqueue), match (enqueue), results_batch (wait for the pass + copy)
+                "breakdown_ms_p50": {k: round(1e3 * float(np.median(v)), 3)
+                                     for k, v in phase.items() if v}},
         # per timed pass: status reset, compare, ordering (one graph replay)
         "gpu_launches": 3 * args.steps,
         "clocks": clk,
@@ -425,6 +475,7 @@ def run_ours(args, rank, world):
                   "e2e": round(1e3 / statistics.mean(platency), 2),
                   "compare_ms": round(statistics.mean(pcmp), 4)},
         "batched_over_plain": round(value / world / plain_ips, 2),
+        "full_gather": full_gather,
         "survivors_per_image": {"min": min(surv), "max": max(surv), "mean": statistics.mean(surv)},
         "dbbuild": {"orientations_per_s": round(N / t_build, 1), "seconds": round(t_build, 3),
                     "hkl_evals_per_s": round(N * len(hkls) / t_build, 1)},
@@ -723,6 +774,8 @@ def main():
                          "single-image GPU executable built for sm_100a")
     ap.add_argument("--n-orient", type=int, default=100_000_000)
     ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--variant", type=int, default=None, choices=[0, 1, 2],
+                    help="pin the compare variant (default: the autotuned shape)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--min-intensity", type=float, default=200.0)
     ap.add_argument("--cpu-sample", type=int, default=10_000_000,

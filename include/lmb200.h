@@ -101,13 +101,24 @@ int lmb_engine_destroy(lmb_engine *e);
 void *lmb_engine_stream(lmb_engine *e);
 
 /* Launch shape of the compare pass: fields = {variant (0 block-barrier ring,
- * 1 warp-specialised), tile_sub (32-orientation sub-tiles per tile), stages,
- * consumer warps, blocks per SM, grid multiplier}; 0 = default.  Written by
- * the autotuner; get returns the shape actually used for this DB.  No
- * reference counterpart (the reference launches <<<ceil(n/1024),1024>>>,
- * LaueMatchingGPU.cu:739-743). */
+ * 1 warp-specialised, 2 warp-specialised over the compact layout),
+ * tile_sub (32-orientation sub-tiles per tile), stages, consumer warps,
+ * blocks per SM, grid multiplier, full_gather}; 0 = default.  full_gather = 1
+ * gathers every spot even of records with fewer spots than MinNrSpots (which
+ * cannot pass; by default they are skipped; results are identical either
+ * way), for measuring the full gather cost.  Written by the autotuner;
+ * get returns the shape actually used for this DB.  No reference counterpart
+ * (the reference launches <<<ceil(n/1024),1024>>>, LaueMatchingGPU.cu:739-743). */
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields);
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields);
+
+/* The compact device layout variant 2 streams: derived from the resident
+ * records on the first variant-2 pass (1 byte per record + 4 bytes per
+ * on-detector spot, in record order; the reference records stay resident).
+ * compact = 1 built, 0 not yet, -1 this DB keeps the reference layout
+ * (MaxNrLaueSpots > 255 or tiles too large).  No reference counterpart. */
+int lmb_engine_layout_info(lmb_engine *e, int32_t *compact, uint64_t *compact_bytes,
+                           int32_t *tiles, int32_t *tile_bytes);
 
 /* lmb_image_load sends a frame whose positive pixels are few (their
  * (uint32 index, value) pairs smaller than half the dense frame) as those

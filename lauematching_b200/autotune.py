@@ -52,6 +52,9 @@ def lookup(R: int, k: int) -> dict | None:
 
 
 def candidate_shapes():
+    # compact layout: the tile comes with the layout; ring depth 0 = as deep as fits
+    for cons, st, gm in itertools.product((8, 12, 16, 17), (0, 4, 8), (1, 2)):
+        yield dict(variant=2, stages=st, consumers=cons, grid_mult=gm)
     for ts, st, cons in itertools.product((4, 8), (4, 6, 8, 12), (8, 12, 16)):
         yield dict(variant=1, tile_sub=ts, stages=st, consumers=cons)
     for ts, st, bps in itertools.product((4, 8), (2, 3, 4), (1, 2, 3)):

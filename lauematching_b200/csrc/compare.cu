@@ -250,10 +250,32 @@ int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_
 
 static constexpr uint64_t kWaitNs = 2000000000ull;  // bounded TMA waits: 2 s
 
+// The spots of one orientation, in record order, as detector pixel indices.
+// RecSpots reads the reference record ({count, x0, y0, ...}) and skips
+// off-detector pixels like LaueMatchingGPU.cu:65; ListSpots reads the compact
+// layout, which holds the on-detector pixels only (same order).
+struct RecSpots {
+  const uint16_t *rec;
+  __device__ __forceinline__ bool pixel(const CmpArgs &a, int s, size_t &p) const {
+    const int x = rec[1 + 2 * s], y = rec[2 + 2 * s];
+    if (x >= a.W || y >= a.H) return false;
+    p = (size_t)y * a.W + x;
+    return true;
+  }
+};
+struct ListSpots {
+  const uint32_t *sp;
+  __device__ __forceinline__ bool pixel(const CmpArgs &, int s, size_t &p) const {
+    p = sp[s];
+    return true;
+  }
+};
+
 // Intensity of slot k over one record, in record order (LaueMatchingCPU.c:671-681
 // for the uint8 image; :649-653 for the float64 image).  Returns the spot
 // count; tot/su receive the FP64 sum and the uint8 sum.
-__device__ __noinline__ int slot_sum(const CmpArgs &a, const uint16_t *rec, int c, int k,
+template <class Spots>
+__device__ __noinline__ int slot_sum(const CmpArgs &a, const Spots sp, int c, int k,
                                      double &tot_out, int &su_out) {
   const uint8_t *img = a.u8 + (size_t)k * a.npx;
   const double *fim = a.f64 ? a.f64 + (size_t)k * a.npx : nullptr;
@@ -261,9 +283,8 @@ __device__ __noinline__ int slot_sum(const CmpArgs &a, const uint16_t *rec, int 
   int ns = 0, su = 0;
   double tot = 0.0;
   for (int s = 0; s < c; s++) {
-    const int x = rec[1 + 2 * s], y = rec[2 + 2 * s];
-    if (x >= a.W || y >= a.H) continue;
-    const size_t p = (size_t)y * a.W + x;
+    size_t p;
+    if (!sp.pixel(a, s, p)) continue;
     const uint8_t raw = img[p];
     if (a.mode == LMB_VALUE_U8) {
       if (raw > 0) {
@@ -285,12 +306,17 @@ __device__ __noinline__ int slot_sum(const CmpArgs &a, const uint16_t *rec, int 
   return ns;
 }
 
-// Called by all 32 lanes of a warp (lanes without a record pass valid=false).
-template <int B>
-__device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, uint64_t oid,
+// Called by all 32 lanes of a warp (lanes without a record pass valid=false,
+// c=0).  c = the record's spot count, clamped to S.
+template <int B, class Spots>
+__device__ __forceinline__ void process(const CmpArgs &a, const Spots sp, int c, uint64_t oid,
                                         uint64_t pol, bool valid) {
-  int c = valid ? rec[0] : 0;
-  if (c > a.S) c = a.S;  // clamp like LaueMatchingGPU.cu:54-55
+  // nSpots <= c, so a record with c < MinNrSpots fails the spot threshold of
+  // LaueMatchingCPU.c:683 in every image: nothing to gather or count
+  if (!a.full_gather && c < a.min_spots) {
+    valid = false;
+    c = 0;
+  }
   unsigned long long cnt[B];
 #pragma unroll
   for (int b = 0; b < B; b++) cnt[b] = 0ull;
@@ -301,11 +327,8 @@ __device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, u
     for (int j = 0; j < 4; j++) {
       m[j] = 0ull;
       const int s = s0 + j;
-      if (s < c) {
-        const int x = rec[1 + 2 * s], y = rec[2 + 2 * s];
-        if (x < a.W && y < a.H)  // skip like LaueMatchingGPU.cu:65
-          m[j] = ld_nc_hint(a.occ + (size_t)y * a.W + x, pol);
-      }
+      size_t p;
+      if (s < c && sp.pixel(a, s, p)) m[j] = ld_nc_hint(a.occ + p, pol);
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -346,7 +369,7 @@ __device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, u
     double tot = 0.0, score = 0.0;
     int ns = 0, su = 0;
     if ((cand >> k) & 1) {
-      ns = slot_sum(a, rec, c, k, tot, su);
+      ns = slot_sum(a, sp, c, k, tot, su);
       pass = ns >= a.min_spots && tot >= a.min_int;
       if (pass) {
         score = dmul(tot, dsqrt((double)ns));
@@ -374,6 +397,15 @@ __device__ __forceinline__ void process(const CmpArgs &a, const uint16_t *rec, u
       }
     }
   }
+}
+
+// One record of the reference layout.
+template <int B>
+__device__ __forceinline__ void process_rec(const CmpArgs &a, const uint16_t *rec, uint64_t oid,
+                                            uint64_t pol, bool valid) {
+  int c = valid ? rec[0] : 0;
+  if (c > a.S) c = a.S;  // clamp like LaueMatchingGPU.cu:54-55
+  process<B>(a, RecSpots{rec}, c, oid, pol, valid);
 }
 
 // Variant 0: every thread consumes; thread 0 refills the ring after a block
@@ -425,10 +457,10 @@ __global__ void __launch_bounds__(256) compare_ring_kernel(const __grid_constant
       }
       const uint16_t *rec = reinterpret_cast<const uint16_t *>(ring + (size_t)s * a.tile_bytes) +
                             (size_t)threadIdx.x * a.R;
-      process<B>(a, rec, oid, pol_occ, true);
+      process_rec<B>(a, rec, oid, pol_occ, true);
     } else {
       const bool v = oid < a.n;  // partial last tile: direct loads, whole warps
-      process<B>(a, v ? a.db + oid * a.R : a.db, oid, pol_occ, v);
+      process_rec<B>(a, v ? a.db + oid * a.R : a.db, oid, pol_occ, v);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -511,13 +543,112 @@ __global__ void __launch_bounds__(576, 1) compare_ws_kernel(const __grid_constan
       }
       const uint16_t *rec = reinterpret_cast<const uint16_t *>(ring + (size_t)s * a.tile_bytes) +
                             (size_t)(sub * 32 + lane) * a.R;
-      process<B>(a, rec, oid, pol_occ, true);
+      process_rec<B>(a, rec, oid, pol_occ, true);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     } else {
       const bool v = oid < a.n;  // partial last tile: direct loads, whole warps
-      process<B>(a, v ? a.db + oid * a.R : a.db, oid, pol_occ, v);
+      process_rec<B>(a, v ? a.db + oid * a.R : a.db, oid, pol_occ, v);
     }
+  }
+}
+
+// Variant 2: warp-specialised over the compact layout (clist.cu): fixed-size
+// tiles of tile_bytes, tile t at cl + t*tile_bytes, each holding nch whole
+// 32-record chunks (header: first record, nch; then the uint8 per-chunk
+// maximum counts, the uint8 counts, the uint32 chunk bases, the uint32
+// on-detector pixel indices in record order).  The producer lane moves whole
+// tiles into the ring (one bulk copy each, no table lookup).  The consumer
+// warps vote over the per-chunk maxima, 32 chunks at a time, for the chunks
+// holding a record with at least MinNrSpots spots (no other record can pass),
+// share those out round-robin (the turn carries over from tile to tile, so
+// tiles with few such chunks still use every warp), find each lane's first
+// spot with a warp prefix sum of the counts, and run the per-record logic of
+// the other variants.
+template <int B>
+__global__ void __launch_bounds__(576, 1) compare_clist_kernel(const __grid_constant__ CmpArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int ST = a.stages;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *empty = full + 16;
+  unsigned char *ring = smem + 256;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int NC = a.consumers;
+  const uint64_t G = gridDim.x;
+  const uint64_t my_tiles = (a.ntiles > blockIdx.x) ? (a.ntiles - 1 - blockIdx.x) / G + 1 : 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NC);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    if (lane != 0) return;
+    const uint64_t pol_db = l2_evict_first();
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < my_tiles; i++) {
+      const int s = (int)(i % ST);
+      if (i >= (uint64_t)ST &&
+          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+        atomicExch(a.err, DEV_TIMEOUT_TMA);
+        break;
+      }
+      const uint64_t t = blockIdx.x + i * G;
+      mbar_expect_tx(&full[s], a.tile_bytes);
+      bulk_g2s_hint(ring + (size_t)s * a.tile_bytes, a.cl + t * a.tile_bytes, a.tile_bytes,
+                    &full[s], pol_db);
+      issued = i + 1;
+    }
+    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
+      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    return;
+  }
+  const int cw = warp - 1;
+  if (cw >= NC) return;
+  const uint64_t pol_occ = l2_evict_last();
+  uint32_t turn = 0;  // the consumer warp that takes the next chunk
+  for (uint64_t i = 0; i < my_tiles; i++) {
+    const int s = (int)(i % ST);
+    const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
+      return;
+    }
+    const unsigned char *tb = ring + (size_t)s * a.tile_bytes;
+    const uint64_t first = *reinterpret_cast<const uint64_t *>(tb);
+    const uint32_t nch = *reinterpret_cast<const uint32_t *>(tb + 8);
+    const unsigned char *cmax = tb + 16;
+    const unsigned char *cnt = tb + clist_cnt_offset(nch);
+    const uint32_t *base = reinterpret_cast<const uint32_t *>(tb + clist_base_offset(nch));
+    const uint32_t *spots = reinterpret_cast<const uint32_t *>(tb + clist_spot_offset(nch));
+    // chunks with a record of at least MinNrSpots spots (every chunk when
+    // gathering everything), 32 per vote; the k-th of them in the block's
+    // running order goes to consumer warp k mod NC
+    const int need = a.full_gather ? 0 : a.min_spots;
+    for (uint32_t j0 = 0; j0 < nch; j0 += 32) {
+      unsigned m = __ballot_sync(0xffffffffu, j0 + lane < nch && cmax[j0 + lane] >= need);
+      while (m) {
+        const uint32_t ch = j0 + (uint32_t)(__ffs(m) - 1);
+        m &= m - 1;
+        const bool mine = turn == (uint32_t)cw;
+        turn = (turn + 1 == (uint32_t)NC) ? 0 : turn + 1;
+        if (!mine) continue;
+        const uint64_t oid = first + ch * 32 + lane;
+        const bool valid = oid < a.n;
+        const int c = valid ? cnt[ch * 32 + lane] : 0;
+        int x = c;  // inclusive prefix sum of the counts over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        process<B>(a, ListSpots{spots + base[ch] + (x - c)}, c, oid, pol_occ, valid);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
   }
 }
 
@@ -603,6 +734,14 @@ static int counter_bits(int S) {
 CompareTuning compare_config(int R, const CompareTuning &req) {
   CompareTuning c = req;
   const size_t rb = (size_t)R * 2;
+  if (c.variant == 2) {  // compact layout: the tile shape comes with the layout
+    c.tile_sub = 0;
+    if (c.consumers <= 0) c.consumers = 16;
+    c.consumers = std::min(c.consumers, 17);
+    c.stages = c.stages > 0 ? std::max(2, std::min(c.stages, 16)) : 0;  // 0: as many as fit
+    c.blocks_per_sm = 1;
+    return c;
+  }
   if (c.variant == 1) {
     if (c.tile_sub <= 0) c.tile_sub = 8;
     while (c.tile_sub > 1 && (size_t)c.tile_sub * 32 * rb * 3 > 200 * 1024) c.tile_sub /= 2;
@@ -630,7 +769,11 @@ CompareTuning compare_config(int R, const CompareTuning &req) {
 template <int B>
 static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, size_t smem,
                     cudaStream_t st) {
-  if (c.variant == 1) {
+  if (c.variant == 2) {
+    const int rc = ensure_smem((const void *)compare_clist_kernel<B>, (int)smem);
+    if (rc) return rc;
+    compare_clist_kernel<B><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
+  } else if (c.variant == 1) {
     const int rc = ensure_smem((const void *)compare_ws_kernel<B>, (int)smem);
     if (rc) return rc;
     compare_ws_kernel<B><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
@@ -646,13 +789,28 @@ static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, siz
 int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_t st) {
   LMB_REQUIRE((reinterpret_cast<uintptr_t>(a.db) & 15) == 0,
               "DB device pointer must be 16-byte aligned");
-  const CompareTuning c = compare_config(a.R, req);
-  a.tile_sub = c.tile_sub;
+  CompareTuning c = compare_config(a.R, req);
   a.consumers = c.consumers;
-  a.tile = (uint32_t)c.tile_sub * 32;
-  a.tile_bytes = (uint32_t)((size_t)a.tile * a.R * 2);  // tile multiple of 8 -> multiple of 16
-  a.full_tiles = a.n / a.tile;
-  a.ntiles = (a.n + a.tile - 1) / a.tile;
+  if (c.variant == 2) {
+    // a.cl_tiles tiles of a.tile_bytes come from the compact layout; every
+    // tile, the last included, is one bulk copy
+    LMB_REQUIRE(a.cl && a.cl_tiles > 0 && a.tile_bytes > 0 && a.tile_bytes % 128 == 0,
+                "compact layout missing or malformed");
+    LMB_REQUIRE((reinterpret_cast<uintptr_t>(a.cl) & 127) == 0, "compact layout misaligned");
+    a.tile_sub = 0;
+    a.tile = 0;
+    a.ntiles = a.cl_tiles;
+    a.full_tiles = a.ntiles;
+    const int fit = (int)std::min<size_t>(16, (227 * 1024 - 256) / a.tile_bytes);
+    LMB_REQUIRE(fit >= 2, "compact tiles of %u bytes leave no room for a ring", a.tile_bytes);
+    c.stages = c.stages > 0 ? std::min(c.stages, fit) : fit;
+  } else {
+    a.tile_sub = c.tile_sub;
+    a.tile = (uint32_t)c.tile_sub * 32;
+    a.tile_bytes = (uint32_t)((size_t)a.tile * a.R * 2);  // tile multiple of 8 -> multiple of 16
+    a.full_tiles = a.n / a.tile;
+    a.ntiles = (a.n + a.tile - 1) / a.tile;
+  }
   a.stages = c.stages;
   if (a.ntiles == 0 || a.active == 0) return LMB_OK;
   const size_t smem = 256 + (size_t)c.stages * a.tile_bytes;

@@ -69,6 +69,12 @@ struct lmb_engine {
   // resident DB
   uint16_t *d_db = nullptr;
   uint64_t n = 0;
+  // compact layout derived from it for compare variant 2 (built on first use)
+  unsigned char *d_cl = nullptr;
+  uint64_t cl_tiles = 0;
+  uint32_t cl_stage = 0;  // bytes per tile
+  uint64_t cl_bytes = 0;
+  int cl_state = 0;  // 0 not built, 1 built, -1 this DB cannot use it
   // image slots
   uint8_t *d_u8 = nullptr;
   double *d_f64 = nullptr;  // allocated on first keep_f64 load
@@ -95,7 +101,7 @@ struct lmb_engine {
   cudaStream_t ld = nullptr;
   cudaEvent_t ev_loaded[LMB_MAX_SLOTS] = {};
   cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
-  CompareTuning tuning{1, 0, 0, 0, 0, 0};  // warp-specialised, default shape
+  CompareTuning tuning{1, 0, 0, 0, 0, 0, 0};  // warp-specialised, default shape
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
   bool sparse_uploads = true;               // frames cross the link as pairs when sparse
@@ -135,6 +141,7 @@ void free_engine(lmb_engine *e) {
   if (e->st) cudaStreamSynchronize(e->st);
   if (e->ld) cudaStreamSynchronize(e->ld);
   cudaFree(e->d_db);
+  cudaFree(e->d_cl);
   cudaFree(e->d_u8);
   cudaFree(e->d_f64);
   cudaFree(e->d_occ);
@@ -228,6 +235,11 @@ int alloc_db(lmb_engine *e, uint64_t n) {
   cudaFree(e->d_db);
   e->d_db = nullptr;
   e->n = 0;
+  cudaFree(e->d_cl);
+  e->d_cl = nullptr;
+  e->cl_tiles = 0;
+  e->cl_state = 0;
+  e->cl_bytes = 0;
   const size_t bytes = (size_t)n * e->R * 2;
   const size_t alloc = ((bytes + 255) / 256) * 256 + 256;
   LMB_CUDA(cudaMalloc(&e->d_db, alloc));
@@ -350,6 +362,85 @@ int try_sparse(lmb_engine *e, const T *px, int slot, int dtype, bool *sparse) {
 }
 
 // One pass: status reset, compare, ordering, status copy-back, on e->st.
+// Derive the compact layout of the resident DB (see clist.cu): spots per
+// 32-record chunk on the device; on the host, the tile size (about 64 chunks
+// of the DB's average size, 4-24 KiB, at least the largest chunk) and a
+// greedy packing of consecutive chunks into tiles; then the tiles on the
+// device.
+int build_compact(lmb_engine *e) {
+  e->cl_state = -1;
+  if (e->S > 255 || e->n == 0) return LMB_OK;  // counts are uint8
+  const uint64_t n = e->n, nch = (n + 31) / 32;
+  uint32_t *d_aux = nullptr;  // chunk spots, then 4 arrays of the packing
+  LMB_CUDA(cudaMalloc(&d_aux, nch * 4 * 4));
+  std::vector<uint32_t> cs(nch);
+  int rc = clist_chunk_launch(e->d_db, n, e->R, e->S, e->geo.nr_px_x, e->geo.nr_px_y, d_aux,
+                              e->st);
+  cudaError_t ce = cudaSuccess;
+  if (rc == LMB_OK) ce = cudaMemcpyAsync(cs.data(), d_aux, nch * 4, cudaMemcpyDeviceToHost, e->st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
+  if (rc || ce != cudaSuccess) {
+    cudaFree(d_aux);
+    return rc ? rc : cuda_fail(ce, "compact layout: chunk counts", __FILE__, __LINE__);
+  }
+  uint64_t total_spots = 0, max_spots = 0;
+  for (uint64_t c = 0; c < nch; c++) {
+    total_spots += cs[c];
+    max_spots = std::max<uint64_t>(max_spots, cs[c]);
+  }
+  auto round128 = [](uint64_t b) { return ((b + 127) / 128) * 128; };
+  const uint64_t avg_chunk = 36 + (4 * total_spots + nch - 1) / nch;
+  uint64_t TB = std::min<uint64_t>(24 * 1024, std::max<uint64_t>(4096, round128(64 * avg_chunk)));
+  TB = std::max<uint64_t>(TB, round128(clist_spot_offset(1) + 4 * max_spots));
+  if (2 * TB + 256 > 227 * 1024) {  // a huge S with dense records: keep the reference layout
+    cudaFree(d_aux);
+    return LMB_OK;
+  }
+  // greedy packing: chunk c into the current tile while it still fits
+  std::vector<uint32_t> ctile(nch), cpos(nch), cbase(nch), tnch;
+  uint32_t nt_chunks = 0;
+  uint64_t t_spots = 0;
+  for (uint64_t c = 0; c < nch; c++) {
+    if (nt_chunks && clist_spot_offset(nt_chunks + 1) + 4 * (t_spots + cs[c]) > TB) {
+      tnch.push_back(nt_chunks);
+      nt_chunks = 0;
+      t_spots = 0;
+    }
+    ctile[c] = (uint32_t)tnch.size();
+    cpos[c] = nt_chunks;
+    cbase[c] = (uint32_t)t_spots;
+    nt_chunks++;
+    t_spots += cs[c];
+  }
+  tnch.push_back(nt_chunks);
+  const uint64_t nt = tnch.size();
+  const uint64_t total = nt * TB;
+  uint32_t *d_tnch = nullptr;
+  ce = cudaMemcpy(d_aux + nch, ctile.data(), nch * 4, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemcpy(d_aux + 2 * nch, cpos.data(), nch * 4, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemcpy(d_aux + 3 * nch, cbase.data(), nch * 4, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMalloc(&d_tnch, nt * 4);
+  if (ce == cudaSuccess) ce = cudaMemcpy(d_tnch, tnch.data(), nt * 4, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_cl, total);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(e->d_cl, 0, total, e->st);
+  if (ce == cudaSuccess)
+    rc = clist_fill_launch(e->d_db, n, e->R, e->S, e->geo.nr_px_x, e->geo.nr_px_y, (uint32_t)TB,
+                           d_aux + nch, d_aux + 2 * nch, d_aux + 3 * nch, d_tnch, e->d_cl, e->st);
+  if (ce == cudaSuccess && rc == LMB_OK) ce = cudaStreamSynchronize(e->st);
+  cudaFree(d_aux);
+  cudaFree(d_tnch);
+  if (ce != cudaSuccess || rc) {
+    cudaFree(e->d_cl);
+    e->d_cl = nullptr;
+    return rc ? rc : cuda_fail(ce, "compact layout", __FILE__, __LINE__);
+  }
+  e->cl_tiles = nt;
+  e->cl_stage = (uint32_t)TB;
+  e->cl_bytes = total;
+  e->cl_state = 1;
+  return LMB_OK;
+}
+
 int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   // timing events recorded inside a captured graph must be external to be
   // observable (and timed) after each replay
@@ -381,6 +472,12 @@ int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   a.surv_cnt = e->d_status;
   a.pass_cnt = e->d_status + LMB_MAX_SLOTS;
   a.err = reinterpret_cast<int *>(e->d_status + 2 * LMB_MAX_SLOTS);
+  a.full_gather = k.tuning.full_gather;
+  if (k.tuning.variant == 2) {
+    a.cl = e->d_cl;
+    a.cl_tiles = e->cl_tiles;
+    a.tile_bytes = e->cl_stage;
+  }
   if (k.min_spots <= e->S && !std::isnan(k.min_int)) {
     const int rc = compare_launch(a, k.tuning, e->num_sms, e->st);
     if (rc) return rc;
@@ -842,6 +939,14 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   LMB_REQUIRE(value_mode == LMB_VALUE_U8 || value_mode == LMB_VALUE_F64, "unknown value mode");
   LMB_REQUIRE(value_mode == LMB_VALUE_U8 || (slot_mask & ~e->f64_mask) == 0,
               "float64 pass needs images loaded with keep_f64");
+  CompareTuning tun = e->tuning;
+  if (tun.variant == 2) {  // compact layout: derive it once per DB
+    if (e->cl_state == 0) {
+      rc = build_compact(e);
+      if (rc) return rc;
+    }
+    if (e->cl_state < 0) tun.variant = 1;  // this DB keeps the reference layout
+  }
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
     if (slot_mask >> k & 1) LMB_CUDA(cudaStreamWaitEvent(e->st, e->ev_loaded[k], 0));
   // The pass (status reset, compare, ordering, status copy-back) replays from
@@ -852,7 +957,7 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   key.min_spots = min_nr_spots;
   key.min_int = min_intensity;
   key.mode = value_mode;
-  key.tuning = e->tuning;
+  key.tuning = tun;
   PassGraph *pg = nullptr;
   for (auto &g : e->graphs)
     if (g.key == key) pg = &g;
@@ -1011,12 +1116,23 @@ int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms) {
 
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields) {
   LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
-  CompareTuning t{1, 0, 0, 0, 0, 0};
-  int32_t *dst[6] = {&t.variant, &t.tile_sub, &t.stages, &t.consumers, &t.blocks_per_sm,
-                     &t.grid_mult};
-  for (int i = 0; i < n_fields && i < 6; i++) *dst[i] = fields[i];
-  LMB_REQUIRE(t.variant == 0 || t.variant == 1, "unknown compare variant %d", t.variant);
+  CompareTuning t{1, 0, 0, 0, 0, 0, 0};
+  int32_t *dst[7] = {&t.variant, &t.tile_sub, &t.stages, &t.consumers, &t.blocks_per_sm,
+                     &t.grid_mult, &t.full_gather};
+  for (int i = 0; i < n_fields && i < 7; i++) *dst[i] = fields[i];
+  LMB_REQUIRE(t.full_gather == 0 || t.full_gather == 1, "full_gather must be 0 or 1");
+  LMB_REQUIRE(t.variant >= 0 && t.variant <= 2, "unknown compare variant %d", t.variant);
   e->tuning = t;
+  return LMB_OK;
+}
+
+int lmb_engine_layout_info(lmb_engine *e, int32_t *compact, uint64_t *compact_bytes,
+                           int32_t *tiles, int32_t *tile_bytes) {
+  LMB_REQUIRE(e, "null engine");
+  if (compact) *compact = e->cl_state;
+  if (compact_bytes) *compact_bytes = e->cl_bytes;
+  if (tiles) *tiles = (int32_t)e->cl_tiles;
+  if (tile_bytes) *tile_bytes = (int32_t)e->cl_stage;
   return LMB_OK;
 }
 
@@ -1029,9 +1145,9 @@ int lmb_engine_set_sparse_uploads(lmb_engine *e, int32_t enable) {
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields) {
   LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
   const CompareTuning c = compare_config(e->R, e->tuning);
-  const int32_t src[6] = {c.variant, c.tile_sub, c.stages, c.consumers, c.blocks_per_sm,
-                          c.grid_mult};
-  for (int i = 0; i < n_fields && i < 6; i++) fields[i] = src[i];
+  const int32_t src[7] = {c.variant, c.tile_sub, c.stages, c.consumers, c.blocks_per_sm,
+                          c.grid_mult, c.full_gather};
+  for (int i = 0; i < n_fields && i < 7; i++) fields[i] = src[i];
   return LMB_OK;
 }
 

@@ -25,6 +25,12 @@ struct CmpArgs {
   unsigned int *surv_cnt;  // [64] survivors (score != 0)
   unsigned int *pass_cnt;  // [64] orientations passing both thresholds
   int *err;                // device error word
+  // compact layout (variant 2): tile t at cl + t * tile_bytes, cl_tiles of them
+  const unsigned char *cl;
+  uint64_t cl_tiles;
+  // 0: a record with fewer spots than MinNrSpots (it cannot pass: its matched
+  // count is at most its spot count) is not gathered; 1: every spot is
+  int full_gather;
   // filled by compare_launch
   uint64_t full_tiles, ntiles;
   uint32_t tile_bytes;
@@ -36,12 +42,13 @@ struct CmpArgs {
 
 // Launch shape of the compare pass (autotuned; zero fields = defaults).
 struct CompareTuning {
-  int variant;        // 0 = block-barrier ring, 1 = warp-specialised
+  int variant;        // 0 = block-barrier ring, 1 = warp-specialised, 2 = compact layout
   int tile_sub;       // 32-orientation sub-tiles per tile
   int stages;         // ring depth
   int consumers;      // consumer warps (variant 1)
   int blocks_per_sm;  // resident blocks per SM (variant 0)
   int grid_mult;      // grid = SMs * blocks_per_sm * grid_mult
+  int full_gather;    // 1: gather every spot even of records that cannot pass
 };
 CompareTuning compare_config(int R, const CompareTuning &req);
 
@@ -89,5 +96,24 @@ int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_
 int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_t st);
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st);
 int status_reset_launch(unsigned int *d_status, uint64_t mask, cudaStream_t st);
+
+// Compact DB layout (clist.cu): on-detector spots per 32-record chunk, then
+// the fixed-size tiles from the host's packing of chunks into tiles.  Byte
+// offsets of the parts of a tile of nch chunks (after the 16-byte header and
+// the uint8 per-chunk maximum counts).
+__host__ __device__ __forceinline__ uint32_t clist_cnt_offset(uint32_t nch) {
+  return 16u + ((nch + 15u) / 16u) * 16u;
+}
+__host__ __device__ __forceinline__ uint32_t clist_base_offset(uint32_t nch) {
+  return clist_cnt_offset(nch) + 32u * nch;
+}
+__host__ __device__ __forceinline__ uint32_t clist_spot_offset(uint32_t nch) {
+  return ((clist_base_offset(nch) + 4u * nch + 15u) / 16u) * 16u;
+}
+int clist_chunk_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H,
+                       uint32_t *d_chunk_spots, cudaStream_t st);
+int clist_fill_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H, uint32_t TB,
+                      const uint32_t *d_ctile, const uint32_t *d_cpos, const uint32_t *d_cbase,
+                      const uint32_t *d_tnch, unsigned char *d_cl, cudaStream_t st);
 
 }  // namespace lmb

@@ -102,21 +102,31 @@ class Engine:
     def stream(self) -> int:
         return int(lib().lmb_engine_stream(self._h) or 0)
 
-    TUNING_FIELDS = ("variant", "tile_sub", "stages", "consumers", "blocks_per_sm", "grid_mult")
+    TUNING_FIELDS = ("variant", "tile_sub", "stages", "consumers", "blocks_per_sm", "grid_mult",
+                     "full_gather")
 
     def set_tuning(self, **kw) -> None:
-        vals = (C.c_int32 * 6)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS])
+        vals = (C.c_int32 * 7)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS])
         if "variant" not in kw:
             vals[0] = 1
-        check(lib().lmb_engine_set_tuning(self._h, vals, 6))
+        check(lib().lmb_engine_set_tuning(self._h, vals, 7))
         self._pinned_shape = True
 
     def set_sparse_uploads(self, enable: bool) -> None:
         check(lib().lmb_engine_set_sparse_uploads(self._h, int(bool(enable))))
 
+    def layout_info(self) -> dict:
+        """State of the compact device layout (compare variant 2)."""
+        st, nb = C.c_int32(0), C.c_uint64(0)
+        tr, tb = C.c_int32(0), C.c_int32(0)
+        check(lib().lmb_engine_layout_info(self._h, C.byref(st), C.byref(nb), C.byref(tr),
+                                           C.byref(tb)))
+        return {"compact": st.value, "bytes": int(nb.value), "tiles": tr.value,
+                "tile_bytes": tb.value}
+
     def get_tuning(self) -> dict:
-        vals = (C.c_int32 * 6)()
-        check(lib().lmb_engine_get_tuning(self._h, vals, 6))
+        vals = (C.c_int32 * 7)()
+        check(lib().lmb_engine_get_tuning(self._h, vals, 7))
         return dict(zip(self.TUNING_FIELDS, list(vals)))
 
     # ---- DB -------------------------------------------------------------------
@@ -208,8 +218,8 @@ class Engine:
         if b != self._shape_bucket:
             shape = lookup(self.R, b)
             if shape:
-                vals = (C.c_int32 * 6)(*[int(shape.get(f, 0)) for f in self.TUNING_FIELDS])
-                check(lib().lmb_engine_set_tuning(self._h, vals, 6))
+                vals = (C.c_int32 * 7)(*[int(shape.get(f, 0)) for f in self.TUNING_FIELDS])
+                check(lib().lmb_engine_set_tuning(self._h, vals, 7))
             self._shape_bucket = b
 
     def match(self, slots, min_nr_spots: int, min_intensity: float, value_mode: int = 0) -> None:

@@ -136,14 +136,17 @@ def test_input_dtypes_f32_u8_match_f64():
         assert np.array_equal(r[0][0], r[k][0]) and r[0][1] == r[k][1]
 
 
-def test_edge_records_partial_tiles_and_thresholds():
+@pytest.mark.parametrize("variant,full_gather", [(1, 0), (1, 1), (2, 0), (2, 1)])
+def test_edge_records_partial_tiles_and_thresholds(variant, full_gather):
     """Counts above S (clamped), pixels off the detector (skipped), DB sizes
-    that are not a multiple of the tile, MinNrSpots <= 0 and > S."""
+    that are not a multiple of the tile, MinNrSpots <= 0 and > S; in the
+    reference layout (variant 1) and the compact one (variant 2), with and
+    without skipping records that have fewer spots than MinNrSpots."""
     rng = np.random.default_rng(1)
     txt = synth.params_text(nr_px=(300, 200), max_nr_spots=7, min_nr_spots=2,
                             min_intensity=3.0)
     p = P.parse_params_text(txt)
-    for n in (0, 1, 7, 255, 256, 257, 1000, 4099):
+    for n in (0, 1, 7, 255, 256, 257, 1000, 4099, 70000):
         rec = np.zeros((n, 15), np.uint16)
         if n:
             rec[:, 0] = rng.integers(0, 12, n)       # some counts exceed S=7
@@ -152,6 +155,7 @@ def test_edge_records_partial_tiles_and_thresholds():
         img = np.where(rng.random(300 * 200) < 0.3, rng.integers(1, 256, 300 * 200), 0)
         img = img.astype(np.float64) * 0.77
         with engine_for(p) as e:
+            e.set_tuning(variant=variant, full_gather=full_gather)
             e.upload_db(rec)
             e.load_image(0, img)
             for ms, mi in ((2, 3.0), (0, 0.0), (-3, -1.0), (8, 0.0), (1, 1e9)):
@@ -160,6 +164,54 @@ def test_edge_records_partial_tiles_and_thresholds():
                 ref = O.compare(rec, 7, img, 300, 200, ms, mi)
                 assert npass == ref.n_pass, (n, ms, mi)
                 assert_same_survivors(got, ref)
+            if variant == 2 and n:
+                assert e.layout_info()["compact"] == 1
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("mode", [0, 1])
+def test_compact_layout_matches_oracle(name, mode):
+    """Variant 2 (compact device layout) on the reference's golden cases."""
+    c = golden_case(name)
+    p = c.params
+    ref = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                    p.min_nr_spots, p.min_intensity, mode=mode)
+    with engine_for(p) as e:
+        e.set_tuning(variant=2)
+        e.upload_db(c.records)
+        e.load_image(5, c.image, keep_f64=(mode == 1))
+        e.load_image(6, c.image * 0.5, keep_f64=(mode == 1))
+        e.match([5, 6], p.min_nr_spots, p.min_intensity, value_mode=mode)
+        got, npass = e.results(5)
+        info = e.layout_info()
+    assert info["compact"] == 1 and 0 < info["bytes"]
+    assert npass == ref.n_pass
+    assert_same_survivors(got, ref)
+
+
+def test_compact_layout_batched_equals_reference_layout():
+    """Twelve uneven frames in one pass: variant 2 == variant 1, slot by slot,
+    on a 300k-orientation device-built DB, for several tile shapes."""
+    p, hk = _batch_case()
+    rng = np.random.default_rng(5)
+    with engine_for(p) as e:
+        e.build_db_synthetic(seed=78, n=300000, hkls=hk)
+        rec = e.download_db(0, 100000)
+        for k in range(12):
+            g = synth.pick_grains(rec, int(rng.integers(1, 21)), 8, rng)
+            e.load_image(k, synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng,
+                                               threshold=None if k == 3 else 20.0))
+        e.set_tuning(variant=1)
+        e.match(range(12), p.min_nr_spots, p.min_intensity)
+        ref = e.results_batch(range(12))
+        for shape in ({}, {"consumers": 4}, {"consumers": 17, "stages": 2}, {"grid_mult": 3},
+                      {"full_gather": 1}):
+            e.set_tuning(variant=2, **shape)
+            e.match(range(12), p.min_nr_spots, p.min_intensity)
+            got = e.results_batch(range(12))
+            for k in range(12):
+                assert got[k][1] == ref[k][1] and np.array_equal(got[k][0], ref[k][0])
+        assert e.layout_info()["compact"] == 1
 
 
 def test_survivor_overflow_is_reported():
