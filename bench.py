@@ -71,59 +71,92 @@ def scratch_dir(need_bytes):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons of one GPU, sampled every ~2 ms through
+    NVML while the timed region runs (nvidia-smi's 100+ ms period would miss a
+    sub-second region; it is the fallback when NVML is unavailable).  Reads
+    only; changes no setting."""
+    REASONS = (("hw_slowdown", "HwSlowdown"), ("hw_thermal_slowdown", "HwThermalSlowdown"),
+               ("sw_thermal_slowdown", "SwThermalSlowdown"), ("sw_power_cap", "SwPowerCap"))
 
     def __init__(self, device):
         self.device = device
-        self.proc = None
-        self.lines = []
+        self.sm, self.reasons, self.mx, self.src = [], set(), None, None
+        self._stop = threading.Event()
+        self.t = None
+
+    def _nvml_index(self):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        parts = [x.strip() for x in vis.split(",") if x.strip()]
+        if parts and all(x.isdigit() for x in parts) and self.device < len(parts):
+            return int(parts[self.device])
+        return self.device
+
+    def _run_nvml(self, nv, h):
+        bits = {}
+        for name, suffix in self.REASONS:
+            v = getattr(nv, "nvmlClocksEventReason" + suffix, None)
+            if v is None:
+                v = getattr(nv, "nvmlClocksThrottleReason" + suffix, 0)
+            bits[name] = v
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = get_reasons(h)
+                for name, bit in bits.items():
+                    if bit and (r & bit):
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def _run_smi(self):
+        proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self._nvml_index()), "--query-gpu=clocks.sm,clocks.max.sm,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+             "--format=csv,noheader,nounits", "-lms", "100"],
+            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self._proc = proc
+        for line in proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 6:
+                continue
+            try:
+                self.sm.append(float(f[0]))
+                self.mx = float(f[1])
+            except ValueError:
+                continue
+            for (name, _), v in zip(self.REASONS, f[2:6]):
+                if v.lower().startswith("active"):
+                    self.reasons.add(name)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-            t0 = time.time()
-            while not self.lines and time.time() - t0 < 5:  # first sample before timing
-                time.sleep(0.02)
-            self.lines.clear()
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self._nvml_index())
+            self.mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.src = "nvml"
+            self.t = threading.Thread(target=self._run_nvml, args=(nv, h), daemon=True)
         except Exception:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.src = "nvidia-smi"
+            self.t = threading.Thread(target=self._run_smi, daemon=True)
+        self.t.start()
+        t0 = time.time()
+        while not self.sm and time.time() - t0 < 5:  # first sample before timing
+            time.sleep(0.001)
+        self.sm.clear()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.t.join(timeout=2)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        self._stop.set()
+        if self.src == "nvidia-smi" and getattr(self, "_proc", None) is not None:
+            self._proc.terminate()
+        if self.t is not None:
+            self.t.join(timeout=5)
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.mx,
+                "reasons": sorted(self.reasons), "samples": len(self.sm), "source": self.src}
 
 
 # ---------------------------------------------------------------------------
@@ -251,6 +284,8 @@ def run_ours(args, rank, world):
     slots = list(range(K))
 
     def timed(nsteps, slot_list):
+        """Passes one at a time (synchronised): per-pass step and compare-kernel
+        times, for the roofline."""
         step_ms, cmp_ms = [], []
         for _ in range(nsteps):
             a = torch.cuda.Event(enable_timing=True)
@@ -263,20 +298,32 @@ def run_ours(args, rank, world):
             cmp_ms.append(e.last_pass_ms()[0])
         return step_ms, cmp_ms
 
+    def timed_stream(nsteps, slot_list):
+        """Passes back to back as a client queues them (no host wait between
+        passes); CUDA events around each pass and around the whole run."""
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(nsteps)]
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for a, b in evs:
+            a.record(stream)
+            e.match(slot_list, p.min_nr_spots, p.min_intensity)
+            b.record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs], t0.elapsed_time(t1)
+
     timed(args.warmup, slots)
+    timed_stream(args.warmup, slots)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    step_ms, cmp_ms = timed(args.steps, slots)
-    t1.record(stream)
-    torch.cuda.synchronize()
-    total_ms = t0.elapsed_time(t1)
+    step_ms, total_ms = timed_stream(args.steps, slots)
     clk = clocks.stop()
+    _, cmp_ms = timed(min(args.steps, 200), slots)  # compare-kernel times, synchronised
     if dist:
         tt = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -287,9 +334,10 @@ def run_ours(args, rank, world):
     shape_main, lay_main = e.get_tuning(), e.layout_info()  # the timed pass's shape
 
     # ---- plain pass (one image) --------------------------------------------
-    timed(args.warmup, [0])
-    pstep, pcmp = timed(args.steps, [0])
-    plain_ips = 1e3 / statistics.mean(pstep)
+    timed_stream(args.warmup, [0])
+    pstep, ptotal = timed_stream(args.steps, [0])
+    plain_ips = args.steps / (ptotal / 1e3)
+    _, pcmp = timed(min(args.steps, 200), [0])
 
     # ---- end to end through the public API from pinned host frames ----------
     pins = []
@@ -396,9 +444,11 @@ def run_ours(args, rank, world):
     for k in range(K):
         e.load_image(k, imgs[k], want_scale=False)
     timed(args.warmup, slots)
-    fg_step, fg_cmp = timed(max(10, args.steps // 4), slots)
+    fg_n = max(10, min(args.steps, 300))
+    _, fg_total = timed_stream(fg_n, slots)
+    _, fg_cmp = timed(min(fg_n, 50), slots)
     fg_surv = [int(e.results(k)[0].shape[0]) for k in range(K)]
-    full_gather = {"value": round(K / (statistics.mean(fg_step) * 1e-3), 2), "unit": UNIT,
+    full_gather = {"value": round(K * fg_n / (fg_total * 1e-3), 2), "unit": UNIT,
                    "compare_ms": round(statistics.mean(fg_cmp), 4),
                    "same_survivor_counts": fg_surv == surv}
 
@@ -767,7 +817,7 @@ def run_serve(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours",
                     help="reference: the reference's CPU path; reference-gpu: its plain "

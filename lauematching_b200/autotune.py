@@ -53,8 +53,11 @@ def lookup(R: int, k: int) -> dict | None:
 
 def candidate_shapes():
     # compact layout: the tile comes with the layout; ring depth 0 = as deep as fits
-    for cons, st, gm in itertools.product((8, 12, 16, 17), (0, 4, 8), (1, 2)):
+    # several small blocks per SM (each its own producer and ring) beat one big one
+    for cons, st, gm in itertools.product((2, 3, 4, 6, 8), (2, 3, 4), (2, 3, 4, 5, 6, 8)):
         yield dict(variant=2, stages=st, consumers=cons, grid_mult=gm)
+    for cons, st in itertools.product((8, 16), (0, 8)):
+        yield dict(variant=2, stages=st, consumers=cons, grid_mult=1)
     for ts, st, cons in itertools.product((4, 8), (4, 6, 8, 12), (8, 12, 16)):
         yield dict(variant=1, tile_sub=ts, stages=st, consumers=cons)
     for ts, st, bps in itertools.product((4, 8), (2, 3, 4), (1, 2, 3)):
