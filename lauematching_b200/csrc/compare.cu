@@ -249,6 +249,8 @@ int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_
 
 
 static constexpr uint64_t kWaitNs = 2000000000ull;  // bounded TMA waits: 2 s
+static constexpr int kGather = 8;                    // spots gathered per group
+static constexpr int kSumGroup = 4;                  // pixel values loaded per group
 
 // The spots of one orientation, in record order, as detector pixel indices.
 // RecSpots reads the reference record ({count, x0, y0, ...}) and skips
@@ -282,22 +284,33 @@ __device__ __noinline__ int slot_sum(const CmpArgs &a, const Spots sp, int c, in
   const double sc = a.scale[k];
   int ns = 0, su = 0;
   double tot = 0.0;
-  for (int s = 0; s < c; s++) {
-    size_t p;
-    if (!sp.pixel(a, s, p)) continue;
-    const uint8_t raw = img[p];
-    if (a.mode == LMB_VALUE_U8) {
-      if (raw > 0) {
-        tot = dadd(tot, dmul((double)raw, sc));
-        ns++;
-        su += raw;
+  // pixel values loaded kSumGroup at a time (independent loads in flight
+  // together), then summed strictly in record order
+  for (int s0 = 0; s0 < c; s0 += kSumGroup) {
+    uint8_t raw[kSumGroup];
+    double fv[kSumGroup];
+#pragma unroll
+    for (int j = 0; j < kSumGroup; j++) {
+      raw[j] = 0;
+      fv[j] = 0.0;
+      size_t p;
+      if (s0 + j < c && sp.pixel(a, s0 + j, p)) {
+        raw[j] = img[p];
+        if (a.mode != LMB_VALUE_U8) fv[j] = fim[p];
       }
-    } else {
-      const double v = fim[p];
-      if (v > 0) {
-        tot = dadd(tot, v);
+    }
+#pragma unroll
+    for (int j = 0; j < kSumGroup; j++) {
+      if (a.mode == LMB_VALUE_U8) {
+        if (raw[j] > 0) {
+          tot = dadd(tot, dmul((double)raw[j], sc));
+          ns++;
+          su += raw[j];
+        }
+      } else if (fv[j] > 0) {
+        tot = dadd(tot, fv[j]);
         ns++;
-        su += raw;
+        su += raw[j];
       }
     }
   }
@@ -320,18 +333,18 @@ __device__ __forceinline__ void process(const CmpArgs &a, const Spots sp, int c,
   unsigned long long cnt[B];
 #pragma unroll
   for (int b = 0; b < B; b++) cnt[b] = 0ull;
-  // gathers issued four at a time so their L2 latencies overlap
-  for (int s0 = 0; s0 < c; s0 += 4) {
-    unsigned long long m[4];
+  // gathers issued kGather at a time so their L2 latencies overlap
+  for (int s0 = 0; s0 < c; s0 += kGather) {
+    unsigned long long m[kGather];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < kGather; j++) {
       m[j] = 0ull;
       const int s = s0 + j;
       size_t p;
       if (s < c && sp.pixel(a, s, p)) m[j] = ld_nc_hint(a.occ + p, pol);
     }
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < kGather; j++) {
       unsigned long long v = m[j] & a.active;
       if (v) {
 #pragma unroll
@@ -841,6 +854,27 @@ __global__ void status_reset_kernel(unsigned int *__restrict__ status, unsigned 
 
 int status_reset_launch(unsigned int *d_status, uint64_t mask, cudaStream_t st) {
   status_reset_kernel<<<1, LMB_MAX_SLOTS, 0, st>>>(d_status, (unsigned long long)mask);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+// blockIdx.y = position in the slot list; 16-byte words of the 32-byte survivors.
+__global__ void gather_kernel(const __grid_constant__ GatherArgs g) {
+  const int i = blockIdx.y;
+  const uint32_t cnt = g.off[i + 1] - g.off[i];
+  const uint4 *src = reinterpret_cast<const uint4 *>(g.src + (size_t)g.slot[i] * g.cap);
+  uint4 *dst = reinterpret_cast<uint4 *>(g.dst + g.off[i]);
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < 2 * cnt; w += gridDim.x * blockDim.x)
+    dst[w] = src[w];
+}
+
+int gather_launch(const GatherArgs &g, cudaStream_t st) {
+  if (g.n <= 0) return LMB_OK;
+  LMB_REQUIRE(g.n <= LMB_MAX_SLOTS, "gather of %d lists", g.n);
+  uint32_t mx = 0;
+  for (int i = 0; i < g.n; i++) mx = std::max(mx, g.off[i + 1] - g.off[i]);
+  const unsigned bx = std::max(1u, std::min(64u, (2 * mx + 255) / 256));
+  gather_kernel<<<dim3(bx, g.n), 256, 0, st>>>(g);
   LMB_CUDA(cudaGetLastError());
   return LMB_OK;
 }

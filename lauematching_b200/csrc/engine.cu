@@ -122,6 +122,9 @@ struct lmb_engine {
   int bt_next = 0;
   void *d_batch = nullptr;
   size_t d_batch_cap = 0;
+  // survivors of a batch of slots packed for one device-to-host copy
+  lmb_survivor *d_gather = nullptr;
+  uint64_t d_gather_cap = 0;
 };
 
 namespace {
@@ -172,6 +175,7 @@ void free_engine(lmb_engine *e) {
     if (e->bt_ev[i]) cudaEventDestroy(e->bt_ev[i]);
   }
   cudaFree(e->d_batch);
+  cudaFree(e->d_gather);
   for (auto &v : e->ev)
     if (v) cudaEventDestroy(v);
   for (int k = 0; k < LMB_MAX_SLOTS; k++) {
@@ -1080,16 +1084,41 @@ int lmb_results_batch(lmb_engine *e, const int32_t *slots, int32_t nslots, lmb_s
               (unsigned long long)out_capacity);
     return LMB_ERR_OVERFLOW;
   }
-  // the survivor lists are final (their passes' events have completed); copy
-  // them on the download stream so a pass queued meanwhile keeps running
-  uint64_t off = 0;
-  for (int i = 0; i < nslots; i++) {
-    if (counts[i])
-      LMB_CUDA(cudaMemcpyAsync(out + off, e->d_sorted + (size_t)slots[i] * e->cap,
-                               counts[i] * sizeof(lmb_survivor), cudaMemcpyDeviceToHost, e->dl));
-    off += counts[i];
+  // the survivor lists are final (their passes' events have completed): pack
+  // them back to back on the device and copy once, on the download stream so
+  // a pass queued meanwhile keeps running
+  if (total) {
+    if (e->d_gather_cap < total) {
+      LMB_CUDA(cudaStreamSynchronize(e->dl));
+      cudaFree(e->d_gather);
+      e->d_gather = nullptr;
+      e->d_gather_cap = 0;
+      const uint64_t want = std::max<uint64_t>(total + total / 4, 4096);
+      LMB_CUDA(cudaMalloc(&e->d_gather, want * sizeof(lmb_survivor)));
+      e->d_gather_cap = want;
+    }
+    GatherArgs g{};
+    g.src = e->d_sorted;
+    g.dst = e->d_gather;
+    g.cap = e->cap;
+    uint64_t off = 0;
+    for (int i0 = 0; i0 < nslots; i0 += LMB_MAX_SLOTS) {  // at most 64 lists per launch
+      const uint64_t base = off;
+      g.dst = e->d_gather + base;
+      g.n = std::min(LMB_MAX_SLOTS, nslots - i0);
+      g.off[0] = 0;
+      for (int i = 0; i < g.n; i++) {
+        g.slot[i] = slots[i0 + i];
+        g.off[i + 1] = g.off[i] + (uint32_t)counts[i0 + i];
+      }
+      off = base + g.off[g.n];
+      rc = gather_launch(g, e->dl);
+      if (rc) return rc;
+    }
+    LMB_CUDA(cudaMemcpyAsync(out, e->d_gather, total * sizeof(lmb_survivor),
+                             cudaMemcpyDeviceToHost, e->dl));
+    LMB_CUDA(cudaStreamSynchronize(e->dl));
   }
-  LMB_CUDA(cudaStreamSynchronize(e->dl));
   e->bytes_d2h += total * sizeof(lmb_survivor);
   return LMB_OK;
 }

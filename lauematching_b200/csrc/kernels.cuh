@@ -95,6 +95,18 @@ int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_
                              cudaStream_t st);
 int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_t st);
 int order_launch(const OrderArgs &a, int nslots, cudaStream_t st);
+
+// Survivor lists of several slots packed back to back (slot i's list at
+// off[i]) for one device-to-host copy.
+struct GatherArgs {
+  const lmb_survivor *src;  // slot k's sorted list at src + k*cap
+  lmb_survivor *dst;
+  uint32_t cap;
+  int n;
+  int slot[LMB_MAX_SLOTS];
+  uint32_t off[LMB_MAX_SLOTS + 1];
+};
+int gather_launch(const GatherArgs &g, cudaStream_t st);
 int status_reset_launch(unsigned int *d_status, uint64_t mask, cudaStream_t st);
 
 // Compact DB layout (clist.cu): on-detector spots per 32-record chunk, then

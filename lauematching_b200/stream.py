@@ -76,7 +76,9 @@ class Geometry:
     engine: object
     free: list = field(default_factory=list)
     loaded: list = field(default_factory=list)  # (slot, Request) uploaded, waiting for a pass
-    inflight: list = field(default_factory=list)  # (slot, Request) in the running pass
+    # passes on the device, oldest first, each a list of (slot, Request); a
+    # second pass queues behind the running one while its results are read
+    inflight: collections.deque = field(default_factory=collections.deque)
 
 
 def _recv_exact(sock, buf, running):
@@ -245,27 +247,30 @@ class StreamServer:
                 break
             # admit arrivals into free slots (uploads overlap the running pass)
             admitted = self._admit(block=idle)
-            # start a pass on every geometry with uploaded images and none running
+            # start a pass over the uploaded images of every geometry; with one
+            # pass already on the device the new one queues behind it
             for g in self.geoms.values():
-                if g.loaded and not g.inflight:
-                    g.inflight, g.loaded = g.loaded, []
+                if g.loaded and len(g.inflight) < 2:
+                    batch, g.loaded = g.loaded, []
                     p = g.params
-                    g.engine.match([s for s, _ in g.inflight], p.min_nr_spots, p.min_intensity)
+                    g.engine.match([s for s, _ in batch], p.min_nr_spots, p.min_intensity)
+                    g.inflight.append(batch)
                     self.passes += 1
-                    self.batch_sizes.append(len(g.inflight))
+                    self.batch_sizes.append(len(batch))
             if not admitted:
                 self._admit(block=False)
-            # collect the passes (sync), free their slots
+            # collect the oldest pass of each geometry (waits for it; a pass
+            # queued behind it keeps the device busy meanwhile), free its slots
             for g in self.geoms.values():
                 if not g.inflight:
                     continue
-                res = g.engine.results_batch([s for s, _ in g.inflight])
+                batch = g.inflight.popleft()
+                res = g.engine.results_batch([s for s, _ in batch])
                 t = time.perf_counter()
-                for s, r in g.inflight:
+                for s, r in batch:
                     surv, npass = res[s]
                     self.done_q.put(Done(r, surv, npass, t))
                     g.free.append(s)
-                g.inflight = []
         self.done_q.put(None)
 
     def _admit(self, block):
