@@ -127,6 +127,14 @@ int lmb_engine_layout_info(lmb_engine *e, int32_t *compact, uint64_t *compact_by
  * (the reference copies the dense float frame, LaueMatchingGPUStream.cu:1204). */
 int lmb_engine_set_sparse_uploads(lmb_engine *e, int32_t enable);
 
+/* Share (0..1) of the page-locked frames of an lmb_image_load_batch call that
+ * are sent dense over the copy engine, enqueued first so that they cross the
+ * link while the host scans the others (results are identical either way).
+ * Default 0.33: the host scan (~120 GB/s over 16 threads) and the copy engine
+ * (~50 GB/s) then finish a batch of 4 MiB frames at about the same time.
+ * No reference counterpart. */
+int lmb_engine_set_dense_share(lmb_engine *e, double share);
+
 /* Upload a forward cache (n records of 1+2S uint16) into device memory.
  * Replaces the chunked synchronous H2D of LaueMatchingGPU.cu:619-749 and
  * the resident upload of LaueMatchingGPUStream.cu:998-1038. */

@@ -29,6 +29,7 @@ EXPORTS = [
     "lmb_version", "lmb_last_error", "lmb_device_info", "lmb_geometry_init", "lmb_engine_create",
     "lmb_engine_destroy", "lmb_engine_stream", "lmb_engine_set_tuning",
     "lmb_engine_get_tuning", "lmb_engine_layout_info", "lmb_engine_set_sparse_uploads",
+    "lmb_engine_set_dense_share",
     "lmb_db_upload", "lmb_db_build",
     "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
     "lmb_image_load_batch",
@@ -107,6 +108,7 @@ def lib():
         "lmb_engine_layout_info": ([vp, C.POINTER(i32), C.POINTER(u64), C.POINTER(i32),
                                     C.POINTER(i32)], C.c_int),
         "lmb_engine_set_sparse_uploads": ([vp, i32], C.c_int),
+        "lmb_engine_set_dense_share": ([vp, dbl], C.c_int),
         "lmb_db_upload": ([vp, vp, u64], C.c_int),
         "lmb_db_build": ([vp, vp, u64, vp, i32], C.c_int),
         "lmb_db_build_ex": ([vp, vp, u64, vp, i32, C.c_uint32], C.c_int),

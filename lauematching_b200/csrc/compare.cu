@@ -251,6 +251,8 @@ int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_
 static constexpr uint64_t kWaitNs = 2000000000ull;  // bounded TMA waits: 2 s
 static constexpr int kGather = 8;                    // spots gathered per group
 static constexpr int kSumGroup = 4;                  // pixel values loaded per group
+static constexpr int kDirect = 16;  // compact pass: a chunk with this many passable records is
+                                    // counted in place, one with fewer goes through the queue
 
 // The spots of one orientation, in record order, as detector pixel indices.
 // RecSpots reads the reference record ({count, x0, y0, ...}) and skips
@@ -621,6 +623,23 @@ __global__ void __launch_bounds__(576, 1) compare_clist_kernel(const __grid_cons
   const int cw = warp - 1;
   if (cw >= NC) return;
   const uint64_t pol_occ = l2_evict_last();
+  // This warp's queue of records that can pass, copied out of the ring (id,
+  // count, pixel indices at an odd stride): a chunk with few of them feeds the
+  // queue, and the queue is counted 32 records at a time on a full warp.
+  const uint32_t SP = clist_queue_stride(a.S);
+  unsigned char *qb = ring + (size_t)ST * a.tile_bytes + (size_t)cw * clist_queue_bytes(a.S);
+  uint64_t *q_oid = reinterpret_cast<uint64_t *>(qb);
+  uint32_t *q_c = reinterpret_cast<uint32_t *>(qb + 256);
+  uint32_t *q_sp = reinterpret_cast<uint32_t *>(qb + 384);
+  int qn = 0;
+  auto flush = [&]() {
+    __syncwarp();
+    const bool v = lane < qn;
+    process<B>(a, ListSpots{q_sp + lane * SP}, v ? (int)q_c[lane] : 0, v ? q_oid[lane] : 0,
+               pol_occ, v);
+    __syncwarp();
+    qn = 0;
+  };
   uint32_t turn = 0;  // the consumer warp that takes the next chunk
   for (uint64_t i = 0; i < my_tiles; i++) {
     const int s = (int)(i % ST);
@@ -657,12 +676,32 @@ __global__ void __launch_bounds__(576, 1) compare_clist_kernel(const __grid_cons
           const int y = __shfl_up_sync(0xffffffffu, x, o);
           if (lane >= o) x += y;
         }
-        process<B>(a, ListSpots{spots + base[ch] + (x - c)}, c, oid, pol_occ, valid);
+        const uint32_t *my = spots + base[ch] + (x - c);
+        unsigned qm = __ballot_sync(0xffffffffu, valid && c >= need);
+        if (__popc(qm) >= kDirect) {  // many can pass: count the chunk in place
+          process<B>(a, ListSpots{my}, c, oid, pol_occ, valid);
+          continue;
+        }
+        while (qm) {  // into the queue, emptying it whenever it fills
+          unsigned rest = qm;
+          for (int r = 32 - qn; r > 0 && rest; r--) rest &= rest - 1;
+          const unsigned take = qm & ~rest;
+          if ((take >> lane) & 1u) {
+            const int pos = qn + __popc(take & ((1u << lane) - 1u));
+            q_oid[pos] = oid;
+            q_c[pos] = (uint32_t)c;
+            for (int k = 0; k < c; k++) q_sp[pos * SP + k] = my[k];
+          }
+          qn += __popc(take);
+          qm = rest;
+          if (qn == 32) flush();
+        }
       }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
+  if (qn) flush();
 }
 
 // ----------------------------------------------------------------------------
@@ -814,7 +853,9 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
     a.tile = 0;
     a.ntiles = a.cl_tiles;
     a.full_tiles = a.ntiles;
-    const int fit = (int)std::min<size_t>(16, (227 * 1024 - 256) / a.tile_bytes);
+    const size_t qbytes = (size_t)c.consumers * clist_queue_bytes(a.S);
+    const size_t room = 227 * 1024 > 256 + qbytes ? 227 * 1024 - 256 - qbytes : 0;
+    const int fit = (int)std::min<size_t>(16, room / a.tile_bytes);
     LMB_REQUIRE(fit >= 2, "compact tiles of %u bytes leave no room for a ring", a.tile_bytes);
     c.stages = c.stages > 0 ? std::min(c.stages, fit) : fit;
   } else {
@@ -826,7 +867,8 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   }
   a.stages = c.stages;
   if (a.ntiles == 0 || a.active == 0) return LMB_OK;
-  const size_t smem = 256 + (size_t)c.stages * a.tile_bytes;
+  size_t smem = 256 + (size_t)c.stages * a.tile_bytes;
+  if (c.variant == 2) smem += (size_t)c.consumers * clist_queue_bytes(a.S);
   LMB_REQUIRE(smem <= 227 * 1024, "compare ring of %zu bytes exceeds shared memory", smem);
   const int mult = c.grid_mult > 0 ? c.grid_mult : 1;
   const unsigned grid = (unsigned)std::min<uint64_t>(

@@ -105,6 +105,7 @@ struct lmb_engine {
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
   bool sparse_uploads = true;               // frames cross the link as pairs when sparse
+  double dense_share = 0.33;                // of page-locked frames in a batch, sent dense
   void *sp_host[kSparseRing] = {};          // pinned (index, value) staging ring (lazy)
   cudaEvent_t sp_ev[kSparseRing] = {};
   int sp_next = 0;
@@ -765,6 +766,23 @@ int lmb_image_load(lmb_engine *e, int32_t slot, const void *pixels, int32_t dtyp
 
 namespace {
 
+// One frame the dense way (copy of the whole frame, max + quantise kernels)
+// on the load stream, without a host scan.
+int dense_load(lmb_engine *e, int slot, const void *pixels, int dtype) {
+  LMB_CUDA(cudaStreamWaitEvent(e->ld, e->ev_released[slot], 0));
+  const size_t bytes = e->npx * dtype_bytes(dtype);
+  LMB_CUDA(cudaMemcpyAsync(e->d_stage, pixels, bytes, cudaMemcpyHostToDevice, e->ld));
+  e->bytes_h2d += bytes;
+  const int rc = quantize_launch(e->d_stage, dtype, e->npx, e->d_max_bits,
+                                 e->d_u8 + (size_t)slot * e->npx, nullptr, e->d_occ, slot,
+                                 e->d_scale + slot, e->num_sms, e->ld);
+  if (rc) return rc;
+  LMB_CUDA(cudaEventRecord(e->ev_loaded[slot], e->ld));
+  e->loaded_mask |= 1ull << slot;
+  e->f64_mask &= ~(1ull << slot);
+  return LMB_OK;
+}
+
 template <typename T>
 int load_batch_sparse(lmb_engine *e, const int32_t *slots, const void *const *frames,
                              int n, int dtype) {
@@ -772,7 +790,8 @@ int load_batch_sparse(lmb_engine *e, const int32_t *slots, const void *const *fr
   const size_t limit = npx * vb / (2 * (4 + vb));
   const size_t capf = std::max<size_t>(1, std::min(limit, npx / 64 + 1));
   const int nt = std::max(1, std::min(16, omp_get_num_procs()));
-  const int nseg = std::max(1, std::min((nt + n - 1) / n, (int)(npx / 4096) + 1));
+  // about four tasks per thread, so the dynamic schedule evens out the threads
+  const int nseg = std::max(1, std::min((4 * nt + n - 1) / n, (int)(npx / 4096) + 1));
   const int ntask = n * nseg;
   if (e->bt_idx.size() < (size_t)ntask * capf) e->bt_idx.resize((size_t)ntask * capf);
   if (e->bt_val.size() < (size_t)ntask * capf * vb) e->bt_val.resize((size_t)ntask * capf * vb);
@@ -919,9 +938,38 @@ int lmb_image_load_batch(lmb_engine *e, const int32_t *slots, const void *const 
     for (int i = 0; i < n && rc == LMB_OK; i++)
       rc = lmb_image_load(e, slots[i], frames[i], dtype, 0, nullptr);
   } else if (n) {
-    rc = dtype == LMB_F64   ? load_batch_sparse<double>(e, slots, frames, n, dtype)
-         : dtype == LMB_F32 ? load_batch_sparse<float>(e, slots, frames, n, dtype)
-                            : load_batch_sparse<uint8_t>(e, slots, frames, n, dtype);
+    // A share of the page-locked frames goes dense over the copy engine
+    // (asynchronous: enqueued first, it runs while the host scans the rest),
+    // so the host's memory reads and the link work side by side.
+    int32_t ss[LMB_MAX_SLOTS];
+    const void *sf[LMB_MAX_SLOTS];
+    int ns = 0;
+    double acc = 0.0;
+    for (int i = 0; i < n && rc == LMB_OK; i++) {
+      bool dense = false;
+      if (e->dense_share > 0.0) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, frames[i]) == cudaSuccess &&
+            at.type == cudaMemoryTypeHost) {
+          acc += e->dense_share;
+          if (acc >= 1.0) {
+            acc -= 1.0;
+            dense = true;
+          }
+        }
+        cudaGetLastError();  // a pageable pointer is not an error here
+      }
+      if (dense) {
+        rc = dense_load(e, slots[i], frames[i], dtype);
+      } else {
+        ss[ns] = slots[i];
+        sf[ns++] = frames[i];
+      }
+    }
+    if (rc == LMB_OK && ns)
+      rc = dtype == LMB_F64   ? load_batch_sparse<double>(e, ss, sf, ns, dtype)
+           : dtype == LMB_F32 ? load_batch_sparse<float>(e, ss, sf, ns, dtype)
+                              : load_batch_sparse<uint8_t>(e, ss, sf, ns, dtype);
   }
   if (rc) return rc;
   if (im_scales && n) {
@@ -1162,6 +1210,13 @@ int lmb_engine_layout_info(lmb_engine *e, int32_t *compact, uint64_t *compact_by
   if (compact_bytes) *compact_bytes = e->cl_bytes;
   if (tiles) *tiles = (int32_t)e->cl_tiles;
   if (tile_bytes) *tile_bytes = (int32_t)e->cl_stage;
+  return LMB_OK;
+}
+
+int lmb_engine_set_dense_share(lmb_engine *e, double share) {
+  LMB_REQUIRE(e, "null engine");
+  LMB_REQUIRE(share >= 0.0 && share <= 1.0, "dense share %g outside [0, 1]", share);
+  e->dense_share = share;
   return LMB_OK;
 }
 

@@ -122,6 +122,15 @@ __host__ __device__ __forceinline__ uint32_t clist_base_offset(uint32_t nch) {
 __host__ __device__ __forceinline__ uint32_t clist_spot_offset(uint32_t nch) {
   return ((clist_base_offset(nch) + 4u * nch + 15u) / 16u) * 16u;
 }
+// Per consumer warp of the compact pass, a shared-memory queue of 32 records:
+// uint64 id[32] | uint32 count[32] | uint32 pixel[32][stride], stride = S
+// rounded up to odd (conflict-free lane-strided reads).
+__host__ __device__ __forceinline__ uint32_t clist_queue_stride(int S) {
+  return (uint32_t)(S < 1 ? 1 : S) | 1u;
+}
+__host__ __device__ __forceinline__ uint32_t clist_queue_bytes(int S) {
+  return 384u + 128u * clist_queue_stride(S);
+}
 int clist_chunk_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H,
                        uint32_t *d_chunk_spots, cudaStream_t st);
 int clist_fill_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H, uint32_t TB,

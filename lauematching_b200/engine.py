@@ -115,6 +115,11 @@ class Engine:
     def set_sparse_uploads(self, enable: bool) -> None:
         check(lib().lmb_engine_set_sparse_uploads(self._h, int(bool(enable))))
 
+    def set_dense_share(self, share: float) -> None:
+        """Share of the page-locked frames of a load_images call sent dense
+        over the copy engine while the host scans the others."""
+        check(lib().lmb_engine_set_dense_share(self._h, float(share)))
+
     def layout_info(self) -> dict:
         """State of the compact device layout (compare variant 2)."""
         st, nb = C.c_int32(0), C.c_uint64(0)

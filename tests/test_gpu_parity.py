@@ -308,6 +308,45 @@ def test_batched_frame_loads_equal_single_loads(dtype):
             e.load_images([3, 3], frames[:2])
 
 
+@pytest.mark.parametrize("share", [0.0, 0.34, 1.0])
+def test_dense_share_of_pinned_frames_gives_same_results(share):
+    """Pinned frames sent dense over the copy engine (a share of each batch)
+    while the host scans the rest: same survivors as single loads."""
+    from lauematching_b200.engine import PinnedBuffer
+    c = golden_case("tilted_fcc")
+    p = c.params
+    npx = p.nr_px_x * p.nr_px_y
+    rng = np.random.default_rng(12)
+    frames = []
+    for k in range(6):
+        img = synth.render_image(c.records[rng.choice(np.nonzero(c.records[:, 0] >= 8)[0], 3)],
+                                 p.nr_px_x, p.nr_px_y, rng)
+        frames.append(np.clip(img, 0, 255).astype(np.uint8))
+    pins = []
+    for f in frames:
+        pb = PinnedBuffer((npx,), np.uint8)
+        pb.array[:] = f.ravel()
+        pins.append(pb)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        singles = []
+        for f in frames:
+            e.load_image(0, f)
+            e.match([0], p.min_nr_spots, p.min_intensity)
+            singles.append(e.results(0))
+        e.set_dense_share(share)
+        for rep in range(2):  # slots reloaded: previous content replaced either way
+            order = list(range(6))[::-1] if rep else list(range(6))
+            e.load_images(list(range(10, 16)), [pins[k].array for k in order])
+            e.match(range(10, 16), p.min_nr_spots, p.min_intensity)
+            got = e.results_batch(range(10, 16))
+            for i, k in enumerate(order):
+                assert got[10 + i][1] == singles[k][1]
+                assert np.array_equal(got[10 + i][0], singles[k][0])
+    for pb in pins:
+        pb.free()
+
+
 def test_queued_passes_keep_each_slots_results():
     """A pass over other slots queued before the previous pass's results are
     read leaves those results intact; a slot's results are those of the last
