@@ -249,7 +249,7 @@ def cpu_baseline(e, p, txt, hkls, img_u8, seed, n_sample, runs=3):
 # scales them to N.
 TRAFFIC_BYTES_PER_ORIENT = {
     "reference": 271.1e6 / 2_000_000,  # compare_ws_kernel, 2M orientations, K=16
-    "compact": 204.6e6 / 30_000_000,   # compare_clist_kernel, 30M orientations, K=64
+    "compact": 205.6e6 / 30_000_000,   # compare_clist_kernel, 30M orientations, K=64
 }
 
 
