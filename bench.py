@@ -253,6 +253,38 @@ TRAFFIC_BYTES_PER_ORIENT = {
 }
 
 
+def merge_timing(space_group, max_angle, device, n_base=800, per=12, seed=5):
+    """The duplicate merge of ~1e4 candidates (near-duplicate families: base
+    orientations and copies rotated by up to 4 degrees, shuffled): host loop
+    (the reference's algorithm, all host threads) against the device merge."""
+    from lauematching_b200 import post, synth
+    rng = np.random.default_rng(seed)
+    base = synth.shoemake_orientations(n_base, seed=seed).reshape(-1, 3, 3)
+    om = []
+    for b in base:
+        om.append(b)
+        for _ in range(per - 1):
+            ax = rng.normal(size=3)
+            ax /= np.linalg.norm(ax)
+            ang = np.deg2rad(rng.uniform(0, 4.0))
+            k = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+            om.append((np.eye(3) + np.sin(ang) * k + (1 - np.cos(ang)) * (k @ k)) @ b)
+    om = np.array(om).reshape(-1, 9)[rng.permutation(n_base * per)]
+    rows = np.arange(om.shape[0], dtype=np.uint64)
+    scores = rng.integers(1, 40, om.shape[0]).astype(np.float64) * 3.5
+    post.merge_clusters(space_group, max_angle, om, rows[:2048], scores[:2048], device=device)
+    t0 = time.perf_counter()
+    dev = post.merge_clusters(space_group, max_angle, om, rows, scores, device=device)
+    t_dev = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    host = post.merge_clusters(space_group, max_angle, om, rows, scores)
+    t_host = time.perf_counter() - t0
+    same = all(np.array_equal(a, b) for a, b in zip(host, dev))
+    return {"candidates": int(om.shape[0]), "clusters": int(host[0].shape[0]),
+            "host_ms": round(t_host * 1e3, 1), "host_threads": os.cpu_count(),
+            "device_ms": round(t_dev * 1e3, 2), "identical": same}
+
+
 def run_ours(args, rank, world):
     import torch
     from lauematching_b200 import synth
@@ -453,6 +485,8 @@ def run_ours(args, rank, world):
                    "compare_ms": round(statistics.mean(fg_cmp), 4),
                    "same_survivor_counts": fg_surv == surv}
 
+    merge = merge_timing(p.space_group, p.max_angle, dev) if rank == 0 else None
+
     # ---- roofline of the compare kernel ----------------------------------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
@@ -527,6 +561,7 @@ def run_ours(args, rank, world):
                   "compare_ms": round(statistics.mean(pcmp), 4)},
         "batched_over_plain": round(value / world / plain_ips, 2),
         "full_gather": full_gather,
+        "merge": merge,
         "survivors_per_image": {"min": min(surv), "max": max(surv), "mean": statistics.mean(surv)},
         "dbbuild": {"orientations_per_s": round(N / t_build, 1), "seconds": round(t_build, 3),
                     "hkl_evals_per_s": round(N * len(hkls) / t_build, 1)},

@@ -249,7 +249,9 @@ typedef struct lmb_post_params {
   int32_t optimizer;     /* 0 = evaluate once */
   int32_t max_results;   /* candidates kept for the merge, top by score;
                             0 = the reference's cap MERGE_MAX_RESULTS 50000 */
-  int32_t reserved;
+  int32_t merge_on_device; /* k > 0: for 1024 or more candidates, the duplicate merge's
+                              pair matrix and greedy pass run on CUDA device k-1 (same
+                              clusters; at most 200000 candidates); 0: on the host */
 } lmb_post_params;
 
 typedef struct lmb_post_output {
@@ -268,6 +270,21 @@ int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *pp,
                      int64_t n_results, const float *image,
                      const int32_t *hkls, int32_t nh, lmb_post_output *out);
 void lmb_post_free(lmb_post_output *out);
+
+/* The duplicate merge alone (mergeDuplicateOrientations, LaueMatchingHeaders.h:
+ * 998-1065, after its cap): candidates rows[0..n) with scores, in input order,
+ * clustered greedily by misorientation <= max_angle (degrees) under the space
+ * group's symmetry.  Out: n_clusters, and per cluster the kept row, its score
+ * and the candidate count (arrays of n entries).  device >= 0 with n >= 1024:
+ * the pair matrix and the greedy pass run on that CUDA device (at most 200000
+ * candidates); pairs whose device angle lies within max(host_band, a 1e-12
+ * relative band) of the float rounding boundary at max_angle are decided with
+ * the host function.  device < 0: the host loop.  Same clusters either way. */
+int lmb_merge_clusters(int32_t device, int32_t space_group, double max_angle,
+                       double host_band, const double *orients, uint64_t n_orients,
+                       const uint64_t *rows, const double *scores, int64_t n,
+                       int32_t num_threads, int32_t *n_clusters, uint64_t *best_rows,
+                       double *best_scores, int32_t *counts);
 
 /* ---- survivor ordering that allocates nothing ------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

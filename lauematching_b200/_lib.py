@@ -34,7 +34,7 @@ EXPORTS = [
     "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
     "lmb_image_load_batch",
     "lmb_match", "lmb_results", "lmb_results_batch", "lmb_last_pass_ms", "lmb_engine_bytes",
-    "lmb_post_process", "lmb_post_free",
+    "lmb_post_process", "lmb_post_free", "lmb_merge_clusters",
     "lmb_order_survivors_noalloc",
     "lmb_host_alloc", "lmb_host_free",
 ]
@@ -60,7 +60,7 @@ class LmbPostParams(C.Structure):
                 ("tol_c_over_a", C.c_double), ("max_angle", C.c_double),
                 ("min_nr_spots", C.c_int32), ("image_num", C.c_int32),
                 ("num_threads", C.c_int32), ("optimizer", C.c_int32),
-                ("max_results", C.c_int32), ("reserved", C.c_int32)]
+                ("max_results", C.c_int32), ("merge_on_device", C.c_int32)]
 
 
 class LmbPostOutput(C.Structure):
@@ -126,6 +126,8 @@ def lib():
         "lmb_post_process": ([C.POINTER(LmbGeometry), C.POINTER(LmbPostParams), vp, u64, vp, vp,
                               C.c_int64, vp, vp, i32, C.POINTER(LmbPostOutput)], C.c_int),
         "lmb_post_free": ([C.POINTER(LmbPostOutput)], None),
+        "lmb_merge_clusters": ([i32, i32, dbl, dbl, vp, u64, vp, vp, C.c_int64, i32,
+                                C.POINTER(i32), vp, vp, vp], C.c_int),
         "lmb_order_survivors_noalloc": ([vp, u64, vp, vp], C.c_int),
         "lmb_host_alloc": ([u64, C.POINTER(vp)], C.c_int),
         "lmb_host_free": ([vp], C.c_int),

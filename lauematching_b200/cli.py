@@ -132,7 +132,8 @@ def main_gpu(argv=None) -> int:
 
     ids, scores = post.collected_matches(surv, n_pass)
     sol, spt, n_unique = post.post_process(p, e.geometry, orients, ids, scores,
-                                           image.astype(np.float32), hkls, num_threads=ncpus)
+                                           image.astype(np.float32), hkls, num_threads=ncpus,
+                                           merge_device=_device())
     try:
         with open(image_fn + ".solutions.txt", "w") as f:
             f.write(post.SOLUTIONS_HEADER + sol)

@@ -107,6 +107,25 @@ struct GatherArgs {
   uint32_t off[LMB_MAX_SLOTS + 1];
 };
 int gather_launch(const GatherArgs &g, cudaStream_t st);
+
+// Duplicate merge on the device (merge.cu).
+struct MergeArgs {
+  double *quat;        // [n][4] candidates' quaternions, input order
+  double *fr;          // [n][4] in the fundamental region
+  double *score;
+  uint32_t *bits;      // [n][W]: column g, bit l = l merges into g
+  uint32_t *unsure;    // [cap][2] (l, g) pairs left to the host
+  unsigned *n_unsure;
+  unsigned cap_unsure;
+  int64_t *out_best;   // per cluster: index of the kept candidate
+  int32_t *out_count;  // per cluster: candidates merged (the reference's dArr)
+  int *n_clusters;
+  int64_t n, W;
+  int nsym;
+  double sym[24][4];
+  double max_angle, rad2deg;
+  double mid, window;  // float rounding boundary at max_angle, and the band left to the host
+};
 int status_reset_launch(unsigned int *d_status, uint64_t mask, cudaStream_t st);
 
 // Compact DB layout (clist.cu): on-detector spots per 32-record chunk, then

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "../../include/lmb200.h"
+#include "merge.h"
 
 namespace lmb {
 void set_error(const char *fmt, ...);
@@ -151,6 +152,69 @@ double misorientation_deg(const Sym &S, const double a[4], const double b[4]) { 
   to_fundamental(S, p, m);
   if (m[0] > 1) m[0] = 1;
   return 2 * (std::acos(m[0])) * kRad2Deg;
+}
+
+// ---- the duplicate merge on the device (merge.cu) ------------------------------
+constexpr int64_t kDeviceMergeMin = 1024;  // fewer candidates: the host loop is quick
+
+struct DecideCtx {
+  const Sym *S;
+  const double *quat;
+  double max_angle;
+};
+
+// The host's own comparison for a pair the device left undecided (l > g, the
+// reference's argument order).
+bool decide_pair(void *ctx, int64_t l, int64_t g) {
+  const DecideCtx *c = static_cast<const DecideCtx *>(ctx);
+  return (float)misorientation_deg(*c->S, &c->quat[l * 4], &c->quat[g * 4]) <= c->max_angle;
+}
+
+int merge_on_gpu(int device, double band, const Sym &S, double max_angle,
+                 const std::vector<double> &quat,
+                 const std::vector<uint64_t> &rows, const std::vector<double> &sc,
+                 std::vector<int> *dcount, std::vector<int> *best_row,
+                 std::vector<double> *best_score) {
+  const int64_t n = (int64_t)rows.size();
+  lmb::MergeHost h{};
+  h.device = device;
+  h.n = n;
+  h.quat = quat.data();
+  h.score = sc.data();
+  h.nsym = S.n;
+  for (int i = 0; i < 24; i++)
+    for (int j = 0; j < 4; j++) h.sym[i][j] = S.q[i][j];
+  h.max_angle = max_angle;
+  h.rad2deg = kRad2Deg;
+  // (float)x <= max_angle changes value where x crosses the midpoint of the
+  // two floats around max_angle; pairs whose device angle is within a band far
+  // wider than the device/host acos difference of it are decided on the host
+  float f1 = (float)max_angle;
+  if ((double)f1 > max_angle) f1 = std::nextafterf(f1, -INFINITY);
+  const float f2 = std::nextafterf(f1, INFINITY);
+  h.mid = ((double)f1 + (double)f2) / 2;
+  h.window = std::isfinite(h.mid) ? std::fmax(1e-12 * std::fmax(1.0, std::fabs(h.mid)), band)
+                                   : -1.0;
+  DecideCtx ctx{&S, quat.data(), max_angle};
+  h.decide = decide_pair;
+  h.ctx = &ctx;
+  std::vector<int64_t> bi((size_t)n);
+  std::vector<int32_t> cnt((size_t)n);
+  int32_t nc = 0;
+  std::vector<std::pair<uint32_t, uint32_t>> unsure;
+  bool overflow = false;
+  const int rc = lmb::merge_device_run(h, &nc, bi.data(), cnt.data(), &unsure, &overflow);
+  if (rc) return rc;
+  if (overflow) {
+    lmb::set_error("device merge: too many candidate pairs at the MaxAngle boundary");
+    return LMB_ERR_OVERFLOW;
+  }
+  for (int32_t c = 0; c < nc; c++) {
+    dcount->push_back(cnt[c]);
+    best_row->push_back((int)rows[bi[c]]);
+    best_score->push_back(sc[bi[c]]);
+  }
+  return LMB_OK;
 }
 
 void om_to_quat(const double m[9], double q[4]) {  // OrientMat2Quat, :262-302
@@ -404,6 +468,50 @@ void appendf(std::string &s, const char *fmt, ...) {
   }
 }
 
+// mergeDuplicateOrientations (:969-1065) after the cap, on candidates rows/sc
+// in input order: clusters (count, kept row, kept score).  device >= 0 and at
+// least kDeviceMergeMin candidates: the pair matrix and greedy pass on that
+// CUDA device (band > 0 widens the band of pairs decided on the host);
+// otherwise the host loop.
+int merge_clusters(int device, double band, const Sym &S, double max_angle,
+                   const double *orients, const std::vector<uint64_t> &rows,
+                   const std::vector<double> &sc, int nthreads, std::vector<int> *dcount,
+                   std::vector<int> *best_row, std::vector<double> *best_score) {
+  const int64_t nr = (int64_t)rows.size();
+  std::vector<double> quat((size_t)nr * 4);
+#pragma omp parallel for num_threads(nthreads)
+  for (int64_t i = 0; i < nr; i++) om_to_quat(orients + rows[i] * 9, &quat[i * 4]);
+  if (device >= 0 && nr >= kDeviceMergeMin)
+    return merge_on_gpu(device, band, S, max_angle, quat, rows, sc, dcount, best_row, best_score);
+  std::vector<float> miso((size_t)nr * (nr > 0 ? nr - 1 : 0) / 2);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic)
+  for (int64_t i = 1; i < nr; i++)
+    for (int64_t j = 0; j < i; j++)
+      miso[(size_t)i * (i - 1) / 2 + j] = (float)misorientation_deg(S, &quat[i * 4], &quat[j * 4]);
+  std::vector<int> done(nr, 0);
+  for (int64_t g = 0; g < nr; g++) {
+    if (done[g]) continue;
+    done[g] = 1;
+    int bs = (int)rows[g];
+    double bsc = sc[g];
+    for (int64_t l = g + 1; l < nr; l++) {
+      if (done[l] > 0) continue;
+      if (miso[(size_t)l * (l - 1) / 2 + g] <= max_angle) {
+        done[l] = 1;
+        done[g]++;
+        if (sc[l] > bsc) {
+          bsc = sc[l];
+          bs = (int)rows[l];
+        }
+      }
+    }
+    dcount->push_back(done[g]);
+    best_row->push_back(bs);
+    best_score->push_back(bsc);
+  }
+  return LMB_OK;
+}
+
 }  // namespace
 
 extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *pp,
@@ -481,35 +589,12 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
     }
     nr = cap;
   }
-  std::vector<double> quat((size_t)nr * 4);
-#pragma omp parallel for num_threads(nthreads)
-  for (int64_t i = 0; i < nr; i++) om_to_quat(orients + rows[i] * 9, &quat[i * 4]);
-  std::vector<float> miso((size_t)nr * (nr > 0 ? nr - 1 : 0) / 2);
-#pragma omp parallel for num_threads(nthreads) schedule(dynamic)
-  for (int64_t i = 1; i < nr; i++)
-    for (int64_t j = 0; j < i; j++)
-      miso[(size_t)i * (i - 1) / 2 + j] = (float)misorientation_deg(S, &quat[i * 4], &quat[j * 4]);
-  std::vector<int> done(nr, 0), dcount, best_row;
+  std::vector<int> dcount, best_row;
   std::vector<double> best_score;
-  for (int64_t g = 0; g < nr; g++) {
-    if (done[g]) continue;
-    done[g] = 1;
-    int bs = (int)rows[g];
-    double bsc = sc[g];
-    for (int64_t l = g + 1; l < nr; l++) {
-      if (done[l] > 0) continue;
-      if (miso[(size_t)l * (l - 1) / 2 + g] <= pp->max_angle) {
-        done[l] = 1;
-        done[g]++;
-        if (sc[l] > bsc) {
-          bsc = sc[l];
-          bs = (int)rows[l];
-        }
-      }
-    }
-    dcount.push_back(done[g]);
-    best_row.push_back(bs);
-    best_score.push_back(bsc);
+  {
+    const int rc = merge_clusters(pp->merge_on_device - 1, 0.0, S, pp->max_angle, orients, rows,
+                                  sc, nthreads, &dcount, &best_row, &best_score);
+    if (rc) return rc;
   }
   const int nsol = (int)dcount.size();
 
@@ -653,6 +738,40 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
   memcpy(out->spots, spt.c_str(), spt.size() + 1);
   out->solutions_len = sol.size();
   out->spots_len = spt.size();
+  return LMB_OK;
+}
+
+extern "C" int lmb_merge_clusters(int32_t device, int32_t space_group, double max_angle,
+                                  double host_band, const double *orients, uint64_t n_orients,
+                                  const uint64_t *rows, const double *scores, int64_t n,
+                                  int32_t num_threads, int32_t *n_clusters, uint64_t *best_rows,
+                                  double *best_scores, int32_t *counts) {
+  if ((n > 0 && (!rows || !scores || !orients || !best_rows || !best_scores || !counts)) ||
+      !n_clusters || n < 0 || !(host_band >= 0.0)) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  for (int64_t i = 0; i < n; i++)
+    if (rows[i] >= n_orients) {
+      lmb::set_error("row %llu outside the %llu orientations", (unsigned long long)rows[i],
+                     (unsigned long long)n_orients);
+      return LMB_ERR_INVALID;
+    }
+  const Sym S = make_sym(space_group);
+  std::vector<uint64_t> rv(rows, rows + n);
+  std::vector<double> sv(scores, scores + n);
+  std::vector<int> dcount, best_row;
+  std::vector<double> best_score;
+  const int rc = merge_clusters(device, host_band, S, max_angle, orients, rv, sv,
+                                num_threads > 0 ? num_threads : 1, &dcount, &best_row,
+                                &best_score);
+  if (rc) return rc;
+  *n_clusters = (int32_t)dcount.size();
+  for (size_t c = 0; c < dcount.size(); c++) {
+    best_rows[c] = (uint64_t)best_row[c];
+    best_scores[c] = best_score[c];
+    counts[c] = dcount[c];
+  }
   return LMB_OK;
 }
 

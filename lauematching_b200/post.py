@@ -32,13 +32,16 @@ STREAM_SPOTS_HEADER = "%ImageNr\t" + SPOTS_HEADER[1:]
 def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndarray,
                  scores: np.ndarray, image_f32: np.ndarray, hkls: np.ndarray,
                  min_nr_spots: int | None = None, image_num: int = 0,
-                 num_threads: int | None = None, max_results: int = 0):
+                 num_threads: int | None = None, max_results: int = 0,
+                 merge_device: int | None = None):
     """Return (solutions_text, spots_text, n_unique) for one image.
 
     ``ids``/``scores`` are the image's collected matches in the reference's
     collection order (ascending orientation ID).  ``max_results`` > 0 keeps
     only that many top-scored candidates for the merge (the reference's own
-    cap path, LaueMatchingHeaders.h:976-997, with its cap of 50000 lowered)."""
+    cap path, LaueMatchingHeaders.h:976-997, with its cap of 50000 lowered).
+    ``merge_device`` (a CUDA device index) runs the duplicate merge of 1024 or
+    more candidates on that device (same clusters); None keeps it on the host."""
     pp = _lib.LmbPostParams()
     for i in range(6):
         pp.lattice[i] = params.lattice[i]
@@ -52,6 +55,7 @@ def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndar
     pp.num_threads = int(num_threads or os.cpu_count() or 1)
     pp.optimizer = 0
     pp.max_results = int(max_results)  # 0: the reference's 50000
+    pp.merge_on_device = 0 if merge_device is None else int(merge_device) + 1
     om = np.ascontiguousarray(orients, dtype=np.float64).reshape(-1, 9)
     idv = np.ascontiguousarray(ids, dtype=np.uint64)
     scv = np.ascontiguousarray(scores, dtype=np.float64)
@@ -82,3 +86,27 @@ def collected_matches(survivors, n_pass: int):
         ids = np.concatenate([ids, np.zeros(extra, np.uint64)])
         sc = np.concatenate([sc, np.zeros(extra, np.float64)])
     return ids, sc
+
+
+def merge_clusters(space_group: int, max_angle: float, orients: np.ndarray, rows, scores,
+                   device: int | None = None, host_band: float = 0.0,
+                   num_threads: int | None = None):
+    """The duplicate merge alone: (best_rows, best_scores, counts) per cluster,
+    in the reference's cluster order.  ``device`` runs it on that CUDA device
+    (1024 or more candidates), None on the host."""
+    om = np.ascontiguousarray(orients, dtype=np.float64).reshape(-1, 9)
+    rv = np.ascontiguousarray(rows, dtype=np.uint64)
+    sv = np.ascontiguousarray(scores, dtype=np.float64)
+    n = rv.shape[0]
+    br = np.zeros(max(n, 1), np.uint64)
+    bs = np.zeros(max(n, 1), np.float64)
+    cn = np.zeros(max(n, 1), np.int32)
+    nc = C.c_int32(0)
+    check(lib().lmb_merge_clusters(-1 if device is None else int(device), int(space_group),
+                                   float(max_angle), float(host_band), om.ctypes.data,
+                                   om.shape[0], rv.ctypes.data, sv.ctypes.data, n,
+                                   int(num_threads or os.cpu_count() or 1), C.byref(nc),
+                                   br.ctypes.data, bs.ctypes.data, cn.ctypes.data))
+    k = nc.value
+    return br[:k].copy(), bs[:k].copy(), cn[:k].copy()
+

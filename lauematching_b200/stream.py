@@ -110,6 +110,7 @@ class StreamServer:
         from . import _lib, formats
         from .engine import Engine
         self.log = log
+        self.device = int(device)
         self.ncpus = max(1, int(ncpus))
         # images are post-processed concurrently, each on few threads
         self.n_writers = max(1, min(8, self.ncpus))
@@ -326,7 +327,8 @@ class StreamServer:
                 sol, spt, nu = post_process(p, g.engine.geometry, self.orients, ids, sc, img,
                                             self.hkls, min_nr_spots=p.min_good_spots,
                                             image_num=d.req.image_num,
-                                            num_threads=self.post_threads)
+                                            num_threads=self.post_threads,
+                                            merge_device=self.device)
             with self._out_lock:
                 if sol or spt:
                     self.sol_f.write(sol)

@@ -48,3 +48,20 @@ def test_post_stage_tolerates_no_survivors():
                                      np.zeros(0, np.uint64), np.zeros(0),
                                      c.image.astype(np.float32), c.hkls)
     assert (sol, spt, nu) == ("", "", 0)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_merge_alone_gives_the_reference_unique_count(name):
+    """lmb_merge_clusters (host path) on the oracle's collected matches gives
+    the reference's "Unique Orientations" count, and counts that add up."""
+    c = golden_case(name)
+    p = c.params
+    s = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                  p.min_nr_spots, p.min_intensity)
+    surv = np.zeros(len(s.ids), [("id", "<u8"), ("score", "<f8")])
+    surv["id"] = s.ids
+    surv["score"] = s.score
+    ids, sc = post.collected_matches(surv, s.n_pass)
+    rows, scores, counts = post.merge_clusters(p.space_group, p.max_angle, c.orients, ids, sc)
+    assert rows.shape[0] == c.meta["cmp_unique"]
+    assert int(counts.sum()) == len(ids)
