@@ -499,7 +499,7 @@ def run_ours(args, rank, world):
     # that layout streams (1 B per orientation + 4 B per on-detector spot +
     # tile headers) plus the occupancy words the gathers read (8 B per pixel).
     lay, shape = lay_main, shape_main
-    compact = shape["variant"] == 2 and lay["compact"] == 1
+    compact = shape.get("last_variant") == 2 and lay["compact"] == 1
     ref_bytes = N * REC_BYTES_PER_ORIENT + K * p.nr_px_x * p.nr_px_y
     alg_bytes = lay["bytes"] + p.nr_px_x * p.nr_px_y * 8 if compact else ref_bytes
     cmp_avg = statistics.mean(cmp_ms)
@@ -774,10 +774,35 @@ def run_reference_gpu(args, rank, world):
 # ---------------------------------------------------------------------------
 # serving: Poisson arrivals of mixed 1024^2 / 2048^2 frames through the daemon
 # ---------------------------------------------------------------------------
-def run_serve(args):
+def _serve_client(port, wire, keys, n_total, rate, nsend):
+    """Poisson arrivals of frames on nsend connections (the extended header:
+    b"LMB2", image number, width, height, dtype uint8)."""
     import socket
     import struct
     import threading as th
+
+    def sender(j):
+        r2 = np.random.default_rng(100 + j)
+        s = socket.create_connection(("127.0.0.1", port))
+        t = time.perf_counter()
+        for i in range(j, n_total, nsend):
+            t += r2.exponential(nsend / rate)
+            dt = t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            key = keys[int(r2.integers(0, 2))]
+            fr = wire[key][int(r2.integers(0, len(wire[key])))]
+            s.sendall(struct.pack("<4sHHHBB", b"LMB2", (i % 65535) + 1, key[0], key[1], 1, 0))
+            s.sendall(fr)
+        s.close()
+    ts = [th.Thread(target=sender, args=(j,)) for j in range(nsend)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+
+
+def run_serve(args):
     from lauematching_b200 import synth, params as P
     from lauematching_b200.engine import Engine
     from lauematching_b200.stream import StreamServer
@@ -802,6 +827,9 @@ def run_serve(args):
             frames.append(synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng).astype(np.uint8))
         pool[(p.nr_px_x, p.nr_px_y)] = frames
     keys = list(pool)
+    wire = {k: [f.tobytes() for f in v] for k, v in pool.items()}
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
     results = []
     port0 = 45000 + (os.getpid() % 200) * 10
     for mode, mb in (("batched", 64), ("plain", 1)):
@@ -813,27 +841,13 @@ def run_serve(args):
                                engines=[e2, e1], max_queue=256).start()
             time.sleep(0.3)
             n_total = int(min(args.serve_images, max(50, rate * args.serve_seconds)))
-            nsend = 4
-            def sender(j):
-                r2 = np.random.default_rng(100 + j)
-                s = socket.create_connection(("127.0.0.1", port0 + 1))
-                t = time.perf_counter()
-                for i in range(j, n_total, nsend):
-                    t += r2.exponential(nsend / rate)
-                    dt = t - time.perf_counter()
-                    if dt > 0:
-                        time.sleep(dt)
-                    key = keys[int(r2.integers(0, 2))]
-                    fr = pool[key][int(r2.integers(0, 16))]
-                    s.sendall(struct.pack("<4sHHHBB", b"LMB2", (i % 65535) + 1, key[0], key[1], 1, 0))
-                    s.sendall(fr.tobytes())
-                s.close()
-            ts = [th.Thread(target=sender, args=(j,)) for j in range(nsend)]
+            # the clients run in a process of their own, as the detector-side
+            # image server does, so they do not share the daemon's interpreter
+            client = ctx.Process(target=_serve_client,
+                                 args=(port0 + 1, wire, keys, n_total, rate, 4))
             t0 = time.perf_counter()
-            for t in ts:
-                t.start()
-            for t in ts:
-                t.join()
+            client.start()
+            client.join()
             deadline = time.time() + 300
             while srv.images_done < n_total and time.time() < deadline:
                 time.sleep(0.02)

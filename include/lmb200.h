@@ -101,7 +101,9 @@ int lmb_engine_destroy(lmb_engine *e);
 void *lmb_engine_stream(lmb_engine *e);
 
 /* Launch shape of the compare pass: fields = {variant (0 block-barrier ring,
- * 1 warp-specialised, 2 warp-specialised over the compact layout),
+ * 1 warp-specialised, 2 warp-specialised over the compact layout, 3 automatic:
+ * variant 2 while the records that can pass hold at most ~3 spots per DB
+ * record on average, variant 1 beyond -- the default),
  * tile_sub (32-orientation sub-tiles per tile), stages, consumer warps,
  * blocks per SM, grid multiplier, full_gather}; 0 = default.  full_gather = 1
  * gathers every spot even of records with fewer spots than MinNrSpots (which
@@ -110,6 +112,7 @@ void *lmb_engine_stream(lmb_engine *e);
  * get returns the shape actually used for this DB.  No reference counterpart
  * (the reference launches <<<ceil(n/1024),1024>>>, LaueMatchingGPU.cu:739-743). */
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields);
+/* get: the same 7 fields, and an 8th: the variant the latest pass ran. */
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields);
 
 /* The compact device layout variant 2 streams: derived from the resident

@@ -35,15 +35,25 @@ __device__ __forceinline__ int clist_count(const uint16_t *db, uint64_t n, int R
   return k;
 }
 
-// Spots per 32-record chunk (one warp per chunk).
+// Spots per 32-record chunk (one warp per chunk), and the histogram of the
+// records' on-detector spot counts (hist[c], c <= S <= 255).
 __global__ void clist_chunk_kernel(const uint16_t *__restrict__ db, uint64_t n, int R, int S, int W,
-                                   int H, uint64_t nchunks, uint32_t *__restrict__ chunk_spots) {
+                                   int H, uint64_t nchunks, uint32_t *__restrict__ chunk_spots,
+                                   unsigned long long *__restrict__ hist) {
+  __shared__ unsigned int h[256];
+  for (int k = threadIdx.x; k < 256; k += blockDim.x) h[k] = 0;
+  __syncthreads();
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t ch = i >> 5;
-  if (ch >= nchunks) return;  // whole warps: blockDim is a multiple of 32
-  int c = clist_count(db, n, R, S, W, H, i);
-  c = __reduce_add_sync(0xffffffffu, c);
-  if ((threadIdx.x & 31) == 0) chunk_spots[ch] = (uint32_t)c;
+  if (ch < nchunks) {  // whole warps: blockDim is a multiple of 32
+    const int c = clist_count(db, n, R, S, W, H, i);
+    if (i < n) atomicAdd(&h[c], 1u);
+    const int sum = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0) chunk_spots[ch] = (uint32_t)sum;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < 256; k += blockDim.x)
+    if (h[k]) atomicAdd(&hist[k], (unsigned long long)h[k]);
 }
 
 // Write the tiles from the host's packing: chunk ch goes to tile ctile[ch] at
@@ -91,12 +101,14 @@ __global__ void clist_fill_kernel(const uint16_t *__restrict__ db, uint64_t n, i
 }
 
 int clist_chunk_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H,
-                       uint32_t *d_chunk_spots, cudaStream_t st) {
+                       uint32_t *d_chunk_spots, unsigned long long *d_hist, cudaStream_t st) {
   const uint64_t nchunks = (n + 31) / 32;
   if (nchunks == 0) return LMB_OK;
+  LMB_REQUIRE(S <= 255, "spot counts above 255 do not fit the histogram");
   const uint64_t threads = nchunks * 32;
-  clist_chunk_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(d_db, n, R, S, W, H,
-                                                                        nchunks, d_chunk_spots);
+  LMB_CUDA(cudaMemsetAsync(d_hist, 0, 256 * sizeof(unsigned long long), st));
+  clist_chunk_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+      d_db, n, R, S, W, H, nchunks, d_chunk_spots, d_hist);
   LMB_CUDA(cudaGetLastError());
   return LMB_OK;
 }

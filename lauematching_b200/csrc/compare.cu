@@ -786,7 +786,7 @@ static int counter_bits(int S) {
 CompareTuning compare_config(int R, const CompareTuning &req) {
   CompareTuning c = req;
   const size_t rb = (size_t)R * 2;
-  if (c.variant == 2) {  // compact layout: the tile shape comes with the layout
+  if (c.variant == 2 || c.variant == 3) {  // compact layout: the tile shape comes with it
     c.tile_sub = 0;
     if (c.consumers <= 0) c.consumers = 16;
     c.consumers = std::min(c.consumers, 17);

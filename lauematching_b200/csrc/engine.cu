@@ -75,6 +75,7 @@ struct lmb_engine {
   uint32_t cl_stage = 0;  // bytes per tile
   uint64_t cl_bytes = 0;
   int cl_state = 0;  // 0 not built, 1 built, -1 this DB cannot use it
+  unsigned long long cl_hist[256] = {};  // records per on-detector spot count
   // image slots
   uint8_t *d_u8 = nullptr;
   double *d_f64 = nullptr;  // allocated on first keep_f64 load
@@ -101,7 +102,10 @@ struct lmb_engine {
   cudaStream_t ld = nullptr;
   cudaEvent_t ev_loaded[LMB_MAX_SLOTS] = {};
   cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
-  CompareTuning tuning{1, 0, 0, 0, 0, 0, 0};  // warp-specialised, default shape
+  // automatic variant with the compact pass's tuned shape (2 stages, 3 consumer
+  // warps, 5 blocks per SM)
+  CompareTuning tuning{3, 0, 2, 3, 1, 5, 0};
+  int last_variant = -1;  // variant the latest pass ran
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
   bool sparse_uploads = true;               // frames cross the link as pairs when sparse
@@ -376,13 +380,16 @@ int build_compact(lmb_engine *e) {
   e->cl_state = -1;
   if (e->S > 255 || e->n == 0) return LMB_OK;  // counts are uint8
   const uint64_t n = e->n, nch = (n + 31) / 32;
-  uint32_t *d_aux = nullptr;  // chunk spots, then 4 arrays of the packing
-  LMB_CUDA(cudaMalloc(&d_aux, nch * 4 * 4));
+  uint32_t *d_aux = nullptr;  // chunk spots, then 4 arrays of the packing; count histogram
+  LMB_CUDA(cudaMalloc(&d_aux, nch * 4 * 4 + 256 * sizeof(unsigned long long)));
+  unsigned long long *d_hist = reinterpret_cast<unsigned long long *>(d_aux + 4 * nch);
   std::vector<uint32_t> cs(nch);
   int rc = clist_chunk_launch(e->d_db, n, e->R, e->S, e->geo.nr_px_x, e->geo.nr_px_y, d_aux,
-                              e->st);
+                              d_hist, e->st);
   cudaError_t ce = cudaSuccess;
   if (rc == LMB_OK) ce = cudaMemcpyAsync(cs.data(), d_aux, nch * 4, cudaMemcpyDeviceToHost, e->st);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(e->cl_hist, d_hist, sizeof(e->cl_hist), cudaMemcpyDeviceToHost, e->st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
   if (rc || ce != cudaSuccess) {
     cudaFree(d_aux);
@@ -444,6 +451,22 @@ int build_compact(lmb_engine *e) {
   e->cl_bytes = total;
   e->cl_state = 1;
   return LMB_OK;
+}
+
+// Automatic variant.  Each spot the pass gathers costs the same in both
+// layouts; what the compact layout saves is the stream of the records'
+// padding.  Measured on B200 at 1e8 records (two detector geometries, K=64),
+// the compact pass is as fast or faster while the records that can pass
+// (at least min_spots on-detector spots) hold up to ~3 spots per DB record
+// on average, and up to 1.4x slower beyond (dense records, where the
+// reference records' stream is no longer the cost).
+constexpr double kAutoGather = 3.0;
+
+double gathered_per_record(const lmb_engine *e, int min_spots) {
+  const int m = std::max(0, min_spots);
+  double g = 0;
+  for (int c = m; c < 256; c++) g += (double)c * (double)e->cl_hist[c];
+  return e->n ? g / (double)e->n : 0.0;
 }
 
 int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
@@ -992,13 +1015,22 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   LMB_REQUIRE(value_mode == LMB_VALUE_U8 || (slot_mask & ~e->f64_mask) == 0,
               "float64 pass needs images loaded with keep_f64");
   CompareTuning tun = e->tuning;
-  if (tun.variant == 2) {  // compact layout: derive it once per DB
+  if (tun.variant == 2 || tun.variant == 3) {  // compact layout: derive it once per DB
     if (e->cl_state == 0) {
       rc = build_compact(e);
       if (rc) return rc;
     }
-    if (e->cl_state < 0) tun.variant = 1;  // this DB keeps the reference layout
+    // variant 3 (automatic): the compact layout while the records that can
+    // pass are few enough, the reference records otherwise (below)
+    bool compact = e->cl_state == 1;
+    if (compact && tun.variant == 3)
+      compact = gathered_per_record(e, tun.full_gather ? 0 : min_nr_spots) <= kAutoGather;
+    if (compact)
+      tun.variant = 2;
+    else
+      tun = CompareTuning{1, 0, 0, 0, 0, 0, tun.full_gather};  // default warp-specialised shape
   }
+  e->last_variant = tun.variant;
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
     if (slot_mask >> k & 1) LMB_CUDA(cudaStreamWaitEvent(e->st, e->ev_loaded[k], 0));
   // The pass (status reset, compare, ordering, status copy-back) replays from
@@ -1198,7 +1230,7 @@ int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields
                      &t.grid_mult, &t.full_gather};
   for (int i = 0; i < n_fields && i < 7; i++) *dst[i] = fields[i];
   LMB_REQUIRE(t.full_gather == 0 || t.full_gather == 1, "full_gather must be 0 or 1");
-  LMB_REQUIRE(t.variant >= 0 && t.variant <= 2, "unknown compare variant %d", t.variant);
+  LMB_REQUIRE(t.variant >= 0 && t.variant <= 3, "unknown compare variant %d", t.variant);
   e->tuning = t;
   return LMB_OK;
 }
@@ -1229,9 +1261,9 @@ int lmb_engine_set_sparse_uploads(lmb_engine *e, int32_t enable) {
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields) {
   LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
   const CompareTuning c = compare_config(e->R, e->tuning);
-  const int32_t src[7] = {c.variant, c.tile_sub, c.stages, c.consumers, c.blocks_per_sm,
-                          c.grid_mult, c.full_gather};
-  for (int i = 0; i < n_fields && i < 7; i++) fields[i] = src[i];
+  const int32_t src[8] = {c.variant, c.tile_sub, c.stages, c.consumers, c.blocks_per_sm,
+                          c.grid_mult, c.full_gather, e->last_variant};
+  for (int i = 0; i < n_fields && i < 8; i++) fields[i] = src[i];
   return LMB_OK;
 }
 

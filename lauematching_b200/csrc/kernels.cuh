@@ -151,7 +151,7 @@ __host__ __device__ __forceinline__ uint32_t clist_queue_bytes(int S) {
   return 384u + 128u * clist_queue_stride(S);
 }
 int clist_chunk_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H,
-                       uint32_t *d_chunk_spots, cudaStream_t st);
+                       uint32_t *d_chunk_spots, unsigned long long *d_hist, cudaStream_t st);
 int clist_fill_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H, uint32_t TB,
                       const uint32_t *d_ctile, const uint32_t *d_cpos, const uint32_t *d_cbase,
                       const uint32_t *d_tnch, unsigned char *d_cl, cudaStream_t st);

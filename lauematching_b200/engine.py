@@ -108,7 +108,7 @@ class Engine:
     def set_tuning(self, **kw) -> None:
         vals = (C.c_int32 * 7)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS])
         if "variant" not in kw:
-            vals[0] = 1
+            vals[0] = 3
         check(lib().lmb_engine_set_tuning(self._h, vals, 7))
         self._pinned_shape = True
 
@@ -130,9 +130,11 @@ class Engine:
                 "tile_bytes": tb.value}
 
     def get_tuning(self) -> dict:
-        vals = (C.c_int32 * 7)()
-        check(lib().lmb_engine_get_tuning(self._h, vals, 7))
-        return dict(zip(self.TUNING_FIELDS, list(vals)))
+        """The shape set (variant 3 = automatic) and ``last_variant``, the
+        variant the latest pass ran."""
+        vals = (C.c_int32 * 8)()
+        check(lib().lmb_engine_get_tuning(self._h, vals, 8))
+        return dict(zip(self.TUNING_FIELDS + ("last_variant",), list(vals)))
 
     # ---- DB -------------------------------------------------------------------
     def upload_db(self, records: np.ndarray) -> None:

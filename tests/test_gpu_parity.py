@@ -169,6 +169,55 @@ def test_edge_records_partial_tiles_and_thresholds(variant, full_gather):
 
 
 @pytest.mark.parametrize("name", golden_names())
+def test_automatic_variant_follows_the_spots_that_can_pass(name):
+    """The default (automatic) variant runs the compact layout while the
+    records that can pass hold at most 3 spots per DB record, the reference
+    records otherwise; both give the oracle's survivors."""
+    c = golden_case(name)
+    p = c.params
+    cnt = np.minimum(c.records[:, 0], p.max_nr_spots).astype(np.int64)  # all on the detector
+    gathered = cnt[cnt >= max(p.min_nr_spots, 0)].sum() / cnt.shape[0]
+    ref = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                    p.min_nr_spots, p.min_intensity)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        e.load_image(1, c.image)
+        e.match([1], p.min_nr_spots, p.min_intensity)
+        got, npass = e.results(1)
+        used = e.get_tuning()
+    assert used["variant"] == 3
+    assert used["last_variant"] == (2 if gathered <= 3.0 else 1), gathered
+    assert npass == ref.n_pass
+    assert_same_survivors(got, ref)
+
+
+def test_many_spots_per_record_keep_the_reference_layout():
+    """MaxNrLaueSpots above 255 (uint8 counts cannot hold it): a pass asked for
+    the compact layout runs over the reference records and matches the oracle."""
+    rng = np.random.default_rng(3)
+    S = 300
+    txt = synth.params_text(nr_px=(256, 256), max_nr_spots=S, min_nr_spots=20,
+                            min_intensity=10.0)
+    p = P.parse_params_text(txt)
+    n = 3000
+    rec = np.zeros((n, 1 + 2 * S), np.uint16)
+    rec[:, 0] = rng.integers(0, S + 5, n)
+    rec[:, 1::2] = rng.integers(0, 260, (n, S))
+    rec[:, 2::2] = rng.integers(0, 260, (n, S))
+    img = np.where(rng.random(256 * 256) < 0.2, rng.integers(1, 256, 256 * 256), 0).astype(np.float64)
+    ref = O.compare(rec, S, img, 256, 256, p.min_nr_spots, p.min_intensity)
+    with engine_for(p) as e:
+        e.set_tuning(variant=2)
+        e.upload_db(rec)
+        e.load_image(0, img)
+        e.match([0], p.min_nr_spots, p.min_intensity)
+        got, npass = e.results(0)
+        assert e.layout_info()["compact"] == -1
+    assert npass == ref.n_pass
+    assert_same_survivors(got, ref)
+
+
+@pytest.mark.parametrize("name", golden_names())
 @pytest.mark.parametrize("mode", [0, 1])
 def test_compact_layout_matches_oracle(name, mode):
     """Variant 2 (compact device layout) on the reference's golden cases."""
