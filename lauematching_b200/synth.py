@@ -235,3 +235,41 @@ def render_image(grain_records: np.ndarray, nr_px_x: int, nr_px_y: int,
             img *= force_max / mx
             img = np.rint(img)
     return img.ravel()
+
+
+def raw_frame(nr_px_y: int, nr_px_x: int, rng: np.random.Generator, n_spots: int = 200,
+              spot_records: np.ndarray | None = None, sigma: float = 1.6,
+              amp_lo: float = 40.0, amp_hi: float = 4000.0, pedestal: float = 100.0,
+              gradient: float = 60.0, noise: float = 5.0, integer: bool = True) -> np.ndarray:
+    """Unprocessed detector frame (float64 [y][x]) as the image server reads
+    it: a smooth pedestal with a gradient, Poisson counting noise and one
+    Gaussian per spot, before any background removal.  Spots come from the
+    given forward-cache records, else at ``n_spots`` seeded positions.
+    ``integer`` rounds to counts (a detector's values); otherwise adds a
+    uniform fraction to every pixel, so nearly all values differ."""
+    yy = np.linspace(0.0, 1.0, nr_px_y)[:, None]
+    xx = np.linspace(0.0, 1.0, nr_px_x)[None, :]
+    img = pedestal + gradient * (0.6 * yy + 0.4 * xx)
+    img = rng.poisson(np.broadcast_to(img, (nr_px_y, nr_px_x)) + noise).astype(np.float64)
+    if spot_records is not None:
+        pts = []
+        for rec in np.atleast_2d(spot_records):
+            c = int(rec[0])
+            pts += [(int(rec[2 + 2 * s]), int(rec[1 + 2 * s])) for s in range(c)]
+        pts = np.array(pts, np.int64).reshape(-1, 2)
+    else:
+        pts = np.stack([rng.integers(0, nr_px_y, n_spots), rng.integers(0, nr_px_x, n_spots)], 1)
+    rad = int(np.ceil(4 * sigma))
+    off = np.arange(-rad, rad + 1)
+    for y, x in pts:
+        a = rng.uniform(amp_lo, amp_hi)
+        s = sigma * rng.uniform(0.6, 1.6)
+        xs, ys = x + off, y + off
+        mx = (xs >= 0) & (xs < nr_px_x)
+        my = (ys >= 0) & (ys < nr_px_y)
+        gx = np.exp(-0.5 * (off[mx] / s) ** 2)
+        gy = np.exp(-0.5 * (off[my] / s) ** 2)
+        img[np.ix_(ys[my], xs[mx])] += a * np.outer(gy, gx)
+    if integer:
+        return np.rint(img)
+    return img + rng.random(img.shape)
