@@ -308,6 +308,81 @@ int lmb_merge_clusters(int32_t device, int32_t space_group, double max_angle,
 int lmb_order_survivors_noalloc(const lmb_survivor *d_in, uint64_t n,
                                 lmb_survivor *d_out, void *stream);
 
+/* ---- frame preprocessing ----------------------------------------------------
+ * Replaces laue_index/preprocess.py:221-338 (preprocess_image; called by
+ * scripts/laue_image_server.py:66-80 and scripts/RunImage.py:150-299) as the
+ * reference runs with numpy, scipy and OpenCV and without diplib or
+ * scikit-image: background = scipy's square median filter
+ * (preprocess.py:42-65), subtraction clipped at 0, threshold
+ * (thresholds.py:29-110; "otsu" falls back to the adaptive noise floor),
+ * float64 -> uint16, 8-connected components numbered as OpenCV numbers them
+ * (preprocess.py:136-151), components below min_area removed and the
+ * intensity-weighted centre of each kept one (preprocess.py:154-188), then
+ * the Gaussian blur of the filtered frame (preprocess.py:315-329).  Every
+ * output is identical to the reference's; the blur weights come from the
+ * caller (numpy's exp, as scipy builds them).  One handle per (device,
+ * frame size); calls on a handle are not re-entrant. */
+typedef struct lmb_pre lmb_pre;
+
+#define LMB_U16 3 /* uint16 detector frame (preprocessing input only) */
+
+#define LMB_THR_ADAPTIVE 0   /* median(nz) + 4 * 1.4826 * MAD(nz), at least 1 */
+#define LMB_THR_PERCENTILE 1 /* np.percentile(frame, threshold_percentile), linear */
+#define LMB_THR_FIXED 2      /* threshold_value */
+
+typedef struct lmb_pre_params {
+  int32_t threshold_method;    /* LMB_THR_* (cfg threshold_method) */
+  int32_t min_area;            /* cfg min_area */
+  double threshold_value;      /* cfg threshold_value (fixed method) */
+  double threshold_percentile; /* cfg threshold_percentile */
+  double override_thresh;      /* > 0: fixed threshold of this value (preprocess.py:280-283) */
+} lmb_pre_params;
+
+typedef struct lmb_pre_counts {
+  double threshold;  /* threshold applied (pixels <= it are zeroed) */
+  double min_dist2;  /* smallest squared distance between two kept centres; +inf below 2 */
+  int32_t n_labels;  /* OpenCV's nlabels: components + 1 */
+  int32_t n_centres; /* components with area >= min_area */
+} lmb_pre_counts;
+
+int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **out);
+int lmb_pre_destroy(lmb_pre *p);
+
+/* scipy.ndimage.median_filter(frame, size) applied `passes` times (mode
+ * reflect), exact for any float64 values (preprocess.py:63-65).  The result
+ * becomes the handle's background and is copied to `out` (may be NULL).
+ * Sizes reaching 8x a frame side (>1 pixel) are refused: scipy's border
+ * handling stops being a mirror there. */
+int lmb_pre_median(lmb_pre *p, const void *frame, int32_t dtype, int32_t size, int32_t passes,
+                   double *out);
+/* The background subtracted from the following frames (float64 [y][x]);
+ * NULL = zeros.  Kept on the device until replaced. */
+int lmb_pre_set_background(lmb_pre *p, const double *background);
+int lmb_pre_get_background(lmb_pre *p, double *out);
+
+/* Steps up to the centres for one raw frame (dtype LMB_F64/F32/U16/U8):
+ * max(frame - background, 0), threshold, uint16 cast, components, small
+ * ones removed, centres.  Results stay on the device for the calls below. */
+int lmb_pre_segment(lmb_pre *p, const void *frame, int32_t dtype, const lmb_pre_params *prm,
+                    lmb_pre_counts *counts);
+/* The same from an already thresholded uint16 frame (find_connected_components
+ * + filter_small_components, preprocess.py:136-188). */
+int lmb_pre_segment_thresholded(lmb_pre *p, const uint16_t *thresholded, int32_t min_area,
+                                lmb_pre_counts *counts);
+/* Centres of the last segment in label order: [label, cx, cy, area] per row
+ * (up to cap rows); bboxes/areas of all components [x, y, w, h, area] (up to
+ * cap rows; may be NULL). */
+int lmb_pre_centres(lmb_pre *p, double *centres, int32_t cap);
+int lmb_pre_stats(lmb_pre *p, int32_t *stats, int32_t cap);
+/* Frames of the last segment; any pointer may be NULL. */
+int lmb_pre_images(lmb_pre *p, uint16_t *thresholded, int32_t *labels, uint16_t *filt_img,
+                   int32_t *filt_labels);
+/* Gaussian blur of the last segment's filtered frame with weights[0..2r]
+ * (scipy.ndimage.gaussian_filter: axis 0 then axis 1, mirrored borders) into
+ * host memory as float64 (LMB_F64) or float32 (LMB_F32, the image server's
+ * wire format, laue_image_server.py:79). */
+int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, int32_t out_dtype);
+
 /* Page-locked host buffers, so image uploads run at full link speed.  No
  * reference counterpart (the reference pins per-stream buffers internally,
  * LaueMatchingGPUStream.cu:1041-1075). */

@@ -19,7 +19,8 @@ LMB_ERR_OOM = -3
 LMB_ERR_OVERFLOW = -4
 LMB_ERR_TIMEOUT = -5
 LMB_MAX_SLOTS = 64
-LMB_F64, LMB_F32, LMB_U8 = 0, 1, 2
+LMB_F64, LMB_F32, LMB_U8, LMB_U16 = 0, 1, 2, 3
+LMB_THR_ADAPTIVE, LMB_THR_PERCENTILE, LMB_THR_FIXED = 0, 1, 2
 LMB_VALUE_U8, LMB_VALUE_F64 = 0, 1
 LMB_BUILD_EXACT_FP64 = 1
 LMB_NOALLOC_ORDER_MAX = 1 << 20
@@ -37,6 +38,9 @@ EXPORTS = [
     "lmb_post_process", "lmb_post_free", "lmb_merge_clusters",
     "lmb_order_survivors_noalloc",
     "lmb_host_alloc", "lmb_host_free",
+    "lmb_pre_create", "lmb_pre_destroy", "lmb_pre_median", "lmb_pre_set_background",
+    "lmb_pre_get_background", "lmb_pre_segment", "lmb_pre_segment_thresholded",
+    "lmb_pre_centres", "lmb_pre_stats", "lmb_pre_images", "lmb_pre_blur",
 ]
 
 
@@ -66,6 +70,17 @@ class LmbPostParams(C.Structure):
 class LmbPostOutput(C.Structure):
     _fields_ = [("solutions", C.c_void_p), ("solutions_len", C.c_uint64),
                 ("spots", C.c_void_p), ("spots_len", C.c_uint64), ("n_unique", C.c_int32)]
+
+
+class LmbPreParams(C.Structure):
+    _fields_ = [("threshold_method", C.c_int32), ("min_area", C.c_int32),
+                ("threshold_value", C.c_double), ("threshold_percentile", C.c_double),
+                ("override_thresh", C.c_double)]
+
+
+class LmbPreCounts(C.Structure):
+    _fields_ = [("threshold", C.c_double), ("min_dist2", C.c_double), ("n_labels", C.c_int32),
+                ("n_centres", C.c_int32)]
 
 
 class LmbError(RuntimeError):
@@ -131,6 +146,18 @@ def lib():
         "lmb_order_survivors_noalloc": ([vp, u64, vp, vp], C.c_int),
         "lmb_host_alloc": ([u64, C.POINTER(vp)], C.c_int),
         "lmb_host_free": ([vp], C.c_int),
+        "lmb_pre_create": ([i32, i32, i32, C.POINTER(vp)], C.c_int),
+        "lmb_pre_destroy": ([vp], C.c_int),
+        "lmb_pre_median": ([vp, vp, i32, i32, i32, vp], C.c_int),
+        "lmb_pre_set_background": ([vp, vp], C.c_int),
+        "lmb_pre_get_background": ([vp, vp], C.c_int),
+        "lmb_pre_segment": ([vp, vp, i32, C.POINTER(LmbPreParams), C.POINTER(LmbPreCounts)],
+                            C.c_int),
+        "lmb_pre_segment_thresholded": ([vp, vp, i32, C.POINTER(LmbPreCounts)], C.c_int),
+        "lmb_pre_centres": ([vp, vp, i32], C.c_int),
+        "lmb_pre_stats": ([vp, vp, i32], C.c_int),
+        "lmb_pre_images": ([vp, vp, vp, vp, vp], C.c_int),
+        "lmb_pre_blur": ([vp, vp, i32, vp, i32], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

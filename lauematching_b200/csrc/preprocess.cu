@@ -1,0 +1,1143 @@
+// Frame preprocessing on the device: the steps of preprocess_image
+// (laue_index/preprocess.py:221-338) as the reference runs them with numpy,
+// scipy and OpenCV, with identical results:
+//
+//   background   exact square median (scipy.ndimage.median_filter, mirrored
+//                borders): pixels become ranks among the frame's distinct
+//                values; one warp per (column, row segment) slides its window
+//                down, keeping 8-bit-digit rank histograms level by level and
+//                refilling a deeper level only when the digit above it moves.
+//   threshold    order statistics (np.median, np.percentile) by radix
+//                selection over order-preserving 64-bit keys, on the device.
+//   components   union-find over 8-neighbours (atomicMin on the parent
+//                array); OpenCV numbers components by the raster order of
+//                the first 2x2 pixel block each touches, so labels come from
+//                a prefix sum over per-block flags.
+//   centres      integer moments per component (exact), one division each.
+//   blur width   closest pair of centres: cell grid, brute force when the
+//                pair is farther apart than a cell.
+//   blur         separable float64 passes in scipy's summation order.
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <type_traits>
+
+#include "common.cuh"
+
+using namespace lmb;
+
+namespace {
+
+constexpr int kT = 256;            // threads of the elementwise kernels
+constexpr int kMedWarps = 8;       // warps per median block
+constexpr int kMedLevels = 4;      // 8-bit digits of a rank (ranks < 2^32)
+constexpr int kCell = 32;          // cell side of the closest-pair grid (pixels)
+constexpr int kSelFramePasses = 3; // selection passes that read the frame
+
+enum SelMode : int { SEL_NZ = 0, SEL_ABSDEV = 1, SEL_ALL = 2 };
+
+// ---- small helpers -----------------------------------------------------------
+// scipy's 'reflect' border (d c b a | a b c d | d c b a), periodic.
+__host__ __device__ __forceinline__ int mirror(int i, int n) {
+  if (i >= 0 && i < n) return i;
+  if (n == 1) return 0;
+  const int p = 2 * n;
+  i %= p;
+  if (i < 0) i += p;
+  return i < n ? i : p - 1 - i;
+}
+
+// Order-preserving key of a double (total order; -0 sorts just below +0).
+__device__ __forceinline__ unsigned long long okey(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double okey_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// numpy's float64 -> uint16 (x86-64): truncate to int32, keep 16 bits.
+__device__ __forceinline__ uint16_t u16_cast(double v) {
+  return (uint16_t)((unsigned)x86_trunc_i32(v) & 0xFFFFu);
+}
+
+template <typename T>
+__device__ __forceinline__ double to_f64(T v) {
+  return (double)v;
+}
+
+size_t grid_for(size_t n, int num_sms) {
+  return std::max<size_t>(1, std::min<size_t>((n + kT - 1) / kT, (size_t)num_sms * 16));
+}
+
+// ---- device state of one frame -----------------------------------------------
+struct Select {
+  unsigned long long n;          // candidates
+  unsigned long long k[2];       // residual ranks sought (k[1] = k[0] + 1 when two)
+  unsigned long long prefix[2];  // key bits fixed so far
+  unsigned long long n_compact;  // candidates kept for the later passes
+  int two;
+  int valid;
+};
+
+struct PreState {
+  Select sel;
+  unsigned int hist[2][256];
+  double med;
+  double thresh;
+  unsigned int n_comp;      // components
+  unsigned int n_labels;    // components + 1
+  unsigned int n_keep;      // components with area >= min_area
+  unsigned int pad;
+  unsigned long long best;  // bits of the smallest squared centre distance
+};
+
+// ---- conversions -------------------------------------------------------------
+template <typename T>
+__global__ void to_f64_kernel(const T *in, double *out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = to_f64(in[i]);
+}
+
+// np.maximum(raw - background, 0.0): NaN stays NaN, -0 stays -0.
+template <typename T>
+__global__ void subtract_kernel(const T *raw, const double *bg, double *sub, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double d = lmb::dsub(to_f64(raw[i]), bg[i]);
+    sub[i] = (d >= 0.0 || isnan(d)) ? d : 0.0;
+  }
+}
+
+// ---- order statistics ----------------------------------------------------------
+__global__ void sel_init_kernel(PreState *st, int mode, unsigned long long n,
+                                unsigned long long k0, int two) {
+  const int t = threadIdx.x;
+  for (int i = t; i < 512; i += blockDim.x) (&st->hist[0][0])[i] = 0;
+  if (t == 0) {
+    Select &s = st->sel;
+    s.n = mode == SEL_ALL ? n : 0;
+    s.k[0] = k0;
+    s.k[1] = k0 + 1;
+    s.prefix[0] = s.prefix[1] = 0;
+    s.n_compact = 0;
+    s.two = mode == SEL_ALL ? two : 0;
+    s.valid = 1;
+  }
+}
+
+__device__ __forceinline__ bool sel_candidate(int mode, double v, double med, double &val) {
+  if (mode != SEL_ALL && !(v > 0.0)) return false;
+  val = mode == SEL_ABSDEV ? fabs(lmb::dsub(v, med)) : v;
+  return true;
+}
+
+// One radix pass: histogram of the digit at `shift` of the candidates whose
+// higher digits equal each sought rank's prefix.  Passes 0..2 read the frame
+// (pass 2 also keeps the surviving keys), later passes read those keys.
+__global__ void sel_hist_kernel(const double *frame, size_t n, PreState *st, int mode, int shift,
+                                unsigned long long *compact) {
+  __shared__ unsigned int h[2][256];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) (&h[0][0])[i] = 0;
+  __syncthreads();
+  const Select s = st->sel;
+  if (s.valid) {
+    const unsigned long long hi = shift >= 56 ? 0ull : (~0ull << (shift + 8));
+    const unsigned long long p0 = s.prefix[0] & hi, p1 = s.prefix[1] & hi;
+    const bool two = s.two != 0 && shift < 56;
+    const double med = st->med;
+    const bool from_frame = shift >= 56 - 8 * (kSelFramePasses - 1);
+    const bool keep = shift == 56 - 8 * (kSelFramePasses - 1);
+    const size_t m = from_frame ? n : (size_t)s.n_compact;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t iters = (m + stride - 1) / stride;
+    for (size_t it = 0; it < iters; ++it) {
+      const size_t i = it * stride + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+      bool hit0 = false, hit1 = false;
+      unsigned long long key = 0;
+      if (i < m) {
+        if (from_frame) {
+          double val;
+          if (sel_candidate(mode, frame[i], med, val)) {
+            key = okey(val);
+            hit0 = (key & hi) == p0;
+            hit1 = two && (key & hi) == p1;
+          }
+        } else {
+          key = compact[i];
+          hit0 = (key & hi) == p0;
+          hit1 = two && (key & hi) == p1;
+        }
+      }
+      const unsigned d = (unsigned)(key >> shift) & 255u;
+      if (hit0) atomicAdd(&h[0][d], 1u);
+      if (hit1) atomicAdd(&h[1][d], 1u);
+      if (keep) {  // warp-aggregated append of the keys still in play
+        const bool k = hit0 || hit1;
+        const unsigned msk = __ballot_sync(0xffffffffu, k);
+        if (msk) {
+          const int lane = threadIdx.x & 31;
+          unsigned long long base = 0;
+          if (lane == __ffs(msk) - 1) base = atomicAdd(&st->sel.n_compact, (unsigned long long)__popc(msk));
+          base = __shfl_sync(0xffffffffu, base, __ffs(msk) - 1);
+          if (k) compact[base + __popc(msk & ((1u << lane) - 1u))] = key;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) {
+    const unsigned v = (&h[0][0])[i];
+    if (v) atomicAdd(&(&st->hist[0][0])[i], v);
+  }
+}
+
+// Digit of `h` (256 bins) holding residual rank k; one warp.
+__device__ __forceinline__ unsigned warp_find_digit(const unsigned *h, unsigned long long &k) {
+  const int lane = threadIdx.x & 31;
+  unsigned c[8];
+  unsigned long long sum = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    c[j] = h[lane * 8 + j];
+    sum += c[j];
+  }
+  unsigned long long incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const unsigned long long excl = incl - sum;
+  const unsigned msk = __ballot_sync(0xffffffffu, k < incl);
+  const int f = msk ? __ffs(msk) - 1 : 31;
+  unsigned digit = 0;
+  unsigned long long r = 0;
+  if (lane == f) {
+    r = k - excl;
+    int j = 0;
+    while (j < 7 && r >= c[j]) r -= c[j++];
+    digit = (unsigned)(lane * 8 + j);
+  }
+  digit = __shfl_sync(0xffffffffu, digit, f);
+  k = __shfl_sync(0xffffffffu, r, f);
+  return digit;
+}
+
+// After a pass: fix the digit of each sought rank, clear the histograms.
+// Pass 0 also learns the candidate count (SEL_NZ / SEL_ABSDEV: the median's
+// ranks, two of them for an even count).
+__global__ void sel_pick_kernel(PreState *st, int mode, int shift) {
+  Select &s = st->sel;
+  const int lane = threadIdx.x;
+  if (shift == 56 && mode != SEL_ALL) {
+    unsigned long long t = 0;
+    for (int j = lane; j < 256; j += 32) t += st->hist[0][j];
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) {
+      s.n = t;
+      s.k[0] = t ? (t - 1) / 2 : 0;
+      s.k[1] = s.k[0] + 1;
+      s.two = t > 0 && (t % 2) == 0;
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && s.n == 0) s.valid = 0;
+  __syncwarp();
+  if (s.valid) {
+    for (int L = 0; L < (s.two ? 2 : 1); ++L) {
+      unsigned long long k = s.k[L];
+      const unsigned d = warp_find_digit(shift == 56 ? st->hist[0] : st->hist[L], k);
+      if (lane == 0) {
+        s.k[L] = k;
+        s.prefix[L] |= (unsigned long long)d << shift;
+      }
+      __syncwarp();
+    }
+  }
+  for (int j = lane; j < 512; j += 32) (&st->hist[0][0])[j] = 0;
+}
+
+__device__ __forceinline__ double sel_value(const Select &s, int L) {
+  return okey_value(s.prefix[L]);
+}
+
+// np.median of the candidates: the middle one, or the mean of the two.
+__device__ __forceinline__ double sel_median(const Select &s) {
+  const double a = sel_value(s, 0);
+  return s.two ? lmb::ddiv(lmb::dadd(a, sel_value(s, 1)), 2.0) : a;
+}
+
+__global__ void finish_median_kernel(PreState *st) {
+  st->med = st->sel.valid ? sel_median(st->sel) : 0.0;
+}
+
+// thresholds.py:35-45: max(med + 4 * (1.4826 * mad), 1.0); 1.0 without candidates.
+__global__ void finish_adaptive_kernel(PreState *st) {
+  if (!st->sel.valid) {
+    st->thresh = 1.0;
+    return;
+  }
+  const double mad = lmb::dmul(1.4826, sel_median(st->sel));
+  const double t = lmb::dadd(st->med, lmb::dmul(4.0, mad));
+  st->thresh = (1.0 > t) ? 1.0 : t;
+}
+
+// numpy's _lerp(a, b, gamma) of the two order statistics.
+__global__ void finish_percentile_kernel(PreState *st, double gamma) {
+  const Select &s = st->sel;
+  const double a = sel_value(s, 0);
+  const double b = s.two ? sel_value(s, 1) : a;
+  const double diff = lmb::dsub(b, a);
+  double r = lmb::dadd(a, lmb::dmul(diff, gamma));
+  if (gamma >= 0.5) r = lmb::dsub(b, lmb::dmul(diff, lmb::dsub(1.0, gamma)));
+  st->thresh = r;
+}
+
+__global__ void set_thresh_kernel(PreState *st, double t) { st->thresh = t; }
+
+__global__ void reset_counts_kernel(PreState *st) {
+  st->n_comp = 0;
+  st->best = 0x7ff0000000000000ull;  // +inf
+}
+
+// ---- threshold, uint16, components ---------------------------------------------
+__global__ void apply_kernel(const double *sub, const PreState *st, uint16_t *t16, int *par,
+                             size_t n) {
+  const double thr = st->thresh;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double v = sub[i];
+    const uint16_t u = (v <= thr) ? (uint16_t)0 : u16_cast(v);
+    t16[i] = u;
+    par[i] = u ? (int)i : -1;
+  }
+}
+
+__global__ void init_parents_kernel(const uint16_t *t16, int *par, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    par[i] = t16[i] ? (int)i : -1;
+}
+
+__device__ __forceinline__ int uf_find(int *L, int x) {
+  int p = __ldcg(L + x);
+  while (p != x) {
+    x = p;
+    p = __ldcg(L + x);
+  }
+  return x;
+}
+
+// Hang the larger root under the smaller; retry when another thread moved it.
+__device__ void uf_union(int *L, int a, int b) {
+  for (;;) {
+    a = uf_find(L, a);
+    b = uf_find(L, b);
+    if (a == b) return;
+    if (a > b) {
+      const int t = a;
+      a = b;
+      b = t;
+    }
+    const int old = atomicMin(L + b, a);
+    if (old == b) return;
+    b = old;
+  }
+}
+
+__global__ void merge_kernel(int *L, int ny, int nx) {
+  const size_t n = (size_t)ny * nx;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (__ldcg(L + i) < 0) continue;
+    const int y = (int)(i / nx), x = (int)(i % nx);
+    const int p = (int)i;
+    if (x > 0 && __ldcg(L + i - 1) >= 0) uf_union(L, p, p - 1);
+    if (y > 0) {
+      const int q = p - nx;
+      if (x > 0 && __ldcg(L + q - 1) >= 0) uf_union(L, p, q - 1);
+      if (__ldcg(L + q) >= 0) uf_union(L, p, q);
+      if (x + 1 < nx && __ldcg(L + q + 1) >= 0) uf_union(L, p, q + 1);
+    }
+  }
+}
+
+__global__ void compress_kernel(int *L, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    if (__ldcg(L + i) >= 0) L[i] = uf_find(L, (int)i);
+}
+
+struct Comps {
+  int *area, *x0, *y0, *x1, *y1;
+  unsigned *fb;  // first 2x2 block (raster index)
+  unsigned long long *sw, *swx, *swy;
+  int *label, *keep;
+};
+
+__global__ void roots_kernel(const int *L, int *cid, PreState *st, Comps c, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (L[i] != (int)i) continue;
+    const unsigned id = atomicAdd(&st->n_comp, 1u);
+    cid[i] = (int)id;
+    c.area[id] = 0;
+    c.x0[id] = INT_MAX;
+    c.y0[id] = INT_MAX;
+    c.x1[id] = -1;
+    c.y1[id] = -1;
+    c.fb[id] = 0xffffffffu;
+    c.sw[id] = c.swx[id] = c.swy[id] = 0;
+  }
+}
+
+__global__ void moments_kernel(const int *L, const int *cid, const uint16_t *t16, Comps c, int ny,
+                               int nx) {
+  const size_t n = (size_t)ny * nx;
+  const unsigned bw = (unsigned)(nx + 1) / 2;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int r = L[i];
+    if (r < 0) continue;
+    const int id = cid[r];
+    const int y = (int)(i / nx), x = (int)(i % nx);
+    const unsigned long long w = t16[i];
+    atomicAdd(c.area + id, 1);
+    atomicMin(c.x0 + id, x);
+    atomicMin(c.y0 + id, y);
+    atomicMax(c.x1 + id, x);
+    atomicMax(c.y1 + id, y);
+    atomicMin(c.fb + id, (unsigned)(y >> 1) * bw + (unsigned)(x >> 1));
+    atomicAdd(c.sw + id, w);
+    atomicAdd(c.swx + id, w * (unsigned long long)x);
+    atomicAdd(c.swy + id, w * (unsigned long long)y);
+  }
+}
+
+// Flag each component's first block: low word counts components, high word
+// kept ones; a prefix sum over blocks then numbers them in OpenCV's order.
+__global__ void flags_kernel(const PreState *st, Comps c, int min_area,
+                             unsigned long long *flags, size_t cap) {
+  const size_t nc = st->n_comp;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < nc && id < cap;
+       id += (size_t)gridDim.x * blockDim.x) {
+    const bool keep = c.area[id] >= min_area;
+    flags[c.fb[id]] = 1ull | (keep ? (1ull << 32) : 0ull);
+  }
+}
+
+__global__ void label_kernel(PreState *st, Comps c, int min_area, const unsigned long long *pos,
+                             size_t nblocks, double *centres, int *stats) {
+  const size_t nc = st->n_comp;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < nc;
+       id += (size_t)gridDim.x * blockDim.x) {
+    const unsigned long long p = pos[c.fb[id]];
+    const int label = (int)(p & 0xffffffffull);
+    const bool keep = c.area[id] >= min_area;
+    c.label[id] = label;
+    const int x0 = c.x0[id], y0 = c.y0[id];
+    int *sr = stats + (size_t)(label - 1) * 5;
+    sr[0] = x0;
+    sr[1] = y0;
+    sr[2] = c.x1[id] - x0 + 1;
+    sr[3] = c.y1[id] - y0 + 1;
+    sr[4] = c.area[id];
+    if (keep) {
+      const int k = (int)(p >> 32) - 1;
+      c.keep[id] = k;
+      const unsigned long long sw = c.sw[id];
+      const double rx = (double)(c.swx[id] - (unsigned long long)x0 * sw);
+      const double ry = (double)(c.swy[id] - (unsigned long long)y0 * sw);
+      double *cr = centres + (size_t)k * 4;
+      cr[0] = (double)label;
+      cr[1] = lmb::dadd(lmb::ddiv(rx, (double)sw), (double)x0);
+      cr[2] = lmb::dadd(lmb::ddiv(ry, (double)sw), (double)y0);
+      cr[3] = (double)c.area[id];
+    } else {
+      c.keep[id] = -1;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long t = nblocks ? pos[nblocks - 1] : 0;
+    st->n_labels = (unsigned)(t & 0xffffffffull) + 1u;
+    st->n_keep = (unsigned)(t >> 32);
+  }
+}
+
+__global__ void images_kernel(const int *L, const int *cid, const uint16_t *t16, Comps c,
+                              int *labels, uint16_t *filt, int *flabels, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int r = L[i];
+    int lab = 0, kept = 0;
+    if (r >= 0) {
+      const int id = cid[r];
+      lab = c.label[id];
+      kept = c.keep[id] >= 0;
+    }
+    labels[i] = lab;
+    flabels[i] = kept ? lab : 0;
+    filt[i] = kept ? t16[i] : (uint16_t)0;
+  }
+}
+
+// ---- closest pair of centres (blur width) ---------------------------------------
+__device__ __forceinline__ double pair_d2(const double *a, const double *b) {
+  const double dx = lmb::dsub(a[1], b[1]), dy = lmb::dsub(a[2], b[2]);
+  return lmb::dadd(lmb::dmul(dx, dx), lmb::dmul(dy, dy));
+}
+
+__global__ void cell_insert_kernel(const PreState *st, const double *centres, int *head, int *next,
+                                   int gcx, int gcy) {
+  const unsigned n = st->n_keep;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int cx = min(max((int)(centres[(size_t)i * 4 + 1] / kCell), 0), gcx - 1);
+    const int cy = min(max((int)(centres[(size_t)i * 4 + 2] / kCell), 0), gcy - 1);
+    next[i] = atomicExch(head + cy * gcx + cx, (int)i);
+  }
+}
+
+__global__ void cell_pairs_kernel(PreState *st, const double *centres, const int *head,
+                                  const int *next, int gcx, int gcy) {
+  const unsigned n = st->n_keep;
+  double best = __longlong_as_double(0x7ff0000000000000ll);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double *a = centres + (size_t)i * 4;
+    const int cx = min(max((int)(a[1] / kCell), 0), gcx - 1);
+    const int cy = min(max((int)(a[2] / kCell), 0), gcy - 1);
+    for (int yy = max(cy - 1, 0); yy <= min(cy + 1, gcy - 1); ++yy)
+      for (int xx = max(cx - 1, 0); xx <= min(cx + 1, gcx - 1); ++xx)
+        for (int j = head[yy * gcx + xx]; j >= 0; j = next[j])
+          if ((unsigned)j > i) best = fmin(best, pair_d2(a, centres + (size_t)j * 4));
+  }
+  atomicMin(&st->best, (unsigned long long)__double_as_longlong(best));
+}
+
+// Pairs in cells that are not neighbours lie more than a cell apart, so the
+// grid's answer is exact when it is within a cell; otherwise every pair.
+__global__ void brute_pairs_kernel(PreState *st, const double *centres) {
+  const double cell2 = (double)kCell * (double)kCell;
+  if (__longlong_as_double((long long)st->best) <= cell2) return;
+  const unsigned n = st->n_keep;
+  double best = __longlong_as_double(0x7ff0000000000000ll);
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (unsigned j = i + 1; j < n; ++j)
+      best = fmin(best, pair_d2(centres + (size_t)i * 4, centres + (size_t)j * 4));
+  atomicMin(&st->best, (unsigned long long)__double_as_longlong(best));
+}
+
+// ---- Gaussian blur ---------------------------------------------------------------
+// scipy's symmetric correlation: w_c*x_0, then + (x_-j + x_+j) * w_j from the
+// outermost pair inwards, every operation rounded on its own.
+template <typename TIn>
+__global__ void blur_rows_kernel(const TIn *in, const double *wts, int r, int ny, int nx,
+                                 double *out) {
+  extern __shared__ double w[];
+  for (int j = threadIdx.x; j <= 2 * r; j += blockDim.x) w[j] = wts[j];
+  __syncthreads();
+  const size_t n = (size_t)ny * nx;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / nx), x = (int)(i % nx);
+    double acc = lmb::dmul(to_f64(in[i]), w[r]);
+    for (int j = r; j >= 1; --j) {
+      const double a = to_f64(in[(size_t)mirror(y - j, ny) * nx + x]);
+      const double b = to_f64(in[(size_t)mirror(y + j, ny) * nx + x]);
+      acc = lmb::dadd(acc, lmb::dmul(lmb::dadd(a, b), w[r - j]));
+    }
+    out[i] = acc;
+  }
+}
+
+template <typename TOut>
+__global__ void blur_cols_kernel(const double *in, const double *wts, int r, int ny, int nx,
+                                 TOut *out) {
+  extern __shared__ double w[];
+  for (int j = threadIdx.x; j <= 2 * r; j += blockDim.x) w[j] = wts[j];
+  __syncthreads();
+  const size_t n = (size_t)ny * nx;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const double *row = in + (i - x);
+    double acc = lmb::dmul(row[x], w[r]);
+    for (int j = r; j >= 1; --j)
+      acc = lmb::dadd(acc, lmb::dmul(lmb::dadd(row[mirror(x - j, nx)], row[mirror(x + j, nx)]), w[r - j]));
+    out[i] = (TOut)acc;
+  }
+}
+
+// ---- median ------------------------------------------------------------------------
+__global__ void rank_keys_kernel(const double *img, unsigned long long *keys, unsigned *idx,
+                                 size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    keys[i] = okey(img[i]);
+    idx[i] = (unsigned)i;
+  }
+}
+
+__global__ void rank_flags_kernel(const unsigned long long *keys, unsigned *flag, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+__global__ void rank_scatter_kernel(const unsigned long long *keys, const unsigned *idx,
+                                    const unsigned *flag, const unsigned *incl, unsigned *rank,
+                                    double *vals, unsigned *n_distinct, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const unsigned r = incl[i] - 1u;
+    rank[idx[i]] = r;
+    if (flag[i]) vals[r] = okey_value(keys[i]);
+    if (i == n - 1) *n_distinct = incl[i];
+  }
+}
+
+struct MedWarp {
+  unsigned *h;     // kMedLevels x 256 counters of this warp
+  int L;           // digits in a rank
+  unsigned pp[kMedLevels];  // rank prefix (digits above level l) of the current path
+  int path[kMedLevels];
+};
+
+__device__ __forceinline__ unsigned med_digit(unsigned r, int l, int L) {
+  return (r >> (8 * (L - 1 - l))) & 255u;
+}
+__device__ __forceinline__ unsigned med_prefix(unsigned r, int l, int L) {
+  const int sh = 8 * (L - l);
+  return sh >= 32 ? 0u : (r >> sh);
+}
+
+__device__ __forceinline__ void med_update(MedWarp &m, unsigned r, unsigned delta) {
+  atomicAdd(m.h + med_digit(r, 0, m.L), delta);
+  for (int l = 1; l < m.L; ++l) {
+    if (med_prefix(r, l, m.L) != m.pp[l]) break;
+    atomicAdd(m.h + l * 256 + med_digit(r, l, m.L), delta);
+  }
+}
+
+// Fill level l from the whole window (ranks whose digits above l follow the path).
+__device__ void med_fill(MedWarp &m, int l, const unsigned *rk, int ny, int nx, int x, int y,
+                         int lo, int hi) {
+  const int lane = threadIdx.x & 31;
+  for (int j = lane; j < 256; j += 32) m.h[l * 256 + j] = 0;
+  __syncwarp();
+  for (int dy = -lo; dy <= hi; ++dy) {
+    const unsigned *row = rk + (size_t)mirror(y + dy, ny) * nx;
+    for (int dx = -lo + lane; dx <= hi; dx += 32) {
+      const unsigned r = row[mirror(x + dx, nx)];
+      if (l == 0 || med_prefix(r, l, m.L) == m.pp[l]) atomicAdd(m.h + l * 256 + med_digit(r, l, m.L), 1u);
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kMedWarps * 32)
+    median_kernel(const unsigned *rk, const double *vals, const unsigned *n_distinct, int ny, int nx,
+                  int s, int seg, double *out) {
+  __shared__ __align__(16) unsigned hist[kMedWarps][kMedLevels * 256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nseg = (ny + seg - 1) / seg;
+  const long long task = (long long)blockIdx.x * kMedWarps + warp;
+  if (task >= (long long)nx * nseg) return;
+  const int x = (int)(task % nx), sg = (int)(task / nx);
+  const int y0 = sg * seg, y1 = min(ny, y0 + seg);
+  const unsigned D = *n_distinct;
+  const int bits = D <= 1 ? 1 : 32 - __clz(D - 1);
+  MedWarp m;
+  m.h = hist[warp];
+  m.L = (bits + 7) / 8;
+  for (int l = 0; l < kMedLevels; ++l) {
+    m.path[l] = -1;
+    m.pp[l] = 0xffffffffu;
+  }
+  m.pp[0] = 0;
+  const int lo = s / 2, hi = s - 1 - lo;
+  const unsigned long long k = ((unsigned long long)s * s) / 2;
+  med_fill(m, 0, rk, ny, nx, x, y0, lo, hi);
+  int rb = 1;  // shallowest level whose histogram must be refilled
+  for (int y = y0; y < y1; ++y) {
+    if (y > y0) {
+      const unsigned *ro = rk + (size_t)mirror(y - 1 - lo, ny) * nx;
+      const unsigned *ri = rk + (size_t)mirror(y + hi, ny) * nx;
+      for (int dx = -lo + lane; dx <= hi; dx += 32) {
+        const int c = mirror(x + dx, nx);
+        med_update(m, ro[c], 0xffffffffu);
+        med_update(m, ri[c], 1u);
+      }
+      __syncwarp();
+    }
+    unsigned long long kres = k;
+    unsigned rank = 0;
+    for (int l = 0; l < m.L; ++l) {
+      if (l >= rb) {
+        med_fill(m, l, rk, ny, nx, x, y, lo, hi);
+        rb = l + 1;
+      }
+      const int d = (int)warp_find_digit(m.h + l * 256, kres);
+      rank = (rank << 8) | (unsigned)d;
+      if (d != m.path[l]) {
+        m.path[l] = d;
+        for (int q = l + 1; q < m.L; ++q) m.pp[q] = 0xffffffffu;
+        if (l + 1 < m.L) m.pp[l + 1] = rank;
+        if (rb > l + 1) rb = l + 1;
+      } else if (l + 1 < m.L) {
+        m.pp[l + 1] = rank;
+      }
+    }
+    // a rank outside the distinct values would mean inconsistent histograms
+    if (lane == 0) out[(size_t)y * nx + x] = rank < D ? vals[rank] : __longlong_as_double(0x7ff8000000000000ll);
+  }
+}
+
+}  // namespace
+
+// ---- handle ------------------------------------------------------------------------
+struct lmb_pre {
+  int device = 0, ny = 0, nx = 0, num_sms = 148;
+  size_t npx = 0, nblocks = 0;
+  cudaStream_t st = nullptr;
+  void *d_raw = nullptr;
+  double *d_bg = nullptr, *d_sub = nullptr, *d_tmp = nullptr;
+  void *d_out = nullptr;
+  uint16_t *d_t16 = nullptr, *d_filt = nullptr;
+  int *d_par = nullptr, *d_cid = nullptr, *d_lab = nullptr, *d_flab = nullptr;
+  Comps c{};
+  unsigned long long *d_flags = nullptr, *d_pos = nullptr, *d_compact = nullptr;
+  double *d_centres = nullptr, *d_w = nullptr;
+  int *d_stats = nullptr, *d_head = nullptr, *d_next = nullptr;
+  int gcx = 1, gcy = 1;
+  PreState *d_state = nullptr, *h_state = nullptr;
+  void *d_cub = nullptr;
+  size_t cub_bytes = 0;
+  // median scratch, allocated on first use
+  unsigned long long *m_keys = nullptr, *m_keys2 = nullptr;
+  unsigned *m_idx = nullptr, *m_idx2 = nullptr, *m_flag = nullptr, *m_incl = nullptr,
+           *m_rank = nullptr, *m_nd = nullptr;
+  double *m_vals = nullptr, *m_img = nullptr;
+  void *m_cub = nullptr;
+  size_t m_cub_bytes = 0;
+  bool segmented = false;
+  lmb_pre_counts last{};
+};
+
+namespace {
+
+int check_pre(lmb_pre *p) {
+  if (!p) {
+    set_error("null preprocessing handle");
+    return LMB_ERR_INVALID;
+  }
+  LMB_CUDA(cudaSetDevice(p->device));
+  return LMB_OK;
+}
+
+void free_pre(lmb_pre *p) {
+  if (!p) return;
+  cudaSetDevice(p->device);
+  if (p->st) cudaStreamSynchronize(p->st);
+  void *bufs[] = {p->d_raw, p->d_bg, p->d_sub, p->d_tmp, p->d_out, p->d_t16, p->d_filt, p->d_par,
+                  p->d_cid, p->d_lab, p->d_flab, p->c.area, p->c.x0, p->c.y0, p->c.x1, p->c.y1,
+                  p->c.fb, p->c.sw, p->c.swx, p->c.swy, p->c.label, p->c.keep, p->d_flags,
+                  p->d_pos, p->d_compact, p->d_centres, p->d_w, p->d_stats, p->d_head, p->d_next,
+                  p->d_state, p->d_cub, p->m_keys, p->m_keys2, p->m_idx, p->m_idx2, p->m_flag,
+                  p->m_incl, p->m_rank, p->m_nd, p->m_vals, p->m_img, p->m_cub};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  if (p->h_state) cudaFreeHost(p->h_state);
+  if (p->st) cudaStreamDestroy(p->st);
+  delete p;
+}
+
+template <typename T>
+int alloc(T **ptr, size_t count) {
+  LMB_CUDA(cudaMalloc(reinterpret_cast<void **>(ptr), std::max<size_t>(count, 1) * sizeof(T)));
+  return LMB_OK;
+}
+
+size_t pre_dtype_bytes(int dtype) {
+  return dtype == LMB_F64 ? 8 : dtype == LMB_F32 ? 4 : dtype == LMB_U16 ? 2 : 1;
+}
+
+template <typename F>
+int by_dtype(int dtype, F &&f) {
+  switch (dtype) {
+    case LMB_F64: return f((const double *)nullptr);
+    case LMB_F32: return f((const float *)nullptr);
+    case LMB_U16: return f((const uint16_t *)nullptr);
+    case LMB_U8: return f((const uint8_t *)nullptr);
+  }
+  set_error("unknown dtype %d", dtype);
+  return LMB_ERR_INVALID;
+}
+
+int upload_frame(lmb_pre *p, const void *frame, int dtype) {
+  LMB_REQUIRE(frame, "null frame");
+  LMB_CUDA(cudaMemcpyAsync(p->d_raw, frame, p->npx * pre_dtype_bytes(dtype),
+                           cudaMemcpyHostToDevice, p->st));
+  return LMB_OK;
+}
+
+// All 8 radix passes of one order-statistic search.
+int run_select(lmb_pre *p, int mode, unsigned long long k0, int two) {
+  sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, mode, p->npx, k0, two);
+  const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 56 - 8 * pass;
+    sel_hist_kernel<<<g, kT, 0, p->st>>>(p->d_sub, p->npx, p->d_state, mode, shift, p->d_compact);
+    sel_pick_kernel<<<1, 32, 0, p->st>>>(p->d_state, mode, shift);
+  }
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+// np.percentile's order statistics and weight for n values (linear method).
+void percentile_plan(size_t n, double pct, unsigned long long *k0, int *two, double *gamma) {
+  const double q = pct / 100.0;
+  const double vi = (double)(n - 1) * q;
+  double prev = std::floor(vi);
+  if (vi >= (double)(n - 1)) {
+    *k0 = n - 1;
+    *two = 0;
+    prev = -1.0;
+  } else if (vi < 0) {
+    *k0 = 0;
+    *two = 0;
+    prev = 0.0;
+  } else {
+    *k0 = (unsigned long long)prev;
+    *two = 1;
+  }
+  *gamma = vi - prev;
+}
+
+// Components, centres and closest pair from d_t16 / d_par.
+int segment_tail(lmb_pre *p, int min_area, lmb_pre_counts *counts) {
+  const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
+  cudaStream_t st = p->st;
+  merge_kernel<<<g, kT, 0, st>>>(p->d_par, p->ny, p->nx);
+  compress_kernel<<<g, kT, 0, st>>>(p->d_par, p->npx);
+  reset_counts_kernel<<<1, 1, 0, st>>>(p->d_state);
+  roots_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_state, p->c, p->npx);
+  moments_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_t16, p->c, p->ny, p->nx);
+  LMB_CUDA(cudaMemsetAsync(p->d_flags, 0, p->nblocks * sizeof(unsigned long long), st));
+  const unsigned gc = (unsigned)grid_for(p->nblocks, p->num_sms);
+  flags_kernel<<<gc, kT, 0, st>>>(p->d_state, p->c, min_area, p->d_flags, p->nblocks);
+  size_t tb = p->cub_bytes;
+  LMB_CUDA(cub::DeviceScan::InclusiveSum(p->d_cub, tb, p->d_flags, p->d_pos, (int)p->nblocks, st));
+  label_kernel<<<gc, kT, 0, st>>>(p->d_state, p->c, min_area, p->d_pos, p->nblocks,
+                                  p->d_centres, p->d_stats);
+  images_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_t16, p->c, p->d_lab, p->d_filt,
+                                  p->d_flab, p->npx);
+  // closest pair of kept centres
+  LMB_CUDA(cudaMemsetAsync(p->d_head, 0xff, (size_t)p->gcx * p->gcy * sizeof(int), st));
+  cell_insert_kernel<<<gc, kT, 0, st>>>(p->d_state, p->d_centres, p->d_head, p->d_next, p->gcx,
+                                        p->gcy);
+  cell_pairs_kernel<<<gc, kT, 0, st>>>(p->d_state, p->d_centres, p->d_head, p->d_next, p->gcx,
+                                       p->gcy);
+  brute_pairs_kernel<<<p->num_sms * 2, kT, 0, st>>>(p->d_state, p->d_centres);
+  LMB_CUDA(cudaGetLastError());
+  PreState *hs = p->h_state;
+  LMB_CUDA(cudaMemcpyAsync(hs, p->d_state, sizeof(PreState), cudaMemcpyDeviceToHost, st));
+  LMB_CUDA(cudaStreamSynchronize(st));
+  lmb_pre_counts out{};
+  out.threshold = hs->thresh;
+  out.n_labels = (int32_t)hs->n_labels;
+  out.n_centres = (int32_t)hs->n_keep;
+  double best;
+  memcpy(&best, &hs->best, sizeof(best));
+  out.min_dist2 = hs->n_keep >= 2 ? best : std::numeric_limits<double>::infinity();
+  p->last = out;
+  p->segmented = true;
+  if (counts) *counts = out;
+  return LMB_OK;
+}
+
+int ensure_median_scratch(lmb_pre *p) {
+  if (p->m_keys) return LMB_OK;
+  int rc;
+  if ((rc = alloc(&p->m_keys, p->npx)) || (rc = alloc(&p->m_keys2, p->npx)) ||
+      (rc = alloc(&p->m_idx, p->npx)) || (rc = alloc(&p->m_idx2, p->npx)) ||
+      (rc = alloc(&p->m_flag, p->npx)) || (rc = alloc(&p->m_incl, p->npx)) ||
+      (rc = alloc(&p->m_rank, p->npx)) || (rc = alloc(&p->m_nd, 1)) ||
+      (rc = alloc(&p->m_vals, p->npx)) || (rc = alloc(&p->m_img, p->npx)))
+    return rc;
+  size_t a = 0, b = 0;
+  LMB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, a, p->m_keys, p->m_keys2, p->m_idx, p->m_idx2,
+                                           (int)p->npx));
+  LMB_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, p->m_flag, p->m_incl, (int)p->npx));
+  p->m_cub_bytes = std::max(a, b);
+  LMB_CUDA(cudaMalloc(&p->m_cub, p->m_cub_bytes));
+  return LMB_OK;
+}
+
+// One median pass of d_in into d_out (both float64 on the device).
+int median_pass(lmb_pre *p, const double *d_in, double *d_out, int size) {
+  cudaStream_t st = p->st;
+  const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
+  rank_keys_kernel<<<g, kT, 0, st>>>(d_in, p->m_keys, p->m_idx, p->npx);
+  size_t tb = p->m_cub_bytes;
+  LMB_CUDA(cub::DeviceRadixSort::SortPairs(p->m_cub, tb, p->m_keys, p->m_keys2, p->m_idx,
+                                           p->m_idx2, (int)p->npx, 0, 64, st));
+  rank_flags_kernel<<<g, kT, 0, st>>>(p->m_keys2, p->m_flag, p->npx);
+  tb = p->m_cub_bytes;
+  LMB_CUDA(cub::DeviceScan::InclusiveSum(p->m_cub, tb, p->m_flag, p->m_incl, (int)p->npx, st));
+  rank_scatter_kernel<<<g, kT, 0, st>>>(p->m_keys2, p->m_idx2, p->m_flag, p->m_incl, p->m_rank,
+                                        p->m_vals, p->m_nd, p->npx);
+  // row segments: enough warps to fill every SM several times over
+  const long long want = (long long)p->num_sms * 64 * 2;
+  int seg = (int)std::max<long long>(16, ((long long)p->ny * p->nx + want - 1) / want);
+  seg = std::min(seg, p->ny);
+  const long long tasks = (long long)p->nx * ((p->ny + seg - 1) / seg);
+  const unsigned blocks = (unsigned)((tasks + kMedWarps - 1) / kMedWarps);
+  median_kernel<<<blocks, kMedWarps * 32, 0, st>>>(p->m_rank, p->m_vals, p->m_nd, p->ny, p->nx,
+                                                   size, seg, d_out);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **out) {
+  LMB_REQUIRE(out, "null output");
+  *out = nullptr;
+  LMB_REQUIRE(nr_px_y > 0 && nr_px_x > 0, "frame size %d x %d", nr_px_y, nr_px_x);
+  LMB_REQUIRE((long long)nr_px_y * nr_px_x < (1ll << 31), "frame of %lld pixels is too large",
+              (long long)nr_px_y * nr_px_x);
+  LMB_CUDA(cudaSetDevice(device));
+  lmb_pre *p = new lmb_pre();
+  p->device = device;
+  p->ny = nr_px_y;
+  p->nx = nr_px_x;
+  p->npx = (size_t)nr_px_y * nr_px_x;
+  p->nblocks = (size_t)((nr_px_y + 1) / 2) * ((nr_px_x + 1) / 2);
+  p->gcx = (nr_px_x + kCell - 1) / kCell;
+  p->gcy = (nr_px_y + kCell - 1) / kCell;
+  cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, device);
+  int rc = LMB_OK;
+  auto fail = [&](int r) {
+    free_pre(p);
+    return r;
+  };
+  if (cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(cuda_fail(cudaGetLastError(), "cudaStreamCreate", __FILE__, __LINE__));
+  const size_t n = p->npx, nb = p->nblocks;
+  if ((rc = alloc(reinterpret_cast<double **>(&p->d_raw), n)) || (rc = alloc(&p->d_bg, n)) ||
+      (rc = alloc(&p->d_sub, n)) || (rc = alloc(&p->d_tmp, n)) ||
+      (rc = alloc(reinterpret_cast<double **>(&p->d_out), n)) || (rc = alloc(&p->d_t16, n)) ||
+      (rc = alloc(&p->d_filt, n)) || (rc = alloc(&p->d_par, n)) || (rc = alloc(&p->d_cid, n)) ||
+      (rc = alloc(&p->d_lab, n)) || (rc = alloc(&p->d_flab, n)) || (rc = alloc(&p->c.area, nb)) ||
+      (rc = alloc(&p->c.x0, nb)) || (rc = alloc(&p->c.y0, nb)) || (rc = alloc(&p->c.x1, nb)) ||
+      (rc = alloc(&p->c.y1, nb)) || (rc = alloc(&p->c.fb, nb)) || (rc = alloc(&p->c.sw, nb)) ||
+      (rc = alloc(&p->c.swx, nb)) || (rc = alloc(&p->c.swy, nb)) ||
+      (rc = alloc(&p->c.label, nb)) || (rc = alloc(&p->c.keep, nb)) ||
+      (rc = alloc(&p->d_flags, nb)) || (rc = alloc(&p->d_pos, nb)) ||
+      (rc = alloc(&p->d_compact, n)) || (rc = alloc(&p->d_centres, nb * 4)) ||
+      (rc = alloc(&p->d_w, 1024)) || (rc = alloc(&p->d_stats, nb * 5)) ||
+      (rc = alloc(&p->d_head, (size_t)p->gcx * p->gcy)) || (rc = alloc(&p->d_next, nb)) ||
+      (rc = alloc(&p->d_state, 1)))
+    return fail(rc);
+  if (cudaMallocHost(&p->h_state, sizeof(PreState)) != cudaSuccess)
+    return fail(cuda_fail(cudaErrorMemoryAllocation, "cudaMallocHost", __FILE__, __LINE__));
+  memset(p->h_state, 0, sizeof(PreState));
+  p->h_state->best = 0x7ff0000000000000ull;
+  if (cudaMemset(p->d_bg, 0, n * sizeof(double)) != cudaSuccess ||
+      cudaMemset(p->d_state, 0, sizeof(PreState)) != cudaSuccess)
+    return fail(cuda_fail(cudaGetLastError(), "cudaMemset", __FILE__, __LINE__));
+  size_t tb = 0;
+  if (cub::DeviceScan::InclusiveSum(nullptr, tb, p->d_flags, p->d_pos, (int)nb) != cudaSuccess)
+    return fail(cuda_fail(cudaGetLastError(), "scan sizing", __FILE__, __LINE__));
+  p->cub_bytes = tb;
+  if (cudaMalloc(&p->d_cub, std::max<size_t>(tb, 1)) != cudaSuccess)
+    return fail(cuda_fail(cudaErrorMemoryAllocation, "cudaMalloc", __FILE__, __LINE__));
+  *out = p;
+  return LMB_OK;
+}
+
+int lmb_pre_destroy(lmb_pre *p) {
+  if (!p) return LMB_OK;
+  free_pre(p);
+  return LMB_OK;
+}
+
+int lmb_pre_set_background(lmb_pre *p, const double *background) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  if (background)
+    LMB_CUDA(cudaMemcpyAsync(p->d_bg, background, p->npx * sizeof(double), cudaMemcpyHostToDevice,
+                             p->st));
+  else
+    LMB_CUDA(cudaMemsetAsync(p->d_bg, 0, p->npx * sizeof(double), p->st));
+  LMB_CUDA(cudaStreamSynchronize(p->st));
+  return LMB_OK;
+}
+
+int lmb_pre_get_background(lmb_pre *p, double *out) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(out, "null output");
+  LMB_CUDA(cudaMemcpyAsync(out, p->d_bg, p->npx * sizeof(double), cudaMemcpyDeviceToHost, p->st));
+  LMB_CUDA(cudaStreamSynchronize(p->st));
+  return LMB_OK;
+}
+
+int lmb_pre_median(lmb_pre *p, const void *frame, int32_t dtype, int32_t size, int32_t passes,
+                   double *out) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(size >= 1, "median size %d", size);
+  LMB_REQUIRE(!(p->ny > 1 && size >= 8 * p->ny) && !(p->nx > 1 && size >= 8 * p->nx),
+              "median size %d reaches 8x the %d x %d frame", size, p->ny, p->nx);
+  if ((rc = upload_frame(p, frame, dtype))) return rc;
+  if ((rc = ensure_median_scratch(p))) return rc;
+  const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
+  rc = by_dtype(dtype, [&](auto tag) {
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
+    to_f64_kernel<T><<<g, kT, 0, p->st>>>(static_cast<const T *>(p->d_raw), p->d_bg, p->npx);
+    return LMB_OK;
+  });
+  if (rc) return rc;
+  if (size > 1) {
+    for (int i = 0; i < passes; ++i) {
+      LMB_CUDA(cudaMemcpyAsync(p->m_img, p->d_bg, p->npx * sizeof(double),
+                               cudaMemcpyDeviceToDevice, p->st));
+      if ((rc = median_pass(p, p->m_img, p->d_bg, size))) return rc;
+    }
+  }
+  if (out)
+    LMB_CUDA(cudaMemcpyAsync(out, p->d_bg, p->npx * sizeof(double), cudaMemcpyDeviceToHost, p->st));
+  LMB_CUDA(cudaStreamSynchronize(p->st));
+  return LMB_OK;
+}
+
+int lmb_pre_segment(lmb_pre *p, const void *frame, int32_t dtype, const lmb_pre_params *prm,
+                    lmb_pre_counts *counts) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(prm, "null parameters");
+  if ((rc = upload_frame(p, frame, dtype))) return rc;
+  const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
+  rc = by_dtype(dtype, [&](auto tag) {
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
+    subtract_kernel<T><<<g, kT, 0, p->st>>>(static_cast<const T *>(p->d_raw), p->d_bg, p->d_sub,
+                                            p->npx);
+    return LMB_OK;
+  });
+  if (rc) return rc;
+  if (prm->override_thresh > 0) {
+    set_thresh_kernel<<<1, 1, 0, p->st>>>(p->d_state, prm->override_thresh);
+  } else if (prm->threshold_method == LMB_THR_FIXED) {
+    set_thresh_kernel<<<1, 1, 0, p->st>>>(p->d_state, prm->threshold_value);
+  } else if (prm->threshold_method == LMB_THR_PERCENTILE) {
+    unsigned long long k0;
+    int two;
+    double gamma;
+    LMB_REQUIRE(prm->threshold_percentile >= 0.0 && prm->threshold_percentile <= 100.0,
+                "Percentiles must be in the range [0, 100]");
+    percentile_plan(p->npx, prm->threshold_percentile, &k0, &two, &gamma);
+    if ((rc = run_select(p, SEL_ALL, k0, two))) return rc;
+    finish_percentile_kernel<<<1, 1, 0, p->st>>>(p->d_state, gamma);
+  } else {
+    LMB_REQUIRE(prm->threshold_method == LMB_THR_ADAPTIVE, "threshold method %d",
+                prm->threshold_method);
+    if ((rc = run_select(p, SEL_NZ, 0, 0))) return rc;
+    finish_median_kernel<<<1, 1, 0, p->st>>>(p->d_state);
+    if ((rc = run_select(p, SEL_ABSDEV, 0, 0))) return rc;
+    finish_adaptive_kernel<<<1, 1, 0, p->st>>>(p->d_state);
+  }
+  apply_kernel<<<g, kT, 0, p->st>>>(p->d_sub, p->d_state, p->d_t16, p->d_par, p->npx);
+  LMB_CUDA(cudaGetLastError());
+  return segment_tail(p, prm->min_area, counts);
+}
+
+int lmb_pre_segment_thresholded(lmb_pre *p, const uint16_t *thresholded, int32_t min_area,
+                                lmb_pre_counts *counts) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(thresholded, "null frame");
+  LMB_CUDA(cudaMemcpyAsync(p->d_t16, thresholded, p->npx * sizeof(uint16_t),
+                           cudaMemcpyHostToDevice, p->st));
+  set_thresh_kernel<<<1, 1, 0, p->st>>>(p->d_state, 0.0);
+  init_parents_kernel<<<(unsigned)grid_for(p->npx, p->num_sms), kT, 0, p->st>>>(p->d_t16,
+                                                                                  p->d_par, p->npx);
+  LMB_CUDA(cudaGetLastError());
+  return segment_tail(p, min_area, counts);
+}
+
+int lmb_pre_centres(lmb_pre *p, double *centres, int32_t cap) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(p->segmented, "no frame segmented yet");
+  const int n = std::min(cap, p->last.n_centres);
+  LMB_REQUIRE(centres || n == 0, "null output");
+  if (n > 0)
+    LMB_CUDA(cudaMemcpy(centres, p->d_centres, (size_t)n * 4 * sizeof(double),
+                        cudaMemcpyDeviceToHost));
+  return LMB_OK;
+}
+
+int lmb_pre_stats(lmb_pre *p, int32_t *stats, int32_t cap) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(p->segmented, "no frame segmented yet");
+  const int n = std::min(cap, p->last.n_labels - 1);
+  LMB_REQUIRE(stats || n == 0, "null output");
+  if (n > 0)
+    LMB_CUDA(cudaMemcpy(stats, p->d_stats, (size_t)n * 5 * sizeof(int32_t),
+                        cudaMemcpyDeviceToHost));
+  return LMB_OK;
+}
+
+int lmb_pre_images(lmb_pre *p, uint16_t *thresholded, int32_t *labels, uint16_t *filt_img,
+                   int32_t *filt_labels) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(p->segmented, "no frame segmented yet");
+  const size_t n = p->npx;
+  if (thresholded)
+    LMB_CUDA(cudaMemcpyAsync(thresholded, p->d_t16, n * 2, cudaMemcpyDeviceToHost, p->st));
+  if (labels) LMB_CUDA(cudaMemcpyAsync(labels, p->d_lab, n * 4, cudaMemcpyDeviceToHost, p->st));
+  if (filt_img)
+    LMB_CUDA(cudaMemcpyAsync(filt_img, p->d_filt, n * 2, cudaMemcpyDeviceToHost, p->st));
+  if (filt_labels)
+    LMB_CUDA(cudaMemcpyAsync(filt_labels, p->d_flab, n * 4, cudaMemcpyDeviceToHost, p->st));
+  LMB_CUDA(cudaStreamSynchronize(p->st));
+  return LMB_OK;
+}
+
+int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, int32_t out_dtype) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(p->segmented, "no frame segmented yet");
+  LMB_REQUIRE(weights && out, "null weights or output");
+  LMB_REQUIRE(radius >= 0 && 2 * radius + 1 <= 1024, "blur radius %d outside 0..511", radius);
+  LMB_REQUIRE(out_dtype == LMB_F64 || out_dtype == LMB_F32, "blur output dtype %d", out_dtype);
+  LMB_CUDA(cudaMemcpyAsync(p->d_w, weights, (size_t)(2 * radius + 1) * sizeof(double),
+                           cudaMemcpyHostToDevice, p->st));
+  const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
+  const size_t sm = (size_t)(2 * radius + 1) * sizeof(double);
+  blur_rows_kernel<uint16_t><<<g, kT, sm, p->st>>>(p->d_filt, p->d_w, radius, p->ny, p->nx,
+                                                   p->d_tmp);
+  if (out_dtype == LMB_F64)
+    blur_cols_kernel<double><<<g, kT, sm, p->st>>>(p->d_tmp, p->d_w, radius, p->ny, p->nx,
+                                                   static_cast<double *>(p->d_out));
+  else
+    blur_cols_kernel<float><<<g, kT, sm, p->st>>>(p->d_tmp, p->d_w, radius, p->ny, p->nx,
+                                                  static_cast<float *>(p->d_out));
+  LMB_CUDA(cudaGetLastError());
+  LMB_CUDA(cudaMemcpyAsync(out, p->d_out, p->npx * (out_dtype == LMB_F64 ? 8 : 4),
+                           cudaMemcpyDeviceToHost, p->st));
+  LMB_CUDA(cudaStreamSynchronize(p->st));
+  return LMB_OK;
+}
+
+}  // extern "C"

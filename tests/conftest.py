@@ -56,8 +56,10 @@ _CACHE = {}
 
 
 def golden_names():
+    """Matching-path cases (the pp_*.npz files are preprocessing fixtures)."""
     return sorted(os.path.splitext(os.path.basename(p))[0]
-                  for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+                  for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if not os.path.basename(p).startswith("pp_"))
 
 
 def golden_case(name) -> GoldenCase:

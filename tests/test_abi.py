@@ -38,6 +38,8 @@ def test_struct_layouts_match_header():
     assert C.sizeof(_lib.LmbSurvivor) == 32
     # 9+9+3 doubles, 4 doubles, 4 int32
     assert C.sizeof(_lib.LmbGeometry) == (21 + 4) * 8 + 4 * 4
+    assert C.sizeof(_lib.LmbPreParams) == 2 * 4 + 3 * 8
+    assert C.sizeof(_lib.LmbPreCounts) == 2 * 8 + 2 * 4
 
 
 def test_geometry_is_bitwise_the_oracle_geometry():
