@@ -383,6 +383,14 @@ int lmb_pre_images(lmb_pre *p, uint16_t *thresholded, int32_t *labels, uint16_t 
  * wire format, laue_image_server.py:79). */
 int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, int32_t out_dtype);
 
+/* Device times (ms, CUDA events on the handle's stream) of the stages of the
+ * last calls: [0] frame upload, [1] subtraction + threshold, [2] components,
+ * centres and closest pair, [3] blur, [4] blur download, [5] median frame
+ * upload, [6] median ranks (last pass), [7] median kernel (last pass).  No
+ * reference counterpart. */
+#define LMB_PRE_STAGES 8
+int lmb_pre_timings(lmb_pre *p, float *ms, int32_t n);
+
 /* Page-locked host buffers, so image uploads run at full link speed.  No
  * reference counterpart (the reference pins per-stream buffers internally,
  * LaueMatchingGPUStream.cu:1041-1075). */

@@ -21,6 +21,7 @@ LMB_ERR_TIMEOUT = -5
 LMB_MAX_SLOTS = 64
 LMB_F64, LMB_F32, LMB_U8, LMB_U16 = 0, 1, 2, 3
 LMB_THR_ADAPTIVE, LMB_THR_PERCENTILE, LMB_THR_FIXED = 0, 1, 2
+LMB_PRE_STAGES = 8
 LMB_VALUE_U8, LMB_VALUE_F64 = 0, 1
 LMB_BUILD_EXACT_FP64 = 1
 LMB_NOALLOC_ORDER_MAX = 1 << 20
@@ -40,7 +41,7 @@ EXPORTS = [
     "lmb_host_alloc", "lmb_host_free",
     "lmb_pre_create", "lmb_pre_destroy", "lmb_pre_median", "lmb_pre_set_background",
     "lmb_pre_get_background", "lmb_pre_segment", "lmb_pre_segment_thresholded",
-    "lmb_pre_centres", "lmb_pre_stats", "lmb_pre_images", "lmb_pre_blur",
+    "lmb_pre_centres", "lmb_pre_stats", "lmb_pre_images", "lmb_pre_blur", "lmb_pre_timings",
 ]
 
 
@@ -158,6 +159,7 @@ def lib():
         "lmb_pre_stats": ([vp, vp, i32], C.c_int),
         "lmb_pre_images": ([vp, vp, vp, vp, vp], C.c_int),
         "lmb_pre_blur": ([vp, vp, i32, vp, i32], C.c_int),
+        "lmb_pre_timings": ([vp, vp, i32], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -34,7 +34,14 @@ constexpr int kT = 256;            // threads of the elementwise kernels
 constexpr int kMedWarps = 8;       // warps per median block
 constexpr int kMedLevels = 4;      // 8-bit digits of a rank (ranks < 2^32)
 constexpr int kCell = 32;          // cell side of the closest-pair grid (pixels)
-constexpr int kSelFramePasses = 3; // selection passes that read the frame
+constexpr int kKeepShift = 40;     // the 8-bit pass that reads the frame and keeps its keys
+constexpr int kHist16Threads = 1024;
+constexpr size_t kHist16Smem = 32768 * sizeof(unsigned);  // 65536 packed 16-bit counters
+constexpr int kPreEvents = 12;
+enum PreEv : int {
+  EV_SEG0 = 0, EV_SEG_UP, EV_SEG_THR, EV_SEG_CC, EV_BLUR0, EV_BLUR_K, EV_BLUR_DL, EV_MED0, EV_MED_UP,
+  EV_MED_RANK, EV_MED_K, EV_MED_PASS
+};
 
 enum SelMode : int { SEL_NZ = 0, SEL_ABSDEV = 1, SEL_ALL = 2 };
 
@@ -79,21 +86,26 @@ struct Select {
   unsigned long long k[2];       // residual ranks sought (k[1] = k[0] + 1 when two)
   unsigned long long prefix[2];  // key bits fixed so far
   unsigned long long n_compact;  // candidates kept for the later passes
+  unsigned long long kmin[2], kmax[2];  // extremes of the keys under each prefix (this pass)
   int two;
   int valid;
+  int done[2];                   // the rank's key is known (all keys under its prefix equal)
+  int pad;
 };
 
 struct PreState {
   Select sel;
-  unsigned int hist[2][256];
+  __align__(16) unsigned int hist[2][256];
   double med;
   double thresh;
+  unsigned int blocks_done;  // blocks of the running selection pass that finished
   unsigned int n_comp;      // components
   unsigned int n_labels;    // components + 1
   unsigned int n_keep;      // components with area >= min_area
-  unsigned int pad;
   unsigned long long best;  // bits of the smallest squared centre distance
 };
+
+static_assert(offsetof(PreState, hist) % 16 == 0, "histogram rows are read as 16-byte vectors");
 
 // ---- conversions -------------------------------------------------------------
 template <typename T>
@@ -125,87 +137,21 @@ __global__ void sel_init_kernel(PreState *st, int mode, unsigned long long n,
     s.k[1] = k0 + 1;
     s.prefix[0] = s.prefix[1] = 0;
     s.n_compact = 0;
+    s.kmin[0] = s.kmin[1] = ~0ull;
+    s.kmax[0] = s.kmax[1] = 0;
+    s.done[0] = s.done[1] = 0;
     s.two = mode == SEL_ALL ? two : 0;
     s.valid = 1;
   }
 }
 
-__device__ __forceinline__ bool sel_candidate(int mode, double v, double med, double &val) {
-  if (mode != SEL_ALL && !(v > 0.0)) return false;
-  val = mode == SEL_ABSDEV ? fabs(lmb::dsub(v, med)) : v;
-  return true;
-}
-
-// One radix pass: histogram of the digit at `shift` of the candidates whose
-// higher digits equal each sought rank's prefix.  Passes 0..2 read the frame
-// (pass 2 also keeps the surviving keys), later passes read those keys.
-__global__ void sel_hist_kernel(const double *frame, size_t n, PreState *st, int mode, int shift,
-                                unsigned long long *compact) {
-  __shared__ unsigned int h[2][256];
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) (&h[0][0])[i] = 0;
-  __syncthreads();
-  const Select s = st->sel;
-  if (s.valid) {
-    const unsigned long long hi = shift >= 56 ? 0ull : (~0ull << (shift + 8));
-    const unsigned long long p0 = s.prefix[0] & hi, p1 = s.prefix[1] & hi;
-    const bool two = s.two != 0 && shift < 56;
-    const double med = st->med;
-    const bool from_frame = shift >= 56 - 8 * (kSelFramePasses - 1);
-    const bool keep = shift == 56 - 8 * (kSelFramePasses - 1);
-    const size_t m = from_frame ? n : (size_t)s.n_compact;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t iters = (m + stride - 1) / stride;
-    for (size_t it = 0; it < iters; ++it) {
-      const size_t i = it * stride + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-      bool hit0 = false, hit1 = false;
-      unsigned long long key = 0;
-      if (i < m) {
-        if (from_frame) {
-          double val;
-          if (sel_candidate(mode, frame[i], med, val)) {
-            key = okey(val);
-            hit0 = (key & hi) == p0;
-            hit1 = two && (key & hi) == p1;
-          }
-        } else {
-          key = compact[i];
-          hit0 = (key & hi) == p0;
-          hit1 = two && (key & hi) == p1;
-        }
-      }
-      const unsigned d = (unsigned)(key >> shift) & 255u;
-      if (hit0) atomicAdd(&h[0][d], 1u);
-      if (hit1) atomicAdd(&h[1][d], 1u);
-      if (keep) {  // warp-aggregated append of the keys still in play
-        const bool k = hit0 || hit1;
-        const unsigned msk = __ballot_sync(0xffffffffu, k);
-        if (msk) {
-          const int lane = threadIdx.x & 31;
-          unsigned long long base = 0;
-          if (lane == __ffs(msk) - 1) base = atomicAdd(&st->sel.n_compact, (unsigned long long)__popc(msk));
-          base = __shfl_sync(0xffffffffu, base, __ffs(msk) - 1);
-          if (k) compact[base + __popc(msk & ((1u << lane) - 1u))] = key;
-        }
-      }
-    }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) {
-    const unsigned v = (&h[0][0])[i];
-    if (v) atomicAdd(&(&st->hist[0][0])[i], v);
-  }
-}
-
-// Digit of `h` (256 bins) holding residual rank k; one warp.
-__device__ __forceinline__ unsigned warp_find_digit(const unsigned *h, unsigned long long &k) {
+// Digit holding residual rank k among 256 bins, lane l holding bins
+// 8l..8l+7 in c[]; one warp.
+__device__ __forceinline__ unsigned warp_find_in(const unsigned (&c)[8], unsigned long long &k) {
   const int lane = threadIdx.x & 31;
-  unsigned c[8];
   unsigned long long sum = 0;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    c[j] = h[lane * 8 + j];
-    sum += c[j];
-  }
+  for (int j = 0; j < 8; ++j) sum += c[j];
   unsigned long long incl = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -228,30 +174,61 @@ __device__ __forceinline__ unsigned warp_find_digit(const unsigned *h, unsigned 
   return digit;
 }
 
-// After a pass: fix the digit of each sought rank, clear the histograms.
-// Pass 0 also learns the candidate count (SEL_NZ / SEL_ABSDEV: the median's
-// ranks, two of them for an even count).
-__global__ void sel_pick_kernel(PreState *st, int mode, int shift) {
-  Select &s = st->sel;
-  const int lane = threadIdx.x;
-  if (shift == 56 && mode != SEL_ALL) {
-    unsigned long long t = 0;
-    for (int j = lane; j < 256; j += 32) t += st->hist[0][j];
-    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (lane == 0) {
-      s.n = t;
-      s.k[0] = t ? (t - 1) / 2 : 0;
-      s.k[1] = s.k[0] + 1;
-      s.two = t > 0 && (t % 2) == 0;
+// The same over a 16-byte aligned shared-memory histogram.
+__device__ __forceinline__ unsigned warp_find_digit(const unsigned *h, unsigned long long &k) {
+  const int lane = threadIdx.x & 31;
+  const uint4 a = reinterpret_cast<const uint4 *>(h)[lane * 2];
+  const uint4 b = reinterpret_cast<const uint4 *>(h)[lane * 2 + 1];
+  const unsigned c[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  return warp_find_in(c, k);
+}
+
+// Per-thread run of equal digits, flushed into the block's histogram when the
+// digit changes: a frame's values crowd a few bins, so most values only bump
+// a register.
+struct DigitRun {
+  unsigned d = 0x100u, n = 0;
+  __device__ __forceinline__ void add(unsigned *hh, unsigned dig) {
+    if (dig == d) {
+      ++n;
+      return;
     }
-    __syncwarp();
+    if (n) atomicAdd(hh + d, n);
+    d = dig;
+    n = 1;
   }
-  if (lane == 0 && s.n == 0) s.valid = 0;
-  __syncwarp();
+  __device__ __forceinline__ void flush(unsigned *hh) {
+    if (n) atomicAdd(hh + d, n);
+    n = 0;
+  }
+};
+
+// After a pass (warp 0 of the grid's last block): fix the digit of each
+// sought rank and clear the histograms.  Pass 0 also learns the candidate
+// count (SEL_NZ / SEL_ABSDEV: the median's ranks, two for an even count).
+__device__ void sel_pick(PreState *st, int mode, int shift) {
+  Select &s = st->sel;
+  const int lane = threadIdx.x & 31;
+  unsigned c0[8], c1[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    c0[j] = __ldcg(&st->hist[0][lane * 8 + j]);
+    c1[j] = __ldcg(&st->hist[1][lane * 8 + j]);
+  }
   if (s.valid) {
     for (int L = 0; L < (s.two ? 2 : 1); ++L) {
+      if (s.done[L]) continue;
+      const int src = L;
+      if (s.kmin[src] == s.kmax[src]) {  // every key under the prefix is this one
+        if (lane == 0) {
+          s.prefix[L] = s.kmin[src];
+          s.done[L] = 1;
+        }
+        __syncwarp();
+        continue;
+      }
       unsigned long long k = s.k[L];
-      const unsigned d = warp_find_digit(shift == 56 ? st->hist[0] : st->hist[L], k);
+      const unsigned d = warp_find_in(src == 0 ? c0 : c1, k);
       if (lane == 0) {
         s.k[L] = k;
         s.prefix[L] |= (unsigned long long)d << shift;
@@ -259,7 +236,320 @@ __global__ void sel_pick_kernel(PreState *st, int mode, int shift) {
       __syncwarp();
     }
   }
+  __syncwarp();
+  if (lane == 0) {
+    s.kmin[0] = s.kmin[1] = ~0ull;
+    s.kmax[0] = s.kmax[1] = 0;
+  }
   for (int j = lane; j < 512; j += 32) (&st->hist[0][0])[j] = 0;
+}
+
+// Key of a selection candidate: non-negative values (every candidate of
+// SEL_NZ and SEL_ABSDEV) only need the sign bit set.
+__device__ __forceinline__ unsigned long long sel_key(int mode, double v) {
+  return mode == SEL_ALL ? okey(v)
+                         : ((unsigned long long)__double_as_longlong(v) | 0x8000000000000000ull);
+}
+
+// One radix pass: histogram of the digit at `shift` of the candidates whose
+// higher digits equal each sought rank's prefix.  Passes 0..2 read the frame
+// (pass 2 also keeps the surviving keys), later passes read those keys.  The
+// last block to finish picks the digits for the next pass.
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void __launch_bounds__(kT, 4)
+    sel_hist_kernel(const double *frame, size_t n, PreState *st, int mode, int shift,
+                    unsigned long long *compact) {
+  constexpr int U = 8;  // values per thread per round
+  __shared__ unsigned int h[2][256];
+  __shared__ Select ss;
+  __shared__ bool last;
+  __shared__ unsigned long long stage[kT * U];  // kept keys of one round
+  __shared__ unsigned n_stage;
+  __shared__ unsigned long long base_s;
+  __shared__ unsigned long long ext[4][kT / 32];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) (&h[0][0])[i] = 0;
+  if (threadIdx.x == 0) {
+    ss = st->sel;
+    n_stage = 0;
+  }
+  __syncthreads();
+  const Select s = ss;
+  const bool two = s.two != 0;
+  // ranks whose key is known already need no more passes
+  if (!s.valid || (s.done[0] && (!two || s.done[1]))) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool act0 = !s.done[0], act1 = two && !s.done[1];
+  const unsigned long long hi = ~0ull << (shift + 8);
+  const unsigned long long p0 = s.prefix[0] & hi, p1 = s.prefix[1] & hi;
+  const double med = st->med;
+  const bool from_frame = shift >= kKeepShift;
+  const bool keep = shift == kKeepShift;
+  const unsigned m = from_frame ? (unsigned)n : (unsigned)s.n_compact;
+  const unsigned stride = gridDim.x * blockDim.x;
+  const unsigned rounds = (m + stride * U - 1) / (stride * U);
+  DigitRun run0, run1;
+  unsigned long long mn0 = ~0ull, mx0 = 0, mn1 = ~0ull, mx1 = 0;
+  for (unsigned it = 0; it < rounds; ++it) {
+    unsigned long long key[U];
+    bool hit0[U], hit1[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned i = (it * U + u) * stride + blockIdx.x * blockDim.x + threadIdx.x;
+      hit0[u] = hit1[u] = false;
+      key[u] = 0;
+      if (i < m) {
+        bool cand = true;
+        if (from_frame) {
+          const double v = frame[i];
+          cand = mode == SEL_ALL || v > 0.0;
+          key[u] = sel_key(mode, mode == SEL_ABSDEV ? fabs(lmb::dsub(v, med)) : v);
+        } else {
+          key[u] = compact[i];
+        }
+        hit0[u] = cand && act0 && (key[u] & hi) == p0;
+        hit1[u] = cand && act1 && (key[u] & hi) == p1;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned d = (unsigned)(key[u] >> shift) & 255u;
+      if (hit0[u]) {
+        run0.add(h[0], d);
+        mn0 = min(mn0, key[u]);
+        mx0 = max(mx0, key[u]);
+      }
+      if (hit1[u]) {
+        run1.add(h[1], d);
+        mn1 = min(mn1, key[u]);
+        mx1 = max(mx1, key[u]);
+      }
+      if (keep) {  // warp-aggregated slot in the block's staging area
+        const bool k = hit0[u] || hit1[u];
+        const unsigned msk = __ballot_sync(0xffffffffu, k);
+        if (msk) {
+          unsigned base = 0;
+          if (lane == __ffs(msk) - 1) base = atomicAdd(&n_stage, (unsigned)__popc(msk));
+          base = __shfl_sync(0xffffffffu, base, __ffs(msk) - 1);
+          if (k) stage[base + __popc(msk & ((1u << lane) - 1u))] = key[u];
+        }
+      }
+    }
+    if (keep) {  // one reservation per block and round for the kept keys
+      __syncthreads();
+      const unsigned ns = n_stage;
+      if (threadIdx.x == 0 && ns) base_s = atomicAdd(&st->sel.n_compact, (unsigned long long)ns);
+      __syncthreads();
+      for (unsigned q = threadIdx.x; q < ns; q += blockDim.x) compact[base_s + q] = stage[q];
+      __syncthreads();
+      if (threadIdx.x == 0) n_stage = 0;
+      __syncthreads();
+    }
+  }
+  run0.flush(h[0]);
+  run1.flush(h[1]);
+  mn0 = warp_min_u64(mn0);
+  mx0 = warp_max_u64(mx0);
+  mn1 = warp_min_u64(mn1);
+  mx1 = warp_max_u64(mx1);
+  if (lane == 0) {
+    ext[0][warp] = mn0;
+    ext[1][warp] = mx0;
+    ext[2][warp] = mn1;
+    ext[3][warp] = mx1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kT / 32; ++w) {
+      mn0 = min(mn0, ext[0][w]);
+      mx0 = max(mx0, ext[1][w]);
+      mn1 = min(mn1, ext[2][w]);
+      mx1 = max(mx1, ext[3][w]);
+    }
+    if (mn0 != ~0ull) {
+      atomicMin(&st->sel.kmin[0], mn0);
+      atomicMax(&st->sel.kmax[0], mx0);
+    }
+    if (mn1 != ~0ull) {
+      atomicMin(&st->sel.kmin[1], mn1);
+      atomicMax(&st->sel.kmax[1], mx1);
+    }
+  }
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) {
+    const unsigned v = (&h[0][0])[i];
+    if (v) atomicAdd(&(&st->hist[0][0])[i], v);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->blocks_done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last && threadIdx.x < 32) {
+    __threadfence();
+    sel_pick(st, mode, shift);
+    if (threadIdx.x == 0) st->blocks_done = 0;
+  }
+}
+
+// ---- first selection pass: 16-bit digits --------------------------------------
+// The top 16 key bits (sign, exponent, 4 mantissa bits) of every candidate are
+// counted in 65536 packed 16-bit counters in shared memory (a block handles at
+// most 65535 values), flushed to a 65536-bin histogram in global memory; the
+// grid's last block finds the bins of the sought ranks with all its threads.
+struct Digit16Run {
+  unsigned d = 0xffffffffu, n = 0;
+  __device__ __forceinline__ void add(unsigned *words, unsigned dig) {
+    if (dig == d) {
+      ++n;
+      return;
+    }
+    flush(words);
+    d = dig;
+    n = 1;
+  }
+  __device__ __forceinline__ void flush(unsigned *words) {
+    if (n) atomicAdd(words + (d >> 1), n << (16 * (d & 1)));
+    n = 0;
+  }
+};
+
+__device__ __forceinline__ unsigned key16(int mode, double v) {
+  return (unsigned)(sel_key(mode, v) >> 48);
+}
+
+// Block of 1024 threads: each owns 64 consecutive bins.
+__device__ void sel_pick16(PreState *st, unsigned *g16, int mode) {
+  __shared__ unsigned long long warp_tot[32];
+  __shared__ unsigned long long total_s;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const uint4 *src = reinterpret_cast<const uint4 *>(g16 + t * 64);
+  unsigned long long mine = 0;
+  {
+    uint4 q[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) q[j] = __ldcg(src + j);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) mine += (unsigned long long)q[j].x + q[j].y + q[j].z + q[j].w;
+  }
+  unsigned long long incl = mine;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    unsigned long long v = warp_tot[lane], x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
+    }
+    warp_tot[lane] = x - v;  // exclusive prefix of the warps
+    if (lane == 31) total_s = x;
+  }
+  __syncthreads();
+  const unsigned long long excl = warp_tot[w] + incl - mine;
+  Select &s = st->sel;
+  if (t == 0) {
+    const unsigned long long tot = total_s;
+    if (mode != SEL_ALL) {
+      s.n = tot;
+      s.k[0] = tot ? (tot - 1) / 2 : 0;
+      s.k[1] = s.k[0] + 1;
+      s.two = tot > 0 && (tot % 2) == 0;
+    }
+    if (s.n == 0) s.valid = 0;
+  }
+  __syncthreads();
+  if (s.valid) {
+    for (int L = 0; L < (s.two ? 2 : 1); ++L) {
+      const unsigned long long k = s.k[L];
+      if (k >= excl && k < excl + mine) {
+        unsigned long long r = k - excl;
+        int jj = 63;
+        for (int j = 0; j < 16 && jj == 63; ++j) {
+          const uint4 q = __ldcg(src + j);
+          const unsigned cc[4] = {q.x, q.y, q.z, q.w};
+          for (int e = 0; e < 4; ++e) {
+            if (4 * j + e == 63) break;
+            if (r < cc[e]) {
+              jj = 4 * j + e;
+              break;
+            }
+            r -= cc[e];
+          }
+        }
+        s.k[L] = r;
+        s.prefix[L] = (unsigned long long)(t * 64 + jj) << 48;
+      }
+    }
+  }
+  __syncthreads();
+  uint4 *dst = reinterpret_cast<uint4 *>(g16 + t * 64);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) dst[j] = make_uint4(0, 0, 0, 0);
+}
+
+// Pass A.  FUSED: also the background subtraction np.maximum(raw - bg, 0),
+// written to `sub` (the selection then costs no extra read of the frame).
+template <typename T, bool FUSED>
+__global__ void __launch_bounds__(kHist16Threads, 1)
+    sel_hist16_kernel(const T *raw, const double *bg, double *sub, unsigned n, PreState *st,
+                      unsigned *g16, int mode) {
+  extern __shared__ unsigned words[];
+  __shared__ bool last;
+  for (int i = threadIdx.x; i < 32768; i += blockDim.x) words[i] = 0;
+  __syncthreads();
+  const double med = st->med;
+  Digit16Run run;
+  constexpr int U = 4;
+  const unsigned stride = gridDim.x * blockDim.x;
+  const unsigned rounds = (n + stride * U - 1) / (stride * U);
+  for (unsigned it = 0; it < rounds; ++it) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned i = (it * U + u) * stride + blockIdx.x * blockDim.x + threadIdx.x;
+      v[u] = 0.0;
+      if (i < n) {
+        if (FUSED) {
+          const double d = lmb::dsub(to_f64(raw[i]), bg[i]);
+          v[u] = (d >= 0.0 || isnan(d)) ? d : 0.0;
+          sub[i] = v[u];
+        } else {
+          v[u] = sub[i];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned i = (it * U + u) * stride + blockIdx.x * blockDim.x + threadIdx.x;
+      if (i < n && (mode == SEL_ALL || v[u] > 0.0))
+        run.add(words, key16(mode, mode == SEL_ABSDEV ? fabs(lmb::dsub(v[u], med)) : v[u]));
+    }
+  }
+  run.flush(words);
+  __syncthreads();
+  for (int wd = threadIdx.x; wd < 32768; wd += blockDim.x) {
+    const unsigned x = words[wd];
+    if (x & 0xffffu) atomicAdd(g16 + 2 * wd, x & 0xffffu);
+    if (x >> 16) atomicAdd(g16 + 2 * wd + 1, x >> 16);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->blocks_done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    sel_pick16(st, g16, mode);
+    if (threadIdx.x == 0) st->blocks_done = 0;
+  }
 }
 
 __device__ __forceinline__ double sel_value(const Select &s, int L) {
@@ -306,22 +596,31 @@ __global__ void reset_counts_kernel(PreState *st) {
 }
 
 // ---- threshold, uint16, components ---------------------------------------------
+// Threshold and uint16 cast (thresholds.py:29-32, preprocess.py:291), and
+// the union-find parents along row runs (see init_parents_kernel).
 __global__ void apply_kernel(const double *sub, const PreState *st, uint16_t *t16, int *par,
-                             size_t n) {
+                             int nx, size_t n) {
   const double thr = st->thresh;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const double v = sub[i];
     const uint16_t u = (v <= thr) ? (uint16_t)0 : u16_cast(v);
     t16[i] = u;
-    par[i] = u ? (int)i : -1;
+    bool left = false;
+    if (u && (i % nx) != 0) {
+      const double vl = sub[i - 1];
+      left = !(vl <= thr) && u16_cast(vl) != 0;
+    }
+    par[i] = u ? (left ? (int)i - 1 : (int)i) : -1;
   }
 }
 
-__global__ void init_parents_kernel(const uint16_t *t16, int *par, size_t n) {
+// Parents start along row runs: a foreground pixel points at its left
+// neighbour when that one is foreground too.
+__global__ void init_parents_kernel(const uint16_t *t16, int *par, int nx, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    par[i] = t16[i] ? (int)i : -1;
+    par[i] = t16[i] ? ((i % nx) != 0 && t16[i - 1] ? (int)i - 1 : (int)i) : -1;
 }
 
 __device__ __forceinline__ int uf_find(int *L, int x) {
@@ -350,28 +649,28 @@ __device__ void uf_union(int *L, int a, int b) {
   }
 }
 
-__global__ void merge_kernel(int *L, int ny, int nx) {
+// Joins each row run S = [s, e] to every run R of the row above that touches
+// it (8-connectivity).  Row runs are already chained, so one join per pair
+// suffices: at q, the leftmost pixel of R within [s-1, e+1], from the pixel
+// max(s, q-1) of S.  Seen from a pixel x of S: the upper-left neighbour when
+// x = s; the upper one when x = s and the upper-left is background; the
+// upper-right one when the upper one is background.
+__global__ void merge_kernel(const uint16_t *t16, int *L, int ny, int nx) {
   const size_t n = (size_t)ny * nx;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    if (__ldcg(L + i) < 0) continue;
     const int y = (int)(i / nx), x = (int)(i % nx);
+    if (y == 0 || !t16[i]) continue;
     const int p = (int)i;
-    if (x > 0 && __ldcg(L + i - 1) >= 0) uf_union(L, p, p - 1);
-    if (y > 0) {
-      const int q = p - nx;
-      if (x > 0 && __ldcg(L + q - 1) >= 0) uf_union(L, p, q - 1);
-      if (__ldcg(L + q) >= 0) uf_union(L, p, q);
-      if (x + 1 < nx && __ldcg(L + q + 1) >= 0) uf_union(L, p, q + 1);
-    }
+    const bool left = x > 0 && t16[i - 1];
+    const uint16_t *up = t16 + (i - nx);
+    const bool ul = x > 0 && up[-1], uc = up[0], ur = x + 1 < nx && up[1];
+    if (ul && !left) uf_union(L, p, p - nx - 1);
+    if (uc && !left && !ul) uf_union(L, p, p - nx);
+    if (ur && !uc) uf_union(L, p, p - nx + 1);
   }
 }
 
-__global__ void compress_kernel(int *L, size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    if (__ldcg(L + i) >= 0) L[i] = uf_find(L, (int)i);
-}
 
 struct Comps {
   int *area, *x0, *y0, *x1, *y1;
@@ -380,10 +679,17 @@ struct Comps {
   int *label, *keep;
 };
 
-__global__ void roots_kernel(const int *L, int *cid, PreState *st, Comps c, size_t n) {
+// Every foreground pixel points straight at its root; each root takes the
+// next component id.
+__global__ void compress_kernel(int *L, int *cid, PreState *st, Comps c, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    if (L[i] != (int)i) continue;
+    if (__ldcg(L + i) < 0) continue;
+    const int r = uf_find(L, (int)i);
+    if (r != (int)i) {
+      L[i] = r;
+      continue;
+    }
     const unsigned id = atomicAdd(&st->n_comp, 1u);
     cid[i] = (int)id;
     c.area[id] = 0;
@@ -492,6 +798,13 @@ __device__ __forceinline__ double pair_d2(const double *a, const double *b) {
   return lmb::dadd(lmb::dmul(dx, dx), lmb::dmul(dy, dy));
 }
 
+// Smallest double over the warp, one atomic per warp that found a pair.
+__device__ __forceinline__ void warp_min_to(unsigned long long *dst, double v) {
+  for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v < __longlong_as_double(0x7ff0000000000000ll))
+    atomicMin(dst, (unsigned long long)__double_as_longlong(v));
+}
+
 __global__ void cell_insert_kernel(const PreState *st, const double *centres, int *head, int *next,
                                    int gcx, int gcy) {
   const unsigned n = st->n_keep;
@@ -515,7 +828,7 @@ __global__ void cell_pairs_kernel(PreState *st, const double *centres, const int
         for (int j = head[yy * gcx + xx]; j >= 0; j = next[j])
           if ((unsigned)j > i) best = fmin(best, pair_d2(a, centres + (size_t)j * 4));
   }
-  atomicMin(&st->best, (unsigned long long)__double_as_longlong(best));
+  warp_min_to(&st->best, best);
 }
 
 // Pairs in cells that are not neighbours lie more than a cell apart, so the
@@ -528,7 +841,7 @@ __global__ void brute_pairs_kernel(PreState *st, const double *centres) {
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     for (unsigned j = i + 1; j < n; ++j)
       best = fmin(best, pair_d2(centres + (size_t)i * 4, centres + (size_t)j * 4));
-  atomicMin(&st->best, (unsigned long long)__double_as_longlong(best));
+  warp_min_to(&st->best, best);
 }
 
 // ---- Gaussian blur ---------------------------------------------------------------
@@ -572,6 +885,54 @@ __global__ void blur_cols_kernel(const double *in, const double *wts, int r, int
   }
 }
 
+// Both passes for a 32x32 output tile: the mirrored input tile with its halo
+// in shared memory, the axis-0 pass over the tile's rows and halo columns,
+// then the axis-1 pass; the same operations in the same order as the two
+// separate passes, without the float64 intermediate in global memory.
+constexpr int kBlurTile = 32;
+constexpr int kBlurTileMaxR = 32;
+
+size_t blur_tile_smem(int r) {
+  const int W = kBlurTile + 2 * r;
+  return (size_t)(2 * r + 1 + kBlurTile * W) * sizeof(double) + (size_t)W * W * sizeof(uint16_t);
+}
+
+template <typename TOut>
+__global__ void __launch_bounds__(256)
+    blur_tile_kernel(const uint16_t *in, const double *wts, int r, int ny, int nx, TOut *out) {
+  extern __shared__ double sm[];
+  const int W = kBlurTile + 2 * r;
+  double *w = sm;
+  double *vert = sm + (2 * r + 1);
+  uint16_t *tile = reinterpret_cast<uint16_t *>(vert + kBlurTile * W);
+  const int x0 = blockIdx.x * kBlurTile, y0 = blockIdx.y * kBlurTile;
+  const int tid = threadIdx.x;
+  for (int j = tid; j <= 2 * r; j += blockDim.x) w[j] = wts[j];
+  for (int idx = tid; idx < W * W; idx += blockDim.x) {
+    const int ty = idx / W, tx = idx - ty * W;
+    tile[idx] = in[(size_t)mirror(y0 - r + ty, ny) * nx + mirror(x0 - r + tx, nx)];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < kBlurTile * W; idx += blockDim.x) {
+    const int ty = idx / W, tx = idx - ty * W;
+    const uint16_t *col = tile + (ty + r) * W + tx;
+    double acc = lmb::dmul((double)col[0], w[r]);
+    for (int j = r; j >= 1; --j)
+      acc = lmb::dadd(acc, lmb::dmul(lmb::dadd((double)col[-j * W], (double)col[j * W]), w[r - j]));
+    vert[idx] = acc;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < kBlurTile * kBlurTile; idx += blockDim.x) {
+    const int ty = idx / kBlurTile, tx = idx - ty * kBlurTile;
+    const int gy = y0 + ty, gx = x0 + tx;
+    if (gy >= ny || gx >= nx) continue;
+    const double *row = vert + ty * W + tx + r;
+    double acc = lmb::dmul(row[0], w[r]);
+    for (int j = r; j >= 1; --j) acc = lmb::dadd(acc, lmb::dmul(lmb::dadd(row[-j], row[j]), w[r - j]));
+    out[(size_t)gy * nx + gx] = (TOut)acc;
+  }
+}
+
 // ---- median ------------------------------------------------------------------------
 __global__ void rank_keys_kernel(const double *img, unsigned long long *keys, unsigned *idx,
                                  size_t n) {
@@ -600,13 +961,6 @@ __global__ void rank_scatter_kernel(const unsigned long long *keys, const unsign
   }
 }
 
-struct MedWarp {
-  unsigned *h;     // kMedLevels x 256 counters of this warp
-  int L;           // digits in a rank
-  unsigned pp[kMedLevels];  // rank prefix (digits above level l) of the current path
-  int path[kMedLevels];
-};
-
 __device__ __forceinline__ unsigned med_digit(unsigned r, int l, int L) {
   return (r >> (8 * (L - 1 - l))) & 255u;
 }
@@ -615,31 +969,46 @@ __device__ __forceinline__ unsigned med_prefix(unsigned r, int l, int L) {
   return sh >= 32 ? 0u : (r >> sh);
 }
 
-__device__ __forceinline__ void med_update(MedWarp &m, unsigned r, unsigned delta) {
-  atomicAdd(m.h + med_digit(r, 0, m.L), delta);
-  for (int l = 1; l < m.L; ++l) {
-    if (med_prefix(r, l, m.L) != m.pp[l]) break;
-    atomicAdd(m.h + l * 256 + med_digit(r, l, m.L), delta);
+// Add `delta` for rank r to every level whose path prefix it follows, and
+// count it into `below` of the levels where its digit lies under the path's.
+__device__ __forceinline__ void med_update(unsigned *h, const unsigned (&pp)[kMedLevels],
+                                           const int (&path)[kMedLevels], int (&below)[kMedLevels],
+                                           int L, unsigned r, int delta) {
+#pragma unroll
+  for (int l = 0; l < kMedLevels; ++l) {
+    if (l >= L || med_prefix(r, l, L) != pp[l]) break;
+    const unsigned d = med_digit(r, l, L);
+    atomicAdd(h + l * 256 + d, (unsigned)delta);
+    below[l] += (int)d < path[l] ? delta : 0;
   }
 }
 
-// Fill level l from the whole window (ranks whose digits above l follow the path).
-__device__ void med_fill(MedWarp &m, int l, const unsigned *rk, int ny, int nx, int x, int y,
-                         int lo, int hi) {
+// Fill level l from the whole window (ranks whose digits above l equal pp).
+__device__ void med_fill(unsigned *h, int l, int L, unsigned pp, const unsigned *rk, int ny,
+                         int nx, int x, int y, int lo, int hi) {
   const int lane = threadIdx.x & 31;
-  for (int j = lane; j < 256; j += 32) m.h[l * 256 + j] = 0;
+  for (int j = lane; j < 256; j += 32) h[l * 256 + j] = 0;
   __syncwarp();
   for (int dy = -lo; dy <= hi; ++dy) {
     const unsigned *row = rk + (size_t)mirror(y + dy, ny) * nx;
     for (int dx = -lo + lane; dx <= hi; dx += 32) {
       const unsigned r = row[mirror(x + dx, nx)];
-      if (l == 0 || med_prefix(r, l, m.L) == m.pp[l]) atomicAdd(m.h + l * 256 + med_digit(r, l, m.L), 1u);
+      if (l == 0 || med_prefix(r, l, L) == pp) atomicAdd(h + l * 256 + med_digit(r, l, L), 1u);
     }
   }
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kMedWarps * 32)
+// One warp per (column x, segment of rows): the window's ranks are kept as
+// per-level histograms of 8-bit digits.  Level 0 counts every rank; level l
+// counts the ranks whose higher digits equal the median's path so far, and
+// below[l] how many of those have a smaller digit at l than the path.  When
+// the window slides down one row, the leaving and entering rows update both.
+// The median's digit at a level is kept while below <= k < below + count
+// (the common case: a background changes slowly); otherwise a short walk
+// over neighbouring bins or a scan of the level finds it, and the levels
+// under a moved digit are refilled from the whole window.
+__global__ void __launch_bounds__(kMedWarps * 32, 4)
     median_kernel(const unsigned *rk, const double *vals, const unsigned *n_distinct, int ny, int nx,
                   int s, int seg, double *out) {
   __shared__ __align__(16) unsigned hist[kMedWarps][kMedLevels * 256];
@@ -651,49 +1020,91 @@ __global__ void __launch_bounds__(kMedWarps * 32)
   const int y0 = sg * seg, y1 = min(ny, y0 + seg);
   const unsigned D = *n_distinct;
   const int bits = D <= 1 ? 1 : 32 - __clz(D - 1);
-  MedWarp m;
-  m.h = hist[warp];
-  m.L = (bits + 7) / 8;
+  const int L = (bits + 7) / 8;
+  unsigned *h = hist[warp];
+  int path[kMedLevels], below[kMedLevels];
+  unsigned pp[kMedLevels];
+#pragma unroll
   for (int l = 0; l < kMedLevels; ++l) {
-    m.path[l] = -1;
-    m.pp[l] = 0xffffffffu;
+    path[l] = -1;
+    below[l] = 0;
+    pp[l] = 0xffffffffu;
   }
-  m.pp[0] = 0;
+  pp[0] = 0;
   const int lo = s / 2, hi = s - 1 - lo;
   const unsigned long long k = ((unsigned long long)s * s) / 2;
-  med_fill(m, 0, rk, ny, nx, x, y0, lo, hi);
-  int rb = 1;  // shallowest level whose histogram must be refilled
+  med_fill(h, 0, L, 0, rk, ny, nx, x, y0, lo, hi);
+  int rb = 0;  // shallowest level whose digit must be found by a full scan
   for (int y = y0; y < y1; ++y) {
     if (y > y0) {
+      int mine[kMedLevels];
+#pragma unroll
+      for (int l = 0; l < kMedLevels; ++l) mine[l] = 0;
       const unsigned *ro = rk + (size_t)mirror(y - 1 - lo, ny) * nx;
       const unsigned *ri = rk + (size_t)mirror(y + hi, ny) * nx;
       for (int dx = -lo + lane; dx <= hi; dx += 32) {
         const int c = mirror(x + dx, nx);
-        med_update(m, ro[c], 0xffffffffu);
-        med_update(m, ri[c], 1u);
+        med_update(h, pp, path, mine, L, ro[c], -1);
+        med_update(h, pp, path, mine, L, ri[c], 1);
       }
+#pragma unroll
+      for (int l = 0; l < kMedLevels; ++l)
+        if (l < L) below[l] += __reduce_add_sync(0xffffffffu, mine[l]);
       __syncwarp();
     }
     unsigned long long kres = k;
     unsigned rank = 0;
-    for (int l = 0; l < m.L; ++l) {
-      if (l >= rb) {
-        med_fill(m, l, rk, ny, nx, x, y, lo, hi);
-        rb = l + 1;
+#pragma unroll
+    for (int l = 0; l < kMedLevels; ++l) {
+      if (l >= L) break;
+      const unsigned *hl = h + l * 256;
+      bool found = false;
+      if (l < rb) {
+        // keep the digit, or walk a few bins from it
+        long long b = below[l];
+        int d = path[l];
+        for (int step = 0; step < 8; ++step) {
+          const long long c = hl[d];
+          if ((long long)kres < b) {
+            if (d == 0) break;
+            --d;
+            b -= hl[d];
+          } else if ((long long)kres >= b + c) {
+            if (d == 255) break;
+            b += c;
+            ++d;
+          } else {
+            found = true;
+            break;
+          }
+        }
+        if (found) {
+          kres -= (unsigned long long)b;
+          below[l] = (int)b;
+          if (d != path[l]) {
+            path[l] = d;
+            if (rb > l + 1) rb = l + 1;
+          }
+        }
+      } else if (l > 0) {
+        med_fill(h, l, L, pp[l], rk, ny, nx, x, y, lo, hi);
       }
-      const int d = (int)warp_find_digit(m.h + l * 256, kres);
-      rank = (rank << 8) | (unsigned)d;
-      if (d != m.path[l]) {
-        m.path[l] = d;
-        for (int q = l + 1; q < m.L; ++q) m.pp[q] = 0xffffffffu;
-        if (l + 1 < m.L) m.pp[l + 1] = rank;
-        if (rb > l + 1) rb = l + 1;
-      } else if (l + 1 < m.L) {
-        m.pp[l + 1] = rank;
+      if (!found) {
+        const unsigned long long k0 = kres;
+        const int d = (int)warp_find_digit(hl, kres);
+        below[l] = (int)(k0 - kres);
+        if (d != path[l]) {
+          path[l] = d;
+          if (rb > l + 1) rb = l + 1;
+        }
+        if (rb <= l) rb = l + 1;
       }
+      rank = (rank << 8) | (unsigned)path[l];
+      if (l + 1 < kMedLevels) pp[l + 1] = rank;
     }
     // a rank outside the distinct values would mean inconsistent histograms
-    if (lane == 0) out[(size_t)y * nx + x] = rank < D ? vals[rank] : __longlong_as_double(0x7ff8000000000000ll);
+    if (lane == 0)
+      out[(size_t)y * nx + x] = rank < D ? vals[rank] : __longlong_as_double(0x7ff8000000000000ll);
   }
 }
 
@@ -711,6 +1122,7 @@ struct lmb_pre {
   int *d_par = nullptr, *d_cid = nullptr, *d_lab = nullptr, *d_flab = nullptr;
   Comps c{};
   unsigned long long *d_flags = nullptr, *d_pos = nullptr, *d_compact = nullptr;
+  unsigned *d_hist16 = nullptr;  // 65536-bin histogram of the first selection pass
   double *d_centres = nullptr, *d_w = nullptr;
   int *d_stats = nullptr, *d_head = nullptr, *d_next = nullptr;
   int gcx = 1, gcy = 1;
@@ -726,6 +1138,9 @@ struct lmb_pre {
   size_t m_cub_bytes = 0;
   bool segmented = false;
   lmb_pre_counts last{};
+  // stage events: frame upload, threshold, components, blur, download, median ranks, median
+  cudaEvent_t ev[kPreEvents] = {};
+  float ms[LMB_PRE_STAGES] = {};
 };
 
 namespace {
@@ -747,11 +1162,13 @@ void free_pre(lmb_pre *p) {
                   p->d_cid, p->d_lab, p->d_flab, p->c.area, p->c.x0, p->c.y0, p->c.x1, p->c.y1,
                   p->c.fb, p->c.sw, p->c.swx, p->c.swy, p->c.label, p->c.keep, p->d_flags,
                   p->d_pos, p->d_compact, p->d_centres, p->d_w, p->d_stats, p->d_head, p->d_next,
-                  p->d_state, p->d_cub, p->m_keys, p->m_keys2, p->m_idx, p->m_idx2, p->m_flag,
+                  p->d_state, p->d_cub, p->d_hist16, p->m_keys, p->m_keys2, p->m_idx, p->m_idx2, p->m_flag,
                   p->m_incl, p->m_rank, p->m_nd, p->m_vals, p->m_img, p->m_cub};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (p->h_state) cudaFreeHost(p->h_state);
+  for (auto &e : p->ev)
+    if (e) cudaEventDestroy(e);
   if (p->st) cudaStreamDestroy(p->st);
   delete p;
 }
@@ -785,17 +1202,36 @@ int upload_frame(lmb_pre *p, const void *frame, int dtype) {
   return LMB_OK;
 }
 
-// All 8 radix passes of one order-statistic search.
-int run_select(lmb_pre *p, int mode, unsigned long long k0, int two) {
-  sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, mode, p->npx, k0, two);
-  const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
-  for (int pass = 0; pass < 8; ++pass) {
-    const int shift = 56 - 8 * pass;
-    sel_hist_kernel<<<g, kT, 0, p->st>>>(p->d_sub, p->npx, p->d_state, mode, shift, p->d_compact);
-    sel_pick_kernel<<<1, 32, 0, p->st>>>(p->d_state, mode, shift);
+// Blocks of the 16-bit pass: each handles at most 65535 values.
+unsigned hist16_grid(const lmb_pre *p) {
+  return (unsigned)std::max<size_t>((size_t)p->num_sms, p->npx / 60000 + 1);
+}
+
+// One order-statistic search.  The 16-bit first pass has run (fused with
+// the subtraction, or launched here when `first_pass`); the 8-bit passes
+// follow, the first over the frame, the rest over the keys it kept.
+int run_select(lmb_pre *p, int mode, bool first_pass) {
+  if (first_pass)
+    sel_hist16_kernel<double, false><<<hist16_grid(p), kHist16Threads, kHist16Smem, p->st>>>(
+        nullptr, nullptr, p->d_sub, (unsigned)p->npx, p->d_state, p->d_hist16, mode);
+  for (int shift = kKeepShift; shift >= 0; shift -= 8) {
+    // one wave of blocks over the frame; the kept keys' count is on the device
+    const unsigned gp = (unsigned)(p->num_sms * (shift == kKeepShift ? 4 : 2));
+    sel_hist_kernel<<<gp, kT, 0, p->st>>>(p->d_sub, p->npx, p->d_state, mode, shift, p->d_compact);
   }
   LMB_CUDA(cudaGetLastError());
   return LMB_OK;
+}
+
+// Subtraction fused with the 16-bit first selection pass of `mode`.
+int subtract_select(lmb_pre *p, int dtype, int mode) {
+  return by_dtype(dtype, [&](auto tag) {
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
+    sel_hist16_kernel<T, true><<<hist16_grid(p), kHist16Threads, kHist16Smem, p->st>>>(
+        static_cast<const T *>(p->d_raw), p->d_bg, p->d_sub, (unsigned)p->npx, p->d_state,
+        p->d_hist16, mode);
+    return LMB_OK;
+  });
 }
 
 // np.percentile's order statistics and weight for n values (linear method).
@@ -819,13 +1255,13 @@ void percentile_plan(size_t n, double pct, unsigned long long *k0, int *two, dou
 }
 
 // Components, centres and closest pair from d_t16 / d_par.
-int segment_tail(lmb_pre *p, int min_area, lmb_pre_counts *counts) {
+int segment_tail(lmb_pre *p, int min_area, lmb_pre_counts *counts, bool parents_ready) {
   const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
   cudaStream_t st = p->st;
-  merge_kernel<<<g, kT, 0, st>>>(p->d_par, p->ny, p->nx);
-  compress_kernel<<<g, kT, 0, st>>>(p->d_par, p->npx);
+  if (!parents_ready) init_parents_kernel<<<g, kT, 0, st>>>(p->d_t16, p->d_par, p->nx, p->npx);
+  merge_kernel<<<g, kT, 0, st>>>(p->d_t16, p->d_par, p->ny, p->nx);
   reset_counts_kernel<<<1, 1, 0, st>>>(p->d_state);
-  roots_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_state, p->c, p->npx);
+  compress_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_state, p->c, p->npx);
   moments_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_t16, p->c, p->ny, p->nx);
   LMB_CUDA(cudaMemsetAsync(p->d_flags, 0, p->nblocks * sizeof(unsigned long long), st));
   const unsigned gc = (unsigned)grid_for(p->nblocks, p->num_sms);
@@ -844,6 +1280,7 @@ int segment_tail(lmb_pre *p, int min_area, lmb_pre_counts *counts) {
                                        p->gcy);
   brute_pairs_kernel<<<p->num_sms * 2, kT, 0, st>>>(p->d_state, p->d_centres);
   LMB_CUDA(cudaGetLastError());
+  LMB_CUDA(cudaEventRecord(p->ev[EV_SEG_CC], st));
   PreState *hs = p->h_state;
   LMB_CUDA(cudaMemcpyAsync(hs, p->d_state, sizeof(PreState), cudaMemcpyDeviceToHost, st));
   LMB_CUDA(cudaStreamSynchronize(st));
@@ -857,6 +1294,14 @@ int segment_tail(lmb_pre *p, int min_area, lmb_pre_counts *counts) {
   p->last = out;
   p->segmented = true;
   if (counts) *counts = out;
+  return LMB_OK;
+}
+
+// Elapsed device time between two recorded events (the stream is synchronised).
+int stage_times(lmb_pre *p, int a, int b, int slot) {
+  float ms = 0.f;
+  LMB_CUDA(cudaEventElapsedTime(&ms, p->ev[a], p->ev[b]));
+  p->ms[slot] = ms;
   return LMB_OK;
 }
 
@@ -882,6 +1327,7 @@ int ensure_median_scratch(lmb_pre *p) {
 int median_pass(lmb_pre *p, const double *d_in, double *d_out, int size) {
   cudaStream_t st = p->st;
   const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
+  LMB_CUDA(cudaEventRecord(p->ev[EV_MED_PASS], st));
   rank_keys_kernel<<<g, kT, 0, st>>>(d_in, p->m_keys, p->m_idx, p->npx);
   size_t tb = p->m_cub_bytes;
   LMB_CUDA(cub::DeviceRadixSort::SortPairs(p->m_cub, tb, p->m_keys, p->m_keys2, p->m_idx,
@@ -897,9 +1343,11 @@ int median_pass(lmb_pre *p, const double *d_in, double *d_out, int size) {
   seg = std::min(seg, p->ny);
   const long long tasks = (long long)p->nx * ((p->ny + seg - 1) / seg);
   const unsigned blocks = (unsigned)((tasks + kMedWarps - 1) / kMedWarps);
+  LMB_CUDA(cudaEventRecord(p->ev[EV_MED_RANK], st));
   median_kernel<<<blocks, kMedWarps * 32, 0, st>>>(p->m_rank, p->m_vals, p->m_nd, p->ny, p->nx,
                                                    size, seg, d_out);
   LMB_CUDA(cudaGetLastError());
+  LMB_CUDA(cudaEventRecord(p->ev[EV_MED_K], st));
   return LMB_OK;
 }
 
@@ -944,8 +1392,32 @@ int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **o
       (rc = alloc(&p->d_compact, n)) || (rc = alloc(&p->d_centres, nb * 4)) ||
       (rc = alloc(&p->d_w, 1024)) || (rc = alloc(&p->d_stats, nb * 5)) ||
       (rc = alloc(&p->d_head, (size_t)p->gcx * p->gcy)) || (rc = alloc(&p->d_next, nb)) ||
-      (rc = alloc(&p->d_state, 1)))
+      (rc = alloc(&p->d_state, 1)) || (rc = alloc(&p->d_hist16, 65536)))
     return fail(rc);
+  if (cudaMemset(p->d_hist16, 0, 65536 * sizeof(unsigned)) != cudaSuccess)
+    return fail(cuda_fail(cudaGetLastError(), "cudaMemset", __FILE__, __LINE__));
+  {
+    // the 16-bit selection pass uses 128 KiB of shared memory per block
+    const int b = (int)kHist16Smem;
+    cudaError_t e = cudaFuncSetAttribute(sel_hist16_kernel<double, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(sel_hist16_kernel<double, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(sel_hist16_kernel<float, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(sel_hist16_kernel<uint16_t, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(sel_hist16_kernel<uint8_t, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__));
+  }
+  for (auto &e : p->ev)
+    if (cudaEventCreate(&e) != cudaSuccess)
+      return fail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
   if (cudaMallocHost(&p->h_state, sizeof(PreState)) != cudaSuccess)
     return fail(cuda_fail(cudaErrorMemoryAllocation, "cudaMallocHost", __FILE__, __LINE__));
   memset(p->h_state, 0, sizeof(PreState));
@@ -997,7 +1469,9 @@ int lmb_pre_median(lmb_pre *p, const void *frame, int32_t dtype, int32_t size, i
   LMB_REQUIRE(size >= 1, "median size %d", size);
   LMB_REQUIRE(!(p->ny > 1 && size >= 8 * p->ny) && !(p->nx > 1 && size >= 8 * p->nx),
               "median size %d reaches 8x the %d x %d frame", size, p->ny, p->nx);
+  LMB_CUDA(cudaEventRecord(p->ev[EV_MED0], p->st));
   if ((rc = upload_frame(p, frame, dtype))) return rc;
+  LMB_CUDA(cudaEventRecord(p->ev[EV_MED_UP], p->st));
   if ((rc = ensure_median_scratch(p))) return rc;
   const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
   rc = by_dtype(dtype, [&](auto tag) {
@@ -1016,7 +1490,10 @@ int lmb_pre_median(lmb_pre *p, const void *frame, int32_t dtype, int32_t size, i
   if (out)
     LMB_CUDA(cudaMemcpyAsync(out, p->d_bg, p->npx * sizeof(double), cudaMemcpyDeviceToHost, p->st));
   LMB_CUDA(cudaStreamSynchronize(p->st));
-  return LMB_OK;
+  if (size > 1 && passes > 0)
+    return stage_times(p, EV_MED0, EV_MED_UP, 5) || stage_times(p, EV_MED_PASS, EV_MED_RANK, 6) ||
+           stage_times(p, EV_MED_RANK, EV_MED_K, 7);
+  return stage_times(p, EV_MED0, EV_MED_UP, 5);
 }
 
 int lmb_pre_segment(lmb_pre *p, const void *frame, int32_t dtype, const lmb_pre_params *prm,
@@ -1024,19 +1501,20 @@ int lmb_pre_segment(lmb_pre *p, const void *frame, int32_t dtype, const lmb_pre_
   int rc = check_pre(p);
   if (rc) return rc;
   LMB_REQUIRE(prm, "null parameters");
+  LMB_CUDA(cudaEventRecord(p->ev[EV_SEG0], p->st));
   if ((rc = upload_frame(p, frame, dtype))) return rc;
+  LMB_CUDA(cudaEventRecord(p->ev[EV_SEG_UP], p->st));
   const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
-  rc = by_dtype(dtype, [&](auto tag) {
-    using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
-    subtract_kernel<T><<<g, kT, 0, p->st>>>(static_cast<const T *>(p->d_raw), p->d_bg, p->d_sub,
-                                            p->npx);
-    return LMB_OK;
-  });
-  if (rc) return rc;
-  if (prm->override_thresh > 0) {
-    set_thresh_kernel<<<1, 1, 0, p->st>>>(p->d_state, prm->override_thresh);
-  } else if (prm->threshold_method == LMB_THR_FIXED) {
-    set_thresh_kernel<<<1, 1, 0, p->st>>>(p->d_state, prm->threshold_value);
+  if (prm->override_thresh > 0 || prm->threshold_method == LMB_THR_FIXED) {
+    rc = by_dtype(dtype, [&](auto tag) {
+      using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
+      subtract_kernel<T><<<g, kT, 0, p->st>>>(static_cast<const T *>(p->d_raw), p->d_bg,
+                                              p->d_sub, p->npx);
+      return LMB_OK;
+    });
+    if (rc) return rc;
+    set_thresh_kernel<<<1, 1, 0, p->st>>>(
+        p->d_state, prm->override_thresh > 0 ? prm->override_thresh : prm->threshold_value);
   } else if (prm->threshold_method == LMB_THR_PERCENTILE) {
     unsigned long long k0;
     int two;
@@ -1044,19 +1522,28 @@ int lmb_pre_segment(lmb_pre *p, const void *frame, int32_t dtype, const lmb_pre_
     LMB_REQUIRE(prm->threshold_percentile >= 0.0 && prm->threshold_percentile <= 100.0,
                 "Percentiles must be in the range [0, 100]");
     percentile_plan(p->npx, prm->threshold_percentile, &k0, &two, &gamma);
-    if ((rc = run_select(p, SEL_ALL, k0, two))) return rc;
+    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_ALL, p->npx, k0, two);
+    if ((rc = subtract_select(p, dtype, SEL_ALL)) || (rc = run_select(p, SEL_ALL, false)))
+      return rc;
     finish_percentile_kernel<<<1, 1, 0, p->st>>>(p->d_state, gamma);
   } else {
     LMB_REQUIRE(prm->threshold_method == LMB_THR_ADAPTIVE, "threshold method %d",
                 prm->threshold_method);
-    if ((rc = run_select(p, SEL_NZ, 0, 0))) return rc;
+    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_NZ, p->npx, 0, 0);
+    if ((rc = subtract_select(p, dtype, SEL_NZ)) || (rc = run_select(p, SEL_NZ, false)))
+      return rc;
     finish_median_kernel<<<1, 1, 0, p->st>>>(p->d_state);
-    if ((rc = run_select(p, SEL_ABSDEV, 0, 0))) return rc;
+    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_ABSDEV, p->npx, 0, 0);
+    if ((rc = run_select(p, SEL_ABSDEV, true))) return rc;
     finish_adaptive_kernel<<<1, 1, 0, p->st>>>(p->d_state);
   }
-  apply_kernel<<<g, kT, 0, p->st>>>(p->d_sub, p->d_state, p->d_t16, p->d_par, p->npx);
+  apply_kernel<<<g, kT, 0, p->st>>>(p->d_sub, p->d_state, p->d_t16, p->d_par, p->nx, p->npx);
   LMB_CUDA(cudaGetLastError());
-  return segment_tail(p, prm->min_area, counts);
+  LMB_CUDA(cudaEventRecord(p->ev[EV_SEG_THR], p->st));
+  rc = segment_tail(p, prm->min_area, counts, true);
+  if (rc) return rc;
+  return stage_times(p, EV_SEG0, EV_SEG_UP, 0) || stage_times(p, EV_SEG_UP, EV_SEG_THR, 1) ||
+         stage_times(p, EV_SEG_THR, EV_SEG_CC, 2);
 }
 
 int lmb_pre_segment_thresholded(lmb_pre *p, const uint16_t *thresholded, int32_t min_area,
@@ -1067,10 +1554,8 @@ int lmb_pre_segment_thresholded(lmb_pre *p, const uint16_t *thresholded, int32_t
   LMB_CUDA(cudaMemcpyAsync(p->d_t16, thresholded, p->npx * sizeof(uint16_t),
                            cudaMemcpyHostToDevice, p->st));
   set_thresh_kernel<<<1, 1, 0, p->st>>>(p->d_state, 0.0);
-  init_parents_kernel<<<(unsigned)grid_for(p->npx, p->num_sms), kT, 0, p->st>>>(p->d_t16,
-                                                                                  p->d_par, p->npx);
   LMB_CUDA(cudaGetLastError());
-  return segment_tail(p, min_area, counts);
+  return segment_tail(p, min_area, counts, false);
 }
 
 int lmb_pre_centres(lmb_pre *p, double *centres, int32_t cap) {
@@ -1121,22 +1606,42 @@ int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, i
   LMB_REQUIRE(weights && out, "null weights or output");
   LMB_REQUIRE(radius >= 0 && 2 * radius + 1 <= 1024, "blur radius %d outside 0..511", radius);
   LMB_REQUIRE(out_dtype == LMB_F64 || out_dtype == LMB_F32, "blur output dtype %d", out_dtype);
+  LMB_CUDA(cudaEventRecord(p->ev[EV_BLUR0], p->st));
   LMB_CUDA(cudaMemcpyAsync(p->d_w, weights, (size_t)(2 * radius + 1) * sizeof(double),
                            cudaMemcpyHostToDevice, p->st));
   const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
-  const size_t sm = (size_t)(2 * radius + 1) * sizeof(double);
-  blur_rows_kernel<uint16_t><<<g, kT, sm, p->st>>>(p->d_filt, p->d_w, radius, p->ny, p->nx,
-                                                   p->d_tmp);
-  if (out_dtype == LMB_F64)
-    blur_cols_kernel<double><<<g, kT, sm, p->st>>>(p->d_tmp, p->d_w, radius, p->ny, p->nx,
-                                                   static_cast<double *>(p->d_out));
-  else
-    blur_cols_kernel<float><<<g, kT, sm, p->st>>>(p->d_tmp, p->d_w, radius, p->ny, p->nx,
-                                                  static_cast<float *>(p->d_out));
+  if (radius <= kBlurTileMaxR) {
+    const dim3 tg((p->nx + kBlurTile - 1) / kBlurTile, (p->ny + kBlurTile - 1) / kBlurTile);
+    const size_t tsm = blur_tile_smem(radius);
+    if (out_dtype == LMB_F64)
+      blur_tile_kernel<double><<<tg, 256, tsm, p->st>>>(p->d_filt, p->d_w, radius, p->ny, p->nx,
+                                                        static_cast<double *>(p->d_out));
+    else
+      blur_tile_kernel<float><<<tg, 256, tsm, p->st>>>(p->d_filt, p->d_w, radius, p->ny, p->nx,
+                                                       static_cast<float *>(p->d_out));
+  } else {
+    const size_t sm = (size_t)(2 * radius + 1) * sizeof(double);
+    blur_rows_kernel<uint16_t><<<g, kT, sm, p->st>>>(p->d_filt, p->d_w, radius, p->ny, p->nx,
+                                                     p->d_tmp);
+    if (out_dtype == LMB_F64)
+      blur_cols_kernel<double><<<g, kT, sm, p->st>>>(p->d_tmp, p->d_w, radius, p->ny, p->nx,
+                                                     static_cast<double *>(p->d_out));
+    else
+      blur_cols_kernel<float><<<g, kT, sm, p->st>>>(p->d_tmp, p->d_w, radius, p->ny, p->nx,
+                                                    static_cast<float *>(p->d_out));
+  }
   LMB_CUDA(cudaGetLastError());
+  LMB_CUDA(cudaEventRecord(p->ev[EV_BLUR_K], p->st));
   LMB_CUDA(cudaMemcpyAsync(out, p->d_out, p->npx * (out_dtype == LMB_F64 ? 8 : 4),
                            cudaMemcpyDeviceToHost, p->st));
+  LMB_CUDA(cudaEventRecord(p->ev[EV_BLUR_DL], p->st));
   LMB_CUDA(cudaStreamSynchronize(p->st));
+  return stage_times(p, EV_BLUR0, EV_BLUR_K, 3) || stage_times(p, EV_BLUR_K, EV_BLUR_DL, 4);
+}
+
+int lmb_pre_timings(lmb_pre *p, float *ms, int32_t n) {
+  LMB_REQUIRE(p && ms, "null argument");
+  for (int i = 0; i < n && i < LMB_PRE_STAGES; ++i) ms[i] = p->ms[i];
   return LMB_OK;
 }
 

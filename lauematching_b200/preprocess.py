@@ -103,6 +103,15 @@ class DevicePreprocessor:
         check(lib().lmb_pre_get_background(self._h, out.ctypes.data))
         return out
 
+    STAGES = ("upload", "threshold", "components", "blur", "blur_download", "median_upload",
+              "median_ranks", "median")
+
+    def timings(self) -> dict:
+        """Device milliseconds of the stages of the last calls."""
+        ms = (C.c_float * _lib.LMB_PRE_STAGES)()
+        check(lib().lmb_pre_timings(self._h, ms, _lib.LMB_PRE_STAGES))
+        return dict(zip(self.STAGES, [round(float(v), 4) for v in ms]))
+
     # -- segmentation ---------------------------------------------------------
     def segment(self, frame: np.ndarray, method: str = "adaptive", threshold_value: float = 0.0,
                 threshold_percentile: float = 90.0, min_area: int = 10,
@@ -140,27 +149,36 @@ class DevicePreprocessor:
         check(lib().lmb_pre_stats(self._h, st.ctypes.data, n))
         return np.ascontiguousarray(st[:n, :4]), np.ascontiguousarray(st[:n, 4])
 
-    def images(self, thresholded=False, labels=False, filt_img=False, filt_labels=False):
+    def images(self, thresholded=False, labels=False, filt_img=False, filt_labels=False,
+               outs: Optional[dict] = None):
+        """The last segment's frames; ``outs`` may supply the arrays to fill."""
         out = {}
         ptr = {}
         for name, want, dt in (("thresholded", thresholded, np.uint16), ("labels", labels, np.int32),
                                ("filt_img", filt_img, np.uint16),
                                ("filt_labels", filt_labels, np.int32)):
             if want:
-                out[name] = np.empty(self.shape, dt)
-                ptr[name] = out[name].ctypes.data
+                a = outs.get(name) if outs else None
+                if a is None or a.shape != self.shape or a.dtype != dt or \
+                        not a.flags.c_contiguous:
+                    a = np.empty(self.shape, dt)
+                out[name] = a
+                ptr[name] = a.ctypes.data
             else:
                 ptr[name] = None
         check(lib().lmb_pre_images(self._h, ptr["thresholded"], ptr["labels"], ptr["filt_img"],
                                    ptr["filt_labels"]))
         return out
 
-    def blur(self, weights: np.ndarray, radius: int, dtype=np.float64) -> np.ndarray:
+    def blur(self, weights: np.ndarray, radius: int, dtype=np.float64,
+             out: Optional[np.ndarray] = None) -> np.ndarray:
         w = np.ascontiguousarray(weights, dtype=np.float64)
         if w.shape != (2 * radius + 1,):
             raise ValueError("weights must have 2*radius+1 entries")
         dt = np.dtype(dtype)
-        out = np.empty(self.shape, dt)
+        if out is None or out.shape != self.shape or out.dtype != dt or \
+                not out.flags.c_contiguous:
+            out = np.empty(self.shape, dt)
         check(lib().lmb_pre_blur(self._h, w.ctypes.data, int(radius), out.ctypes.data,
                                  _lib.LMB_F64 if dt == np.float64 else _lib.LMB_F32))
         return out
@@ -291,7 +309,7 @@ def _threshold_method(cfg) -> str:
 
 
 def _run(h: DevicePreprocessor, raw_image, cfg, override_thresh, return_intermediates,
-         blur_dtype):
+         blur_dtype, outs=None):
     cnt = h.segment(raw_image, _threshold_method(cfg), cfg["threshold_value"],
                     cfg["threshold_percentile"], cfg["min_area"], override_thresh)
     shape = h.shape
@@ -304,7 +322,7 @@ def _run(h: DevicePreprocessor, raw_image, cfg, override_thresh, return_intermed
                     "labels_unfiltered": im["labels"], "filt_img": im["thresholded"],
                     "filt_labels": im["labels"], "blurred": blurred, "centers": []}
         return blurred, im["thresholded"], im["labels"], []
-    im = h.images(thresholded=inter, labels=inter, filt_img=True, filt_labels=True)
+    im = h.images(thresholded=inter, labels=inter, filt_img=True, filt_labels=True, outs=outs)
     centers = h.centres(int(cnt.n_centres))
     if not centers:
         blurred = np.zeros(shape, dtype=np.float64)
@@ -312,7 +330,7 @@ def _run(h: DevicePreprocessor, raw_image, cfg, override_thresh, return_intermed
         sigma = _sigma_from(len(centers), cnt.min_dist2, cfg["px_x"], cfg["distance"],
                             cfg["orientation_spacing"])
         w, r = gaussian_weights(sigma)
-        blurred = h.blur(w, r, blur_dtype)
+        blurred = h.blur(w, r, blur_dtype, out=outs.get("blurred") if outs else None)
     if inter:
         return {"background": h.background(), "thresholded": im["thresholded"],
                 "labels_unfiltered": im["labels"], "filt_img": im["filt_img"],
@@ -356,11 +374,24 @@ class Preprocessor:
     one device handle and the background uploaded once."""
 
     def __init__(self, cfg: Dict[str, Any], background: Optional[np.ndarray] = None,
-                 *, device: int = 0, blur_dtype=np.float64):
+                 *, device: int = 0, blur_dtype=np.float64, reuse_outputs: bool = False):
+        """``reuse_outputs``: the returned blurred frame, filtered frame and
+        filtered labels are views of page-locked buffers owned by this object
+        and overwritten by the next call (no page faults on fresh arrays,
+        full-speed copies); by default every call returns new arrays, as the
+        reference does."""
         self.cfg = cfg
         self.background = background
         self.blur_dtype = blur_dtype
         self._h = DevicePreprocessor(cfg["nr_px_y"], cfg["nr_px_x"], device)
+        self._outs = None
+        if reuse_outputs:
+            from .engine import PinnedBuffer
+            shape = self._h.shape
+            self._pinned = [PinnedBuffer(shape, blur_dtype), PinnedBuffer(shape, np.uint16),
+                            PinnedBuffer(shape, np.int32)]
+            self._outs = {"blurred": self._pinned[0].array, "filt_img": self._pinned[1].array,
+                          "filt_labels": self._pinned[2].array}
         if background is not None:
             self._h.set_background(background, token=("fixed",))
 
@@ -372,7 +403,7 @@ class Preprocessor:
         if self.background is None:
             _prepare_background(self._h, raw, self.cfg, None)
         return _run(self._h, raw, self.cfg, override_thresh, return_intermediates,
-                    self.blur_dtype)
+                    self.blur_dtype, self._outs)
 
     def close(self):
         self._h.close()

@@ -172,3 +172,21 @@ def test_preprocessor_keeps_its_background_and_float32_output():
         assert np.array_equal(b, z["blurred"].astype(np.float32))
         assert np.array_equal(fl, z["filt_labels"])
     pre.close()
+
+
+def test_reused_page_locked_outputs_hold_the_same_frames():
+    from lauematching_b200 import preprocess as PP
+    from lauematching_b200.engine import PinnedBuffer
+    z = np.load(os.path.join(HERE, "golden", "pp_adaptive_bgmedian.npz"))
+    cfg = json.loads(str(z["cfg"]))
+    pre = PP.Preprocessor(cfg, z["background"], reuse_outputs=True)
+    src = PinnedBuffer(z["raw"].shape, np.float64)
+    src.array[...] = z["raw"]
+    for _ in range(3):
+        b, fi, fl, cen = pre(src.array)
+        assert np.array_equal(bits(b), bits(z["blurred"]))
+        assert np.array_equal(fi, z["filt_img"]) and np.array_equal(fl, z["filt_labels"])
+        assert np.array_equal(bits(centres_array(cen)), bits(z["centers"]))
+    b2 = pre(src.array)[0]
+    assert b2.ctypes.data == b.ctypes.data  # the same buffer, refilled
+    pre.close()
