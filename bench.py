@@ -285,6 +285,77 @@ def merge_timing(space_group, max_angle, device, n_base=800, per=12, seed=5):
             "device_ms": round(t_dev * 1e3, 2), "identical": same}
 
 
+def preprocess_timing(device, parity=True, cpu_port=True, frames=20):
+    """Frame preprocessing (laue_index.preprocess_image's steps) of a 2048^2
+    detector frame on the device: the image server's flow (background from
+    the first frame's median, then per frame subtraction, adaptive threshold,
+    components, centres, blur), timed through the public API, plus the CPU
+    port of the same steps on one frame."""
+    from lauematching_b200 import preprocess as PP, synth
+    from lauematching_b200.engine import PinnedBuffer
+    rng = np.random.default_rng(21)
+    raw = synth.raw_frame(2048, 2048, rng, n_spots=600)
+    cfg = dict(nr_px_x=2048, nr_px_y=2048, filter_radius=101, median_passes=1,
+               threshold_method="adaptive", threshold_value=0.0, threshold_percentile=90.0,
+               min_area=10, px_x=0.2, distance=0.513, orientation_spacing=0.4)
+    h = PP.DevicePreprocessor(2048, 2048, device)
+    med_ms, med_kernel = [], []
+    for i in range(4):
+        t0 = time.perf_counter()
+        bg = h.median(raw, 101, 1)
+        if i:
+            med_ms.append(1e3 * (time.perf_counter() - t0))
+            tm = h.timings()
+            med_kernel.append(tm["median_ranks"] + tm["median"])
+    h.close()
+
+    def run(pre, frame):
+        for _ in range(3):
+            pre(frame)
+        wall, devm = [], []
+        for _ in range(frames):
+            t0 = time.perf_counter()
+            out = pre(frame)
+            wall.append(1e3 * (time.perf_counter() - t0))
+            tm = pre._h.timings()
+            devm.append(tm["threshold"] + tm["components"] + tm["blur"])
+        return float(np.median(wall)), float(np.median(devm)), pre._h.timings(), out
+
+    fresh = PP.Preprocessor(cfg, bg)
+    w_fresh, d_fresh, _, out = run(fresh, raw)
+    pin = PinnedBuffer(raw.shape, np.uint16)
+    pin.array[...] = raw.astype(np.uint16)
+    fast = PP.Preprocessor(cfg, bg, blur_dtype=np.float32, reuse_outputs=True)
+    w_fast, d_fast, stages, _ = run(fast, pin.array)
+    res = {"workload": "2048x2048 detector frame (pedestal + Poisson + 600 spots), background "
+                       "= median of radius 101 computed once, adaptive threshold, min_area 10",
+           "centres": len(out[3]),
+           "device_ms_per_frame": round(d_fast, 4),
+           "device_frames_per_s": round(1e3 / d_fast, 1),
+           "e2e_ms_per_frame": {"float64_frame_new_arrays": round(w_fresh, 3),
+                                "pinned_uint16_frame_reused_outputs_float32_blur": round(w_fast, 3)},
+           "e2e_frames_per_s": round(1e3 / w_fast, 1),
+           "stages_ms": {k: v for k, v in stages.items() if not k.startswith("median")},
+           "median_background_ms": {"radius": 101, "device": round(float(np.median(med_kernel)), 3),
+                                    "e2e": round(float(np.median(med_ms)), 3)}}
+    if parity or cpu_port:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import preprocess_oracle as PO
+        t0 = time.perf_counter()
+        want = PO.preprocess_image(raw, cfg, background=bg)
+        t_port = time.perf_counter() - t0
+        if parity:
+            res["identical_to_oracle"] = bool(
+                np.array_equal(out[0].view(np.uint8), want["blurred"].view(np.uint8))
+                and np.array_equal(out[2], want["filt_labels"]))
+        if cpu_port:
+            res["cpu_port_s_per_frame"] = round(t_port, 3)
+    fresh.close()
+    fast.close()
+    pin.free()
+    return res
+
+
 def run_ours(args, rank, world):
     import torch
     from lauematching_b200 import synth
@@ -486,6 +557,8 @@ def run_ours(args, rank, world):
                    "same_survivor_counts": fg_surv == surv}
 
     merge = merge_timing(p.space_group, p.max_angle, dev) if rank == 0 else None
+    prep = preprocess_timing(dev, parity=not args.no_parity,
+                             cpu_port=not args.no_cpu_baseline) if rank == 0 else None
 
     # ---- roofline of the compare kernel ----------------------------------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -562,6 +635,7 @@ def run_ours(args, rank, world):
         "batched_over_plain": round(value / world / plain_ips, 2),
         "full_gather": full_gather,
         "merge": merge,
+        "preprocess": prep,
         "survivors_per_image": {"min": min(surv), "max": max(surv), "mean": statistics.mean(surv)},
         "dbbuild": {"orientations_per_s": round(N / t_build, 1), "seconds": round(t_build, 3),
                     "hkl_evals_per_s": round(N * len(hkls) / t_build, 1)},
@@ -884,6 +958,8 @@ def main():
                     help="orientations per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--preprocess", action="store_true",
+                    help="only the frame-preprocessing leg (2048^2 frames; --steps frames)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (Poisson arrivals)")
     ap.add_argument("--serve-rates", type=str, default="50,200,500,1000,2000")
     ap.add_argument("--serve-seconds", type=float, default=4.0)
@@ -898,6 +974,10 @@ def main():
         run_reference_gpu(args, rank, world)
     elif args.serve:
         run_serve(args)
+    elif args.preprocess:
+        print(json.dumps(preprocess_timing(0, parity=not args.no_parity,
+                                           cpu_port=not args.no_cpu_baseline,
+                                           frames=max(1, min(args.steps, 200)))), flush=True)
     else:
         run_ours(args, rank, world)
 

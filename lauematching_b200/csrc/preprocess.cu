@@ -109,7 +109,7 @@ static_assert(offsetof(PreState, hist) % 16 == 0, "histogram rows are read as 16
 
 // ---- conversions -------------------------------------------------------------
 template <typename T>
-__global__ void to_f64_kernel(const T *in, double *out, size_t n) {
+__global__ void to_f64_kernel(const T *__restrict__ in, double *__restrict__ out, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
     out[i] = to_f64(in[i]);
@@ -117,7 +117,8 @@ __global__ void to_f64_kernel(const T *in, double *out, size_t n) {
 
 // np.maximum(raw - background, 0.0): NaN stays NaN, -0 stays -0.
 template <typename T>
-__global__ void subtract_kernel(const T *raw, const double *bg, double *sub, size_t n) {
+__global__ void subtract_kernel(const T *__restrict__ raw, const double *__restrict__ bg,
+                                double *__restrict__ sub, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const double d = lmb::dsub(to_f64(raw[i]), bg[i]);
@@ -500,8 +501,8 @@ __device__ void sel_pick16(PreState *st, unsigned *g16, int mode) {
 // written to `sub` (the selection then costs no extra read of the frame).
 template <typename T, bool FUSED>
 __global__ void __launch_bounds__(kHist16Threads, 1)
-    sel_hist16_kernel(const T *raw, const double *bg, double *sub, unsigned n, PreState *st,
-                      unsigned *g16, int mode) {
+    sel_hist16_kernel(const T *__restrict__ raw, const double *__restrict__ bg,
+                      double *__restrict__ sub, unsigned n, PreState *st, unsigned *g16, int mode) {
   extern __shared__ unsigned words[];
   __shared__ bool last;
   for (int i = threadIdx.x; i < 32768; i += blockDim.x) words[i] = 0;
@@ -598,8 +599,8 @@ __global__ void reset_counts_kernel(PreState *st) {
 // ---- threshold, uint16, components ---------------------------------------------
 // Threshold and uint16 cast (thresholds.py:29-32, preprocess.py:291), and
 // the union-find parents along row runs (see init_parents_kernel).
-__global__ void apply_kernel(const double *sub, const PreState *st, uint16_t *t16, int *par,
-                             int nx, size_t n) {
+__global__ void apply_kernel(const double *__restrict__ sub, const PreState *st,
+                             uint16_t *__restrict__ t16, int *__restrict__ par, int nx, size_t n) {
   const double thr = st->thresh;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -775,8 +776,9 @@ __global__ void label_kernel(PreState *st, Comps c, int min_area, const unsigned
   }
 }
 
-__global__ void images_kernel(const int *L, const int *cid, const uint16_t *t16, Comps c,
-                              int *labels, uint16_t *filt, int *flabels, size_t n) {
+__global__ void images_kernel(const int *__restrict__ L, const int *__restrict__ cid,
+                              const uint16_t *__restrict__ t16, Comps c, int *__restrict__ labels,
+                              uint16_t *__restrict__ filt, int *__restrict__ flabels, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const int r = L[i];
@@ -899,7 +901,8 @@ size_t blur_tile_smem(int r) {
 
 template <typename TOut>
 __global__ void __launch_bounds__(256)
-    blur_tile_kernel(const uint16_t *in, const double *wts, int r, int ny, int nx, TOut *out) {
+    blur_tile_kernel(const uint16_t *__restrict__ in, const double *__restrict__ wts, int r, int ny,
+                     int nx, TOut *__restrict__ out) {
   extern __shared__ double sm[];
   const int W = kBlurTile + 2 * r;
   double *w = sm;
