@@ -383,6 +383,18 @@ int lmb_pre_images(lmb_pre *p, uint16_t *thresholded, int32_t *labels, uint16_t 
  * wire format, laue_image_server.py:79). */
 int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, int32_t out_dtype);
 
+/* The blur of lmb_pre_blur straight into image slot `slot` of an engine on the
+ * same device, quantised there as lmb_image_load quantises a host frame, with no
+ * host round trip of the blurred frame.  frame_dtype is the form in which the
+ * reference hands the blurred frame to its matcher: LMB_F32 for the stream
+ * daemon (the image server sends float32, laue_image_server.py:79), LMB_F64 for
+ * the LaueMatchingGPU executable (RunImage writes float64, RunImage.py:290-292);
+ * the slot then holds exactly what loading that frame from the host would give.
+ * im_scale (may be NULL) receives the slot's imScale.  No reference
+ * counterpart: the reference moves the blurred frame through a file or TCP. */
+int lmb_pre_blur_to_slot(lmb_pre *p, const double *weights, int32_t radius, lmb_engine *e,
+                         int32_t slot, int32_t frame_dtype, double *im_scale);
+
 /* Device times (ms, CUDA events on the handle's stream) of the stages of the
  * last calls: [0] frame upload, [1] subtraction + threshold, [2] components,
  * centres and closest pair, [3] blur, [4] blur download, [5] median frame

@@ -42,6 +42,7 @@ EXPORTS = [
     "lmb_pre_create", "lmb_pre_destroy", "lmb_pre_median", "lmb_pre_set_background",
     "lmb_pre_get_background", "lmb_pre_segment", "lmb_pre_segment_thresholded",
     "lmb_pre_centres", "lmb_pre_stats", "lmb_pre_images", "lmb_pre_blur", "lmb_pre_timings",
+    "lmb_pre_blur_to_slot",
 ]
 
 
@@ -160,6 +161,7 @@ def lib():
         "lmb_pre_images": ([vp, vp, vp, vp, vp], C.c_int),
         "lmb_pre_blur": ([vp, vp, i32, vp, i32], C.c_int),
         "lmb_pre_timings": ([vp, vp, i32], C.c_int),
+        "lmb_pre_blur_to_slot": ([vp, vp, i32, vp, i32, i32, dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -1267,6 +1267,49 @@ int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields) {
   return LMB_OK;
 }
 
+}  // extern "C"
+
+namespace lmb {
+
+// A frame already in this engine's device memory (written on another stream
+// that recorded `ready`) into a slot: the dense quantisation of
+// lmb_image_load without any host copy; `consumed` is recorded once the
+// frame has been read, so its producer may overwrite it.
+int engine_load_device_frame(lmb_engine *e, int slot, const void *d_img, int dtype,
+                             int nr_px_y, int nr_px_x, cudaEvent_t ready, cudaEvent_t consumed,
+                             double *im_scale) {
+  int rc = check_engine(e);
+  if (rc) return rc;
+  LMB_REQUIRE(slot >= 0 && slot < LMB_MAX_SLOTS, "slot %d outside 0..%d", slot,
+              LMB_MAX_SLOTS - 1);
+  LMB_REQUIRE(dtype == LMB_F64 || dtype == LMB_F32, "device frame dtype %d", dtype);
+  LMB_REQUIRE(nr_px_y == e->geo.nr_px_y && nr_px_x == e->geo.nr_px_x,
+              "frame of %d x %d pixels, detector of %d x %d", nr_px_y, nr_px_x, e->geo.nr_px_y,
+              e->geo.nr_px_x);
+  LMB_CUDA(cudaStreamWaitEvent(e->ld, e->ev_released[slot], 0));
+  LMB_CUDA(cudaStreamWaitEvent(e->ld, ready, 0));
+  rc = quantize_launch(d_img, dtype, e->npx, e->d_max_bits, e->d_u8 + (size_t)slot * e->npx,
+                       nullptr, e->d_occ, slot, e->d_scale + slot, e->num_sms, e->ld);
+  if (rc) return rc;
+  LMB_CUDA(cudaEventRecord(consumed, e->ld));
+  LMB_CUDA(cudaEventRecord(e->ev_loaded[slot], e->ld));
+  e->loaded_mask |= 1ull << slot;
+  e->f64_mask &= ~(1ull << slot);
+  if (im_scale) {
+    LMB_CUDA(cudaMemcpyAsync(im_scale, e->d_scale + slot, sizeof(double), cudaMemcpyDeviceToHost,
+                             e->ld));
+    e->bytes_d2h += sizeof(double);
+    LMB_CUDA(cudaStreamSynchronize(e->ld));
+  }
+  return LMB_OK;
+}
+
+int engine_device(const lmb_engine *e) { return e ? e->device : -1; }
+
+}  // namespace lmb
+
+extern "C" {
+
 int lmb_host_alloc(uint64_t bytes, void **out) {
   LMB_REQUIRE(out, "null output");
   *out = nullptr;

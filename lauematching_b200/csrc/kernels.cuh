@@ -70,6 +70,10 @@ int synth_orient_launch(uint64_t seed, uint64_t first, uint64_t n, double *d_out
 int quantize_launch(const void *d_img, int dtype, size_t npx, unsigned long long *d_max_bits,
                     uint8_t *d_u8, double *d_f64_keep, unsigned long long *d_occ, int slot,
                     double *d_scale_slot, int num_sms, cudaStream_t st);
+int engine_load_device_frame(lmb_engine *e, int slot, const void *d_img, int dtype,
+                             int nr_px_y, int nr_px_x, cudaEvent_t ready, cudaEvent_t consumed,
+                             double *im_scale);
+int engine_device(const lmb_engine *e);
 int sparse_load_launch(const uint32_t *d_idx, const void *d_val, int dtype, size_t nnz, double mx,
                        uint8_t *d_u8, unsigned long long *d_occ, int slot, double *d_scale_slot,
                        size_t npx, int num_sms, cudaStream_t st);

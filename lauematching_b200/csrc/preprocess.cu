@@ -25,6 +25,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "kernels.cuh"
 
 using namespace lmb;
 
@@ -1144,6 +1145,10 @@ struct lmb_pre {
   // stage events: frame upload, threshold, components, blur, download, median ranks, median
   cudaEvent_t ev[kPreEvents] = {};
   float ms[LMB_PRE_STAGES] = {};
+  // blurred frame handed to an engine: ready on this stream, free once the
+  // engine's quantisation has read it
+  cudaEvent_t ev_out_ready = nullptr, ev_out_free = nullptr;
+  bool out_in_use = false;
 };
 
 namespace {
@@ -1172,6 +1177,8 @@ void free_pre(lmb_pre *p) {
   if (p->h_state) cudaFreeHost(p->h_state);
   for (auto &e : p->ev)
     if (e) cudaEventDestroy(e);
+  if (p->ev_out_ready) cudaEventDestroy(p->ev_out_ready);
+  if (p->ev_out_free) cudaEventDestroy(p->ev_out_free);
   if (p->st) cudaStreamDestroy(p->st);
   delete p;
 }
@@ -1421,6 +1428,9 @@ int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **o
   for (auto &e : p->ev)
     if (cudaEventCreate(&e) != cudaSuccess)
       return fail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
+  if (cudaEventCreateWithFlags(&p->ev_out_ready, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->ev_out_free, cudaEventDisableTiming) != cudaSuccess)
+    return fail(cuda_fail(cudaGetLastError(), "cudaEventCreate", __FILE__, __LINE__));
   if (cudaMallocHost(&p->h_state, sizeof(PreState)) != cudaSuccess)
     return fail(cuda_fail(cudaErrorMemoryAllocation, "cudaMallocHost", __FILE__, __LINE__));
   memset(p->h_state, 0, sizeof(PreState));
@@ -1602,13 +1612,20 @@ int lmb_pre_images(lmb_pre *p, uint16_t *thresholded, int32_t *labels, uint16_t 
   return LMB_OK;
 }
 
-int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, int32_t out_dtype) {
-  int rc = check_pre(p);
-  if (rc) return rc;
+}  // extern "C"
+
+namespace {
+
+// Both blur passes of the last segment's filtered frame into p->d_out.
+int blur_launch(lmb_pre *p, const double *weights, int32_t radius, int32_t out_dtype) {
   LMB_REQUIRE(p->segmented, "no frame segmented yet");
-  LMB_REQUIRE(weights && out, "null weights or output");
+  LMB_REQUIRE(weights, "null weights");
   LMB_REQUIRE(radius >= 0 && 2 * radius + 1 <= 1024, "blur radius %d outside 0..511", radius);
   LMB_REQUIRE(out_dtype == LMB_F64 || out_dtype == LMB_F32, "blur output dtype %d", out_dtype);
+  if (p->out_in_use) {  // an engine may still be reading the previous blurred frame
+    LMB_CUDA(cudaStreamWaitEvent(p->st, p->ev_out_free, 0));
+    p->out_in_use = false;
+  }
   LMB_CUDA(cudaEventRecord(p->ev[EV_BLUR0], p->st));
   LMB_CUDA(cudaMemcpyAsync(p->d_w, weights, (size_t)(2 * radius + 1) * sizeof(double),
                            cudaMemcpyHostToDevice, p->st));
@@ -1635,11 +1652,40 @@ int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, i
   }
   LMB_CUDA(cudaGetLastError());
   LMB_CUDA(cudaEventRecord(p->ev[EV_BLUR_K], p->st));
+  return LMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lmb_pre_blur(lmb_pre *p, const double *weights, int32_t radius, void *out, int32_t out_dtype) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(out, "null output");
+  if ((rc = blur_launch(p, weights, radius, out_dtype))) return rc;
   LMB_CUDA(cudaMemcpyAsync(out, p->d_out, p->npx * (out_dtype == LMB_F64 ? 8 : 4),
                            cudaMemcpyDeviceToHost, p->st));
   LMB_CUDA(cudaEventRecord(p->ev[EV_BLUR_DL], p->st));
   LMB_CUDA(cudaStreamSynchronize(p->st));
   return stage_times(p, EV_BLUR0, EV_BLUR_K, 3) || stage_times(p, EV_BLUR_K, EV_BLUR_DL, 4);
+}
+
+int lmb_pre_blur_to_slot(lmb_pre *p, const double *weights, int32_t radius, lmb_engine *e,
+                         int32_t slot, int32_t frame_dtype, double *im_scale) {
+  int rc = check_pre(p);
+  if (rc) return rc;
+  LMB_REQUIRE(e, "null engine");
+  LMB_REQUIRE(engine_device(e) == p->device, "engine on device %d, preprocessing on device %d",
+              engine_device(e), p->device);
+  if ((rc = blur_launch(p, weights, radius, frame_dtype))) return rc;
+  LMB_CUDA(cudaEventRecord(p->ev_out_ready, p->st));
+  rc = engine_load_device_frame(e, slot, p->d_out, frame_dtype, p->ny, p->nx, p->ev_out_ready,
+                                p->ev_out_free, im_scale);
+  if (rc) return rc;
+  p->out_in_use = true;
+  LMB_CUDA(cudaStreamSynchronize(p->st));
+  return stage_times(p, EV_BLUR0, EV_BLUR_K, 3);
 }
 
 int lmb_pre_timings(lmb_pre *p, float *ms, int32_t n) {

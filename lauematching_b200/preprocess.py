@@ -170,6 +170,22 @@ class DevicePreprocessor:
                                    ptr["filt_labels"]))
         return out
 
+    def blur_to_slot(self, weights: np.ndarray, radius: int, engine, slot: int,
+                     frame_dtype=np.float32) -> float:
+        """The blurred frame straight into an engine slot on this device,
+        quantised as if ``frame_dtype`` copies of it had been loaded from the
+        host; returns the slot's imScale."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        if w.shape != (2 * radius + 1,):
+            raise ValueError("weights must have 2*radius+1 entries")
+        dt = np.dtype(frame_dtype)
+        sc = C.c_double(0.0)
+        check(lib().lmb_pre_blur_to_slot(self._h, w.ctypes.data, int(radius), engine._h,
+                                         int(slot),
+                                         _lib.LMB_F64 if dt == np.float64 else _lib.LMB_F32,
+                                         C.byref(sc)))
+        return sc.value
+
     def blur(self, weights: np.ndarray, radius: int, dtype=np.float64,
              out: Optional[np.ndarray] = None) -> np.ndarray:
         w = np.ascontiguousarray(weights, dtype=np.float64)
@@ -404,6 +420,32 @@ class Preprocessor:
             _prepare_background(self._h, raw, self.cfg, None)
         return _run(self._h, raw, self.cfg, override_thresh, return_intermediates,
                     self.blur_dtype, self._outs)
+
+    def to_slot(self, engine, slot: int, raw_image: np.ndarray, *,
+                override_thresh: float = 0.0, frame_dtype=np.float32, want_centres: bool = False):
+        """Preprocess a raw frame straight into image slot ``slot`` of
+        ``engine`` (same device, same frame size): the slot then holds what
+        loading ``preprocess_image``'s blurred frame, as ``frame_dtype`` (float32:
+        the image server's wire format; float64: RunImage's .bin), would give,
+        without the frame leaving the GPU.  Returns the number of centres (or
+        the centre list with ``want_centres``); ``None`` when the frame has no
+        spots, as the image server then sends nothing (laue_image_server.py:76-77)
+        and the slot is left untouched."""
+        raw = np.asarray(raw_image)
+        if raw.shape != self._h.shape:
+            raise ValueError(f"frame of shape {raw.shape}, expected {self._h.shape}")
+        if self.background is None:
+            _prepare_background(self._h, raw, self.cfg, None)
+        cfg = self.cfg
+        cnt = self._h.segment(raw, _threshold_method(cfg), cfg["threshold_value"],
+                              cfg["threshold_percentile"], cfg["min_area"], override_thresh)
+        if cnt.n_labels <= 1 or cnt.n_centres == 0:
+            return None
+        sigma = _sigma_from(int(cnt.n_centres), cnt.min_dist2, cfg["px_x"], cfg["distance"],
+                            cfg["orientation_spacing"])
+        w, r = gaussian_weights(sigma)
+        self._h.blur_to_slot(w, r, engine, slot, frame_dtype)
+        return self._h.centres(int(cnt.n_centres)) if want_centres else int(cnt.n_centres)
 
     def close(self):
         self._h.close()

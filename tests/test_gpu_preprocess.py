@@ -190,3 +190,42 @@ def test_reused_page_locked_outputs_hold_the_same_frames():
     b2 = pre(src.array)[0]
     assert b2.ctypes.data == b.ctypes.data  # the same buffer, refilled
     pre.close()
+
+
+@pytest.mark.parametrize("frame_dtype", [np.float32, np.float64])
+def test_raw_frames_straight_into_engine_slots(frame_dtype):
+    """Preprocessing into a slot matches exactly as loading the reference's
+    blurred frame (as float32 from the image server, or float64 from RunImage)
+    from the host does."""
+    from lauematching_b200 import params as P, preprocess as PP, synth
+    from lauematching_b200.engine import Engine
+    names = ["adaptive_bgmedian", "override", "fixed_given_bg", "no_components"]
+    zs = [np.load(os.path.join(HERE, "golden", f"pp_{n}.npz")) for n in names]
+    by_shape = {}
+    for n, z in zip(names, zs):
+        by_shape.setdefault(z["raw"].shape, []).append((n, z))
+    for shape, cases in by_shape.items():
+        ny, nx = shape
+        txt = synth.params_text(nr_px=(nx, ny), px=0.0002 * 2048 / max(nx, ny),
+                                min_nr_spots=2, min_intensity=5.0)
+        p = P.parse_params_text(txt)
+        with Engine(p) as e:
+            e.build_db_synthetic(3, 60000, synth.hkls_cubic(6))
+            for n, z in cases:
+                cfg = json.loads(str(z["cfg"]))
+                bg = z["background_in"] if z["background_in"].size else None
+                pre = PP.Preprocessor(cfg, bg)
+                got = pre.to_slot(e, 0, z["raw"], override_thresh=float(z["override_thresh"]),
+                                  frame_dtype=frame_dtype)
+                if z["centers"].shape[0] == 0:
+                    assert got is None
+                    pre.close()
+                    continue
+                assert got == z["centers"].shape[0]
+                e.load_image(1, z["blurred"].astype(frame_dtype))
+                e.match([0, 1], p.min_nr_spots, p.min_intensity)
+                a, na = e.results(0)
+                b, nb = e.results(1)
+                assert na == nb and np.array_equal(a, b), n
+                assert na > 0, n
+                pre.close()
