@@ -68,6 +68,7 @@ class PinnedBuffer:
 class Engine:
     def __init__(self, params: LaueParams, device: int = 0, survivor_capacity: int = 0):
         self.params = params
+        self.device = int(device)
         self.geometry = geometry_from_params(params)
         self.S = int(params.max_nr_spots)
         self.R = 1 + 2 * self.S

@@ -35,7 +35,7 @@ __all__ = [
     "compute_background", "load_background", "enhance_image",
     "find_connected_components", "filter_small_components",
     "calculate_gaussian_sigma", "gaussian_weights", "preprocess_image", "Preprocessor",
-    "DevicePreprocessor",
+    "DevicePreprocessor", "PreprocessPool",
 ]
 
 _DTYPES = {np.dtype(np.float64): _lib.LMB_F64, np.dtype(np.float32): _lib.LMB_F32,
@@ -449,3 +449,56 @@ class Preprocessor:
 
     def close(self):
         self._h.close()
+
+
+class PreprocessPool:
+    """Several frames preprocessed at once into an engine's slots: one
+    :class:`Preprocessor` (device handle and CUDA stream) per worker thread, so
+    one frame's upload and host steps overlap another's kernels.  Calls into
+    the engine are serialised (an engine is not re-entrant)."""
+
+    def __init__(self, cfg: Dict[str, Any], background: Optional[np.ndarray] = None, *,
+                 device: int = 0, workers: int = 3):
+        from concurrent.futures import ThreadPoolExecutor
+        self.cfg, self.background, self.device = cfg, background, device
+        self._pres = [Preprocessor(cfg, background, device=device) for _ in range(workers)]
+        self._free = list(range(workers))
+        self._lock = threading.Lock()
+        self._engine_lock = threading.Lock()
+        self._pool = ThreadPoolExecutor(max_workers=workers)
+
+    def _one(self, engine, slot, frame, frame_dtype):
+        with self._lock:
+            w = self._free.pop()
+        try:
+            pre = self._pres[w]
+            raw = np.asarray(frame)
+            if pre.background is None:
+                _prepare_background(pre._h, raw, self.cfg, None)
+            cfg = self.cfg
+            cnt = pre._h.segment(raw, _threshold_method(cfg), cfg["threshold_value"],
+                                 cfg["threshold_percentile"], cfg["min_area"], 0.0)
+            if cnt.n_labels <= 1 or cnt.n_centres == 0:
+                return None
+            sigma = _sigma_from(int(cnt.n_centres), cnt.min_dist2, cfg["px_x"], cfg["distance"],
+                                cfg["orientation_spacing"])
+            wts, r = gaussian_weights(sigma)
+            with self._engine_lock:
+                pre._h.blur_to_slot(wts, r, engine, slot, frame_dtype)
+            return int(cnt.n_centres)
+        finally:
+            with self._lock:
+                self._free.append(w)
+
+    def to_slots(self, engine, slots, frames, frame_dtype=np.float32) -> List:
+        """Preprocess frames[i] into slots[i] (``Preprocessor.to_slot`` for
+        each, several at a time); returns each frame's centre count, ``None``
+        for frames without spots (their slots are left untouched)."""
+        futs = [self._pool.submit(self._one, engine, s, f, frame_dtype)
+                for s, f in zip(slots, frames)]
+        return [f.result() for f in futs]
+
+    def close(self):
+        self._pool.shutdown(wait=True)
+        for p in self._pres:
+            p.close()

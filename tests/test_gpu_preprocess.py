@@ -229,3 +229,32 @@ def test_raw_frames_straight_into_engine_slots(frame_dtype):
                 assert na == nb and np.array_equal(a, b), n
                 assert na > 0, n
                 pre.close()
+
+
+def test_pool_loads_the_same_slots_as_one_frame_at_a_time():
+    from lauematching_b200 import params as P, preprocess as PP, synth
+    from lauematching_b200.engine import Engine
+    z = np.load(os.path.join(HERE, "golden", "pp_many_values.npz"))
+    cfg = json.loads(str(z["cfg"]))
+    ny, nx = z["raw"].shape
+    txt = synth.params_text(nr_px=(nx, ny), px=0.0002 * 2048 / max(nx, ny), min_nr_spots=2,
+                            min_intensity=5.0)
+    p = P.parse_params_text(txt)
+    rng = np.random.default_rng(4)
+    frames = [z["raw"]] + [synth.raw_frame(ny, nx, rng, n_spots=40, integer=bool(i % 2))
+                           for i in range(7)]
+    with Engine(p) as e:
+        e.build_db_synthetic(5, 60000, synth.hkls_cubic(6))
+        pool = PP.PreprocessPool(cfg, z["background"], workers=3)
+        got = pool.to_slots(e, list(range(8)), frames)
+        pre = PP.Preprocessor(cfg, z["background"])
+        for k, f in enumerate(frames):
+            assert pre.to_slot(e, 8 + k, f) == got[k]
+        slots = [k for k in range(8) if got[k] is not None]
+        e.match(slots + [8 + k for k in slots], p.min_nr_spots, p.min_intensity)
+        for k in slots:
+            a, na = e.results(k)
+            b, nb = e.results(8 + k)
+            assert na == nb and np.array_equal(a, b)
+        pool.close()
+        pre.close()
