@@ -192,8 +192,36 @@ def dbbuild_parity_sample(e, p, hkls, seed, n_orient, per_block=20000, blocks=5)
     return {"sampled_orientations": total, "records_differing": mism}
 
 
-def cpu_baseline(e, p, txt, hkls, img_u8, seed, n_sample, runs=3):
-    """The reference LaueMatchingCPU (or the oracle port) on a bounded sample."""
+def survivor_parity(e, p, img_u8, n_sample=2_000_000):
+    """This run's survivors of one bench image against the oracle on the DB's
+    first n_sample records: ids, spot counts, uint8 sums and the FP64
+    intensity sums and scores bit for bit.  Returns (summary, our survivors
+    over the whole DB) -- the reference's own count is checked in
+    cpu_baseline."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    e.load_image(0, img_u8, want_scale=False)
+    e.match([0], p.min_nr_spots, p.min_intensity)
+    ours, npass = e.results(0)
+    n_sample = min(n_sample, e.n_orient)
+    want = O.compare(e.download_db(0, n_sample), p.max_nr_spots, img_u8.astype(np.float64),
+                     p.nr_px_x, p.nr_px_y, p.min_nr_spots, p.min_intensity,
+                     nthreads=os.cpu_count() or 1)
+    sub = ours[ours["id"] < n_sample]
+    same = (np.array_equal(sub["id"], want.ids.astype(np.uint64))
+            and np.array_equal(sub["n_spots"], want.n_spots)
+            and np.array_equal(sub["sum_u8"], want.sum_u8)
+            and np.array_equal(sub["tot_int"].view(np.uint64), want.tot_int.view(np.uint64))
+            and np.array_equal(sub["score"].view(np.uint64), want.score.view(np.uint64)))
+    return {"records": n_sample, "survivors": int(sub.shape[0]),
+            "oracle_survivors": int(want.ids.shape[0]), "identical": bool(same)}, ours
+
+
+def cpu_baseline(e, p, txt, hkls, img_u8, seed, n_sample, runs=3, ours=None):
+    """The reference LaueMatchingCPU (or the oracle port) on a bounded sample;
+    with ``ours`` (this run's survivors of the same image over the whole DB),
+    the reference's "Initial solutions" count on the sample is compared with
+    ours over the same records."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from lauematching_b200 import formats
@@ -224,15 +252,21 @@ def cpu_baseline(e, p, txt, hkls, img_u8, seed, n_sample, runs=3):
             times.append(r.compare_seconds)
             walls.append(r.wall_seconds)
         t = statistics.median(times)
+        ref_initial = r.initial_solutions
         for fn in os.listdir(wd):
             os.remove(os.path.join(wd, fn))
         os.rmdir(wd)
         per_image = t * (1e8 / n_sample)
-        return {"value": 1.0 / per_image, "unit": UNIT, "cores": cores, "kind": "reference",
-                "sample": f"LaueMatchingCPU DoFwd 0 compare stage on {n_sample} of the DB's "
-                          f"records (1 image), median of {runs} runs = {t:.4f} s, scaled x"
-                          f"{1e8 / n_sample:g} to the 1e8-orientation DB; whole-process wall "
-                          f"{statistics.median(walls):.2f} s per run"}
+        res = {"value": 1.0 / per_image, "unit": UNIT, "cores": cores, "kind": "reference",
+               "sample": f"LaueMatchingCPU DoFwd 0 compare stage on {n_sample} of the DB's "
+                         f"records (1 image), median of {runs} runs = {t:.4f} s, scaled x"
+                         f"{1e8 / n_sample:g} to the 1e8-orientation DB; whole-process wall "
+                         f"{statistics.median(walls):.2f} s per run"}
+        if ours is not None:
+            mine = int((ours["id"] < n_sample).sum())
+            res["initial_solutions"] = {"reference": ref_initial, "ours": mine,
+                                        "identical": ref_initial == mine}
+        return res
     t0 = time.perf_counter()
     for _ in range(runs):
         O.compare(rec, p.max_nr_spots, img, p.nr_px_x, p.nr_px_y, p.min_nr_spots,
@@ -721,8 +755,12 @@ def run_ours(args, rank, world):
     }
     if rank == 0 and world == 1 and not args.no_parity:
         out["dbbuild"]["parity"] = dbbuild_parity_sample(e, p, hkls, args.seed, N)
+    ours0 = None
+    if rank == 0 and world == 1 and not args.no_parity:
+        out["survivor_parity"], ours0 = survivor_parity(e, p, imgs[0])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(e, p, txt, hkls, imgs[0], args.seed, args.cpu_sample)
+        out["cpu_baseline"] = cpu_baseline(e, p, txt, hkls, imgs[0], args.seed, args.cpu_sample,
+                                           ours=ours0)
     for pb in pins:
         pb.free()
     e.close()
