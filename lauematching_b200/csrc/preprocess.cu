@@ -100,6 +100,8 @@ struct PreState {
   double med;
   double thresh;
   unsigned int blocks_done;  // blocks of the running selection pass that finished
+  unsigned int nonint;       // a candidate value was not an integer in [0, 65535]
+  unsigned int value_path;   // the threshold came from the value histogram
   unsigned int n_comp;      // components
   unsigned int n_labels;    // components + 1
   unsigned int n_keep;      // components with area >= min_area
@@ -129,10 +131,14 @@ __global__ void subtract_kernel(const T *__restrict__ raw, const double *__restr
 
 // ---- order statistics ----------------------------------------------------------
 __global__ void sel_init_kernel(PreState *st, int mode, unsigned long long n,
-                                unsigned long long k0, int two) {
+                                unsigned long long k0, int two, int new_frame) {
   const int t = threadIdx.x;
   for (int i = t; i < 512; i += blockDim.x) (&st->hist[0][0])[i] = 0;
   if (t == 0) {
+    if (new_frame) {
+      st->nonint = 0;
+      st->value_path = 0;
+    }
     Select &s = st->sel;
     s.n = mode == SEL_ALL ? n : 0;
     s.k[0] = k0;
@@ -550,6 +556,208 @@ __global__ void __launch_bounds__(kHist16Threads, 1)
   if (last) {
     __threadfence();
     sel_pick16(st, g16, mode);
+    if (threadIdx.x == 0) st->blocks_done = 0;
+  }
+}
+
+// ---- threshold statistics of integer-valued frames ---------------------------------
+// A detector frame minus a median background holds integers.  When every
+// candidate value is an integer in [0, 65535], one pass counts the values
+// themselves (65536 packed 16-bit counters per block, flushed into the global
+// histogram); the grid's last block turns the histogram into prefix sums and
+// finds the order statistics by binary search: np.median / np.percentile
+// directly, and the median of |v - median| as the smallest distance d with
+// more than k values within d of the median.  Any other value (fraction,
+// negative zero, NaN, above 65535) leaves the work to the radix selection.
+__device__ __forceinline__ unsigned long long vh_count_le(const unsigned *P, int v) {
+  return v < 0 ? 0ull : (unsigned long long)__ldcg(P + v);
+}
+
+// Smallest x in [lo, hi] with pred(x), pred monotone and true at hi; the
+// whole warp probes 32 points per round.
+template <typename Pred>
+__device__ long long warp_search(long long lo, long long hi, Pred pred) {
+  const int lane = threadIdx.x & 31;
+  while (hi - lo + 1 > 32) {
+    const long long step = (hi - lo + 1 + 31) / 32;
+    long long x = lo + (long long)(lane + 1) * step - 1;
+    if (x > hi) x = hi;
+    const unsigned m = __ballot_sync(0xffffffffu, pred(x));
+    const int f = __ffs(m) - 1;
+    long long nhi = lo + (long long)(f + 1) * step - 1;
+    if (nhi > hi) nhi = hi;
+    lo = lo + (long long)f * step;
+    hi = nhi;
+  }
+  const long long x = lo + lane;
+  const unsigned m = __ballot_sync(0xffffffffu, x <= hi && pred(x));
+  return lo + __ffs(m) - 1;
+}
+
+// Smallest value v >= lo with more than r values in [lo, v].
+__device__ int vh_rank(const unsigned *P, int lo, unsigned long long r) {
+  const unsigned long long base = vh_count_le(P, lo - 1);
+  return (int)warp_search(lo, 65535, [&](long long v) {
+    return vh_count_le(P, (int)v) - base > r;
+  });
+}
+
+// Values in [lo, 65535] within t/2 of med.
+__device__ unsigned long long vh_within(const unsigned *P, int lo, double med, long long t) {
+  const double h = 0.5 * (double)t;
+  long long a = (long long)ceil(med - h), b = (long long)floor(med + h);
+  if (a < lo) a = lo;
+  if (b > 65535) b = 65535;
+  if (b < a) return 0ull;
+  return vh_count_le(P, (int)b) - vh_count_le(P, (int)a - 1);
+}
+
+// Smallest distance (a multiple of 1/2) with more than r values within it.
+__device__ double vh_dist(const unsigned *P, int lo, double med, unsigned long long r) {
+  const long long t = warp_search(0, 2 * 65536, [&](long long x) {
+    return vh_within(P, lo, med, x) > r;
+  });
+  return 0.5 * (double)t;
+}
+
+// Last block (1024 threads): prefix sums in place, then the threshold (warp 0).
+__device__ void vh_finish(PreState *st, unsigned *g16, int mode, unsigned long long k0, int two,
+                          double gamma) {
+  __shared__ unsigned long long warp_tot[32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  uint4 *src = reinterpret_cast<uint4 *>(g16 + t * 64);
+  unsigned mine = 0;
+  {
+    uint4 q[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) q[j] = __ldcg(src + j);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) mine += q[j].x + q[j].y + q[j].z + q[j].w;
+  }
+  unsigned long long incl = mine;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    unsigned long long v = warp_tot[lane], x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
+    }
+    warp_tot[lane] = x - v;
+  }
+  __syncthreads();
+  unsigned run = (unsigned)(warp_tot[w] + incl - mine);  // counts fit 32 bits (frames < 2^31 px)
+  for (int j = 0; j < 16; ++j) {
+    uint4 q = __ldcg(src + j);
+    q.x = (run += q.x);
+    q.y = (run += q.y);
+    q.z = (run += q.z);
+    q.w = (run += q.w);
+    src[j] = q;
+  }
+  __threadfence();
+  __syncthreads();
+  if (w == 0) {
+    const unsigned *P = g16;
+    double thresh;
+    if (mode == SEL_ALL) {  // np.percentile over every pixel
+      const double a = (double)vh_rank(P, 0, k0);
+      const double b = two ? (double)vh_rank(P, 0, k0 + 1) : a;
+      const double diff = lmb::dsub(b, a);
+      thresh = lmb::dadd(a, lmb::dmul(diff, gamma));
+      if (gamma >= 0.5) thresh = lmb::dsub(b, lmb::dmul(diff, lmb::dsub(1.0, gamma)));
+    } else {  // the adaptive noise floor over the nonzero pixels
+      const unsigned long long n = vh_count_le(P, 65535) - vh_count_le(P, 0);
+      if (n == 0) {
+        thresh = 1.0;
+      } else {
+        const unsigned long long k = (n - 1) / 2;
+        const bool even = (n % 2) == 0;
+        const double a = (double)vh_rank(P, 1, k);
+        const double med =
+            even ? lmb::ddiv(lmb::dadd(a, (double)vh_rank(P, 1, k + 1)), 2.0) : a;
+        const double m1 = vh_dist(P, 1, med, k);
+        const double md = even ? lmb::ddiv(lmb::dadd(m1, vh_dist(P, 1, med, k + 1)), 2.0) : m1;
+        const double mad = lmb::dmul(1.4826, md);
+        const double thr = lmb::dadd(med, lmb::dmul(4.0, mad));
+        thresh = (1.0 > thr) ? 1.0 : thr;
+      }
+    }
+    if (lane == 0) {
+      st->thresh = thresh;
+      st->value_path = 1;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 16; ++j) src[j] = make_uint4(0, 0, 0, 0);
+}
+
+// Subtraction fused with the value histogram (see above).
+template <typename T>
+__global__ void __launch_bounds__(kHist16Threads, 1)
+    value_hist_kernel(const T *__restrict__ raw, const double *__restrict__ bg,
+                      double *__restrict__ sub, unsigned n, PreState *st, unsigned *g16, int mode,
+                      unsigned long long k0, int two, double gamma) {
+  extern __shared__ unsigned words[];
+  __shared__ bool last;
+  __shared__ int nonint_s;
+  for (int i = threadIdx.x; i < 32768; i += blockDim.x) words[i] = 0;
+  if (threadIdx.x == 0) nonint_s = 0;
+  __syncthreads();
+  Digit16Run run;
+  bool nonint = false;
+  constexpr int U = 4;
+  const unsigned stride = gridDim.x * blockDim.x;
+  const unsigned rounds = (n + stride * U - 1) / (stride * U);
+  for (unsigned it = 0; it < rounds; ++it) {
+    double v[U];
+    bool in[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned i = (it * U + u) * stride + blockIdx.x * blockDim.x + threadIdx.x;
+      in[u] = i < n;
+      v[u] = 0.0;
+      if (in[u]) {
+        const double d = lmb::dsub(to_f64(raw[i]), bg[i]);
+        v[u] = (d >= 0.0 || isnan(d)) ? d : 0.0;
+        sub[i] = v[u];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!in[u] || !(mode == SEL_ALL || v[u] > 0.0)) continue;
+      const double x = v[u];
+      if (x == trunc(x) && x <= 65535.0 && !signbit(x)) run.add(words, (unsigned)x);
+      else nonint = true;  // also NaN: every comparison with it is false
+    }
+  }
+  run.flush(words);
+  if (nonint) nonint_s = 1;
+  __syncthreads();
+  if (threadIdx.x == 0 && nonint_s) atomicOr(&st->nonint, 1u);
+  for (int wd = threadIdx.x; wd < 32768; wd += blockDim.x) {
+    const unsigned x = words[wd];
+    if (x & 0xffffu) atomicAdd(g16 + 2 * wd, x & 0xffffu);
+    if (x >> 16) atomicAdd(g16 + 2 * wd + 1, x >> 16);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->blocks_done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    if (__ldcg(&st->nonint) == 0) {
+      vh_finish(st, g16, mode, k0, two, gamma);
+    } else {  // leave an empty histogram for the radix selection
+      uint4 *src = reinterpret_cast<uint4 *>(g16 + threadIdx.x * 64);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) src[j] = make_uint4(0, 0, 0, 0);
+    }
     if (threadIdx.x == 0) st->blocks_done = 0;
   }
 }
@@ -1233,6 +1441,27 @@ int run_select(lmb_pre *p, int mode, bool first_pass) {
   return LMB_OK;
 }
 
+// Subtraction fused with the value histogram; *done when every candidate was
+// an integer in [0, 65535] and the threshold is set (else the frame's
+// subtraction is in place for the radix selection).
+int value_select(lmb_pre *p, int dtype, int mode, unsigned long long k0, int two, double gamma,
+                 bool *done) {
+  int rc = by_dtype(dtype, [&](auto tag) {
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
+    value_hist_kernel<T><<<hist16_grid(p), kHist16Threads, kHist16Smem, p->st>>>(
+        static_cast<const T *>(p->d_raw), p->d_bg, p->d_sub, (unsigned)p->npx, p->d_state,
+        p->d_hist16, mode, k0, two, gamma);
+    return LMB_OK;
+  });
+  if (rc) return rc;
+  LMB_CUDA(cudaGetLastError());
+  LMB_CUDA(cudaMemcpyAsync(&p->h_state->value_path, &p->d_state->value_path, sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, p->st));
+  LMB_CUDA(cudaStreamSynchronize(p->st));
+  *done = p->h_state->value_path != 0;
+  return LMB_OK;
+}
+
 // Subtraction fused with the 16-bit first selection pass of `mode`.
 int subtract_select(lmb_pre *p, int dtype, int mode) {
   return by_dtype(dtype, [&](auto tag) {
@@ -1423,6 +1652,18 @@ int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **o
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(sel_hist16_kernel<uint8_t, true>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(value_hist_kernel<double>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(value_hist_kernel<float>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(value_hist_kernel<uint16_t>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(value_hist_kernel<uint8_t>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__));
   }
   for (auto &e : p->ev)
@@ -1535,20 +1776,26 @@ int lmb_pre_segment(lmb_pre *p, const void *frame, int32_t dtype, const lmb_pre_
     LMB_REQUIRE(prm->threshold_percentile >= 0.0 && prm->threshold_percentile <= 100.0,
                 "Percentiles must be in the range [0, 100]");
     percentile_plan(p->npx, prm->threshold_percentile, &k0, &two, &gamma);
-    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_ALL, p->npx, k0, two);
-    if ((rc = subtract_select(p, dtype, SEL_ALL)) || (rc = run_select(p, SEL_ALL, false)))
-      return rc;
-    finish_percentile_kernel<<<1, 1, 0, p->st>>>(p->d_state, gamma);
+    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_ALL, p->npx, k0, two, 1);
+    bool done = false;
+    if ((rc = value_select(p, dtype, SEL_ALL, k0, two, gamma, &done))) return rc;
+    if (!done) {
+      if ((rc = run_select(p, SEL_ALL, true))) return rc;
+      finish_percentile_kernel<<<1, 1, 0, p->st>>>(p->d_state, gamma);
+    }
   } else {
     LMB_REQUIRE(prm->threshold_method == LMB_THR_ADAPTIVE, "threshold method %d",
                 prm->threshold_method);
-    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_NZ, p->npx, 0, 0);
-    if ((rc = subtract_select(p, dtype, SEL_NZ)) || (rc = run_select(p, SEL_NZ, false)))
-      return rc;
-    finish_median_kernel<<<1, 1, 0, p->st>>>(p->d_state);
-    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_ABSDEV, p->npx, 0, 0);
-    if ((rc = run_select(p, SEL_ABSDEV, true))) return rc;
-    finish_adaptive_kernel<<<1, 1, 0, p->st>>>(p->d_state);
+    sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_NZ, p->npx, 0, 0, 1);
+    bool done = false;
+    if ((rc = value_select(p, dtype, SEL_NZ, 0, 0, 0.0, &done))) return rc;
+    if (!done) {
+      if ((rc = run_select(p, SEL_NZ, true))) return rc;
+      finish_median_kernel<<<1, 1, 0, p->st>>>(p->d_state);
+      sel_init_kernel<<<1, kT, 0, p->st>>>(p->d_state, SEL_ABSDEV, p->npx, 0, 0, 0);
+      if ((rc = run_select(p, SEL_ABSDEV, true))) return rc;
+      finish_adaptive_kernel<<<1, 1, 0, p->st>>>(p->d_state);
+    }
   }
   apply_kernel<<<g, kT, 0, p->st>>>(p->d_sub, p->d_state, p->d_t16, p->d_par, p->nx, p->npx);
   LMB_CUDA(cudaGetLastError());

@@ -104,16 +104,20 @@ def test_full_size_median_radius_101_on_sampled_pixels():
         assert bg[y, x] == np.partition(w, (s * s) // 2)[(s * s) // 2], (y, x)
 
 
-@pytest.mark.parametrize("method,extra", [("adaptive", {}), ("percentile", {"threshold_percentile": 99.5}),
-                                          ("fixed", {"threshold_value": 40.0}),
-                                          ("otsu", {})])
-def test_full_size_frame_against_the_oracle(method, extra):
+@pytest.mark.parametrize("method,extra,integer", [
+    ("adaptive", {}, True), ("percentile", {"threshold_percentile": 99.5}, True),
+    ("fixed", {"threshold_value": 40.0}, False), ("otsu", {}, True),
+    # fractional values: the radix selection instead of the value histogram
+    ("adaptive", {}, False), ("percentile", {"threshold_percentile": 97.25}, False)])
+def test_full_size_frame_against_the_oracle(method, extra, integer):
     """2048^2 frames with a given background (the image server's flow)."""
     from lauematching_b200 import preprocess as PP, synth
-    rng = np.random.default_rng(abs(hash(method)) % 1000)
-    raw = synth.raw_frame(2048, 2048, rng, n_spots=600, integer=method != "fixed")
+    rng = np.random.default_rng(sum(map(ord, method)) + int(integer))
+    raw = synth.raw_frame(2048, 2048, rng, n_spots=600, integer=integer)
     yy, xx = np.mgrid[0:2048, 0:2048]
     bg = 100.0 + 0.02 * yy + 0.01 * xx
+    if integer:  # integer frames minus an integer background: the value-histogram path
+        bg = np.rint(bg)
     cfg = dict(nr_px_x=2048, nr_px_y=2048, filter_radius=101, median_passes=1,
                threshold_method=method, threshold_value=0.0, threshold_percentile=90.0,
                min_area=10, px_x=0.2, distance=0.513, orientation_spacing=0.4)
