@@ -18,6 +18,7 @@
 //                pair is farther apart than a cell.
 //   blur         separable float64 passes in scipy's summation order.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <cmath>
 #include <cstring>
@@ -865,12 +866,13 @@ __device__ void uf_union(int *L, int a, int b) {
 // max(s, q-1) of S.  Seen from a pixel x of S: the upper-left neighbour when
 // x = s; the upper one when x = s and the upper-left is background; the
 // upper-right one when the upper one is background.
-__global__ void merge_kernel(const uint16_t *t16, int *L, int ny, int nx) {
-  const size_t n = (size_t)ny * nx;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
+__global__ void merge_kernel(const uint16_t *t16, int *L, int nx, const unsigned *fg,
+                             const unsigned *n_fg) {
+  const unsigned nf = *n_fg;
+  for (unsigned f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    const unsigned i = fg[f];
     const int y = (int)(i / nx), x = (int)(i % nx);
-    if (y == 0 || !t16[i]) continue;
+    if (y == 0) continue;
     const int p = (int)i;
     const bool left = x > 0 && t16[i - 1];
     const uint16_t *up = t16 + (i - nx);
@@ -891,10 +893,11 @@ struct Comps {
 
 // Every foreground pixel points straight at its root; each root takes the
 // next component id.
-__global__ void compress_kernel(int *L, int *cid, PreState *st, Comps c, size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    if (__ldcg(L + i) < 0) continue;
+__global__ void compress_kernel(int *L, int *cid, PreState *st, Comps c, const unsigned *fg,
+                                const unsigned *n_fg) {
+  const unsigned nf = *n_fg;
+  for (unsigned f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    const unsigned i = fg[f];
     const int r = uf_find(L, (int)i);
     if (r != (int)i) {
       L[i] = r;
@@ -912,14 +915,13 @@ __global__ void compress_kernel(int *L, int *cid, PreState *st, Comps c, size_t 
   }
 }
 
-__global__ void moments_kernel(const int *L, const int *cid, const uint16_t *t16, Comps c, int ny,
-                               int nx) {
-  const size_t n = (size_t)ny * nx;
+__global__ void moments_kernel(const int *L, const int *cid, const uint16_t *t16, Comps c, int nx,
+                               const unsigned *fg, const unsigned *n_fg) {
+  const unsigned nf = *n_fg;
   const unsigned bw = (unsigned)(nx + 1) / 2;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
+  for (unsigned f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    const unsigned i = fg[f];
     const int r = L[i];
-    if (r < 0) continue;
     const int id = cid[r];
     const int y = (int)(i / nx), x = (int)(i % nx);
     const unsigned long long w = t16[i];
@@ -985,23 +987,37 @@ __global__ void label_kernel(PreState *st, Comps c, int min_area, const unsigned
   }
 }
 
-__global__ void images_kernel(const int *__restrict__ L, const int *__restrict__ cid,
-                              const uint16_t *__restrict__ t16, Comps c, int *__restrict__ labels,
-                              uint16_t *__restrict__ filt, int *__restrict__ flabels, size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const int r = L[i];
-    int lab = 0, kept = 0;
-    if (r >= 0) {
-      const int id = cid[r];
-      lab = c.label[id];
-      kept = c.keep[id] >= 0;
-    }
-    labels[i] = lab;
-    flabels[i] = kept ? lab : 0;
-    filt[i] = kept ? t16[i] : (uint16_t)0;
+// The filtered frame (kept components' pixels) over a zeroed frame.
+__global__ void filt_kernel(const int *__restrict__ L, const int *__restrict__ cid,
+                            const uint16_t *__restrict__ t16, Comps c, uint16_t *__restrict__ filt,
+                            const unsigned *fg, const unsigned *n_fg) {
+  const unsigned nf = *n_fg;
+  for (unsigned f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    const unsigned i = fg[f];
+    if (c.keep[cid[L[i]]] >= 0) filt[i] = t16[i];
   }
 }
+
+// Labels of all and of the kept components over zeroed frames (built only
+// when a caller asks for them).
+__global__ void labels_kernel(const int *__restrict__ L, const int *__restrict__ cid, Comps c,
+                              int *__restrict__ labels, int *__restrict__ flabels,
+                              const unsigned *fg, const unsigned *n_fg) {
+  const unsigned nf = *n_fg;
+  for (unsigned f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    const unsigned i = fg[f];
+    const int id = cid[L[i]];
+    const int lab = c.label[id];
+    labels[i] = lab;
+    if (c.keep[id] >= 0) flabels[i] = lab;
+  }
+}
+
+// Foreground test of the list selection.
+struct IsForeground {
+  const uint16_t *t16;
+  __device__ __forceinline__ bool operator()(const unsigned &i) const { return t16[i] != 0; }
+};
 
 // ---- closest pair of centres (blur width) ---------------------------------------
 __device__ __forceinline__ double pair_d2(const double *a, const double *b) {
@@ -1335,6 +1351,10 @@ struct lmb_pre {
   Comps c{};
   unsigned long long *d_flags = nullptr, *d_pos = nullptr, *d_compact = nullptr;
   unsigned *d_hist16 = nullptr;  // 65536-bin histogram of the first selection pass
+  unsigned *d_fg = nullptr, *d_nfg = nullptr;  // foreground pixel list and its length
+  void *d_fg_tmp = nullptr;
+  size_t fg_bytes = 0;
+  bool labels_ready = false;  // label images of the last segment built
   double *d_centres = nullptr, *d_w = nullptr;
   int *d_stats = nullptr, *d_head = nullptr, *d_next = nullptr;
   int gcx = 1, gcy = 1;
@@ -1378,7 +1398,7 @@ void free_pre(lmb_pre *p) {
                   p->d_cid, p->d_lab, p->d_flab, p->c.area, p->c.x0, p->c.y0, p->c.x1, p->c.y1,
                   p->c.fb, p->c.sw, p->c.swx, p->c.swy, p->c.label, p->c.keep, p->d_flags,
                   p->d_pos, p->d_compact, p->d_centres, p->d_w, p->d_stats, p->d_head, p->d_next,
-                  p->d_state, p->d_cub, p->d_hist16, p->m_keys, p->m_keys2, p->m_idx, p->m_idx2, p->m_flag,
+                  p->d_state, p->d_cub, p->d_hist16, p->d_fg, p->d_nfg, p->d_fg_tmp, p->m_keys, p->m_keys2, p->m_idx, p->m_idx2, p->m_flag,
                   p->m_incl, p->m_rank, p->m_nd, p->m_vals, p->m_img, p->m_cub};
   for (void *b : bufs)
     if (b) cudaFree(b);
@@ -1462,16 +1482,6 @@ int value_select(lmb_pre *p, int dtype, int mode, unsigned long long k0, int two
   return LMB_OK;
 }
 
-// Subtraction fused with the 16-bit first selection pass of `mode`.
-int subtract_select(lmb_pre *p, int dtype, int mode) {
-  return by_dtype(dtype, [&](auto tag) {
-    using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
-    sel_hist16_kernel<T, true><<<hist16_grid(p), kHist16Threads, kHist16Smem, p->st>>>(
-        static_cast<const T *>(p->d_raw), p->d_bg, p->d_sub, (unsigned)p->npx, p->d_state,
-        p->d_hist16, mode);
-    return LMB_OK;
-  });
-}
 
 // np.percentile's order statistics and weight for n values (linear method).
 void percentile_plan(size_t n, double pct, unsigned long long *k0, int *two, double *gamma) {
@@ -1498,10 +1508,14 @@ int segment_tail(lmb_pre *p, int min_area, lmb_pre_counts *counts, bool parents_
   const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
   cudaStream_t st = p->st;
   if (!parents_ready) init_parents_kernel<<<g, kT, 0, st>>>(p->d_t16, p->d_par, p->nx, p->npx);
-  merge_kernel<<<g, kT, 0, st>>>(p->d_t16, p->d_par, p->ny, p->nx);
+  // the foreground pixels, in raster order; the component kernels run over them
+  size_t sb = p->fg_bytes;
+  LMB_CUDA(cub::DeviceSelect::If(p->d_fg_tmp, sb, thrust::counting_iterator<unsigned>(0u),
+                                 p->d_fg, p->d_nfg, (int)p->npx, IsForeground{p->d_t16}, st));
+  merge_kernel<<<g, kT, 0, st>>>(p->d_t16, p->d_par, p->nx, p->d_fg, p->d_nfg);
   reset_counts_kernel<<<1, 1, 0, st>>>(p->d_state);
-  compress_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_state, p->c, p->npx);
-  moments_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_t16, p->c, p->ny, p->nx);
+  compress_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_state, p->c, p->d_fg, p->d_nfg);
+  moments_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_t16, p->c, p->nx, p->d_fg, p->d_nfg);
   LMB_CUDA(cudaMemsetAsync(p->d_flags, 0, p->nblocks * sizeof(unsigned long long), st));
   const unsigned gc = (unsigned)grid_for(p->nblocks, p->num_sms);
   flags_kernel<<<gc, kT, 0, st>>>(p->d_state, p->c, min_area, p->d_flags, p->nblocks);
@@ -1509,8 +1523,9 @@ int segment_tail(lmb_pre *p, int min_area, lmb_pre_counts *counts, bool parents_
   LMB_CUDA(cub::DeviceScan::InclusiveSum(p->d_cub, tb, p->d_flags, p->d_pos, (int)p->nblocks, st));
   label_kernel<<<gc, kT, 0, st>>>(p->d_state, p->c, min_area, p->d_pos, p->nblocks,
                                   p->d_centres, p->d_stats);
-  images_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_t16, p->c, p->d_lab, p->d_filt,
-                                  p->d_flab, p->npx);
+  LMB_CUDA(cudaMemsetAsync(p->d_filt, 0, p->npx * sizeof(uint16_t), st));
+  filt_kernel<<<g, kT, 0, st>>>(p->d_par, p->d_cid, p->d_t16, p->c, p->d_filt, p->d_fg, p->d_nfg);
+  p->labels_ready = false;
   // closest pair of kept centres
   LMB_CUDA(cudaMemsetAsync(p->d_head, 0xff, (size_t)p->gcx * p->gcy * sizeof(int), st));
   cell_insert_kernel<<<gc, kT, 0, st>>>(p->d_state, p->d_centres, p->d_head, p->d_next, p->gcx,
@@ -1631,8 +1646,17 @@ int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **o
       (rc = alloc(&p->d_compact, n)) || (rc = alloc(&p->d_centres, nb * 4)) ||
       (rc = alloc(&p->d_w, 1024)) || (rc = alloc(&p->d_stats, nb * 5)) ||
       (rc = alloc(&p->d_head, (size_t)p->gcx * p->gcy)) || (rc = alloc(&p->d_next, nb)) ||
-      (rc = alloc(&p->d_state, 1)) || (rc = alloc(&p->d_hist16, 65536)))
+      (rc = alloc(&p->d_state, 1)) || (rc = alloc(&p->d_hist16, 65536)) ||
+      (rc = alloc(&p->d_fg, n)) || (rc = alloc(&p->d_nfg, 1)))
     return fail(rc);
+  {
+    size_t fb = 0;
+    if (cub::DeviceSelect::If(nullptr, fb, thrust::counting_iterator<unsigned>(0u), p->d_fg,
+                              p->d_nfg, (int)n, IsForeground{p->d_t16}) != cudaSuccess ||
+        cudaMalloc(&p->d_fg_tmp, std::max<size_t>(fb, 1)) != cudaSuccess)
+      return fail(cuda_fail(cudaGetLastError(), "foreground list set-up", __FILE__, __LINE__));
+    p->fg_bytes = fb;
+  }
   if (cudaMemset(p->d_hist16, 0, 65536 * sizeof(unsigned)) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "cudaMemset", __FILE__, __LINE__));
   {
@@ -1640,18 +1664,6 @@ int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **o
     const int b = (int)kHist16Smem;
     cudaError_t e = cudaFuncSetAttribute(sel_hist16_kernel<double, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(sel_hist16_kernel<double, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(sel_hist16_kernel<float, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(sel_hist16_kernel<uint16_t, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(sel_hist16_kernel<uint8_t, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(value_hist_kernel<double>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, b);
@@ -1848,6 +1860,14 @@ int lmb_pre_images(lmb_pre *p, uint16_t *thresholded, int32_t *labels, uint16_t 
   if (rc) return rc;
   LMB_REQUIRE(p->segmented, "no frame segmented yet");
   const size_t n = p->npx;
+  if ((labels || filt_labels) && !p->labels_ready) {
+    LMB_CUDA(cudaMemsetAsync(p->d_lab, 0, n * sizeof(int), p->st));
+    LMB_CUDA(cudaMemsetAsync(p->d_flab, 0, n * sizeof(int), p->st));
+    labels_kernel<<<(unsigned)grid_for(n, p->num_sms), kT, 0, p->st>>>(
+        p->d_par, p->d_cid, p->c, p->d_lab, p->d_flab, p->d_fg, p->d_nfg);
+    LMB_CUDA(cudaGetLastError());
+    p->labels_ready = true;
+  }
   if (thresholded)
     LMB_CUDA(cudaMemcpyAsync(thresholded, p->d_t16, n * 2, cudaMemcpyDeviceToHost, p->st));
   if (labels) LMB_CUDA(cudaMemcpyAsync(labels, p->d_lab, n * 4, cudaMemcpyDeviceToHost, p->st));
