@@ -505,12 +505,10 @@ __device__ void sel_pick16(PreState *st, unsigned *g16, int mode) {
   for (int j = 0; j < 16; ++j) dst[j] = make_uint4(0, 0, 0, 0);
 }
 
-// Pass A.  FUSED: also the background subtraction np.maximum(raw - bg, 0),
-// written to `sub` (the selection then costs no extra read of the frame).
-template <typename T, bool FUSED>
+// Pass A over the subtracted frame.
 __global__ void __launch_bounds__(kHist16Threads, 1)
-    sel_hist16_kernel(const T *__restrict__ raw, const double *__restrict__ bg,
-                      double *__restrict__ sub, unsigned n, PreState *st, unsigned *g16, int mode) {
+    sel_hist16_kernel(const double *__restrict__ sub, unsigned n, PreState *st, unsigned *g16,
+                      int mode) {
   extern __shared__ unsigned words[];
   __shared__ bool last;
   for (int i = threadIdx.x; i < 32768; i += blockDim.x) words[i] = 0;
@@ -525,16 +523,7 @@ __global__ void __launch_bounds__(kHist16Threads, 1)
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const unsigned i = (it * U + u) * stride + blockIdx.x * blockDim.x + threadIdx.x;
-      v[u] = 0.0;
-      if (i < n) {
-        if (FUSED) {
-          const double d = lmb::dsub(to_f64(raw[i]), bg[i]);
-          v[u] = (d >= 0.0 || isnan(d)) ? d : 0.0;
-          sub[i] = v[u];
-        } else {
-          v[u] = sub[i];
-        }
-      }
+      v[u] = i < n ? sub[i] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -626,12 +615,13 @@ __device__ void vh_finish(PreState *st, unsigned *g16, int mode, unsigned long l
                           double gamma) {
   __shared__ unsigned long long warp_tot[32];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  uint4 *src = reinterpret_cast<uint4 *>(g16 + t * 64);
+  const int nq = 65536 / 4 / blockDim.x;  // uint4 words of bins per thread
+  uint4 *src = reinterpret_cast<uint4 *>(g16) + (size_t)t * nq;
   unsigned mine = 0;
-  {
+  for (int j0 = 0; j0 < nq; j0 += 16) {
     uint4 q[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) q[j] = __ldcg(src + j);
+    for (int j = 0; j < 16; ++j) q[j] = __ldcg(src + j0 + j);
 #pragma unroll
     for (int j = 0; j < 16; ++j) mine += q[j].x + q[j].y + q[j].z + q[j].w;
   }
@@ -643,16 +633,17 @@ __device__ void vh_finish(PreState *st, unsigned *g16, int mode, unsigned long l
   if (lane == 31) warp_tot[w] = incl;
   __syncthreads();
   if (w == 0) {
-    unsigned long long v = warp_tot[lane], x = v;
+    const int nw = blockDim.x >> 5;
+    unsigned long long v = lane < nw ? warp_tot[lane] : 0ull, x = v;
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned long long u = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= o) x += u;
     }
-    warp_tot[lane] = x - v;
+    if (lane < nw) warp_tot[lane] = x - v;
   }
   __syncthreads();
   unsigned run = (unsigned)(warp_tot[w] + incl - mine);  // counts fit 32 bits (frames < 2^31 px)
-  for (int j = 0; j < 16; ++j) {
+  for (int j = 0; j < nq; ++j) {
     uint4 q = __ldcg(src + j);
     q.x = (run += q.x);
     q.y = (run += q.y);
@@ -694,25 +685,29 @@ __device__ void vh_finish(PreState *st, unsigned *g16, int mode, unsigned long l
     }
   }
   __syncthreads();
-#pragma unroll
-  for (int j = 0; j < 16; ++j) src[j] = make_uint4(0, 0, 0, 0);
+  for (int j = 0; j < nq; ++j) src[j] = make_uint4(0, 0, 0, 0);
 }
 
-// Subtraction fused with the value histogram (see above).
+// Subtraction fused with the value histogram (see above).  Each block counts
+// values below kVhLocal in shared memory (runs of equal values in registers)
+// and adds larger ones straight into the global 65536-bin histogram.
+constexpr int kVhLocal = 4096;
+constexpr int kVhThreads = 256;
+
 template <typename T>
-__global__ void __launch_bounds__(kHist16Threads, 1)
+__global__ void __launch_bounds__(kVhThreads, 4)
     value_hist_kernel(const T *__restrict__ raw, const double *__restrict__ bg,
                       double *__restrict__ sub, unsigned n, PreState *st, unsigned *g16, int mode,
                       unsigned long long k0, int two, double gamma) {
-  extern __shared__ unsigned words[];
+  __shared__ unsigned h[kVhLocal];
   __shared__ bool last;
   __shared__ int nonint_s;
-  for (int i = threadIdx.x; i < 32768; i += blockDim.x) words[i] = 0;
+  for (int i = threadIdx.x; i < kVhLocal; i += blockDim.x) h[i] = 0;
   if (threadIdx.x == 0) nonint_s = 0;
   __syncthreads();
-  Digit16Run run;
+  DigitRun run;  // bins below kVhLocal
   bool nonint = false;
-  constexpr int U = 4;
+  constexpr int U = 8;
   const unsigned stride = gridDim.x * blockDim.x;
   const unsigned rounds = (n + stride * U - 1) / (stride * U);
   for (unsigned it = 0; it < rounds; ++it) {
@@ -733,19 +728,21 @@ __global__ void __launch_bounds__(kHist16Threads, 1)
     for (int u = 0; u < U; ++u) {
       if (!in[u] || !(mode == SEL_ALL || v[u] > 0.0)) continue;
       const double x = v[u];
-      if (x == trunc(x) && x <= 65535.0 && !signbit(x)) run.add(words, (unsigned)x);
-      else nonint = true;  // also NaN: every comparison with it is false
+      if (x == trunc(x) && x <= 65535.0 && !signbit(x)) {
+        const unsigned b = (unsigned)x;
+        if (b < (unsigned)kVhLocal) run.add(h, b);
+        else atomicAdd(g16 + b, 1u);
+      } else {
+        nonint = true;  // also NaN: every comparison with it is false
+      }
     }
   }
-  run.flush(words);
+  run.flush(h);
   if (nonint) nonint_s = 1;
   __syncthreads();
   if (threadIdx.x == 0 && nonint_s) atomicOr(&st->nonint, 1u);
-  for (int wd = threadIdx.x; wd < 32768; wd += blockDim.x) {
-    const unsigned x = words[wd];
-    if (x & 0xffffu) atomicAdd(g16 + 2 * wd, x & 0xffffu);
-    if (x >> 16) atomicAdd(g16 + 2 * wd + 1, x >> 16);
-  }
+  for (int b = threadIdx.x; b < kVhLocal; b += blockDim.x)
+    if (h[b]) atomicAdd(g16 + b, h[b]);
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(&st->blocks_done, 1u) == gridDim.x - 1;
@@ -755,9 +752,8 @@ __global__ void __launch_bounds__(kHist16Threads, 1)
     if (__ldcg(&st->nonint) == 0) {
       vh_finish(st, g16, mode, k0, two, gamma);
     } else {  // leave an empty histogram for the radix selection
-      uint4 *src = reinterpret_cast<uint4 *>(g16 + threadIdx.x * 64);
-#pragma unroll
-      for (int j = 0; j < 16; ++j) src[j] = make_uint4(0, 0, 0, 0);
+      for (int q = threadIdx.x; q < 65536 / 4; q += blockDim.x)
+        reinterpret_cast<uint4 *>(g16)[q] = make_uint4(0, 0, 0, 0);
     }
     if (threadIdx.x == 0) st->blocks_done = 0;
   }
@@ -1161,6 +1157,82 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The same for radius R known at compile time (1..8; sigma 1 gives R = 4):
+// each thread keeps a 4-output segment of a column (axis-0 pass) and then of
+// a row (axis-1 pass) in registers, 4 + 2R inputs, each converted once.
+constexpr int kBlurFixedMaxR = 8;
+
+template <int R, typename TOut>
+__global__ void __launch_bounds__(256)
+    blur_tile_r_kernel(const uint16_t *__restrict__ in, const double *__restrict__ wts, int ny,
+                       int nx, TOut *__restrict__ out) {
+  constexpr int W = kBlurTile + 2 * R;
+  __shared__ double w[2 * R + 1];
+  __shared__ double vert[kBlurTile * W];
+  __shared__ uint16_t tile[W * W];
+  const int x0 = blockIdx.x * kBlurTile, y0 = blockIdx.y * kBlurTile;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t <= 2 * R) w[t] = wts[t];
+  // mirrored source columns of this lane (W <= 48 < 64)
+  const int c0 = mirror(x0 - R + lane, nx);
+  const int c1 = lane + 32 < W ? mirror(x0 - R + lane + 32, nx) : 0;
+  for (int row = warp; row < W; row += 8) {
+    const uint16_t *src = in + (size_t)mirror(y0 - R + row, ny) * nx;
+    tile[row * W + lane] = src[c0];
+    if (lane + 32 < W) tile[row * W + lane + 32] = src[c1];
+  }
+  __syncthreads();
+  // axis 0: task = (group of 4 output rows, tile column)
+  for (int task = t; task < 8 * W; task += 256) {
+    const int rg = task / W, col = task - rg * W;
+    double v[4 + 2 * R];
+#pragma unroll
+    for (int q = 0; q < 4 + 2 * R; ++q) v[q] = (double)tile[(rg * 4 + q) * W + col];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      double acc = lmb::dmul(v[o + R], w[R]);
+#pragma unroll
+      for (int j = R; j >= 1; --j)
+        acc = lmb::dadd(acc, lmb::dmul(lmb::dadd(v[o + R - j], v[o + R + j]), w[R - j]));
+      vert[(rg * 4 + o) * W + col] = acc;
+    }
+  }
+  __syncthreads();
+  // axis 1: task = (output row, group of 4 output columns)
+  {
+    const int row = t >> 3, cg = (t & 7) * 4;
+    const double *src = vert + row * W + cg;
+    double v[4 + 2 * R];
+#pragma unroll
+    for (int q = 0; q < 4 + 2 * R; ++q) v[q] = src[q];
+    const int gy = y0 + row;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      double acc = lmb::dmul(v[o + R], w[R]);
+#pragma unroll
+      for (int j = R; j >= 1; --j)
+        acc = lmb::dadd(acc, lmb::dmul(lmb::dadd(v[o + R - j], v[o + R + j]), w[R - j]));
+      const int gx = x0 + cg + o;
+      if (gy < ny && gx < nx) out[(size_t)gy * nx + gx] = (TOut)acc;
+    }
+  }
+}
+
+template <typename TOut>
+void blur_tile_r_launch(int r, dim3 grid, const uint16_t *in, const double *w, int ny, int nx,
+                        TOut *out, cudaStream_t st) {
+  switch (r) {
+    case 1: blur_tile_r_kernel<1, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+    case 2: blur_tile_r_kernel<2, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+    case 3: blur_tile_r_kernel<3, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+    case 4: blur_tile_r_kernel<4, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+    case 5: blur_tile_r_kernel<5, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+    case 6: blur_tile_r_kernel<6, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+    case 7: blur_tile_r_kernel<7, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+    default: blur_tile_r_kernel<8, TOut><<<grid, 256, 0, st>>>(in, w, ny, nx, out); break;
+  }
+}
+
 // ---- median ------------------------------------------------------------------------
 __global__ void rank_keys_kernel(const double *img, unsigned long long *keys, unsigned *idx,
                                  size_t n) {
@@ -1450,8 +1522,8 @@ unsigned hist16_grid(const lmb_pre *p) {
 // follow, the first over the frame, the rest over the keys it kept.
 int run_select(lmb_pre *p, int mode, bool first_pass) {
   if (first_pass)
-    sel_hist16_kernel<double, false><<<hist16_grid(p), kHist16Threads, kHist16Smem, p->st>>>(
-        nullptr, nullptr, p->d_sub, (unsigned)p->npx, p->d_state, p->d_hist16, mode);
+    sel_hist16_kernel<<<hist16_grid(p), kHist16Threads, kHist16Smem, p->st>>>(
+        p->d_sub, (unsigned)p->npx, p->d_state, p->d_hist16, mode);
   for (int shift = kKeepShift; shift >= 0; shift -= 8) {
     // one wave of blocks over the frame; the kept keys' count is on the device
     const unsigned gp = (unsigned)(p->num_sms * (shift == kKeepShift ? 4 : 2));
@@ -1468,7 +1540,7 @@ int value_select(lmb_pre *p, int dtype, int mode, unsigned long long k0, int two
                  bool *done) {
   int rc = by_dtype(dtype, [&](auto tag) {
     using T = std::remove_const_t<std::remove_pointer_t<decltype(tag)>>;
-    value_hist_kernel<T><<<hist16_grid(p), kHist16Threads, kHist16Smem, p->st>>>(
+    value_hist_kernel<T><<<(unsigned)(p->num_sms * 4), kVhThreads, 0, p->st>>>(
         static_cast<const T *>(p->d_raw), p->d_bg, p->d_sub, (unsigned)p->npx, p->d_state,
         p->d_hist16, mode, k0, two, gamma);
     return LMB_OK;
@@ -1662,20 +1734,8 @@ int lmb_pre_create(int32_t device, int32_t nr_px_y, int32_t nr_px_x, lmb_pre **o
   {
     // the 16-bit selection pass uses 128 KiB of shared memory per block
     const int b = (int)kHist16Smem;
-    cudaError_t e = cudaFuncSetAttribute(sel_hist16_kernel<double, false>,
+    cudaError_t e = cudaFuncSetAttribute(sel_hist16_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(value_hist_kernel<double>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(value_hist_kernel<float>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(value_hist_kernel<uint16_t>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(value_hist_kernel<uint8_t>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__));
   }
   for (auto &e : p->ev)
@@ -1897,7 +1957,15 @@ int blur_launch(lmb_pre *p, const double *weights, int32_t radius, int32_t out_d
   LMB_CUDA(cudaMemcpyAsync(p->d_w, weights, (size_t)(2 * radius + 1) * sizeof(double),
                            cudaMemcpyHostToDevice, p->st));
   const unsigned g = (unsigned)grid_for(p->npx, p->num_sms);
-  if (radius <= kBlurTileMaxR) {
+  if (radius >= 1 && radius <= kBlurFixedMaxR) {
+    const dim3 tg((p->nx + kBlurTile - 1) / kBlurTile, (p->ny + kBlurTile - 1) / kBlurTile);
+    if (out_dtype == LMB_F64)
+      blur_tile_r_launch<double>(radius, tg, p->d_filt, p->d_w, p->ny, p->nx,
+                                 static_cast<double *>(p->d_out), p->st);
+    else
+      blur_tile_r_launch<float>(radius, tg, p->d_filt, p->d_w, p->ny, p->nx,
+                                static_cast<float *>(p->d_out), p->st);
+  } else if (radius <= kBlurTileMaxR) {
     const dim3 tg((p->nx + kBlurTile - 1) / kBlurTile, (p->ny + kBlurTile - 1) / kBlurTile);
     const size_t tsm = blur_tile_smem(radius);
     if (out_dtype == LMB_F64)

@@ -262,3 +262,23 @@ def test_pool_loads_the_same_slots_as_one_frame_at_a_time():
             assert na == nb and np.array_equal(a, b)
         pool.close()
         pre.close()
+
+
+@pytest.mark.parametrize("shape", [(100, 70), (33, 65), (5, 3), (1, 40)])
+def test_blur_every_kernel_radius_against_scipy_order(shape):
+    """Radii 1-8 (register kernels), 9-32 (shared-memory tile), above (two
+    passes), on frames that are not multiples of the tile and on frames
+    narrower than the window (mirrored periodically)."""
+    from lauematching_b200 import preprocess as PP
+    rng = np.random.default_rng(sum(shape))
+    t = ((rng.random(shape) < 0.3) * rng.integers(1, 60000, shape)).astype(np.uint16)
+    h = PP.DevicePreprocessor(*shape)
+    h.segment_thresholded(t, 1)
+    for sigma in (0.3, 0.5, 0.7, 1.0, 1.2, 1.4, 1.7, 1.9, 2.5, 5.0, 8.0, 9.0):
+        w, r = PP.gaussian_weights(sigma)
+        want = PO.gaussian_blur(t, sigma)
+        got = h.blur(w, r, np.float64)
+        assert np.array_equal(bits(got), bits(want)), (sigma, r)
+        got32 = h.blur(w, r, np.float32)
+        assert np.array_equal(got32, want.astype(np.float32)), (sigma, r)
+    h.close()
