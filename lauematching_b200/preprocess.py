@@ -35,7 +35,7 @@ __all__ = [
     "compute_background", "load_background", "enhance_image",
     "find_connected_components", "filter_small_components",
     "calculate_gaussian_sigma", "gaussian_weights", "preprocess_image", "Preprocessor",
-    "DevicePreprocessor", "PreprocessPool",
+    "DevicePreprocessor", "PreprocessPool", "config_from_params_text",
 ]
 
 _DTYPES = {np.dtype(np.float64): _lib.LMB_F64, np.dtype(np.float32): _lib.LMB_F32,
@@ -319,6 +319,48 @@ def gaussian_weights(sigma: float, truncate: float = 4.0) -> Tuple[np.ndarray, i
     return phi / phi.sum(), radius
 
 
+# Preprocessing keys of a LaueMatching parameter file and their defaults, as
+# the image server reads them (scripts/laue_stream_utils.py:89-220).
+_CONFIG_DEFAULTS = {"nr_px_x": 2048, "nr_px_y": 2048, "px_x": 0.2, "px_y": 0.2,
+                    "distance": 0.513, "threshold_method": "adaptive", "threshold_value": 0.0,
+                    "threshold_percentile": 90.0, "min_area": 10, "filter_radius": 101,
+                    "median_passes": 1, "orientation_spacing": 0.4, "background_file": ""}
+
+
+def config_from_params_text(text: str) -> Dict[str, Any]:
+    """The preprocessing configuration of a parameter file's text, with the
+    rules of ``scripts/laue_stream_utils.py:parse_config`` (141-220): ``#``
+    comments, the first token is the key, malformed values are skipped."""
+    cfg = dict(_CONFIG_DEFAULTS)
+    conv = {"NrPxX": ("nr_px_x", int), "NrPxY": ("nr_px_y", int), "PxX": ("px_x", float),
+            "PxY": ("px_y", float), "ThresholdMethod": ("threshold_method", str.lower),
+            "Threshold": ("threshold_value", float),
+            "ThresholdPercentile": ("threshold_percentile", float),
+            "MinArea": ("min_area", int), "FilterRadius": ("filter_radius", int),
+            "NMeadianPasses": ("median_passes", int),
+            "OrientationSpacing": ("orientation_spacing", float),
+            "BackgroundFile": ("background_file", str)}
+    for line in text.splitlines():
+        line = line.strip()
+        if not line or line.startswith("#"):
+            continue
+        if "#" in line:
+            line = line[: line.index("#")].strip()
+        parts = line.split()
+        if len(parts) < 2:
+            continue
+        key, rest = parts[0], parts[1:]
+        try:
+            if key == "P_Array" and len(rest) >= 3:
+                cfg["distance"] = float(rest[2])
+            elif key in conv:
+                name, f = conv[key]
+                cfg[name] = f(rest[0])
+        except (ValueError, IndexError):
+            logger.warning(f"Skipping malformed config line '{line}'")
+    return cfg
+
+
 def _threshold_method(cfg) -> str:
     m = cfg["threshold_method"]
     return m if m in ("percentile", "fixed") else "adaptive"
@@ -467,7 +509,7 @@ class PreprocessPool:
         self._engine_lock = threading.Lock()
         self._pool = ThreadPoolExecutor(max_workers=workers)
 
-    def _one(self, engine, slot, frame, frame_dtype):
+    def _one(self, engine, slot, frame, frame_dtype, host_copy=False):
         with self._lock:
             w = self._free.pop()
         try:
@@ -485,16 +527,21 @@ class PreprocessPool:
             wts, r = gaussian_weights(sigma)
             with self._engine_lock:
                 pre._h.blur_to_slot(wts, r, engine, slot, frame_dtype)
+            if host_copy:  # the blurred frame as the matcher read it, for the post-stage
+                return int(cnt.n_centres), pre._h.blur(wts, r, frame_dtype)
             return int(cnt.n_centres)
         finally:
             with self._lock:
                 self._free.append(w)
 
-    def to_slots(self, engine, slots, frames, frame_dtype=np.float32) -> List:
+    def to_slots(self, engine, slots, frames, frame_dtype=np.float32,
+                 host_copy: bool = False) -> List:
         """Preprocess frames[i] into slots[i] (``Preprocessor.to_slot`` for
-        each, several at a time); returns each frame's centre count, ``None``
-        for frames without spots (their slots are left untouched)."""
-        futs = [self._pool.submit(self._one, engine, s, f, frame_dtype)
+        each, several at a time); returns each frame's centre count (with
+        ``host_copy``, the pair (count, blurred frame as ``frame_dtype`` in host
+        memory)), ``None`` for frames without spots (their slots are left
+        untouched)."""
+        futs = [self._pool.submit(self._one, engine, s, f, frame_dtype, host_copy)
                 for s, f in zip(slots, frames)]
         return [f.result() for f in futs]
 

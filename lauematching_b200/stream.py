@@ -25,7 +25,17 @@ What changes (the serving side of the B200 design):
 * mixed detector sizes -- ``--extra-params`` adds further detector
   geometries, each with its own resident DB; frames for them arrive on port
   60518 with an extended header (``b"LMB2"``, uint16 image number, uint16
-  width, uint16 height, uint8 dtype 0=float32/1=uint8, one pad byte);
+  width, uint16 height, uint8 dtype 0=float32/1=uint8/2=raw uint16, one pad
+  byte);
+* raw detector frames -- dtype 2 on the extended port is an unprocessed
+  uint16 frame: the daemon runs the image server's preprocessing
+  (``laue_index.preprocess.preprocess_image``, configured by the same keys
+  of the parameter file, background from BackgroundFile or the median of
+  the geometry's first raw frame, as ``scripts/laue_image_server.py:160-176``)
+  on the device, straight into the frame's slot; the blurred frame the
+  matcher read (float32, as the image server would have sent it) feeds the
+  post-stage; a frame without spots is finished without lines (the image
+  server does not send it, ``laue_image_server.py:76-77``);
 * the post-stage (merge, refinement, text) runs on a writer thread, off the
   GPU loop; per-image latency (arrival -> lines written) is recorded and
   p50/p99 reported.
@@ -52,6 +62,8 @@ MAX_CONNECTIONS = 10
 MAX_QUEUE = 32
 EXT_MAGIC = b"LMB2"
 EXT_HEADER = struct.Struct("<4sHHHBB")
+_SURV_DTYPE = np.dtype([("id", "<u8"), ("n_spots", "<i4"), ("sum_u8", "<i4"),
+                        ("tot_int", "<f8"), ("score", "<f8")])
 
 
 @dataclass
@@ -60,6 +72,7 @@ class Request:
     key: tuple  # (NrPxX, NrPxY)
     pixels: np.ndarray
     t_arrival: float
+    raw: bool = False  # an unprocessed detector frame, preprocessed on the device
 
 
 @dataclass
@@ -79,6 +92,8 @@ class Geometry:
     # passes on the device, oldest first, each a list of (slot, Request); a
     # second pass queues behind the running one while its results are read
     inflight: collections.deque = field(default_factory=collections.deque)
+    pre_cfg: dict = None  # preprocessing configuration for raw frames
+    pool: object = None   # PreprocessPool, made on the first raw frame
 
 
 def _recv_exact(sock, buf, running):
@@ -106,7 +121,7 @@ class StreamServer:
 
     def __init__(self, params_list, orients, hkls, ncpus=1, max_batch=64, device=0,
                  result_dir=None, port=PORT, ext_port=EXT_PORT, host="0.0.0.0",
-                 log=print, max_queue=MAX_QUEUE, engines=None):
+                 log=print, max_queue=MAX_QUEUE, engines=None, preprocess_cfgs=None):
         from . import _lib, formats
         from .engine import Engine
         self.log = log
@@ -125,8 +140,9 @@ class StreamServer:
             key = (int(p.nr_px_x), int(p.nr_px_y))
             if key in self.geoms:
                 raise ValueError(f"two parameter files describe a {key} detector")
+            pcfg = preprocess_cfgs[i] if preprocess_cfgs else None
             if engines is not None:  # DBs already resident (in-process use)
-                self.geoms[key] = Geometry(p, engines[i])
+                self.geoms[key] = Geometry(p, engines[i], pre_cfg=pcfg)
                 continue
             e = Engine(p, device=device)
             fwd = p.forward_file
@@ -144,7 +160,7 @@ class StreamServer:
                         _write_cache(e, fwd, orients.shape[0])
                     except OSError as exc:
                         log(f"Could not write the forward simulation to {fwd}: {exc}")
-            self.geoms[key] = Geometry(p, e)
+            self.geoms[key] = Geometry(p, e, pre_cfg=pcfg)
         # admission: slots per geometry within the free HBM after the DBs
         info = _lib.device_info(device)
         per_slot = max(int(k[0]) * int(k[1]) * 5 for k in self.geoms)  # u8 frame + wire staging
@@ -211,11 +227,11 @@ class StreamServer:
                     if not _recv_exact(c, hb, run):
                         break
                     magic, num, w, h, dt, _ = EXT_HEADER.unpack(hb)
-                    if magic != EXT_MAGIC or dt not in (0, 1):
+                    if magic != EXT_MAGIC or dt not in (0, 1, 2):
                         self.log("bad extended header; closing connection")
                         break
                     key = (w, h)
-                    dtype = np.float32 if dt == 0 else np.uint8
+                    dtype = (np.float32, np.uint8, np.uint16)[dt]
                 else:
                     hb = bytearray(2)
                     if not _recv_exact(c, hb, run):
@@ -233,7 +249,8 @@ class StreamServer:
                 # blocks while MAX_QUEUE images wait (back-pressure, as queue_push)
                 while self.running:
                     try:
-                        self.queue.put(Request(num, key, payload, t), timeout=0.5)
+                        self.queue.put(Request(num, key, payload, t, raw=dtype == np.uint16),
+                                       timeout=0.5)
                         break
                     except queue.Full:
                         continue
@@ -296,17 +313,54 @@ class StreamServer:
                 continue
             admitted.setdefault(r.key, []).append((g.free.pop(), r))
             n += 1
-        # one batched upload per geometry and pixel type
+        # one batched upload per geometry and pixel type; raw frames are
+        # preprocessed on the device straight into their slots
         for key, items in admitted.items():
             g = self.geoms[key]
+            raw = [(s, r) for s, r in items if r.raw]
+            items = [(s, r) for s, r in items if not r.raw]
+            if raw:
+                items += self._preprocess_raw(g, raw)
             by_type = collections.defaultdict(list)
             for s, r in items:
-                by_type[r.pixels.dtype].append((s, r))
+                if not r.raw:
+                    by_type[r.pixels.dtype].append((s, r))
             for its in by_type.values():
                 g.engine.load_images([s for s, _ in its], [r.pixels for _, r in its])
             g.loaded.extend(items)
         self._backlog = keep
         return n
+
+    def _preprocess_raw(self, g, raw):
+        """Raw frames into their slots; returns the loaded (slot, request)
+        pairs, each request now holding its blurred frame.  Frames without
+        spots are finished at once without lines and free their slots."""
+        from . import preprocess as PP
+        if g.pool is None:
+            cfg = dict(g.pre_cfg) if g.pre_cfg else PP.config_from_params_text("")
+            cfg["nr_px_x"], cfg["nr_px_y"] = int(g.params.nr_px_x), int(g.params.nr_px_y)
+            bg = PP.load_background(cfg.get("background_file", ""), cfg["nr_px_x"],
+                                    cfg["nr_px_y"])
+            if np.count_nonzero(bg) == 0:  # the image server: median of the first frame
+                bg = PP.compute_background(raw[0][1].pixels.reshape(cfg["nr_px_y"],
+                                                                    cfg["nr_px_x"]),
+                                           cfg["filter_radius"], cfg["median_passes"],
+                                           device=self.device)
+            g.pool = PP.PreprocessPool(cfg, bg, device=self.device)
+        shape = (int(g.params.nr_px_y), int(g.params.nr_px_x))
+        res = g.pool.to_slots(g.engine, [s for s, _ in raw],
+                              [r.pixels.reshape(shape) for _, r in raw], np.float32,
+                              host_copy=True)
+        loaded = []
+        t = time.perf_counter()
+        for (s, r), out in zip(raw, res):
+            if out is None:
+                g.free.append(s)
+                self.done_q.put(Done(r, np.zeros(0, _SURV_DTYPE), 0, t))
+                continue
+            r.pixels = out[1].ravel()
+            loaded.append((s, r))
+        return loaded
 
     # ---- post-stage + output ----------------------------------------------------
     def _writer(self):
@@ -382,6 +436,9 @@ class StreamServer:
             t.join(timeout=drain_timeout)
         self.sol_f.close()
         self.spt_f.close()
+        for g in self.geoms.values():
+            if g.pool is not None:
+                g.pool.close()
         if close_engines:
             for g in self.geoms.values():
                 g.engine.close()
@@ -430,9 +487,14 @@ def main(argv=None) -> int:
     orients = formats.read_orientations(orient_fn)
     hkls = formats.read_hkls(hkl_fn)
     print(f"{orients.shape[0]} orientations, {len(hkls)} hkls", flush=True)
+    from .preprocess import config_from_params_text
+    pcfgs = []
+    for fn in [param_fn] + opts.extra_params:
+        with open(fn) as f:
+            pcfgs.append(config_from_params_text(f.read()))
     srv = StreamServer(plist, orients, hkls, ncpus=int(ncpu_s), max_batch=opts.max_batch,
                        device=opts.device, port=opts.port, ext_port=opts.ext_port,
-                       log=lambda *a: print(*a, flush=True))
+                       log=lambda *a: print(*a, flush=True), preprocess_cfgs=pcfgs)
     stop = threading.Event()
 
     def on_signal(signum, frame):

@@ -65,3 +65,18 @@ def test_zero_radius_background_needs_no_device():
     a = np.arange(12.0).reshape(3, 4)
     assert not PP.compute_background(a, 0, 1).any()
     assert not PP.compute_background(a, 101, 0).any()
+
+
+def test_config_from_a_parameter_file_follows_the_image_server_rules():
+    txt = ("NrPxX 1024\n# ThresholdMethod fixed\nP_Array 0 0 0.61  # metres\n"
+           "ThresholdMethod Percentile\nThreshold 12.5\nThresholdPercentile 99\n"
+           "MinArea bad\nFilterRadius 51\nNMeadianPasses 2\nOrientationSpacing 0.25\n"
+           "PxX 0.0002\nBackgroundFile /tmp/bg.bin\nLatticeParameter 0.3 0.3 0.3 90 90 90\n")
+    cfg = PP.config_from_params_text(txt)
+    assert cfg["nr_px_x"] == 1024 and cfg["nr_px_y"] == 2048
+    assert cfg["distance"] == 0.61 and cfg["px_x"] == 0.0002
+    assert cfg["threshold_method"] == "percentile" and cfg["threshold_value"] == 12.5
+    assert cfg["threshold_percentile"] == 99.0 and cfg["min_area"] == 10  # malformed: default
+    assert cfg["filter_radius"] == 51 and cfg["median_passes"] == 2
+    assert cfg["orientation_spacing"] == 0.25 and cfg["background_file"] == "/tmp/bg.bin"
+    assert PP.config_from_params_text("")["threshold_method"] == "adaptive"

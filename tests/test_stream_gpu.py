@@ -92,11 +92,12 @@ def _expected(c_params, orients, hkls, img_f32, num):
     return sol.splitlines(), spt.splitlines()
 
 
-def _server(plist, orients, hkls, tmp, max_batch, ports):
+def _server(plist, orients, hkls, tmp, max_batch, ports, preprocess_cfgs=None):
     from lauematching_b200.stream import StreamServer
     return StreamServer(plist, orients, hkls, ncpus=4, max_batch=max_batch,
                         result_dir=str(tmp), port=ports[0], ext_port=ports[1],
-                        host="127.0.0.1", log=lambda *a: None).start()
+                        host="127.0.0.1", log=lambda *a: None,
+                        preprocess_cfgs=preprocess_cfgs).start()
 
 
 def test_stream_mix_equals_alone_equals_oracle(tmp_path):
@@ -167,3 +168,52 @@ def test_stream_mixed_detector_sizes(tmp_path):
         assert sol.get(10 + i, []) == _expected(p2, c.orients, c.hkls, f2[i], 10 + i)[0]
         assert sol.get(20 + i, []) == _expected(p1, c.orients, c.hkls,
                                                 f1[i].astype(np.float32), 20 + i)[0]
+
+
+def test_stream_raw_frames_preprocessed_on_the_device(tmp_path):
+    """Raw uint16 detector frames (extended header, dtype 2) are preprocessed
+    on the device into their slots: each image's lines equal those of the
+    blurred frame preprocess_image makes (as float32, what the image server
+    sends), and a frame without spots is finished without lines."""
+    from lauematching_b200 import preprocess as PP
+    c = golden_case("tilted_fcc")
+    p = P.parse_params_text(_params_text(c), binary="stream")
+    ny, nx = p.nr_px_y, p.nr_px_x
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    bg = np.rint(100.0 + 0.01 * yy + 0.02 * xx)
+    bg_path = tmp_path / "background.bin"
+    bg.tofile(bg_path)
+    cfg = PP.config_from_params_text(_params_text(c) + f"BackgroundFile {bg_path}\nMinArea 5\n")
+    assert cfg["background_file"] == str(bg_path) and cfg["min_area"] == 5
+    rng = np.random.default_rng(5)
+    raws = []
+    for _ in range(5):
+        g = synth.pick_grains(c.records, int(rng.integers(1, 5)), 8, rng)
+        f = synth.raw_frame(ny, nx, rng, spot_records=c.records[g], sigma=1.2, amp_lo=300.0,
+                            amp_hi=4000.0)
+        raws.append(np.clip(f, 0, 65535).astype(np.uint16))
+    raws.append(bg.astype(np.uint16))  # nothing above the background: no spots
+    ports = _ports()
+    srv = _server([p], c.orients, c.hkls, tmp_path / "raw", 64, ports, preprocess_cfgs=[cfg])
+    try:
+        time.sleep(0.3)
+        sock = socket.create_connection(("127.0.0.1", ports[1]))
+        for i, f in enumerate(raws):
+            sock.sendall(struct.pack("<4sHHHBB", b"LMB2", 30 + i, nx, ny, 2, 0))
+            sock.sendall(f.tobytes())
+        sock.close()
+        _wait_done(srv, len(raws))
+    finally:
+        srv.stop()
+    sol = _lines_by_image(tmp_path / "raw" / "solutions.txt")
+    spt = _lines_by_image(tmp_path / "raw" / "spots.txt")
+    _expected.records = {(nx, ny): c.records}
+    n_lines = 0
+    for i, f in enumerate(raws[:-1]):
+        blurred = PP.preprocess_image(f, cfg, background=bg)[0].astype(np.float32)
+        es, ep = _expected(p, c.orients, c.hkls, blurred, 30 + i)
+        assert sol.get(30 + i, []) == es
+        assert spt.get(30 + i, []) == ep
+        n_lines += len(es)
+    assert 30 + len(raws) - 1 not in sol
+    assert n_lines > 0
