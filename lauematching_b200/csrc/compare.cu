@@ -279,8 +279,8 @@ struct ListSpots {
 // for the uint8 image; :649-653 for the float64 image).  Returns the spot
 // count; tot/su receive the FP64 sum and the uint8 sum.
 template <class Spots>
-__device__ __noinline__ int slot_sum(const CmpArgs &a, const Spots sp, int c, int k,
-                                     double &tot_out, int &su_out) {
+__device__ __forceinline__ int slot_sum_body(const CmpArgs &a, const Spots sp, int c, int k,
+                                             double &tot_out, int &su_out) {
   const uint8_t *img = a.u8 + (size_t)k * a.npx;
   const double *fim = a.f64 ? a.f64 + (size_t)k * a.npx : nullptr;
   const double sc = a.scale[k];
@@ -321,9 +321,17 @@ __device__ __noinline__ int slot_sum(const CmpArgs &a, const Spots sp, int c, in
   return ns;
 }
 
+// Called out of line by kernels without a tight register bound; kernels
+// bounded for high occupancy (TAG > 1) take it inline, within their bound.
+template <class Spots>
+__device__ __noinline__ int slot_sum(const CmpArgs &a, const Spots sp, int c, int k,
+                                     double &tot_out, int &su_out) {
+  return slot_sum_body(a, sp, c, k, tot_out, su_out);
+}
+
 // Called by all 32 lanes of a warp (lanes without a record pass valid=false,
 // c=0).  c = the record's spot count, clamped to S.
-template <int B, class Spots>
+template <int B, class Spots, int TAG = 1>
 __device__ __forceinline__ void process(const CmpArgs &a, const Spots sp, int c, uint64_t oid,
                                         uint64_t pol, bool valid) {
   // nSpots <= c, so a record with c < MinNrSpots fails the spot threshold of
@@ -384,7 +392,10 @@ __device__ __forceinline__ void process(const CmpArgs &a, const Spots sp, int c,
     double tot = 0.0, score = 0.0;
     int ns = 0, su = 0;
     if ((cand >> k) & 1) {
-      ns = slot_sum(a, sp, c, k, tot, su);
+      if constexpr (TAG > 1)
+        ns = slot_sum_body(a, sp, c, k, tot, su);
+      else
+        ns = slot_sum(a, sp, c, k, tot, su);
       pass = ns >= a.min_spots && tot >= a.min_int;
       if (pass) {
         score = dmul(tot, dsqrt((double)ns));
@@ -580,8 +591,9 @@ __global__ void __launch_bounds__(576, 1) compare_ws_kernel(const __grid_constan
 // tiles with few such chunks still use every warp), find each lane's first
 // spot with a warp prefix sum of the counts, and run the per-record logic of
 // the other variants.
-template <int B>
-__global__ void __launch_bounds__(576, 1) compare_clist_kernel(const __grid_constant__ CmpArgs a) {
+template <int B, int MINB>
+__global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
+    compare_clist_kernel(const __grid_constant__ CmpArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int ST = a.stages;
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
@@ -635,7 +647,8 @@ __global__ void __launch_bounds__(576, 1) compare_clist_kernel(const __grid_cons
   auto flush = [&]() {
     __syncwarp();
     const bool v = lane < qn;
-    process<B>(a, ListSpots{q_sp + lane * SP}, v ? (int)q_c[lane] : 0, v ? q_oid[lane] : 0,
+    process<B, ListSpots, MINB>(a, ListSpots{q_sp + lane * SP}, v ? (int)q_c[lane] : 0,
+                                v ? q_oid[lane] : 0,
                pol_occ, v);
     __syncwarp();
     qn = 0;
@@ -679,7 +692,7 @@ __global__ void __launch_bounds__(576, 1) compare_clist_kernel(const __grid_cons
         const uint32_t *my = spots + base[ch] + (x - c);
         unsigned qm = __ballot_sync(0xffffffffu, valid && c >= need);
         if (__popc(qm) >= kDirect) {  // many can pass: count the chunk in place
-          process<B>(a, ListSpots{my}, c, oid, pol_occ, valid);
+          process<B, ListSpots, MINB>(a, ListSpots{my}, c, oid, pol_occ, valid);
           continue;
         }
         while (qm) {  // into the queue, emptying it whenever it fills
@@ -820,11 +833,16 @@ CompareTuning compare_config(int R, const CompareTuning &req) {
 
 template <int B>
 static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, size_t smem,
-                    cudaStream_t st) {
-  if (c.variant == 2) {
-    const int rc = ensure_smem((const void *)compare_clist_kernel<B>, (int)smem);
+                    bool six, cudaStream_t st) {
+  if (c.variant == 2 && six) {
+    // six 128-thread blocks per SM: registers bounded for that occupancy
+    const int rc = ensure_smem((const void *)compare_clist_kernel<B, 6>, (int)smem);
     if (rc) return rc;
-    compare_clist_kernel<B><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
+    compare_clist_kernel<B, 6><<<grid, 128, smem, st>>>(a);
+  } else if (c.variant == 2) {
+    const int rc = ensure_smem((const void *)compare_clist_kernel<B, 1>, (int)smem);
+    if (rc) return rc;
+    compare_clist_kernel<B, 1><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
   } else if (c.variant == 1) {
     const int rc = ensure_smem((const void *)compare_ws_kernel<B>, (int)smem);
     if (rc) return rc;
@@ -874,13 +892,16 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   const unsigned grid = (unsigned)std::min<uint64_t>(
       a.ntiles, (uint64_t)num_sms * c.blocks_per_sm * (uint64_t)mult);
   const int B = counter_bits(a.S);
-  if (B <= 3) return launch_b<3>(a, c, grid, smem, st);
-  if (B <= 5) return launch_b<5>(a, c, grid, smem, st);
-  if (B <= 6) return launch_b<6>(a, c, grid, smem, st);
-  if (B <= 7) return launch_b<7>(a, c, grid, smem, st);
-  if (B <= 9) return launch_b<9>(a, c, grid, smem, st);
-  if (B <= 11) return launch_b<11>(a, c, grid, smem, st);
-  return launch_b<16>(a, c, grid, smem, st);
+  // six 128-thread compact-pass blocks per SM (the tuned shape) get a kernel
+  // whose registers are bounded for that occupancy
+  const bool six = c.variant == 2 && c.consumers == 3 && mult >= 6;
+  if (B <= 3) return launch_b<3>(a, c, grid, smem, six, st);
+  if (B <= 5) return launch_b<5>(a, c, grid, smem, six, st);
+  if (B <= 6) return launch_b<6>(a, c, grid, smem, six, st);
+  if (B <= 7) return launch_b<7>(a, c, grid, smem, six, st);
+  if (B <= 9) return launch_b<9>(a, c, grid, smem, six, st);
+  if (B <= 11) return launch_b<11>(a, c, grid, smem, six, st);
+  return launch_b<16>(a, c, grid, smem, six, st);
 }
 
 // Zero the survivor and pass counters of the pass's slots only: the counters

@@ -103,8 +103,8 @@ struct lmb_engine {
   cudaEvent_t ev_loaded[LMB_MAX_SLOTS] = {};
   cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
   // automatic variant with the compact pass's tuned shape (2 stages, 3 consumer
-  // warps, 5 blocks per SM)
-  CompareTuning tuning{3, 0, 2, 3, 1, 5, 0};
+  // warps, 6 blocks per SM)
+  CompareTuning tuning{3, 0, 2, 3, 1, 6, 0};
   int last_variant = -1;  // variant the latest pass ran
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
@@ -403,6 +403,16 @@ int build_compact(lmb_engine *e) {
   auto round128 = [](uint64_t b) { return ((b + 127) / 128) * 128; };
   const uint64_t avg_chunk = 36 + (4 * total_spots + nch - 1) / nch;
   uint64_t TB = std::min<uint64_t>(24 * 1024, std::max<uint64_t>(4096, round128(64 * avg_chunk)));
+  {
+    // room for six blocks of the default pass shape (three consumer warps, a
+    // two-stage ring) on an SM, when the largest chunk allows it
+    int per_sm = 0, reserved = 0;
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, e->device);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, e->device);
+    const int64_t room =
+        (int64_t)per_sm / 6 - reserved - 256 - 3 * (int64_t)clist_queue_bytes(e->S);
+    if (room > 2 * 4096) TB = std::min<uint64_t>(TB, (uint64_t)(room / 2) / 128 * 128);
+  }
   TB = std::max<uint64_t>(TB, round128(clist_spot_offset(1) + 4 * max_spots));
   if (2 * TB + 256 > 227 * 1024) {  // a huge S with dense records: keep the reference layout
     cudaFree(d_aux);

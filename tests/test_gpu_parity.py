@@ -254,7 +254,8 @@ def test_compact_layout_batched_equals_reference_layout():
         e.match(range(12), p.min_nr_spots, p.min_intensity)
         ref = e.results_batch(range(12))
         for shape in ({}, {"consumers": 4}, {"consumers": 17, "stages": 2}, {"grid_mult": 3},
-                      {"full_gather": 1}):
+                      {"full_gather": 1}, {"consumers": 3, "stages": 2, "grid_mult": 6},
+                      {"consumers": 3, "stages": 2, "grid_mult": 6, "full_gather": 1}):
             e.set_tuning(variant=2, **shape)
             e.match(range(12), p.min_nr_spots, p.min_intensity)
             got = e.results_batch(range(12))
