@@ -319,6 +319,117 @@ def merge_timing(space_group, max_angle, device, n_base=800, per=12, seed=5):
             "device_ms": round(t_dev * 1e3, 2), "identical": same}
 
 
+# The tilted detector of APS 34-ID-E (P_Array, R_Array as the reference's
+# example parameter files give them); spots per orientation ~20, so the
+# refinement objective sees realistic valid-HKL lists.
+TILTED_P = (0.028745, 0.002788, 0.513115)
+TILTED_R = (-1.20131258, -1.21399082, -1.21881158)
+
+
+def refine_scene(device, n_frames, per_frame, seed=17, min_spots=8):
+    """Frames rendered from true grains and coarse matrices 0.05-0.3 degrees
+    off them (a DB grid's neighbour), tilted detector, fcc Ni, 1240 HKLs.
+    The true grains' spots come from the device DB build."""
+    from lauematching_b200 import params as P, synth
+    from lauematching_b200.engine import Engine
+    txt = synth.params_text(p=TILTED_P, r=TILTED_R, max_nr_spots=30, min_nr_spots=5)
+    p = P.parse_params_text(txt)
+    hk = synth.hkls_cubic(8)
+    rng = np.random.default_rng(seed)
+    n_cand = 40 * n_frames * per_frame
+    e = Engine(p, device=device)
+    try:
+        e.build_db_synthetic(seed, n_cand, hk)
+        rec = e.download_db(0, n_cand)
+        om_all = e.synth_orientations(seed, 0, n_cand)
+    finally:
+        e.close()
+    ok = np.nonzero(rec[:, 0] >= min_spots)[0][:n_frames * per_frame]
+    frames, image = [], []
+    for f in range(n_frames):
+        sel = ok[f * per_frame:(f + 1) * per_frame]
+        img = synth.render_image(rec[sel], p.nr_px_x, p.nr_px_y, rng)
+        frames.append(img.astype(np.float32).reshape(p.nr_px_y, p.nr_px_x))
+        image += [f] * per_frame
+    om_c = synth.perturb_orientations(om_all[ok], rng, 0.05, 0.3)
+    return p, hk, frames, np.array(image, np.int32), om_c
+
+
+def refine_timing(device, sizes=((32, 24), (32, 192)), max_eval=200, reps=3, cpu=True):
+    """Refinement of the grains of a batch (FitOrientation of every grain,
+    200 evaluations at most): this library's lockstep Nelder-Mead with the
+    objective on the device (one launch per group round) against the same fit
+    with the objective on all host threads (identical results), at a few
+    grains per frame and at many (polycrystal frames), and the reference's
+    own problem_function timed on one host thread."""
+    from lauematching_b200.engine import geometry_from_params
+    from lauematching_b200.refine import Refiner
+    out = {"runs": []}
+    for n_frames, per_frame in sizes:
+        p, hk, frames, image, om_c = refine_scene(device, n_frames, per_frame)
+        geo = geometry_from_params(p)
+        run = {"workload": f"{len(om_c)} grains over {n_frames} 2048x2048 float frames "
+                           f"(tilted detector, fcc, {len(hk)} HKLs), coarse matrices 0.05-0.3 deg "
+                           f"off the true grains, Nelder-Mead <= {max_eval} evaluations per grain"}
+        res = {}
+        for name, dev in (("device", device), ("host", None)):
+            with Refiner(p, geo, hk, device=dev) as r:
+                t0 = time.perf_counter()
+                r.set_images(frames)
+                nv = r.set_grains(om_c, image)
+                t_setup = time.perf_counter() - t0
+                _, ov0, _ = r.fit("once")
+                ts, kms = [], []
+                for _ in range(reps if dev is not None else 1):
+                    t0 = time.perf_counter()
+                    x, ov, ev = r.fit("nelder-mead", max_eval)
+                    ts.append(time.perf_counter() - t0)
+                    kms.append(r.last_stats()["kernel_ms"])
+                st = r.last_stats()
+                res[name] = (x, ov, ev)
+                fit_s = statistics.median(ts)
+                run[name] = {"fit_ms": round(fit_s * 1e3, 2),
+                             "grains_per_s": round(len(om_c) / fit_s, 1),
+                             "evaluations_per_s": round(st["points"] / fit_s, 1),
+                             "rounds": st["rounds"], "evaluations": st["points"],
+                             "setup_ms": round(t_setup * 1e3, 1)}
+                if dev is not None:
+                    km = statistics.median(kms)
+                    run[name]["objective_kernel_ms"] = round(km, 3)
+                    run[name]["kernel_evaluations_per_s"] = round(st["points"] / (km * 1e-3), 1)
+                    run["valid_hkls_per_grain"] = round(float(nv.mean()), 1)
+                    run["overlap_start_mean"] = round(float(ov0.mean()), 1)
+                    run["overlap_fit_mean"] = round(float(ov.mean()), 1)
+                    run["improved_grains"] = int((ov > ov0).sum())
+                else:
+                    run[name]["threads"] = os.cpu_count()
+        run["identical"] = all(np.array_equal(a, b) for a, b in zip(res["device"], res["host"]))
+        run["device_over_host"] = round(run["host"]["fit_ms"] / run["device"]["fit_ms"], 2)
+        out["runs"].append(run)
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ref_objective as RO
+        if RO.available():
+            ref = RO.RefObjective(p, geo, hk)
+            x0 = [ref.start(om_c[g])[0] for g in range(min(64, len(om_c)))]
+            valid = [ref.prefilter(x[:3]) for x in x0]
+            n_ev = 0
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 2.0:
+                for g, x in enumerate(x0):
+                    ref.problem(x, frames[int(image[g])], valid[g])
+                    n_ev += 1
+            dt = time.perf_counter() - t0
+            out["cpu_baseline"] = {
+                "kind": "reference", "cores": 1,
+                "value": round(n_ev / dt, 1), "unit": "evaluations/s",
+                "sample": f"the reference's problem_function (LaueMatchingHeaders.h, compiled "
+                          f"from the reference tree) at the start points of {len(x0)} grains, "
+                          f"{n_ev} evaluations in {dt:.2f} s on one thread; the reference runs "
+                          f"one grain per OpenMP thread"}
+    return out
+
+
 def preprocess_timing(device, parity=True, cpu_port=True, frames=20):
     """Frame preprocessing (laue_index.preprocess_image's steps) of a 2048^2
     detector frame on the device: the image server's flow (background from
@@ -668,6 +779,7 @@ def run_ours(args, rank, world):
                    "same_survivor_counts": fg_surv == surv}
 
     merge = merge_timing(p.space_group, p.max_angle, dev) if rank == 0 else None
+    refine = refine_timing(dev, cpu=not args.no_cpu_baseline) if rank == 0 else None
     prep = preprocess_timing(dev, parity=not args.no_parity,
                              cpu_port=not args.no_cpu_baseline) if rank == 0 else None
     if prep is not None:
@@ -748,6 +860,7 @@ def run_ours(args, rank, world):
         "batched_over_plain": round(value / world / plain_ips, 2),
         "full_gather": full_gather,
         "merge": merge,
+        "refine": refine,
         "preprocess": prep,
         "survivors_per_image": {"min": min(surv), "max": max(surv), "mean": statistics.mean(surv)},
         "dbbuild": {"orientations_per_s": round(N / t_build, 1), "seconds": round(t_build, 3),
@@ -1077,6 +1190,8 @@ def main():
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--preprocess", action="store_true",
                     help="only the frame-preprocessing leg (2048^2 frames; --steps frames)")
+    ap.add_argument("--refine", action="store_true",
+                    help="only the batched refinement leg (device against host threads)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (Poisson arrivals)")
     ap.add_argument("--serve-rates", type=str, default="50,200,500,1000,2000")
     ap.add_argument("--serve-seconds", type=float, default=4.0)
@@ -1091,6 +1206,8 @@ def main():
         run_reference_gpu(args, rank, world)
     elif args.serve:
         run_serve(args)
+    elif args.refine:
+        print(json.dumps(refine_timing(0, cpu=not args.no_cpu_baseline)), flush=True)
     elif args.preprocess:
         print(json.dumps(preprocess_timing(0, parity=not args.no_parity,
                                            cpu_port=not args.no_cpu_baseline,

@@ -289,6 +289,49 @@ int lmb_merge_clusters(int32_t device, int32_t space_group, double max_angle,
                        int32_t num_threads, int32_t *n_clusters, uint64_t *best_rows,
                        double *best_scores, int32_t *counts);
 
+/* ---- batched orientation refinement ----------------------------------------
+ * FitOrientation (LaueMatchingHeaders.h:696-801) for many grains at once, as
+ * fitAndWriteOrientations (:1072-1153) sets it up: per grain the Euler angles
+ * of its coarse matrix (OrientMat2Euler), the HKLs valid there
+ * (prefilterHKLs, :513-561, with the parameters' lattice), the start point
+ * and box (Euler +-3 degrees, lattice entries x (1 +- tol_LatC), or c/a x
+ * (1 +- tol_c_over_a)), and problem_function (:640-694 with
+ * calcOverlapFiltered :564-636) as the objective: -(nrPos * sqrt(sum)) over
+ * at most 3 x max_nr_spots spots.  device >= 0: objective evaluations run on
+ * that CUDA device, one launch per round for all grains; device < 0: on
+ * pp->num_threads host threads.  Both give bit-identical values.  The
+ * images are float frames of nr_px_y rows of nr_px_x (image[py * nr_px_x +
+ * px]), copied at lmb_refine_set_images; set_images drops the grains. */
+typedef struct lmb_refine lmb_refine;
+int lmb_refine_create(int32_t device, const lmb_geometry *geo, const lmb_post_params *pp,
+                      const int32_t *hkls, int32_t nh, lmb_refine **out);
+int lmb_refine_destroy(lmb_refine *r);
+/* n: the fit's dimension count (3 + lattice entries with a tolerance, or 4) */
+int lmb_refine_dims(lmb_refine *r, int32_t *n);
+int lmb_refine_set_images(lmb_refine *r, const float *const *frames, int32_t n_images);
+/* orients[n_grains][9]: coarse orientation matrices; image[n_grains]: frame
+ * index of each grain; n_valid (optional, [n_grains]): prefiltered HKL counts */
+int lmb_refine_set_grains(lmb_refine *r, const double *orients, const int32_t *image,
+                          int32_t n_grains, int32_t *n_valid);
+/* start points and box of every grain, [n_grains][n] each (any may be NULL) */
+int lmb_refine_start(lmb_refine *r, double *x0, double *lower, double *upper);
+/* problem_function at m points: x[m][n] of grain[m] -> objective[m] */
+int lmb_refine_evaluate(lmb_refine *r, const int32_t *grain, const double *x, int64_t m,
+                        double *objective);
+/* Fit every grain.  optimizer 0: evaluate once at the start point (the
+ * reference built with an evaluate-once NLopt stand-in gives the same
+ * result); 1: this library's bounded Nelder-Mead, all grains in lockstep,
+ * at most max_eval evaluations per grain, stopping at relative changes of
+ * 1e-6 in value or position (NLopt is not available; NLopt's own
+ * NELDERMEAD / BOBYQA take other steps).  The start simplex steps each
+ * coordinate by init_step x its box width (<= 0: 0.02).  Out: x_fit[n_grains][n],
+ * overlap[n_grains] (= -objective at x_fit), evals[n_grains] (optional). */
+int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval, double init_step,
+                   double *x_fit, double *overlap, int32_t *evals);
+/* Of the last evaluate / fit call: points evaluated, rounds (launches on a
+ * device), summed device time of the objective kernel (0 on the host). */
+int lmb_refine_last_stats(lmb_refine *r, int64_t *points, int32_t *rounds, float *kernel_ms);
+
 /* ---- survivor ordering that allocates nothing ------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory themselves (code running inside another framework's memory pool, or

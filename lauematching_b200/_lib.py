@@ -43,6 +43,9 @@ EXPORTS = [
     "lmb_pre_get_background", "lmb_pre_segment", "lmb_pre_segment_thresholded",
     "lmb_pre_centres", "lmb_pre_stats", "lmb_pre_images", "lmb_pre_blur", "lmb_pre_timings",
     "lmb_pre_blur_to_slot",
+    "lmb_refine_create", "lmb_refine_destroy", "lmb_refine_dims", "lmb_refine_set_images",
+    "lmb_refine_set_grains", "lmb_refine_start", "lmb_refine_evaluate", "lmb_refine_fit",
+    "lmb_refine_last_stats",
 ]
 
 
@@ -162,6 +165,17 @@ def lib():
         "lmb_pre_blur": ([vp, vp, i32, vp, i32], C.c_int),
         "lmb_pre_timings": ([vp, vp, i32], C.c_int),
         "lmb_pre_blur_to_slot": ([vp, vp, i32, vp, i32, i32, dp], C.c_int),
+        "lmb_refine_create": ([i32, C.POINTER(LmbGeometry), C.POINTER(LmbPostParams), vp, i32,
+                               C.POINTER(vp)], C.c_int),
+        "lmb_refine_destroy": ([vp], C.c_int),
+        "lmb_refine_dims": ([vp, C.POINTER(i32)], C.c_int),
+        "lmb_refine_set_images": ([vp, vp, i32], C.c_int),
+        "lmb_refine_set_grains": ([vp, vp, vp, i32, vp], C.c_int),
+        "lmb_refine_start": ([vp, vp, vp, vp], C.c_int),
+        "lmb_refine_evaluate": ([vp, vp, vp, C.c_int64, vp], C.c_int),
+        "lmb_refine_fit": ([vp, i32, i32, dbl, vp, vp, vp], C.c_int),
+        "lmb_refine_last_stats": ([vp, C.POINTER(C.c_int64), C.POINTER(i32),
+                                   C.POINTER(C.c_float)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -23,6 +23,7 @@
 // with one thread).
 #include <omp.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -33,6 +34,7 @@
 
 #include "../../include/lmb200.h"
 #include "merge.h"
+#include "refine.h"
 
 namespace lmb {
 void set_error(const char *fmt, ...);
@@ -396,11 +398,10 @@ struct Crystal {
   double cell_vol, phi_vol;  // calcV of the params lattice, :371-377
 };
 
-// Objective of the refinement at x (problem_function, :640-694 with
-// calcOverlapFiltered :564-636).
-double objective(unsigned n, const double *x, const Crystal &cr, const double recip0[3][3],
-                 const Detector &d, const float *img, const int32_t *hkls, const int *valid,
-                 int nvalid, int max_spots, std::vector<double> &acc) {
+// The matrix OM . recip of the refinement at x (problem_function :651-673 and
+// calcOverlapFiltered :567-570): the lattice of x when n > 3, else recip0.
+void point_matrix(unsigned n, const double *x, const Crystal &cr, const double recip0[3][3],
+                  double OM[3][3]) {
   double recip[3][3];
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) recip[i][j] = recip0[i][j];
@@ -422,9 +423,16 @@ double objective(unsigned n, const double *x, const Crystal &cr, const double re
     recip_of(lat, cr.sg, recip);
   }
   const double eul[3] = {x[0], x[1], x[2]};
-  double OMt[3][3], OM[3][3];
+  double OMt[3][3];
   euler_to_om(eul, OMt);
   mat33(OMt, recip, OM);
+}
+
+// calcOverlapFiltered (:564-636) at the matrix OM, with problem_function's
+// sign: -(nrPos * sqrt(sum of the kept spots' positive pixels)).
+double overlap_at(const double OM[3][3], const Detector &d, const float *img,
+                  const int32_t *hkls, const int *valid, int nvalid, int max_spots,
+                  std::vector<double> &acc) {
   double result = 0;
   int nspot = 0, npos = 0;
   for (int vi = 0; vi < nvalid; vi++) {
@@ -442,6 +450,61 @@ double objective(unsigned n, const double *x, const Crystal &cr, const double re
     if (++nspot == max_spots) break;
   }
   return -(npos * std::sqrt(result));
+}
+
+// Objective of the refinement at x (problem_function, :640-694 with
+// calcOverlapFiltered :564-636).
+double objective(unsigned n, const double *x, const Crystal &cr, const double recip0[3][3],
+                 const Detector &d, const float *img, const int32_t *hkls, const int *valid,
+                 int nvalid, int max_spots, std::vector<double> &acc) {
+  double OM[3][3];
+  point_matrix(n, x, cr, recip0, OM);
+  return overlap_at(OM, d, img, hkls, valid, nvalid, max_spots, acc);
+}
+
+// The crystal of the refinement (tol_c_over_a != 0 zeroes tol_LatC, as the
+// reference's parameter reader does) with calcV's volumes (:371-377).
+Crystal make_crystal(const lmb_post_params *pp) {
+  Crystal cr;
+  for (int i = 0; i < 6; i++) {
+    cr.lat[i] = pp->lattice[i];
+    cr.tol_latc[i] = pp->tol_c_over_a != 0 ? 0.0 : pp->tol_latc[i];
+  }
+  cr.sg = pp->space_group;
+  cr.tol_c_over_a = pp->tol_c_over_a;
+  cr.c_over_a_orig = cr.lat[2] / cr.lat[0];
+  const double ca = std::cos(cr.lat[3] * kDeg2Rad), cb = std::cos(cr.lat[4] * kDeg2Rad);
+  const double cg = std::cos(cr.lat[5] * kDeg2Rad);
+  cr.phi_vol = std::sqrt(1.0 - ca * ca - cb * cb - cg * cg + 2 * ca * cb * cg);
+  cr.cell_vol = cr.lat[0] * cr.lat[1] * cr.lat[2] * cr.phi_vol;
+  return cr;
+}
+
+void make_detector(const lmb_geometry *geo, Detector *d, double recip[3][3]) {
+  for (int i = 0; i < 3; i++) {
+    d->p[i] = geo->p[i];
+    for (int j = 0; j < 3; j++) {
+      recip[i][j] = geo->recip[i * 3 + j];
+      d->rt[i][j] = geo->rot_t[i * 3 + j];
+    }
+  }
+  d->px_x = geo->px_x;
+  d->px_y = geo->px_y;
+  d->elo = geo->elo;
+  d->ehi = geo->ehi;
+  d->W = geo->nr_px_x;
+  d->H = geo->nr_px_y;
+}
+
+// FitOrientation's dimension count (:705-716): 3 Euler angles plus the
+// lattice entries with a tolerance, or 4 with a c/a tolerance.
+unsigned fit_dims(const Crystal &cr) {
+  int nz = 0;
+  for (int i = 0; i < 6; i++)
+    if (cr.tol_latc[i] != 0) nz++;
+  unsigned n = 3 + nz;
+  if (cr.tol_c_over_a != 0) n = 4;
+  return n;
 }
 
 struct GrainOut {
@@ -531,35 +594,10 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
     }
   const int nthreads = pp->num_threads > 0 ? pp->num_threads : 1;
   const Sym S = make_sym(pp->space_group);
-  Crystal cr;
-  for (int i = 0; i < 6; i++) {
-    cr.lat[i] = pp->lattice[i];
-    cr.tol_latc[i] = pp->tol_c_over_a != 0 ? 0.0 : pp->tol_latc[i];
-  }
-  cr.sg = pp->space_group;
-  cr.tol_c_over_a = pp->tol_c_over_a;
-  cr.c_over_a_orig = cr.lat[2] / cr.lat[0];
-  {
-    const double ca = std::cos(cr.lat[3] * kDeg2Rad), cb = std::cos(cr.lat[4] * kDeg2Rad);
-    const double cg = std::cos(cr.lat[5] * kDeg2Rad);
-    cr.phi_vol = std::sqrt(1.0 - ca * ca - cb * cb - cg * cg + 2 * ca * cb * cg);
-    cr.cell_vol = cr.lat[0] * cr.lat[1] * cr.lat[2] * cr.phi_vol;
-  }
+  const Crystal cr = make_crystal(pp);
   double recip[3][3];
   Detector d;
-  for (int i = 0; i < 3; i++) {
-    d.p[i] = geo->p[i];
-    for (int j = 0; j < 3; j++) {
-      recip[i][j] = geo->recip[i * 3 + j];
-      d.rt[i][j] = geo->rot_t[i * 3 + j];
-    }
-  }
-  d.px_x = geo->px_x;
-  d.px_y = geo->px_y;
-  d.elo = geo->elo;
-  d.ehi = geo->ehi;
-  d.W = geo->nr_px_x;
-  d.H = geo->nr_px_y;
+  make_detector(geo, &d, recip);
   const int max_spots = 3 * geo->max_nr_spots;  // LaueMatchingCPU.c:740
   const double tol = 3 * kDeg2Rad;                // :739
 
@@ -619,14 +657,7 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
       }
     }
     // FitOrientation (:696-801) with the evaluate-once optimiser
-    unsigned n = 3;
-    {
-      int nz = 0;
-      for (int i = 0; i < 6; i++)
-        if (cr.tol_latc[i] != 0) nz++;
-      n = 3 + nz;
-      if (cr.tol_c_over_a != 0) n = 4;
-    }
+    const unsigned n = fit_dims(cr);
     std::vector<double> x(n);
     x[0] = eb[0];
     x[1] = eb[1];
@@ -781,4 +812,605 @@ extern "C" void lmb_post_free(lmb_post_output *out) {
   free(out->spots);
   out->solutions = out->spots = nullptr;
   out->solutions_len = out->spots_len = 0;
+}
+
+// ---- batched refinement (FitOrientation :696-801 over many grains) -------------
+//
+// One context holds the detector, the crystal and the HKL list of a
+// parameter set, the float images of a batch and the grains to refine (their
+// coarse orientations and prefiltered HKL lists).  Evaluations run on a CUDA
+// device (device >= 0, refine.cu) or on host threads (device < 0) with the
+// same arithmetic, so both give identical objective values.
+struct lmb_refine {
+  int device = -1;
+  Detector d{};
+  Crystal cr{};
+  double recip[3][3];
+  int max_spots = 0, nthreads = 1;
+  unsigned n = 3;
+  std::vector<int32_t> hkls;
+  int nh = 0;
+  std::vector<float> frames;  // host evaluation: the images, W x H each
+  int n_img = 0;
+  lmb::RefineDev *dev = nullptr;
+  std::vector<double> hout[lmb::kRefineBufs];  // host evaluation: values per buffer
+  int ng = 0;
+  std::vector<int32_t> gimg, nvalid;
+  std::vector<std::vector<int>> valid;  // host evaluation: per grain
+  std::vector<double> x0, xl, xu;
+  // statistics of the last evaluate / fit call
+  int64_t last_points = 0;
+  int32_t last_rounds = 0;
+  float last_kernel_ms = 0.f;
+};
+
+namespace {
+
+// problem_function at m points (grain[k], x[k][n]), in evaluation buffer b:
+// eval_submit forms the points' matrices (into page-locked memory for the
+// device) and queues the evaluation (on the host: computes it), eval_collect
+// waits for it and hands out the m values (valid until b is submitted again).
+int eval_submit(lmb_refine *r, int b, const int32_t *grain, const double *x, int64_t m) {
+  const int nt = m >= 64 ? r->nthreads : 1;
+  if (r->device >= 0) {
+    double *T = nullptr;
+    int32_t *gd = nullptr;
+    int rc = lmb::refine_dev_stage(r->dev, b, m, &T, &gd);
+    if (rc) return rc;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t k = 0; k < m; k++) {
+      double OM[3][3];
+      point_matrix(r->n, x + (size_t)k * r->n, r->cr, r->recip, OM);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) T[(size_t)k * 9 + i * 3 + j] = OM[i][j];
+      gd[k] = grain[k];
+    }
+    return lmb::refine_dev_submit(r->dev, b, r->max_spots);
+  }
+  std::vector<double> &out = r->hout[b];
+  out.resize((size_t)m);
+  const size_t npx = (size_t)r->d.W * r->d.H;
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<double> acc((size_t)3 * r->max_spots, 0.0);
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t k = 0; k < m; k++) {
+      const int g = grain[k];
+      double OM[3][3];
+      point_matrix(r->n, x + (size_t)k * r->n, r->cr, r->recip, OM);
+      out[k] = overlap_at(OM, r->d, r->frames.data() + npx * r->gimg[g], r->hkls.data(),
+                          r->valid[g].data(), r->nvalid[g], r->max_spots, acc);
+    }
+  }
+  return LMB_OK;
+}
+
+int eval_collect(lmb_refine *r, int b, const double **obj, float *kernel_ms) {
+  if (r->device >= 0) return lmb::refine_dev_collect(r->dev, b, obj, kernel_ms);
+  *obj = r->hout[b].data();
+  if (kernel_ms) *kernel_ms = 0.f;
+  return LMB_OK;
+}
+
+// The two steps at once, values into obj[m].
+int refine_eval(lmb_refine *r, const int32_t *grain, const double *x, int64_t m, double *obj,
+                float *kernel_ms) {
+  int rc = eval_submit(r, 0, grain, x, m);
+  if (rc) return rc;
+  const double *v = nullptr;
+  rc = eval_collect(r, 0, &v, kernel_ms);
+  if (rc) return rc;
+  if (m) memcpy(obj, v, sizeof(double) * m);
+  return LMB_OK;
+}
+
+// Bounded Nelder-Mead (Nelder & Mead 1965, with the coefficients of Lagarias,
+// Reeds, Wright & Wright 1998: reflection 1, expansion 2, contraction 1/2,
+// shrink 1/2), trial points clamped into the box.  This library's own
+// optimiser, not NLopt's: its steps and stopping differ from NLopt's
+// NELDERMEAD and BOBYQA.  One state per grain; every round each running
+// grain proposes its next points and all of them are evaluated together.
+struct NMGrain {
+  std::vector<double> v, f;  // (n+1) x n vertices, n+1 values
+  std::vector<double> xr, xb;  // reflection, centroid of the n best
+  double fr = 0;
+  int phase = 0;  // 0 start simplex, 1 reflect, 2 expand, 3 outside / 4 inside contraction,
+                  // 5 shrink, 6 done
+  int evals = 0;
+  std::vector<double> pend;  // points to evaluate this round
+};
+
+constexpr double kTolRel = 1e-6;  // ftol_rel and xtol_rel of FitOrientation (:773-774)
+// Start simplex: x0 and x0 + h_i e_i, h_i this fraction of coordinate i's box
+// (Euler: 6 degrees wide).  Spots are a few pixels wide, so large first steps
+// land every vertex off all spots.
+constexpr double kInitStep = 0.02;
+// From this many grains on, the fit runs them as two alternating groups.
+constexpr int kSplitGrains = 64;
+
+void nm_clamp(const lmb_refine *r, int g, double *x) {
+  for (unsigned i = 0; i < r->n; i++)
+    x[i] = std::min(std::max(x[i], r->xl[(size_t)g * r->n + i]), r->xu[(size_t)g * r->n + i]);
+}
+
+void nm_sort(NMGrain &s, unsigned n) {
+  std::vector<int> idx(n + 1);
+  for (unsigned i = 0; i <= n; i++) idx[i] = (int)i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return s.f[a] < s.f[b]; });
+  std::vector<double> v2(s.v.size()), f2(n + 1);
+  for (unsigned i = 0; i <= n; i++) {
+    f2[i] = s.f[idx[i]];
+    for (unsigned j = 0; j < n; j++) v2[i * n + j] = s.v[(size_t)idx[i] * n + j];
+  }
+  s.v.swap(v2);
+  s.f.swap(f2);
+}
+
+// Order the simplex, test the stopping rules, propose the reflection.
+void nm_step(const lmb_refine *r, int g, NMGrain &s, int max_eval) {
+  const unsigned n = r->n;
+  nm_sort(s, n);
+  s.pend.clear();
+  bool stop = s.evals + 1 > max_eval;
+  if (!stop && s.f[n] - s.f[0] <= kTolRel * std::fabs(s.f[0])) stop = true;
+  if (!stop) {
+    bool small = true;
+    for (unsigned j = 1; j <= n && small; j++)
+      for (unsigned i = 0; i < n; i++)
+        if (std::fabs(s.v[j * n + i] - s.v[i]) > kTolRel * std::fabs(s.v[i])) {
+          small = false;
+          break;
+        }
+    stop = small;
+  }
+  if (stop) {
+    s.phase = 6;
+    return;
+  }
+  std::vector<double> xb(n, 0.0);
+  for (unsigned j = 0; j < n; j++)
+    for (unsigned i = 0; i < n; i++) xb[i] += s.v[j * n + i];
+  for (unsigned i = 0; i < n; i++) xb[i] /= n;
+  s.xb = xb;
+  s.xr.resize(n);
+  for (unsigned i = 0; i < n; i++) s.xr[i] = xb[i] + (xb[i] - s.v[n * n + i]);
+  nm_clamp(r, g, s.xr.data());
+  s.pend = s.xr;
+  s.phase = 1;
+}
+
+void nm_replace_worst(NMGrain &s, unsigned n, const std::vector<double> &x, double fx) {
+  for (unsigned i = 0; i < n; i++) s.v[n * n + i] = x[i];
+  s.f[n] = fx;
+}
+
+void nm_shrink(const lmb_refine *r, int g, NMGrain &s, int max_eval) {
+  const unsigned n = r->n;
+  if (s.evals + (int)n > max_eval) {
+    nm_sort(s, n);
+    s.pend.clear();
+    s.phase = 6;
+    return;
+  }
+  for (unsigned j = 1; j <= n; j++)
+    for (unsigned i = 0; i < n; i++) s.v[j * n + i] = s.v[i] + 0.5 * (s.v[j * n + i] - s.v[i]);
+  s.pend.assign(s.v.begin() + n, s.v.end());
+  s.phase = 5;
+}
+
+// Take this round's values (res[0..) in the order of s.pend) and move on.
+void nm_consume(const lmb_refine *r, int g, NMGrain &s, const double *res, int max_eval) {
+  const unsigned n = r->n;
+  const std::vector<double> &xb = s.xb;
+  switch (s.phase) {
+    case 0:
+      for (unsigned j = 0; j <= n; j++) s.f[j] = res[j];
+      s.evals += n + 1;
+      nm_step(r, g, s, max_eval);
+      return;
+    case 1: {
+      s.fr = res[0];
+      s.evals++;
+      if (s.fr >= s.f[0] && s.fr < s.f[n - 1]) {
+        nm_replace_worst(s, n, s.xr, s.fr);
+        nm_step(r, g, s, max_eval);
+      } else if (s.fr < s.f[0]) {
+        if (s.evals + 1 > max_eval) {
+          nm_replace_worst(s, n, s.xr, s.fr);
+          nm_step(r, g, s, max_eval);
+          return;
+        }
+        std::vector<double> x(n);
+        for (unsigned i = 0; i < n; i++) x[i] = xb[i] + 2.0 * (xb[i] - s.v[n * n + i]);
+        nm_clamp(r, g, x.data());
+        s.pend = x;
+        s.phase = 2;
+      } else {
+        if (s.evals + 1 > max_eval) {
+          nm_step(r, g, s, max_eval);
+          return;
+        }
+        std::vector<double> x(n);
+        if (s.fr < s.f[n]) {
+          for (unsigned i = 0; i < n; i++) x[i] = xb[i] + 0.5 * (s.xr[i] - xb[i]);
+          s.phase = 3;
+        } else {
+          for (unsigned i = 0; i < n; i++) x[i] = xb[i] + 0.5 * (s.v[n * n + i] - xb[i]);
+          s.phase = 4;
+        }
+        s.pend = x;
+      }
+      return;
+    }
+    case 2:
+      s.evals++;
+      if (res[0] < s.fr)
+        nm_replace_worst(s, n, s.pend, res[0]);
+      else
+        nm_replace_worst(s, n, s.xr, s.fr);
+      nm_step(r, g, s, max_eval);
+      return;
+    case 3:
+      s.evals++;
+      if (res[0] <= s.fr) {
+        nm_replace_worst(s, n, s.pend, res[0]);
+        nm_step(r, g, s, max_eval);
+      } else {
+        nm_shrink(r, g, s, max_eval);
+      }
+      return;
+    case 4:
+      s.evals++;
+      if (res[0] < s.f[n]) {
+        nm_replace_worst(s, n, s.pend, res[0]);
+        nm_step(r, g, s, max_eval);
+      } else {
+        nm_shrink(r, g, s, max_eval);
+      }
+      return;
+    case 5:
+      for (unsigned j = 1; j <= n; j++) s.f[j] = res[j - 1];
+      s.evals += n;
+      nm_step(r, g, s, max_eval);
+      return;
+    default:
+      return;
+  }
+}
+
+}  // namespace
+
+extern "C" int lmb_refine_create(int32_t device, const lmb_geometry *geo,
+                                 const lmb_post_params *pp, const int32_t *hkls, int32_t nh,
+                                 lmb_refine **out) {
+  if (!geo || !pp || !out || nh < 0 || (!hkls && nh) || geo->nr_px_x <= 0 ||
+      geo->nr_px_y <= 0 || geo->max_nr_spots <= 0) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  lmb_refine *r = new lmb_refine();
+  r->device = device;
+  r->cr = make_crystal(pp);
+  make_detector(geo, &r->d, r->recip);
+  r->max_spots = 3 * geo->max_nr_spots;  // LaueMatchingCPU.c:740
+  r->nthreads = pp->num_threads > 0 ? pp->num_threads : 1;
+  r->n = fit_dims(r->cr);
+  r->hkls.assign(hkls, hkls + 3 * (size_t)nh);
+  r->nh = nh;
+  if (device >= 0) {
+    lmb::RefineGeoHost g{};
+    for (int i = 0; i < 3; i++) {
+      g.p[i] = r->d.p[i];
+      for (int j = 0; j < 3; j++) g.rt[i * 3 + j] = r->d.rt[i][j];
+    }
+    g.px_x = r->d.px_x;
+    g.px_y = r->d.px_y;
+    g.elo = r->d.elo;
+    g.ehi = r->d.ehi;
+    g.W = r->d.W;
+    g.H = r->d.H;
+    const int rc = lmb::refine_dev_create(device, g, hkls, nh, &r->dev);
+    if (rc) {
+      delete r;
+      return rc;
+    }
+  }
+  *out = r;
+  return LMB_OK;
+}
+
+extern "C" int lmb_refine_destroy(lmb_refine *r) {
+  if (!r) return LMB_OK;
+  lmb::refine_dev_destroy(r->dev);
+  delete r;
+  return LMB_OK;
+}
+
+extern "C" int lmb_refine_dims(lmb_refine *r, int32_t *n) {
+  if (!r || !n) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  *n = (int32_t)r->n;
+  return LMB_OK;
+}
+
+extern "C" int lmb_refine_set_images(lmb_refine *r, const float *const *frames,
+                                     int32_t n_images) {
+  if (!r || n_images < 0 || (!frames && n_images)) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  for (int i = 0; i < n_images; i++)
+    if (!frames[i]) {
+      lmb::set_error("null frame %d", i);
+      return LMB_ERR_INVALID;
+    }
+  r->ng = 0;
+  if (r->device >= 0) {
+    const int rc = lmb::refine_dev_images(r->dev, frames, n_images);
+    if (rc) return rc;
+  } else {
+    const size_t npx = (size_t)r->d.W * r->d.H;
+    r->frames.resize(npx * n_images);
+    for (int i = 0; i < n_images; i++)
+      memcpy(r->frames.data() + npx * i, frames[i], npx * sizeof(float));
+  }
+  r->n_img = n_images;
+  return LMB_OK;
+}
+
+extern "C" int lmb_refine_set_grains(lmb_refine *r, const double *orients, const int32_t *image,
+                                     int32_t n_grains, int32_t *n_valid) {
+  if (!r || n_grains < 0 || (n_grains && (!orients || !image))) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  for (int g = 0; g < n_grains; g++)
+    if (image[g] < 0 || image[g] >= r->n_img) {
+      lmb::set_error("grain %d: image %d outside the %d images", g, image[g], r->n_img);
+      return LMB_ERR_INVALID;
+    }
+  const unsigned n = r->n;
+  const double tol = 3 * kDeg2Rad;  // LaueMatchingCPU.c:739
+  r->ng = 0;
+  r->gimg.assign(image, image + n_grains);
+  r->x0.assign((size_t)n_grains * n, 0.0);
+  r->xl = r->x0;
+  r->xu = r->x0;
+  std::vector<double> T((size_t)n_grains * 9);
+#pragma omp parallel for num_threads(r->nthreads) schedule(static)
+  for (int g = 0; g < n_grains; g++) {
+    // fitAndWriteOrientations (:1090-1112): Euler angles of the coarse matrix,
+    // FitOrientation's start point and box (:718-743)
+    double ob[3][3], eb[3], OMt[3][3], OM[3][3];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) ob[i][j] = orients[(size_t)g * 9 + i * 3 + j];
+    om_to_euler(ob, eb);
+    double *x = &r->x0[(size_t)g * n], *xl = &r->xl[(size_t)g * n], *xu = &r->xu[(size_t)g * n];
+    for (int i = 0; i < 3; i++) {
+      x[i] = eb[i];
+      xl[i] = eb[i] - tol;
+      xu[i] = eb[i] + tol;
+    }
+    int c = 3;
+    for (int i = 0; i < 6; i++)
+      if (r->cr.tol_latc[i] != 0) {
+        x[c] = r->cr.lat[i];
+        xl[c] = r->cr.lat[i] * (1 - r->cr.tol_latc[i]);
+        xu[c] = r->cr.lat[i] * (1 + r->cr.tol_latc[i]);
+        c++;
+      }
+    if (r->cr.tol_c_over_a != 0) {
+      x[3] = r->cr.c_over_a_orig;
+      xl[3] = r->cr.c_over_a_orig * (1 - r->cr.tol_c_over_a);
+      xu[3] = r->cr.c_over_a_orig * (1 + r->cr.tol_c_over_a);
+    }
+    // prefilterHKLs (:513-561) at the coarse angles with the parameters' lattice
+    euler_to_om(eb, OMt);
+    mat33(OMt, r->recip, OM);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) T[(size_t)g * 9 + i * 3 + j] = OM[i][j];
+  }
+  r->nvalid.assign(n_grains, 0);
+  if (r->device >= 0) {
+    const int rc = lmb::refine_dev_prefilter(r->dev, T.data(), image, n_grains, r->nvalid.data(),
+                                             nullptr);
+    if (rc) return rc;
+  } else {
+    r->valid.assign(n_grains, {});
+#pragma omp parallel for num_threads(r->nthreads) schedule(dynamic)
+    for (int g = 0; g < n_grains; g++) {
+      double OM[3][3];
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) OM[i][j] = T[(size_t)g * 9 + i * 3 + j];
+      for (int h = 0; h < r->nh; h++) {
+        double qh[3], px, py, ql;
+        if (project(OM, r->hkls.data() + 3 * h, r->d, qh, px, py, ql)) r->valid[g].push_back(h);
+      }
+      r->nvalid[g] = (int32_t)r->valid[g].size();
+    }
+  }
+  if (n_valid) memcpy(n_valid, r->nvalid.data(), sizeof(int32_t) * n_grains);
+  r->ng = n_grains;
+  return LMB_OK;
+}
+
+extern "C" int lmb_refine_start(lmb_refine *r, double *x0, double *lower, double *upper) {
+  if (!r) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  const size_t k = (size_t)r->ng * r->n;
+  if (x0) memcpy(x0, r->x0.data(), k * sizeof(double));
+  if (lower) memcpy(lower, r->xl.data(), k * sizeof(double));
+  if (upper) memcpy(upper, r->xu.data(), k * sizeof(double));
+  return LMB_OK;
+}
+
+extern "C" int lmb_refine_evaluate(lmb_refine *r, const int32_t *grain, const double *x,
+                                   int64_t m, double *objective) {
+  if (!r || m < 0 || (m && (!grain || !x || !objective))) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  for (int64_t k = 0; k < m; k++)
+    if (grain[k] < 0 || grain[k] >= r->ng) {
+      lmb::set_error("point %lld: grain %d outside the %d grains", (long long)k, grain[k], r->ng);
+      return LMB_ERR_INVALID;
+    }
+  float ms = 0.f;
+  const int rc = refine_eval(r, grain, x, m, objective, &ms);
+  r->last_points = m;
+  r->last_rounds = 1;
+  r->last_kernel_ms = ms;
+  return rc;
+}
+
+extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval,
+                              double init_step, double *x_fit, double *overlap, int32_t *evals) {
+  if (!r || (optimizer != 0 && optimizer != 1) || max_eval < 1 || !(init_step < 1.0) ||
+      (r->ng && (!x_fit || !overlap))) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  const unsigned n = r->n;
+  const int ng = r->ng;
+  r->last_points = 0;
+  r->last_rounds = 0;
+  r->last_kernel_ms = 0.f;
+  if (ng == 0) return LMB_OK;
+  if (optimizer == 0 || max_eval < (int)n + 1) {
+    // the evaluate-once stand-in: x stays at the start point
+    std::vector<int32_t> gi(ng);
+    std::vector<double> f(ng);
+    for (int g = 0; g < ng; g++) gi[g] = g;
+    float ms = 0.f;
+    const int rc = refine_eval(r, gi.data(), r->x0.data(), ng, f.data(), &ms);
+    if (rc) return rc;
+    memcpy(x_fit, r->x0.data(), sizeof(double) * ng * n);
+    for (int g = 0; g < ng; g++) {
+      overlap[g] = -f[g];
+      if (evals) evals[g] = 1;
+    }
+    r->last_points = ng;
+    r->last_rounds = 1;
+    r->last_kernel_ms = ms;
+    return LMB_OK;
+  }
+  std::vector<NMGrain> st(ng);
+  for (int g = 0; g < ng; g++) {
+    NMGrain &s = st[g];
+    const double *x0 = &r->x0[(size_t)g * n];
+    s.v.assign((size_t)(n + 1) * n, 0.0);
+    s.f.assign(n + 1, 0.0);
+    for (unsigned j = 0; j <= n; j++)
+      for (unsigned i = 0; i < n; i++) s.v[j * n + i] = x0[i];
+    for (unsigned i = 0; i < n; i++) {
+      const double lo = r->xl[(size_t)g * n + i], hi = r->xu[(size_t)g * n + i];
+      const double h = (init_step > 0 ? init_step : kInitStep) * (hi - lo);
+      double y = x0[i] + h;
+      if (y > hi) y = x0[i] - h;
+      s.v[(i + 1) * n + i] = y;
+    }
+    s.pend = s.v;
+    s.phase = 0;
+  }
+  // Two groups of grains alternate: while the device evaluates one group's
+  // round, the host takes the other group's values and forms its next points.
+  // Each grain's steps depend on its own values only, so the grouping changes
+  // no result.
+  struct Group {
+    int g0 = 0, g1 = 0;
+    std::vector<int32_t> pg;
+    std::vector<double> px;
+    std::vector<int64_t> off;
+    bool pending = false;
+  };
+  const int ngroups = ng >= kSplitGrains ? 2 : 1;
+  Group grp[2];
+  for (int b = 0; b < ngroups; b++) {
+    grp[b].g0 = (int)((int64_t)ng * b / ngroups);
+    grp[b].g1 = (int)((int64_t)ng * (b + 1) / ngroups);
+    grp[b].off.assign(grp[b].g1 - grp[b].g0 + 1, 0);
+  }
+  const int nt = r->nthreads;
+  auto build = [&](Group &G) {  // the group's pending points, in grain order
+    const int cnt = G.g1 - G.g0;
+    int64_t tot = 0;
+    for (int g = G.g0; g < G.g1; g++) {
+      G.off[g - G.g0] = tot;
+      if (st[g].phase != 6) tot += (int64_t)(st[g].pend.size() / n);
+    }
+    G.off[cnt] = tot;
+    G.pg.resize((size_t)tot);
+    G.px.resize((size_t)tot * n);
+#pragma omp parallel for num_threads(nt) schedule(static) if (cnt >= 256)
+    for (int g = G.g0; g < G.g1; g++) {
+      if (st[g].phase == 6) continue;
+      const int64_t o = G.off[g - G.g0], k = G.off[g - G.g0 + 1] - o;
+      for (int64_t j = 0; j < k; j++) G.pg[(size_t)(o + j)] = g;
+      std::copy(st[g].pend.begin(), st[g].pend.end(), G.px.begin() + (size_t)o * n);
+    }
+    return tot;
+  };
+  auto drain = [&]() {  // after an error: wait for what is still queued
+    for (int b = 0; b < ngroups; b++)
+      if (grp[b].pending) {
+        const double *v;
+        eval_collect(r, b, &v, nullptr);
+        grp[b].pending = false;
+      }
+  };
+  int rc = LMB_OK;
+  for (int b = 0; b < ngroups && !rc; b++)
+    if (build(grp[b]) > 0) {
+      rc = eval_submit(r, b, grp[b].pg.data(), grp[b].px.data(), (int64_t)grp[b].pg.size());
+      grp[b].pending = rc == LMB_OK;
+    }
+  for (bool any = true; any && !rc;) {
+    any = false;
+    for (int b = 0; b < ngroups && !rc; b++) {
+      Group &G = grp[b];
+      if (!G.pending) continue;
+      any = true;
+      const double *pf = nullptr;
+      float ms = 0.f;
+      G.pending = false;
+      rc = eval_collect(r, b, &pf, &ms);
+      if (rc) break;
+      r->last_points += (int64_t)G.pg.size();
+      r->last_rounds++;
+      r->last_kernel_ms += ms;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 32) if (G.g1 - G.g0 >= 256)
+      for (int g = G.g0; g < G.g1; g++)
+        if (st[g].phase != 6) nm_consume(r, g, st[g], pf + G.off[g - G.g0], max_eval);
+      if (build(G) > 0) {
+        rc = eval_submit(r, b, G.pg.data(), G.px.data(), (int64_t)G.pg.size());
+        G.pending = rc == LMB_OK;
+      }
+    }
+  }
+  if (rc) {
+    drain();
+    return rc;
+  }
+  for (int g = 0; g < ng; g++) {
+    memcpy(x_fit + (size_t)g * n, st[g].v.data(), sizeof(double) * n);
+    overlap[g] = -st[g].f[0];
+    if (evals) evals[g] = st[g].evals;
+  }
+  return LMB_OK;
+}
+
+extern "C" int lmb_refine_last_stats(lmb_refine *r, int64_t *points, int32_t *rounds,
+                                     float *kernel_ms) {
+  if (!r) {
+    lmb::set_error("bad argument");
+    return LMB_ERR_INVALID;
+  }
+  if (points) *points = r->last_points;
+  if (rounds) *rounds = r->last_rounds;
+  if (kernel_ms) *kernel_ms = r->last_kernel_ms;
+  return LMB_OK;
 }

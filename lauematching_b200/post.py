@@ -29,6 +29,23 @@ STREAM_SOLUTIONS_HEADER = "%ImageNr\t" + SOLUTIONS_HEADER[1:]
 STREAM_SPOTS_HEADER = "%ImageNr\t" + SPOTS_HEADER[1:]
 
 
+def make_post_params(params: LaueParams, min_nr_spots: int | None = None,
+                     num_threads: int | None = None) -> _lib.LmbPostParams:
+    """The post-stage's crystal and merge parameters from a parameter file."""
+    pp = _lib.LmbPostParams()
+    for i in range(6):
+        pp.lattice[i] = params.lattice[i]
+        pp.tol_latc[i] = params.tol_latc[i]
+    pp.space_group = int(params.space_group)
+    pp.max_nr_spots = int(params.max_nr_spots)
+    pp.tol_c_over_a = float(params.tol_c_over_a)
+    pp.max_angle = float(params.max_angle)
+    pp.min_nr_spots = int(params.min_nr_spots if min_nr_spots is None else min_nr_spots)
+    pp.num_threads = int(num_threads or os.cpu_count() or 1)
+    pp.optimizer = 0
+    return pp
+
+
 def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndarray,
                  scores: np.ndarray, image_f32: np.ndarray, hkls: np.ndarray,
                  min_nr_spots: int | None = None, image_num: int = 0,
@@ -42,18 +59,8 @@ def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndar
     cap path, LaueMatchingHeaders.h:976-997, with its cap of 50000 lowered).
     ``merge_device`` (a CUDA device index) runs the duplicate merge of 1024 or
     more candidates on that device (same clusters); None keeps it on the host."""
-    pp = _lib.LmbPostParams()
-    for i in range(6):
-        pp.lattice[i] = params.lattice[i]
-        pp.tol_latc[i] = params.tol_latc[i]
-    pp.space_group = int(params.space_group)
-    pp.max_nr_spots = int(params.max_nr_spots)
-    pp.tol_c_over_a = float(params.tol_c_over_a)
-    pp.max_angle = float(params.max_angle)
-    pp.min_nr_spots = int(params.min_nr_spots if min_nr_spots is None else min_nr_spots)
+    pp = make_post_params(params, min_nr_spots, num_threads)
     pp.image_num = int(image_num)
-    pp.num_threads = int(num_threads or os.cpu_count() or 1)
-    pp.optimizer = 0
     pp.max_results = int(max_results)  # 0: the reference's 50000
     pp.merge_on_device = 0 if merge_device is None else int(merge_device) + 1
     om = np.ascontiguousarray(orients, dtype=np.float64).reshape(-1, 9)

@@ -199,6 +199,23 @@ def pick_grains(records: np.ndarray, n_grains: int, min_spots: int,
     return np.sort(pick) + id_offset
 
 
+def perturb_orientations(om: np.ndarray, rng: np.random.Generator, lo_deg: float,
+                         hi_deg: float) -> np.ndarray:
+    """Each orientation matrix (n, 9) turned by an angle uniform in
+    [lo_deg, hi_deg] about a random axis (left-multiplied rotation): coarse
+    starting points of a refinement, as a DB grid's nearest neighbour is."""
+    om = np.asarray(om, np.float64).reshape(-1, 3, 3)
+    ax = rng.normal(size=(om.shape[0], 3))
+    ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+    ang = np.deg2rad(rng.uniform(lo_deg, hi_deg, size=om.shape[0]))
+    K = np.zeros((om.shape[0], 3, 3))
+    K[:, 0, 1], K[:, 0, 2], K[:, 1, 2] = -ax[:, 2], ax[:, 1], -ax[:, 0]
+    K[:, 1, 0], K[:, 2, 0], K[:, 2, 1] = ax[:, 2], -ax[:, 1], ax[:, 0]
+    s, c = np.sin(ang)[:, None, None], np.cos(ang)[:, None, None]
+    R = np.eye(3)[None] + s * K + (1 - c) * (K @ K)
+    return (R @ om).reshape(-1, 9)
+
+
 def render_image(grain_records: np.ndarray, nr_px_x: int, nr_px_y: int,
                  rng: np.random.Generator, sigma: float = 2.0,
                  amp_lo: float = 50.0, amp_hi: float = 255.0,
