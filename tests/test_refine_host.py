@@ -19,7 +19,8 @@ from lauematching_b200.refine import Refiner
 
 pytestmark = pytest.mark.skipif(not RO.available(), reason="oracle/_ref/libref_objective.so not built")
 
-CASES = ["tilted_fcc", "tilted_hex_ca", "tilted_dense", "beamnormal_fcc"]
+CASES = ["tilted_fcc", "tilted_hex_ca", "tilted_dense", "beamnormal_fcc", "tilted_rhomb",
+         "tilted_hex"]
 
 
 def scene(name, crystal="params", n_grains=24):
