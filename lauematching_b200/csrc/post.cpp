@@ -910,14 +910,18 @@ int refine_eval(lmb_refine *r, const int32_t *grain, const double *x, int64_t m,
 // optimiser, not NLopt's: its steps and stopping differ from NLopt's
 // NELDERMEAD and BOBYQA.  One state per grain; every round each running
 // grain proposes its next points and all of them are evaluated together.
+constexpr int kMaxDims = 9;  // 3 Euler angles + 6 lattice parameters
+
 struct NMGrain {
-  std::vector<double> v, f;  // (n+1) x n vertices, n+1 values
-  std::vector<double> xr, xb;  // reflection, centroid of the n best
+  double v[(kMaxDims + 1) * kMaxDims];  // n+1 vertices of n coordinates
+  double f[kMaxDims + 1];               // their values
+  double xr[kMaxDims], xb[kMaxDims];    // reflection, centroid of the n best
   double fr = 0;
   int phase = 0;  // 0 start simplex, 1 reflect, 2 expand, 3 outside / 4 inside contraction,
                   // 5 shrink, 6 done
   int evals = 0;
-  std::vector<double> pend;  // points to evaluate this round
+  int npend = 0;                                // points to evaluate this round
+  double pend[(kMaxDims + 1) * kMaxDims];
 };
 
 constexpr double kTolRel = 1e-6;  // ftol_rel and xtol_rel of FitOrientation (:773-774)
@@ -933,24 +937,32 @@ void nm_clamp(const lmb_refine *r, int g, double *x) {
     x[i] = std::min(std::max(x[i], r->xl[(size_t)g * r->n + i]), r->xu[(size_t)g * r->n + i]);
 }
 
+void nm_propose(NMGrain &s, unsigned n, const double *x) {
+  for (unsigned i = 0; i < n; i++) s.pend[i] = x[i];
+  s.npend = 1;
+}
+
+// Vertices in ascending value, ties in their current order (a stable sort).
 void nm_sort(NMGrain &s, unsigned n) {
-  std::vector<int> idx(n + 1);
-  for (unsigned i = 0; i <= n; i++) idx[i] = (int)i;
-  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return s.f[a] < s.f[b]; });
-  std::vector<double> v2(s.v.size()), f2(n + 1);
-  for (unsigned i = 0; i <= n; i++) {
-    f2[i] = s.f[idx[i]];
-    for (unsigned j = 0; j < n; j++) v2[i * n + j] = s.v[(size_t)idx[i] * n + j];
+  for (unsigned i = 1; i <= n; i++) {
+    const double fi = s.f[i];
+    double vi[kMaxDims];
+    for (unsigned c = 0; c < n; c++) vi[c] = s.v[i * n + c];
+    unsigned j = i;
+    for (; j > 0 && s.f[j - 1] > fi; j--) {
+      s.f[j] = s.f[j - 1];
+      for (unsigned c = 0; c < n; c++) s.v[j * n + c] = s.v[(j - 1) * n + c];
+    }
+    s.f[j] = fi;
+    for (unsigned c = 0; c < n; c++) s.v[j * n + c] = vi[c];
   }
-  s.v.swap(v2);
-  s.f.swap(f2);
 }
 
 // Order the simplex, test the stopping rules, propose the reflection.
 void nm_step(const lmb_refine *r, int g, NMGrain &s, int max_eval) {
   const unsigned n = r->n;
   nm_sort(s, n);
-  s.pend.clear();
+  s.npend = 0;
   bool stop = s.evals + 1 > max_eval;
   if (!stop && s.f[n] - s.f[0] <= kTolRel * std::fabs(s.f[0])) stop = true;
   if (!stop) {
@@ -967,41 +979,41 @@ void nm_step(const lmb_refine *r, int g, NMGrain &s, int max_eval) {
     s.phase = 6;
     return;
   }
-  std::vector<double> xb(n, 0.0);
+  for (unsigned i = 0; i < n; i++) s.xb[i] = 0.0;
   for (unsigned j = 0; j < n; j++)
-    for (unsigned i = 0; i < n; i++) xb[i] += s.v[j * n + i];
-  for (unsigned i = 0; i < n; i++) xb[i] /= n;
-  s.xb = xb;
-  s.xr.resize(n);
-  for (unsigned i = 0; i < n; i++) s.xr[i] = xb[i] + (xb[i] - s.v[n * n + i]);
-  nm_clamp(r, g, s.xr.data());
-  s.pend = s.xr;
+    for (unsigned i = 0; i < n; i++) s.xb[i] += s.v[j * n + i];
+  for (unsigned i = 0; i < n; i++) s.xb[i] /= n;
+  for (unsigned i = 0; i < n; i++) s.xr[i] = s.xb[i] + (s.xb[i] - s.v[n * n + i]);
+  nm_clamp(r, g, s.xr);
+  nm_propose(s, n, s.xr);
   s.phase = 1;
 }
 
-void nm_replace_worst(NMGrain &s, unsigned n, const std::vector<double> &x, double fx) {
+void nm_replace_worst(NMGrain &s, unsigned n, const double *x, double fx) {
   for (unsigned i = 0; i < n; i++) s.v[n * n + i] = x[i];
   s.f[n] = fx;
 }
 
 void nm_shrink(const lmb_refine *r, int g, NMGrain &s, int max_eval) {
+  (void)g;
   const unsigned n = r->n;
   if (s.evals + (int)n > max_eval) {
     nm_sort(s, n);
-    s.pend.clear();
+    s.npend = 0;
     s.phase = 6;
     return;
   }
   for (unsigned j = 1; j <= n; j++)
     for (unsigned i = 0; i < n; i++) s.v[j * n + i] = s.v[i] + 0.5 * (s.v[j * n + i] - s.v[i]);
-  s.pend.assign(s.v.begin() + n, s.v.end());
+  for (unsigned k = 0; k < n * n; k++) s.pend[k] = s.v[n + k];
+  s.npend = (int)n;
   s.phase = 5;
 }
 
 // Take this round's values (res[0..) in the order of s.pend) and move on.
 void nm_consume(const lmb_refine *r, int g, NMGrain &s, const double *res, int max_eval) {
   const unsigned n = r->n;
-  const std::vector<double> &xb = s.xb;
+  const double *xb = s.xb;
   switch (s.phase) {
     case 0:
       for (unsigned j = 0; j <= n; j++) s.f[j] = res[j];
@@ -1020,17 +1032,17 @@ void nm_consume(const lmb_refine *r, int g, NMGrain &s, const double *res, int m
           nm_step(r, g, s, max_eval);
           return;
         }
-        std::vector<double> x(n);
+        double x[kMaxDims];
         for (unsigned i = 0; i < n; i++) x[i] = xb[i] + 2.0 * (xb[i] - s.v[n * n + i]);
-        nm_clamp(r, g, x.data());
-        s.pend = x;
+        nm_clamp(r, g, x);
+        nm_propose(s, n, x);
         s.phase = 2;
       } else {
         if (s.evals + 1 > max_eval) {
           nm_step(r, g, s, max_eval);
           return;
         }
-        std::vector<double> x(n);
+        double x[kMaxDims];
         if (s.fr < s.f[n]) {
           for (unsigned i = 0; i < n; i++) x[i] = xb[i] + 0.5 * (s.xr[i] - xb[i]);
           s.phase = 3;
@@ -1038,7 +1050,7 @@ void nm_consume(const lmb_refine *r, int g, NMGrain &s, const double *res, int m
           for (unsigned i = 0; i < n; i++) x[i] = xb[i] + 0.5 * (s.v[n * n + i] - xb[i]);
           s.phase = 4;
         }
-        s.pend = x;
+        nm_propose(s, n, x);
       }
       return;
     }
@@ -1302,10 +1314,10 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
   for (int g = 0; g < ng; g++) {
     NMGrain &s = st[g];
     const double *x0 = &r->x0[(size_t)g * n];
-    s.v.assign((size_t)(n + 1) * n, 0.0);
-    s.f.assign(n + 1, 0.0);
-    for (unsigned j = 0; j <= n; j++)
+    for (unsigned j = 0; j <= n; j++) {
+      s.f[j] = 0.0;
       for (unsigned i = 0; i < n; i++) s.v[j * n + i] = x0[i];
+    }
     for (unsigned i = 0; i < n; i++) {
       const double lo = r->xl[(size_t)g * n + i], hi = r->xu[(size_t)g * n + i];
       const double h = (init_step > 0 ? init_step : kInitStep) * (hi - lo);
@@ -1313,7 +1325,8 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
       if (y > hi) y = x0[i] - h;
       s.v[(i + 1) * n + i] = y;
     }
-    s.pend = s.v;
+    for (unsigned k = 0; k < (n + 1) * n; k++) s.pend[k] = s.v[k];
+    s.npend = (int)n + 1;
     s.phase = 0;
   }
   // Two groups of grains alternate: while the device evaluates one group's
@@ -1340,7 +1353,7 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
     int64_t tot = 0;
     for (int g = G.g0; g < G.g1; g++) {
       G.off[g - G.g0] = tot;
-      if (st[g].phase != 6) tot += (int64_t)(st[g].pend.size() / n);
+      if (st[g].phase != 6) tot += st[g].npend;
     }
     G.off[cnt] = tot;
     G.pg.resize((size_t)tot);
@@ -1350,7 +1363,7 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
       if (st[g].phase == 6) continue;
       const int64_t o = G.off[g - G.g0], k = G.off[g - G.g0 + 1] - o;
       for (int64_t j = 0; j < k; j++) G.pg[(size_t)(o + j)] = g;
-      std::copy(st[g].pend.begin(), st[g].pend.end(), G.px.begin() + (size_t)o * n);
+      std::copy(st[g].pend, st[g].pend + (size_t)k * n, G.px.begin() + (size_t)o * n);
     }
     return tot;
   };
@@ -1396,7 +1409,7 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
     return rc;
   }
   for (int g = 0; g < ng; g++) {
-    memcpy(x_fit + (size_t)g * n, st[g].v.data(), sizeof(double) * n);
+    memcpy(x_fit + (size_t)g * n, st[g].v, sizeof(double) * n);
     overlap[g] = -st[g].f[0];
     if (evals) evals[g] = st[g].evals;
   }
