@@ -30,7 +30,7 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
   } while (0)
 
 // ---- device error flag codes ---------------------------------------------
-enum DevErr : int { DEV_OK = 0, DEV_TIMEOUT_TMA = 1, DEV_BAD_ALIGN = 2 };
+enum DevErr : int { DEV_OK = 0, DEV_TIMEOUT_TMA = 1, DEV_BAD_ALIGN = 2, DEV_BAD_QUEUE = 3 };
 
 // ---- exact FP64 (round to nearest, never contracted into FMA) -------------
 // The reference CPU build has no fused multiply-add (x86-64 SSE2, -O3 without

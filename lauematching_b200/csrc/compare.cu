@@ -638,8 +638,8 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
   // This warp's queue of records that can pass, copied out of the ring (id,
   // count, pixel indices at an odd stride): a chunk with few of them feeds the
   // queue, and the queue is counted 32 records at a time on a full warp.
-  const uint32_t SP = clist_queue_stride(a.S);
-  unsigned char *qb = ring + (size_t)ST * a.tile_bytes + (size_t)cw * clist_queue_bytes(a.S);
+  const uint32_t SP = clist_queue_stride(a.qS);
+  unsigned char *qb = ring + (size_t)ST * a.tile_bytes + (size_t)cw * clist_queue_bytes(a.qS);
   uint64_t *q_oid = reinterpret_cast<uint64_t *>(qb);
   uint32_t *q_c = reinterpret_cast<uint32_t *>(qb + 256);
   uint32_t *q_sp = reinterpret_cast<uint32_t *>(qb + 384);
@@ -690,7 +690,10 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
           if (lane >= o) x += y;
         }
         const uint32_t *my = spots + base[ch] + (x - c);
-        unsigned qm = __ballot_sync(0xffffffffu, valid && c >= need);
+        // a record longer than a queue entry cannot come from a layout whose
+        // largest count sized the queue; should one appear, fail the pass
+        if (valid && c >= need && c > a.qS) atomicExch(a.err, DEV_BAD_QUEUE);
+        unsigned qm = __ballot_sync(0xffffffffu, valid && c >= need && c <= a.qS);
         if (__popc(qm) >= kDirect) {  // many can pass: count the chunk in place
           process<B, ListSpots, MINB>(a, ListSpots{my}, c, oid, pol_occ, valid);
           continue;
@@ -831,14 +834,23 @@ CompareTuning compare_config(int R, const CompareTuning &req) {
   return c;
 }
 
+template <int B, int MINB>
+static int launch_clist_bounded(const CmpArgs &a, unsigned grid, size_t smem, cudaStream_t st) {
+  const int rc = ensure_smem((const void *)compare_clist_kernel<B, MINB>, (int)smem);
+  if (rc) return rc;
+  compare_clist_kernel<B, MINB><<<grid, 128, smem, st>>>(a);
+  return LMB_OK;
+}
+
 template <int B>
 static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, size_t smem,
-                    bool six, cudaStream_t st) {
-  if (c.variant == 2 && six) {
-    // six 128-thread blocks per SM: registers bounded for that occupancy
-    const int rc = ensure_smem((const void *)compare_clist_kernel<B, 6>, (int)smem);
+                    int nblk, cudaStream_t st) {
+  if (c.variant == 2 && nblk >= 6) {
+    // six to eight 128-thread blocks per SM: registers bounded for that occupancy
+    const int rc = nblk >= 8   ? launch_clist_bounded<B, 8>(a, grid, smem, st)
+                   : nblk == 7 ? launch_clist_bounded<B, 7>(a, grid, smem, st)
+                               : launch_clist_bounded<B, 6>(a, grid, smem, st);
     if (rc) return rc;
-    compare_clist_kernel<B, 6><<<grid, 128, smem, st>>>(a);
   } else if (c.variant == 2) {
     const int rc = ensure_smem((const void *)compare_clist_kernel<B, 1>, (int)smem);
     if (rc) return rc;
@@ -871,7 +883,8 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
     a.tile = 0;
     a.ntiles = a.cl_tiles;
     a.full_tiles = a.ntiles;
-    const size_t qbytes = (size_t)c.consumers * clist_queue_bytes(a.S);
+    LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "compact pass queue entry of %d spots", a.qS);
+    const size_t qbytes = (size_t)c.consumers * clist_queue_bytes(a.qS);
     const size_t room = 227 * 1024 > 256 + qbytes ? 227 * 1024 - 256 - qbytes : 0;
     const int fit = (int)std::min<size_t>(16, room / a.tile_bytes);
     LMB_REQUIRE(fit >= 2, "compact tiles of %u bytes leave no room for a ring", a.tile_bytes);
@@ -886,22 +899,22 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   a.stages = c.stages;
   if (a.ntiles == 0 || a.active == 0) return LMB_OK;
   size_t smem = 256 + (size_t)c.stages * a.tile_bytes;
-  if (c.variant == 2) smem += (size_t)c.consumers * clist_queue_bytes(a.S);
+  if (c.variant == 2) smem += (size_t)c.consumers * clist_queue_bytes(a.qS);
   LMB_REQUIRE(smem <= 227 * 1024, "compare ring of %zu bytes exceeds shared memory", smem);
   const int mult = c.grid_mult > 0 ? c.grid_mult : 1;
   const unsigned grid = (unsigned)std::min<uint64_t>(
       a.ntiles, (uint64_t)num_sms * c.blocks_per_sm * (uint64_t)mult);
   const int B = counter_bits(a.S);
-  // six 128-thread compact-pass blocks per SM (the tuned shape) get a kernel
-  // whose registers are bounded for that occupancy
-  const bool six = c.variant == 2 && c.consumers == 3 && mult >= 6;
-  if (B <= 3) return launch_b<3>(a, c, grid, smem, six, st);
-  if (B <= 5) return launch_b<5>(a, c, grid, smem, six, st);
-  if (B <= 6) return launch_b<6>(a, c, grid, smem, six, st);
-  if (B <= 7) return launch_b<7>(a, c, grid, smem, six, st);
-  if (B <= 9) return launch_b<9>(a, c, grid, smem, six, st);
-  if (B <= 11) return launch_b<11>(a, c, grid, smem, six, st);
-  return launch_b<16>(a, c, grid, smem, six, st);
+  // six to eight 128-thread compact-pass blocks per SM (the tuned shapes) get
+  // a kernel whose registers are bounded for that occupancy
+  const int nblk = (c.variant == 2 && c.consumers == 3) ? std::min(mult, 8) : 0;
+  if (B <= 3) return launch_b<3>(a, c, grid, smem, nblk, st);
+  if (B <= 5) return launch_b<5>(a, c, grid, smem, nblk, st);
+  if (B <= 6) return launch_b<6>(a, c, grid, smem, nblk, st);
+  if (B <= 7) return launch_b<7>(a, c, grid, smem, nblk, st);
+  if (B <= 9) return launch_b<9>(a, c, grid, smem, nblk, st);
+  if (B <= 11) return launch_b<11>(a, c, grid, smem, nblk, st);
+  return launch_b<16>(a, c, grid, smem, nblk, st);
 }
 
 // Zero the survivor and pass counters of the pass's slots only: the counters

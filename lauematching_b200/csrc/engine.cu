@@ -76,6 +76,7 @@ struct lmb_engine {
   uint64_t cl_bytes = 0;
   int cl_state = 0;  // 0 not built, 1 built, -1 this DB cannot use it
   unsigned long long cl_hist[256] = {};  // records per on-detector spot count
+  int cl_qs = 0;  // largest on-detector spot count of a record (sizes the pass's queues)
   // image slots
   uint8_t *d_u8 = nullptr;
   double *d_f64 = nullptr;  // allocated on first keep_f64 load
@@ -103,8 +104,8 @@ struct lmb_engine {
   cudaEvent_t ev_loaded[LMB_MAX_SLOTS] = {};
   cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
   // automatic variant with the compact pass's tuned shape (2 stages, 3 consumer
-  // warps, 6 blocks per SM)
-  CompareTuning tuning{3, 0, 2, 3, 1, 6, 0};
+  // warps, 8 blocks per SM)
+  CompareTuning tuning{3, 0, 2, 3, 1, 8, 0};
   int last_variant = -1;  // variant the latest pass ran
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
@@ -249,6 +250,7 @@ int alloc_db(lmb_engine *e, uint64_t n) {
   e->cl_tiles = 0;
   e->cl_state = 0;
   e->cl_bytes = 0;
+  e->cl_qs = 0;
   const size_t bytes = (size_t)n * e->R * 2;
   const size_t alloc = ((bytes + 255) / 256) * 256 + 256;
   LMB_CUDA(cudaMalloc(&e->d_db, alloc));
@@ -395,6 +397,12 @@ int build_compact(lmb_engine *e) {
     cudaFree(d_aux);
     return rc ? rc : cuda_fail(ce, "compact layout: chunk counts", __FILE__, __LINE__);
   }
+  e->cl_qs = 1;
+  for (int c = 255; c >= 1; c--)
+    if (e->cl_hist[c]) {
+      e->cl_qs = c;
+      break;
+    }
   uint64_t total_spots = 0, max_spots = 0;
   for (uint64_t c = 0; c < nch; c++) {
     total_spots += cs[c];
@@ -404,13 +412,15 @@ int build_compact(lmb_engine *e) {
   const uint64_t avg_chunk = 36 + (4 * total_spots + nch - 1) / nch;
   uint64_t TB = std::min<uint64_t>(24 * 1024, std::max<uint64_t>(4096, round128(64 * avg_chunk)));
   {
-    // room for six blocks of the default pass shape (three consumer warps, a
-    // two-stage ring) on an SM, when the largest chunk allows it
+    // room for the pass shape's blocks (three consumer warps, a two-stage
+    // ring; six per SM, or up to eight when the tuning asks for more) on an
+    // SM, when the largest chunk allows it
     int per_sm = 0, reserved = 0;
     cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, e->device);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, e->device);
+    const int nb = std::max(6, std::min(8, e->tuning.grid_mult));
     const int64_t room =
-        (int64_t)per_sm / 6 - reserved - 256 - 3 * (int64_t)clist_queue_bytes(e->S);
+        (int64_t)per_sm / nb - reserved - 256 - 3 * (int64_t)clist_queue_bytes(e->cl_qs);
     if (room > 2 * 4096) TB = std::min<uint64_t>(TB, (uint64_t)(room / 2) / 128 * 128);
   }
   TB = std::max<uint64_t>(TB, round128(clist_spot_offset(1) + 4 * max_spots));
@@ -493,6 +503,7 @@ int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   a.n = e->n;
   a.R = e->R;
   a.S = e->S;
+  a.qS = e->cl_qs > 0 ? e->cl_qs : e->S;
   a.W = e->geo.nr_px_x;
   a.H = e->geo.nr_px_y;
   a.occ = e->d_occ;
@@ -1109,6 +1120,10 @@ int slot_status(lmb_engine *e, int slot, const unsigned int **st) {
   LMB_CUDA(cudaEventSynchronize(e->ev_done[r]));
   *st = e->h_status + (size_t)r * kStatusWords;
   const int derr = (int)(*st)[2 * LMB_MAX_SLOTS];
+  if (derr == DEV_BAD_QUEUE) {
+    set_error("compare pass: a compact-layout record longer than the pass's queue entries");
+    return LMB_ERR_INVALID;
+  }
   if (derr != DEV_OK) {
     set_error("device wait gave up in the compare pass (code %d)", derr);
     return LMB_ERR_TIMEOUT;

@@ -11,6 +11,7 @@ struct CmpArgs {
   const uint16_t *db;  // n records of R uint16, 16-byte aligned
   uint64_t n;
   int R, S, W, H;
+  int qS;  // compact pass: spots per record-queue entry (the layout's largest count)
   const unsigned long long *occ;  // per pixel: bit k = slot k's uint8 pixel > 0
   unsigned long long active;      // slots of this pass
   const uint8_t *u8;              // slot k image at u8 + k*npx

@@ -238,6 +238,27 @@ def test_compact_layout_matches_oracle(name, mode):
     assert_same_survivors(got, ref)
 
 
+@pytest.mark.parametrize("nb", [7, 8])
+def test_compact_layout_sized_for_more_blocks_matches_oracle(nb):
+    """The compact layout built for 7 or 8 blocks per SM (smaller tiles) and
+    passes at that block count: the oracle's survivors on two golden cases."""
+    for name in ("tilted_fcc", "beamnormal_fcc"):
+        c = golden_case(name)
+        p = c.params
+        ref = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                        p.min_nr_spots, p.min_intensity)
+        with engine_for(p) as e:
+            e.set_tuning(variant=2, consumers=3, stages=2, grid_mult=nb)
+            e.upload_db(c.records)
+            e.load_image(0, c.image)
+            e.match([0], p.min_nr_spots, p.min_intensity)
+            got, npass = e.results(0)
+            info = e.layout_info()
+        assert info["compact"] == 1 and info["tile_bytes"] % 128 == 0
+        assert npass == ref.n_pass
+        assert_same_survivors(got, ref)
+
+
 def test_compact_layout_batched_equals_reference_layout():
     """Twelve uneven frames in one pass: variant 2 == variant 1, slot by slot,
     on a 300k-orientation device-built DB, for several tile shapes."""
@@ -255,7 +276,10 @@ def test_compact_layout_batched_equals_reference_layout():
         ref = e.results_batch(range(12))
         for shape in ({}, {"consumers": 4}, {"consumers": 17, "stages": 2}, {"grid_mult": 3},
                       {"full_gather": 1}, {"consumers": 3, "stages": 2, "grid_mult": 6},
-                      {"consumers": 3, "stages": 2, "grid_mult": 6, "full_gather": 1}):
+                      {"consumers": 3, "stages": 2, "grid_mult": 6, "full_gather": 1},
+                      {"consumers": 3, "stages": 2, "grid_mult": 7},
+                      {"consumers": 3, "stages": 2, "grid_mult": 8},
+                      {"consumers": 3, "stages": 2, "grid_mult": 8, "full_gather": 1}):
             e.set_tuning(variant=2, **shape)
             e.match(range(12), p.min_nr_spots, p.min_intensity)
             got = e.results_batch(range(12))
