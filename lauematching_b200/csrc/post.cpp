@@ -1335,9 +1335,10 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
   // no result.
   struct Group {
     int g0 = 0, g1 = 0;
-    std::vector<int32_t> pg;
-    std::vector<double> px;
+    std::vector<int32_t> pg;  // host evaluation: grain of each point
+    std::vector<double> px;   // host evaluation: the points
     std::vector<int64_t> off;
+    int64_t m = 0;
     bool pending = false;
   };
   const int ngroups = ng >= kSplitGrains ? 2 : 1;
@@ -1348,24 +1349,69 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
     grp[b].off.assign(grp[b].g1 - grp[b].g0 + 1, 0);
   }
   const int nt = r->nthreads;
-  auto build = [&](Group &G) {  // the group's pending points, in grain order
+  // One round of group b in one parallel region: the optimiser steps on the
+  // values pf (none on the first round), the round's points in grain order,
+  // and (device) their matrices straight into the page-locked staging
+  // buffer; then the evaluation is queued (device) or done (host).
+  auto round = [&](int b, const double *pf) -> int {
+    Group &G = grp[b];
     const int cnt = G.g1 - G.g0;
+    const bool dev = r->device >= 0;
     int64_t tot = 0;
-    for (int g = G.g0; g < G.g1; g++) {
-      G.off[g - G.g0] = tot;
-      if (st[g].phase != 6) tot += st[g].npend;
+    int lrc = LMB_OK;
+    double *T = nullptr;
+    int32_t *gd = nullptr;
+#pragma omp parallel num_threads(nt) if (cnt >= 256)
+    {
+      if (pf) {
+#pragma omp for schedule(dynamic, 32)
+        for (int g = G.g0; g < G.g1; g++)
+          if (st[g].phase != 6) nm_consume(r, g, st[g], pf + G.off[g - G.g0], max_eval);
+      }
+#pragma omp master
+      {
+        for (int g = G.g0; g < G.g1; g++) {
+          G.off[g - G.g0] = tot;
+          if (st[g].phase != 6) tot += st[g].npend;
+        }
+        G.off[cnt] = tot;
+        if (tot > 0 && dev) {
+          lrc = lmb::refine_dev_stage(r->dev, b, tot, &T, &gd);
+        } else if (tot > 0) {
+          G.pg.resize((size_t)tot);
+          G.px.resize((size_t)tot * n);
+        }
+      }
+#pragma omp barrier
+      if (tot > 0 && lrc == LMB_OK) {
+#pragma omp for schedule(static)
+        for (int g = G.g0; g < G.g1; g++) {
+          if (st[g].phase == 6) continue;
+          const int64_t o = G.off[g - G.g0], k = G.off[g - G.g0 + 1] - o;
+          for (int64_t j = 0; j < k; j++) {
+            const double *x = st[g].pend + (size_t)j * n;
+            if (dev) {
+              double OM[3][3];
+              point_matrix(n, x, r->cr, r->recip, OM);
+              double *t = T + (size_t)(o + j) * 9;
+              for (int i = 0; i < 3; i++)
+                for (int c = 0; c < 3; c++) t[i * 3 + c] = OM[i][c];
+              gd[o + j] = g;
+            } else {
+              G.pg[(size_t)(o + j)] = g;
+              std::copy(x, x + n, G.px.begin() + (size_t)(o + j) * n);
+            }
+          }
+        }
+      }
     }
-    G.off[cnt] = tot;
-    G.pg.resize((size_t)tot);
-    G.px.resize((size_t)tot * n);
-#pragma omp parallel for num_threads(nt) schedule(static) if (cnt >= 256)
-    for (int g = G.g0; g < G.g1; g++) {
-      if (st[g].phase == 6) continue;
-      const int64_t o = G.off[g - G.g0], k = G.off[g - G.g0 + 1] - o;
-      for (int64_t j = 0; j < k; j++) G.pg[(size_t)(o + j)] = g;
-      std::copy(st[g].pend, st[g].pend + (size_t)k * n, G.px.begin() + (size_t)o * n);
-    }
-    return tot;
+    if (lrc) return lrc;
+    G.m = tot;
+    if (tot == 0) return LMB_OK;
+    lrc = dev ? lmb::refine_dev_submit(r->dev, b, r->max_spots)
+              : eval_submit(r, b, G.pg.data(), G.px.data(), tot);
+    G.pending = lrc == LMB_OK;
+    return lrc;
   };
   auto drain = [&]() {  // after an error: wait for what is still queued
     for (int b = 0; b < ngroups; b++)
@@ -1376,11 +1422,7 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
       }
   };
   int rc = LMB_OK;
-  for (int b = 0; b < ngroups && !rc; b++)
-    if (build(grp[b]) > 0) {
-      rc = eval_submit(r, b, grp[b].pg.data(), grp[b].px.data(), (int64_t)grp[b].pg.size());
-      grp[b].pending = rc == LMB_OK;
-    }
+  for (int b = 0; b < ngroups && !rc; b++) rc = round(b, nullptr);
   for (bool any = true; any && !rc;) {
     any = false;
     for (int b = 0; b < ngroups && !rc; b++) {
@@ -1392,16 +1434,10 @@ extern "C" int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval
       G.pending = false;
       rc = eval_collect(r, b, &pf, &ms);
       if (rc) break;
-      r->last_points += (int64_t)G.pg.size();
+      r->last_points += G.m;
       r->last_rounds++;
       r->last_kernel_ms += ms;
-#pragma omp parallel for num_threads(nt) schedule(dynamic, 32) if (G.g1 - G.g0 >= 256)
-      for (int g = G.g0; g < G.g1; g++)
-        if (st[g].phase != 6) nm_consume(r, g, st[g], pf + G.off[g - G.g0], max_eval);
-      if (build(G) > 0) {
-        rc = eval_submit(r, b, G.pg.data(), G.px.data(), (int64_t)G.pg.size());
-        G.pending = rc == LMB_OK;
-      }
+      rc = round(b, pf);
     }
   }
   if (rc) {
