@@ -249,7 +249,9 @@ typedef struct lmb_post_params {
   int32_t min_nr_spots;  /* MinNrSpots (CLI) or MinGoodSpots (daemon) */
   int32_t image_num;     /* > 0: prepend the ImageNr column (daemon format) */
   int32_t num_threads;   /* host threads */
-  int32_t optimizer;     /* 0 = evaluate once */
+  int32_t optimizer;     /* 0 = evaluate once (the reference built without NLopt);
+                            1 = this library's bounded Nelder-Mead, all grains at once
+                            (lmb_refine_fit, 200 evaluations; not NLopt's steps) */
   int32_t max_results;   /* candidates kept for the merge, top by score;
                             0 = the reference's cap MERGE_MAX_RESULTS 50000 */
   int32_t merge_on_device; /* k > 0: for 1024 or more candidates, the duplicate merge's

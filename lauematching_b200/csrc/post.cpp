@@ -47,6 +47,7 @@ constexpr double kRad2Deg = 57.2957795130823;    // :33
 constexpr double kEps = 1E-12;                    // :42
 constexpr double kHc = 1.2398419739;              // :41
 constexpr int kMergeMax = 50000;                  // :953
+constexpr int kFitMaxEval = 200;                  // nlopt_set_maxeval, :775
 
 // Symmetry quaternions (w, x, y, z) per crystal system, LaueMatchingHeaders.h:83-145.
 const double kTric[1][4] = {{1, 0, 0, 0}};
@@ -582,7 +583,7 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
                                 const double *scores, int64_t n_results, const float *image,
                                 const int32_t *hkls, int32_t nh, lmb_post_output *out) {
   if (!geo || !pp || !out || (!orients && n_orients) || (n_results > 0 && (!ids || !scores)) ||
-      !image || (!hkls && nh)) {
+      !image || (!hkls && nh) || (pp->optimizer != 0 && pp->optimizer != 1)) {
     lmb::set_error("null argument");
     return LMB_ERR_INVALID;
   }
@@ -637,6 +638,29 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
   const int nsol = (int)dcount.size();
 
   // ---- refine + write (:1072-1153) ---------------------------------------------
+  // optimizer 1: this library's bounded Nelder-Mead over all grains at once
+  // (lmb_refine_fit on host threads); optimizer 0 (below): evaluate once, as
+  // the reference built without NLopt does
+  std::vector<double> nm_x, nm_ov;
+  if (pp->optimizer == 1 && nsol > 0) {
+    lmb_refine *rf = nullptr;
+    int rc = lmb_refine_create(-1, geo, pp, hkls, nh, &rf);
+    std::vector<double> om((size_t)nsol * 9);
+    std::vector<int32_t> im((size_t)nsol, 0);
+    for (int it = 0; it < nsol; it++)
+      memcpy(&om[(size_t)it * 9], orients + (size_t)best_row[it] * 9, 9 * sizeof(double));
+    int32_t nd = 0;
+    if (!rc) rc = lmb_refine_set_images(rf, &image, 1);
+    if (!rc) rc = lmb_refine_set_grains(rf, om.data(), im.data(), nsol, nullptr);
+    if (!rc) rc = lmb_refine_dims(rf, &nd);
+    if (!rc) {
+      nm_x.resize((size_t)nsol * nd);
+      nm_ov.resize((size_t)nsol);
+      rc = lmb_refine_fit(rf, 1, kFitMaxEval, 0.0, nm_x.data(), nm_ov.data(), nullptr);
+    }
+    lmb_refine_destroy(rf);
+    if (rc) return rc;
+  }
   std::vector<GrainOut> go(nsol);
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic)
   for (int it = 0; it < nsol; it++) {
@@ -668,11 +692,16 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
         if (cr.tol_latc[i] != 0) x[c++] = cr.lat[i];
       if (cr.tol_c_over_a != 0) x[3] = cr.c_over_a_orig;
     }
-    (void)tol;  // bounds of the search box; unused by the evaluate-once optimiser
+    (void)tol;  // bounds of the search box (used by lmb_refine_set_grains)
     std::vector<double> acc((size_t)3 * max_spots, 0.0);
-    const double minf = objective(n, x.data(), cr, recip, d, image, hkls, valid.data(),
-                                  (int)valid.size(), max_spots, acc);
-    const double mv = -minf;
+    double mv;
+    if (pp->optimizer == 1) {
+      for (unsigned i = 0; i < n; i++) x[i] = nm_x[(size_t)it * n + i];
+      mv = nm_ov[it];
+    } else {
+      mv = -objective(n, x.data(), cr, recip, d, image, hkls, valid.data(), (int)valid.size(),
+                      max_spots, acc);
+    }
     for (int i = 0; i < 3; i++) ef[i] = x[i];
     double latf[6];
     {

@@ -42,7 +42,10 @@ def make_post_params(params: LaueParams, min_nr_spots: int | None = None,
     pp.max_angle = float(params.max_angle)
     pp.min_nr_spots = int(params.min_nr_spots if min_nr_spots is None else min_nr_spots)
     pp.num_threads = int(num_threads or os.cpu_count() or 1)
-    pp.optimizer = 0
+    # "Optimizer NelderMead" in the parameter file: this library's bounded
+    # Nelder-Mead (NLopt is not available); BOBYQA, the reference's default,
+    # needs NLopt and is run as the evaluate-once stand-in
+    pp.optimizer = 1 if params.optimizer == "NelderMead" else 0
     return pp
 
 
@@ -50,7 +53,7 @@ def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndar
                  scores: np.ndarray, image_f32: np.ndarray, hkls: np.ndarray,
                  min_nr_spots: int | None = None, image_num: int = 0,
                  num_threads: int | None = None, max_results: int = 0,
-                 merge_device: int | None = None):
+                 merge_device: int | None = None, optimizer: str | None = None):
     """Return (solutions_text, spots_text, n_unique) for one image.
 
     ``ids``/``scores`` are the image's collected matches in the reference's
@@ -58,8 +61,12 @@ def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndar
     only that many top-scored candidates for the merge (the reference's own
     cap path, LaueMatchingHeaders.h:976-997, with its cap of 50000 lowered).
     ``merge_device`` (a CUDA device index) runs the duplicate merge of 1024 or
-    more candidates on that device (same clusters); None keeps it on the host."""
+    more candidates on that device (same clusters); None keeps it on the host.
+    ``optimizer`` ("once" or "nelder-mead") overrides the parameter file's
+    Optimizer (NelderMead: this library's Nelder-Mead; otherwise once)."""
     pp = make_post_params(params, min_nr_spots, num_threads)
+    if optimizer is not None:
+        pp.optimizer = {"once": 0, "nelder-mead": 1}[optimizer]
     pp.image_num = int(image_num)
     pp.max_results = int(max_results)  # 0: the reference's 50000
     pp.merge_on_device = 0 if merge_device is None else int(merge_device) + 1

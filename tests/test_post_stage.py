@@ -65,3 +65,42 @@ def test_merge_alone_gives_the_reference_unique_count(name):
     rows, scores, counts = post.merge_clusters(p.space_group, p.max_angle, c.orients, ids, sc)
     assert rows.shape[0] == c.meta["cmp_unique"]
     assert int(counts.sum()) == len(ids)
+
+
+def test_post_stage_nelder_mead_refines_the_grains():
+    """optimizer 1 (the parameter file's "Optimizer NelderMead"): this library's
+    Nelder-Mead moves the grains off their coarse orientations and never
+    lowers NMatches*sqrt(Intensity); the same clusters; deterministic."""
+    import copy
+    c = golden_case("tilted_dense")
+    p = copy.deepcopy(c.params)
+    s = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                  p.min_nr_spots, p.min_intensity)
+    surv = np.zeros(len(s.ids), [("id", "<u8"), ("score", "<f8")])
+    surv["id"] = s.ids
+    surv["score"] = s.score
+    ids, sc = post.collected_matches(surv, s.n_pass)
+    geo = geometry_from_params(p)
+    img = c.image.astype(np.float32)
+    sol0, _, nu0 = post.post_process(p, geo, c.orients, ids, sc, img, c.hkls, num_threads=4)
+    sol1, spt1, nu1 = post.post_process(p, geo, c.orients, ids, sc, img, c.hkls, num_threads=4,
+                                        optimizer="nelder-mead")
+    p.optimizer = "NelderMead"
+    sol2, spt2, nu2 = post.post_process(p, geo, c.orients, ids, sc, img, c.hkls, num_threads=2)
+    assert (sol2, spt2, nu2) == (sol1, spt1, nu1)
+    assert nu0 == nu1
+
+    def rows(txt):
+        return {int(f[0]): [float(v) for v in f[2:]]
+                for f in (ln.split() for ln in txt.splitlines() if ln.strip())}
+    r0, r1 = rows(sol0), rows(sol1)
+    common = sorted(set(r0) & set(r1))
+    assert len(common) >= 0.8 * len(r0)
+    # columns after GrainNr, NumberOfSolutions: Intensity, NMatches*Intensity,
+    # NMatches*sqrt(Intensity), ...; misorientation is the second to last
+    moved = improved = 0
+    for g in common:
+        assert r1[g][2] >= r0[g][2] - 1e-9 * abs(r0[g][2])
+        improved += r1[g][2] > r0[g][2]
+        moved += r1[g][-2] > 0
+    assert improved > 0 and moved >= improved
