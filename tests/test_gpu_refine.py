@@ -91,3 +91,36 @@ def test_device_objective_many_points_and_spot_cap():
         pts = lo[grains] + rng.random((m, d.dims)) * (hi[grains] - lo[grains])
         assert np.array_equal(d.evaluate(grains, pts), h.evaluate(grains, pts))
         assert d.evaluate([], np.zeros((0, d.dims))).shape == (0,)
+
+
+def test_device_fit_reproduces_the_post_stage_nelder_mead_text():
+    """The post-stage with "Optimizer NelderMead" fits on host threads; the same
+    grains fitted on the device give the same overlaps, printed as the
+    post-stage prints them (NMatches*sqrt(Intensity), %-13.4lf)."""
+    import copy
+
+    import oracle as O
+    from conftest import golden_case
+    from lauematching_b200 import post
+
+    c = golden_case("tilted_dense")
+    p = copy.deepcopy(c.params)
+    s = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                  p.min_nr_spots, p.min_intensity)
+    surv = np.zeros(len(s.ids), [("id", "<u8"), ("score", "<f8")])
+    surv["id"] = s.ids
+    surv["score"] = s.score
+    ids, sc = post.collected_matches(surv, s.n_pass)
+    geo = geometry_from_params(p)
+    img = c.image.astype(np.float32)
+    sol, _, _ = post.post_process(p, geo, c.orients, ids, sc, img, c.hkls, num_threads=8,
+                                  optimizer="nelder-mead")
+    rows, _, _ = post.merge_clusters(p.space_group, p.max_angle, c.orients, ids, sc)
+    with Refiner(p, geo, c.hkls, device=0) as r:
+        r.set_images([img.reshape(p.nr_px_y, p.nr_px_x)])
+        r.set_grains(c.orients[rows.astype(np.int64)], 0)
+        _, ov, _ = r.fit("nelder-mead", 200)
+    printed = {int(f[0]): f[4] for f in (ln.split() for ln in sol.splitlines() if ln.strip())}
+    assert len(printed) > 100
+    for g, txt in printed.items():
+        assert txt == "%.4f" % ov[g - 1]
