@@ -104,3 +104,21 @@ def test_post_stage_nelder_mead_refines_the_grains():
         improved += r1[g][2] > r0[g][2]
         moved += r1[g][-2] > 0
     assert improved > 0 and moved >= improved
+
+
+def test_post_stage_rejects_unknown_optimizer():
+    import ctypes as C
+    from lauematching_b200 import _lib
+    c = golden_case("tilted_fcc")
+    p = c.params
+    pp = post.make_post_params(p)
+    pp.optimizer = 2
+    geo = geometry_from_params(p)
+    img = c.image.astype(np.float32)
+    hk = np.ascontiguousarray(c.hkls, np.int32)
+    om = np.ascontiguousarray(c.orients, np.float64)
+    out = _lib.LmbPostOutput()
+    rc = _lib.lib().lmb_post_process(C.byref(geo), C.byref(pp), om.ctypes.data, om.shape[0],
+                                     None, None, 0, img.ctypes.data, hk.ctypes.data,
+                                     hk.shape[0], C.byref(out))
+    assert rc == _lib.LMB_ERR_INVALID
