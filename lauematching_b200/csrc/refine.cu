@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(128) prefilter_kernel(const double *__restrict
 // calcOverlapFiltered + problem_function's sign: obj[k] = -(nrPos * sqrt(sum))
 // for point k (matrix T[k], grain grain[k]).  acc: per warp, the directions
 // of the spots kept so far (max_spots x 3 doubles, outArrThis).
-__global__ void __launch_bounds__(128) objective_kernel(
+__global__ void __launch_bounds__(128, 7) objective_kernel(
     const double *__restrict__ T, const int32_t *__restrict__ grain, int64_t m,
     const int4 *__restrict__ hkl, int nh, const int32_t *__restrict__ valid,
     const int32_t *__restrict__ nvalid, const int32_t *__restrict__ gimg,
