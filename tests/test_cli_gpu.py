@@ -60,3 +60,30 @@ def test_cli_usage_and_fatal_errors(tmp_path):
     r = subprocess.run([sys.executable, EXE, str(tmp_path / "nope.txt"), "o", "h", "i", "1"],
                        capture_output=True, text=True)
     assert r.returncode == 1 and "Could not open parameter file" in r.stdout
+
+
+def test_cli_nelder_mead_writes_the_refined_solutions(tmp_path):
+    """"Optimizer NelderMead" in the parameter file: the CLI's solutions.txt is
+    the post-stage's Nelder-Mead text for the oracle's survivors (not the
+    evaluate-once text of the reference built without NLopt)."""
+    import oracle as O
+    from lauematching_b200 import post
+    from lauematching_b200.engine import geometry_from_params
+    c = golden_case("tilted_dense")
+    pp, op, hp, ip, fwd = _case_files(c, tmp_path, 0)
+    with open(pp, "a") as f:
+        f.write("Optimizer NelderMead\n")
+    r = subprocess.run([sys.executable, EXE, pp, op, hp, ip, "4"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    p = c.params
+    s = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                  p.min_nr_spots, p.min_intensity)
+    surv = np.zeros(len(s.ids), [("id", "<u8"), ("score", "<f8")])
+    surv["id"] = s.ids
+    surv["score"] = s.score
+    ids, sc = post.collected_matches(surv, s.n_pass)
+    sol, _, _ = post.post_process(p, geometry_from_params(p), c.orients, ids, sc,
+                                  c.image.astype(np.float32), c.hkls, optimizer="nelder-mead")
+    got = open(ip + ".solutions.txt").read()
+    assert got == post.SOLUTIONS_HEADER + sol
+    assert got != c.cmp_solutions
