@@ -256,7 +256,9 @@ typedef struct lmb_post_params {
                             0 = the reference's cap MERGE_MAX_RESULTS 50000 */
   int32_t merge_on_device; /* k > 0: for 1024 or more candidates, the duplicate merge's
                               pair matrix and greedy pass run on CUDA device k-1 (same
-                              clusters; at most 200000 candidates); 0: on the host */
+                              clusters; at most 200000 candidates), and with optimizer 1
+                              and 2048 or more grains the refinement's evaluations too
+                              (same fits); 0: all on the host */
 } lmb_post_params;
 
 typedef struct lmb_post_output {

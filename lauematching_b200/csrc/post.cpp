@@ -48,6 +48,9 @@ constexpr double kEps = 1E-12;                    // :42
 constexpr double kHc = 1.2398419739;              // :41
 constexpr int kMergeMax = 50000;                  // :953
 constexpr int kFitMaxEval = 200;                  // nlopt_set_maxeval, :775
+// From this many grains on, a post-stage with a device refines on it (fewer:
+// host threads are as fast, the per-round launch latency dominates).
+constexpr int kDeviceRefineMin = 2048;
 
 // Symmetry quaternions (w, x, y, z) per crystal system, LaueMatchingHeaders.h:83-145.
 const double kTric[1][4] = {{1, 0, 0, 0}};
@@ -639,12 +642,17 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
 
   // ---- refine + write (:1072-1153) ---------------------------------------------
   // optimizer 1: this library's bounded Nelder-Mead over all grains at once
-  // (lmb_refine_fit on host threads); optimizer 0 (below): evaluate once, as
-  // the reference built without NLopt does
+  // (lmb_refine_fit; its evaluations on the merge's device when there is one
+  // and the grains are many, on host threads otherwise; the same fits either
+  // way); optimizer 0 (below): evaluate once, as the reference built without
+  // NLopt does
   std::vector<double> nm_x, nm_ov;
   if (pp->optimizer == 1 && nsol > 0) {
     lmb_refine *rf = nullptr;
-    int rc = lmb_refine_create(-1, geo, pp, hkls, nh, &rf);
+    const int rdev = (pp->merge_on_device > 0 && nsol >= kDeviceRefineMin)
+                         ? pp->merge_on_device - 1
+                         : -1;
+    int rc = lmb_refine_create(rdev, geo, pp, hkls, nh, &rf);
     std::vector<double> om((size_t)nsol * 9);
     std::vector<int32_t> im((size_t)nsol, 0);
     for (int it = 0; it < nsol; it++)

@@ -124,3 +124,20 @@ def test_device_fit_reproduces_the_post_stage_nelder_mead_text():
     assert len(printed) > 100
     for g, txt in printed.items():
         assert txt == "%.4f" % ov[g - 1]
+
+
+def test_post_stage_refines_many_grains_on_the_device_with_the_host_text():
+    """2200 grains on one frame, "Optimizer NelderMead", merge device given:
+    the post-stage refines on the device (2048 or more grains) and writes the
+    same solutions and spots text as on host threads."""
+    from lauematching_b200 import post
+    c, p, geo, frames, image, om_true, om_c = synthetic_scene(n_frames=1, per_frame=2200)
+    ids = np.arange(om_c.shape[0], dtype=np.uint64)
+    sc = np.linspace(100.0, 500.0, om_c.shape[0])
+    img = frames[0].ravel()
+    host = post.post_process(p, geo, om_c, ids, sc, img, c.hkls, num_threads=8,
+                             optimizer="nelder-mead")
+    dev = post.post_process(p, geo, om_c, ids, sc, img, c.hkls, num_threads=8,
+                            optimizer="nelder-mead", merge_device=0)
+    assert host[2] >= 2048
+    assert dev == host
