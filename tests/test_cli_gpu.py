@@ -87,3 +87,41 @@ def test_cli_nelder_mead_writes_the_refined_solutions(tmp_path):
     got = open(ip + ".solutions.txt").read()
     assert got == post.SOLUTIONS_HEADER + sol
     assert got != c.cmp_solutions
+
+
+def test_reference_indexer_invocation_writes_reference_files(tmp_path):
+    """The invocation the reference's laue_index.indexer.run_indexer makes for
+    compute_type="GPU" (recorded from the reference's module in
+    tests/golden/indexer_invocation.json: the selected executable, argv,
+    LD_LIBRARY_PATH, the caller's working directory, stdout/stderr into
+    <output_path>.LaueMatching_std{out,err}.txt), replayed against this
+    repository on a golden case: exit 0 (the reference's success), and
+    solutions/spots byte-equal to the reference binary's files."""
+    import json
+    with open(os.path.join(ROOT, "tests", "golden", "indexer_invocation.json")) as f:
+        fx = json.load(f)
+    sel = {(r["compute_type"], r["do_forward"]): r["executable"] for r in fx["resolve"]}
+    run = [r for r in fx["gpu_runs"] if r["exit_code"] == 0][0]
+    c = golden_case("tilted_fcc")
+    pp, op, hp, ip, _ = _case_files(c, tmp_path, 0)
+    call = run["call"]
+    actual = {call["config_file"]: pp, call["orient_db_file"]: op, call["hkl_file"]: hp,
+              call["image_bin"]: ip, str(call["ncpus"]): "4"}
+    exe = os.path.join(ROOT, sel[("GPU", False)])
+    env = dict(os.environ)
+    env["LD_LIBRARY_PATH"] = ":".join(
+        os.path.join(ROOT, p) if p and not p.startswith("/") else env.get("LD_LIBRARY_PATH", "")
+        for p in run["ld_library_path"])
+    work = tmp_path / "work"
+    work.mkdir()
+    r = subprocess.run([exe] + [actual[a] for a in run["argv"]], env=env, cwd=str(work),
+                       capture_output=True, text=True)
+    outp = str(tmp_path / "image.bin")
+    with open(outp + run["result"]["stdout_log"], "w") as f:
+        f.write(r.stdout)
+    with open(outp + run["result"]["stderr_log"], "w") as f:
+        f.write(r.stderr)
+    assert r.returncode == 0, r.stdout + r.stderr  # run_indexer's success
+    assert f"Initial solutions: {c.meta['cmp_initial']} " in r.stdout
+    assert open(ip + ".solutions.txt").read() == c.cmp_solutions
+    assert open(ip + ".spots.txt").read() == c.cmp_spots
