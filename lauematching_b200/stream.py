@@ -121,7 +121,8 @@ class StreamServer:
 
     def __init__(self, params_list, orients, hkls, ncpus=1, max_batch=64, device=0,
                  result_dir=None, port=PORT, ext_port=EXT_PORT, host="0.0.0.0",
-                 log=print, max_queue=MAX_QUEUE, engines=None, preprocess_cfgs=None):
+                 log=print, max_queue=MAX_QUEUE, engines=None, preprocess_cfgs=None,
+                 free_bytes=None):
         from . import _lib, formats
         from .engine import Engine
         self.log = log
@@ -162,9 +163,10 @@ class StreamServer:
                         log(f"Could not write the forward simulation to {fwd}: {exc}")
             self.geoms[key] = Geometry(p, e, pre_cfg=pcfg)
         # admission: slots per geometry within the free HBM after the DBs
-        info = _lib.device_info(device)
+        # (free_bytes: the caller's figure, for engines it manages itself)
+        free = _lib.device_info(device)["free"] if free_bytes is None else int(free_bytes)
         per_slot = max(int(k[0]) * int(k[1]) * 5 for k in self.geoms)  # u8 frame + wire staging
-        budget = max(1, int(0.5 * info["free"] // per_slot))
+        budget = max(1, int(0.5 * free // per_slot))
         self.max_batch = int(min(max_batch, 64, budget))
         for g in self.geoms.values():
             g.free = list(range(self.max_batch))[::-1]
@@ -495,6 +497,14 @@ def main(argv=None) -> int:
     srv = StreamServer(plist, orients, hkls, ncpus=int(ncpu_s), max_batch=opts.max_batch,
                        device=opts.device, port=opts.port, ext_port=opts.ext_port,
                        log=lambda *a: print(*a, flush=True), preprocess_cfgs=pcfgs)
+    return serve_until_signalled(srv)
+
+
+def serve_until_signalled(srv) -> int:
+    """Run the daemon until SIGINT or SIGTERM (LaueMatchingGPUStream.cu:542-551):
+    the first signal stops accepting and drains -- every image already
+    received is matched and written -- then returns 0 (:1288); a second
+    signal exits at once with status 1."""
     stop = threading.Event()
 
     def on_signal(signum, frame):
@@ -505,7 +515,7 @@ def main(argv=None) -> int:
     signal.signal(signal.SIGINT, on_signal)
     signal.signal(signal.SIGTERM, on_signal)
     srv.start()
-    print(f"Listening on port {opts.port} (extended header on {opts.ext_port}); "
+    print(f"Listening on port {srv.port} (extended header on {srv.ext_port}); "
           f"up to {srv.max_batch} images per DB pass", flush=True)
     while not stop.wait(0.5):
         pass
