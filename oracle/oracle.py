@@ -18,6 +18,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import re
+import shutil
 import subprocess
 import tempfile
 import time
@@ -29,6 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblmoracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "LaueMatchingCPU")
 REF_GPU_BIN = os.path.join(HERE, "_ref", "LaueMatchingGPU")
+REF_STREAM_BIN = os.path.join(HERE, "_ref", "LaueMatchingGPUStream")
 
 _lib = None
 
@@ -201,6 +203,65 @@ def run_reference_gpu(params_path, orient_path, hkl_path, image_path, ncpus=1,
                      grab(r"Time elapsed to match on the GPU: " + num),
                      grab(r"Finished comparing, time elapsed after comparing with forward "
                           r"simulation: " + num), wall)
+
+
+def have_ref_stream() -> bool:
+    return os.path.exists(REF_STREAM_BIN)
+
+
+class RefStream:
+    """The reference's LaueMatchingGPUStream daemon (sm_100a build) run through
+    its own command line (LaueMatchingGPUStream.cu:536-540) in ``cwd``.  A
+    reader thread time-stamps (time.monotonic) each image's last report line
+    -- "[Image N] No matches, skipping fitting." or "[Image N] Total: ..."
+    (finalize_stream, :452-533) -- so a client can measure per-image
+    latency and throughput from outside.  stdout is line-buffered through
+    stdbuf so a line appears when the daemon prints it."""
+
+    READY = "LaueMatchingGPUStream ready"
+
+    def __init__(self, params_path, orient_path, hkl_path, ncpus, cwd, env=None):
+        import threading
+        cmd = [REF_STREAM_BIN, params_path, orient_path, hkl_path, str(ncpus)]
+        if shutil.which("stdbuf"):
+            cmd = ["stdbuf", "-oL", "-eL"] + cmd
+        self.proc = subprocess.Popen(cmd, cwd=cwd, stdout=subprocess.PIPE,
+                                     stderr=subprocess.STDOUT, text=True, env=env)
+        self.done = {}          # image number -> monotonic time of its last line
+        self.lines = []
+        self.ready = threading.Event()
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        pat = re.compile(r"^\[Image (\d+)\] (No matches|Total:)")
+        for line in self.proc.stdout:
+            t = time.monotonic()
+            if len(self.lines) < 20000:
+                self.lines.append(line)
+            if self.READY in line:
+                self.ready.set()
+            m = pat.match(line)
+            if m:
+                self.done[int(m.group(1))] = t
+        self.ready.set()
+
+    def wait_ready(self, timeout=900.0) -> bool:
+        self.ready.wait(timeout)
+        return self.proc.poll() is None and any(self.READY in ln for ln in self.lines)
+
+    def stop(self, timeout=120.0) -> int:
+        """SIGINT: the daemon drains its streams and exits (:542-551, :1288)."""
+        import signal
+        if self.proc.poll() is None:
+            self.proc.send_signal(signal.SIGINT)
+        try:
+            self.proc.wait(timeout)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            self.proc.wait()
+        self._t.join(5)
+        return self.proc.returncode
 
 
 def reference_case(workdir, params_text, orients, hkls, image, ncpus=1):

@@ -77,8 +77,9 @@ def make_frame(ny, nx, seed, kw, bg_kind):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LAUE_REFERENCE_ROOT",
-                                                                      "/root/reference")
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LAUE_REFERENCE_ROOT")
+    if not ref_root:
+        sys.exit("give the reference tree as the argument or in LAUE_REFERENCE_ROOT")
     sys.path.insert(0, ref_root)
     from laue_index import preprocess as RP
     for name, (ny, nx, seed, kw, over, bg_kind, ovt) in CASES.items():
