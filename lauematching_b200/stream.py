@@ -96,6 +96,35 @@ class Geometry:
     pool: object = None   # PreprocessPool, made on the first raw frame
 
 
+class FramePool:
+    """Receive buffers reused across messages, per (pixel count, dtype): a
+    fresh 16 MiB array per frame costs its page faults on every message.  A
+    buffer goes back to the pool when its image is finished (or dropped);
+    arrays the pool did not make are ignored on return."""
+
+    def __init__(self):
+        self._lock = threading.Lock()
+        self._free: dict = collections.defaultdict(list)
+        self._mine: set = set()
+
+    def get(self, n, dtype):
+        k = (int(n), np.dtype(dtype).str)
+        with self._lock:
+            if self._free[k]:
+                return self._free[k].pop()
+        a = np.empty(int(n), dtype)
+        with self._lock:
+            self._mine.add(id(a))
+        return a
+
+    def put(self, a):
+        if a is None:
+            return
+        with self._lock:
+            if id(a) in self._mine:
+                self._free[(a.size, a.dtype.str)].append(a)
+
+
 def _recv_exact(sock, buf, running):
     view = memoryview(buf)
     got = 0
@@ -171,11 +200,13 @@ class StreamServer:
         for g in self.geoms.values():
             g.free = list(range(self.max_batch))[::-1]
         self.queue: queue.Queue = queue.Queue(maxsize=max_queue)
+        self.frames = FramePool()
         self._backlog = collections.deque()
         self.done_q: queue.Queue = queue.Queue()
         self.running = False
         self.latencies_ms: list = []
         self.gpu_latencies_ms: list = []
+        self.done_at: dict = {}  # image number -> time.monotonic() its lines were written
         self.passes = 0
         self.images_done = 0
         self.batch_sizes: list = []
@@ -241,21 +272,27 @@ class StreamServer:
                     num = int.from_bytes(hb, sys.byteorder)  # host-endian, as memcpy
                     key, dtype = (W, H), np.float32
                     w, h = W, H
-                payload = np.empty(w * h, dtype)
+                payload = self.frames.get(w * h, dtype)
                 if not _recv_exact(c, payload.view(np.uint8), run):
+                    self.frames.put(payload)
                     break
                 t = time.perf_counter()
                 if key not in self.geoms:
                     self.log(f"image {num}: no DB for a {w}x{h} detector; dropped")
+                    self.frames.put(payload)
                     continue
                 # blocks while MAX_QUEUE images wait (back-pressure, as queue_push)
+                queued = False
                 while self.running:
                     try:
                         self.queue.put(Request(num, key, payload, t, raw=dtype == np.uint16),
                                        timeout=0.5)
+                        queued = True
                         break
                     except queue.Full:
                         continue
+                if not queued:
+                    self.frames.put(payload)
         finally:
             c.close()
 
@@ -360,6 +397,7 @@ class StreamServer:
                 g.free.append(s)
                 self.done_q.put(Done(r, np.zeros(0, _SURV_DTYPE), 0, t))
                 continue
+            self.frames.put(r.pixels)  # the raw frame; the blurred one replaces it
             r.pixels = out[1].ravel()
             loaded.append((s, r))
         return loaded
@@ -391,7 +429,9 @@ class StreamServer:
                     self.spt_f.write(spt)
                     self.sol_f.flush()
                     self.spt_f.flush()
+                self.frames.put(d.req.pixels)
                 t = time.perf_counter()
+                self.done_at[d.req.image_num] = time.monotonic()
                 self.latencies_ms.append((t - d.req.t_arrival) * 1e3)
                 self.gpu_latencies_ms.append((d.t_gpu_done - d.req.t_arrival) * 1e3)
                 self.images_done += 1
