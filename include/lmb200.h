@@ -101,18 +101,27 @@ int lmb_engine_destroy(lmb_engine *e);
 void *lmb_engine_stream(lmb_engine *e);
 
 /* Launch shape of the compare pass: fields = {variant (0 block-barrier ring,
- * 1 warp-specialised, 2 warp-specialised over the compact layout, 3 automatic:
- * variant 2 while the records that can pass hold at most ~3 spots per DB
- * record on average, variant 1 beyond -- the default),
- * tile_sub (32-orientation sub-tiles per tile), stages, consumer warps,
- * blocks per SM, grid multiplier, full_gather}; 0 = default.  full_gather = 1
+ * 1 warp-specialised, 2 warp-specialised over the compact layout, 3 automatic
+ * -- the default: variant 2 while the records that can pass hold at most ~3
+ * spots per DB record on average, variant 4 beyond, variant 1 when the
+ * compact layout cannot be built --, 4 the compact layout filtered by the
+ * cell mask of the pass's frames), tile_sub (32-orientation sub-tiles per
+ * tile), stages, consumer warps, blocks per SM, grid multiplier,
+ * full_gather, test_consumer_wait_us, cell_consumers, cell_stages}; 0 =
+ * default.  cell_consumers and cell_stages shape variant 4 when the
+ * automatic variant picks it (the autotuner's dense-DB entry).  full_gather = 1
  * gathers every spot even of records with fewer spots than MinNrSpots (which
  * cannot pass; by default they are skipped; results are identical either
- * way), for measuring the full gather cost.  Written by the autotuner;
- * get returns the shape actually used for this DB.  No reference counterpart
+ * way), for measuring the full gather cost.  test_consumer_wait_us (tests
+ * only, compact-layout variants) makes the pass's consumer warps wait that
+ * long on a barrier nothing arrives at, so the pass gives up and its results
+ * report LMB_ERR_TIMEOUT; the engine's device error word is sticky, so that
+ * engine reports the timeout from then on.  Written by the autotuner; get
+ * returns the shape actually used for this DB.  No reference counterpart
  * (the reference launches <<<ceil(n/1024),1024>>>, LaueMatchingGPU.cu:739-743). */
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields);
-/* get: the same 7 fields, and an 8th: the variant the latest pass ran. */
+/* get: fields 0-6 as set, 7: the variant the latest pass ran, 8: the test
+ * wait, 9-10: the cell-mask pass's shape for the automatic variant. */
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields);
 
 /* The compact device layout variant 2 streams: derived from the resident
@@ -169,6 +178,20 @@ int lmb_db_build_synthetic(lmb_engine *e, uint64_t seed, uint64_t n,
  * above (n*9 doubles to out), bitwise the ones lmb_db_build_synthetic used. */
 int lmb_synth_orientations(lmb_engine *e, uint64_t seed, uint64_t first,
                            uint64_t n, double *out);
+
+/* Synthetic builds with flags: LMB_BUILD_EXACT_FP64 as for lmb_db_build_ex;
+ * LMB_BUILD_SYNTH_HEX_FZ reduces every generated rotation to the hexagonal
+ * (622) fundamental zone -- of its 12 equivalents under the operators of
+ * LaueMatchingHeaders.h:111-122 the one with the largest |scalar part|, the
+ * reference's own merge criterion -- since the reference never generates
+ * zone-restricted DBs (scripts/GenerateOrientations.py:5-9).
+ * lmb_synth_orientations_ex gives the same matrices for the same flags. */
+#define LMB_BUILD_SYNTH_HEX_FZ 2
+int lmb_db_build_synthetic_ex(lmb_engine *e, uint64_t seed, uint64_t n,
+                              const int32_t *hkls, int32_t nh, double *orients_out,
+                              uint32_t flags);
+int lmb_synth_orientations_ex(lmb_engine *e, uint64_t seed, uint64_t first,
+                              uint64_t n, double *out, uint32_t flags);
 
 /* Copy records [first, first+count) of the resident DB to the host (to write
  * the ForwardFile, LaueMatchingCPU.c:694-711). */
@@ -335,22 +358,34 @@ int lmb_refine_fit(lmb_refine *r, int32_t optimizer, int32_t max_eval, double in
 /* Of the last evaluate / fit call: points evaluated, rounds (launches on a
  * device), summed device time of the objective kernel (0 on the host). */
 int lmb_refine_last_stats(lmb_refine *r, int64_t *points, int32_t *rounds, float *kernel_ms);
+/* What the calling thread's last lmb_post_process refined (optimizer 1):
+ * device -2 = no refinement, -1 = host threads, else the device ordinal;
+ * points, rounds and objective-kernel time as lmb_refine_last_stats gives
+ * them.  The post-stage keeps its refinement handles between calls (no
+ * allocation per image once a handle exists for that device, geometry,
+ * parameters and HKL list). */
+int lmb_post_last_refine_stats(int32_t *device, int64_t *points, int32_t *rounds,
+                               float *kernel_ms);
 
 /* ---- survivor ordering that allocates nothing ------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory themselves (code running inside another framework's memory pool, or
  * on a thread that must not take cudaMalloc's implicit device
  * synchronisation) but hold device buffers: sorts d_in[0..n) (unsorted
- * survivors, ids < 2^40) by orientation id into d_out (no aliasing), with the
- * same order as lmb_results delivers, on `stream` (a cudaStream_t; NULL =
- * legacy default stream).  Makes no cudaMalloc/cudaFree call: lists above 8192
+ * survivors) by orientation id, ties by position, into d_out (the two ranges
+ * must not overlap), with the same order as lmb_results delivers, on
+ * `stream` (a cudaStream_t; NULL = legacy default stream).  Ids of 2^40 and
+ * above are ordered too (by a slower comparison that reads the ids from
+ * d_in).  Makes no cudaMalloc/cudaFree call: lists above 8192
  * entries use a fixed 8 MiB device array inside the library as key scratch,
  * which every GPU that loads the library holds until the process exits.
  * n above LMB_NOALLOC_ORDER_MAX is rejected with LMB_ERR_INVALID.  The first
  * call on a device resolves that array's address (cudaGetSymbolAddress) and
  * sets the kernel's shared-memory limit; make it before any stream capture.
- * All calls share the one scratch array, so calls that overlap on the GPU
- * (other streams, other threads) race: serialise them. */
+ * That set-up is kept for the life of the process: a cudaDeviceReset of the
+ * device afterwards is not supported (later calls would launch with the
+ * stale address).  All calls share the one scratch array, so calls that
+ * overlap on the GPU (other streams, other threads) race: serialise them. */
 #define LMB_NOALLOC_ORDER_MAX (1u << 20)
 int lmb_order_survivors_noalloc(const lmb_survivor *d_in, uint64_t n,
                                 lmb_survivor *d_out, void *stream);

@@ -24,6 +24,7 @@ LMB_THR_ADAPTIVE, LMB_THR_PERCENTILE, LMB_THR_FIXED = 0, 1, 2
 LMB_PRE_STAGES = 8
 LMB_VALUE_U8, LMB_VALUE_F64 = 0, 1
 LMB_BUILD_EXACT_FP64 = 1
+LMB_BUILD_SYNTH_HEX_FZ = 2
 LMB_NOALLOC_ORDER_MAX = 1 << 20
 
 # Every function the header declares (checked by the CPU test suite).
@@ -33,7 +34,8 @@ EXPORTS = [
     "lmb_engine_get_tuning", "lmb_engine_layout_info", "lmb_engine_set_sparse_uploads",
     "lmb_engine_set_dense_share",
     "lmb_db_upload", "lmb_db_build",
-    "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations", "lmb_db_download", "lmb_db_info", "lmb_image_load",
+    "lmb_db_build_ex", "lmb_db_build_synthetic", "lmb_synth_orientations",
+    "lmb_db_build_synthetic_ex", "lmb_synth_orientations_ex", "lmb_db_download", "lmb_db_info", "lmb_image_load",
     "lmb_image_load_batch",
     "lmb_match", "lmb_results", "lmb_results_batch", "lmb_last_pass_ms", "lmb_engine_bytes",
     "lmb_post_process", "lmb_post_free", "lmb_merge_clusters",
@@ -45,7 +47,7 @@ EXPORTS = [
     "lmb_pre_blur_to_slot",
     "lmb_refine_create", "lmb_refine_destroy", "lmb_refine_dims", "lmb_refine_set_images",
     "lmb_refine_set_grains", "lmb_refine_start", "lmb_refine_evaluate", "lmb_refine_fit",
-    "lmb_refine_last_stats",
+    "lmb_refine_last_stats", "lmb_post_last_refine_stats",
 ]
 
 
@@ -98,6 +100,10 @@ class OverflowError_(LmbError):
     pass
 
 
+class TimeoutError_(LmbError):
+    """A bounded device wait gave up (LMB_ERR_TIMEOUT)."""
+
+
 _lib = None
 
 
@@ -134,6 +140,8 @@ def lib():
         "lmb_db_build_ex": ([vp, vp, u64, vp, i32, C.c_uint32], C.c_int),
         "lmb_db_build_synthetic": ([vp, u64, u64, vp, i32, vp], C.c_int),
         "lmb_synth_orientations": ([vp, u64, u64, u64, vp], C.c_int),
+        "lmb_db_build_synthetic_ex": ([vp, u64, u64, vp, i32, vp, C.c_uint32], C.c_int),
+        "lmb_synth_orientations_ex": ([vp, u64, u64, u64, vp, C.c_uint32], C.c_int),
         "lmb_db_download": ([vp, u64, u64, vp], C.c_int),
         "lmb_db_info": ([vp, C.POINTER(u64), C.POINTER(i32)], C.c_int),
         "lmb_image_load": ([vp, i32, vp, i32, i32, dp], C.c_int),
@@ -176,6 +184,8 @@ def lib():
         "lmb_refine_fit": ([vp, i32, i32, dbl, vp, vp, vp], C.c_int),
         "lmb_refine_last_stats": ([vp, C.POINTER(C.c_int64), C.POINTER(i32),
                                    C.POINTER(C.c_float)], C.c_int),
+        "lmb_post_last_refine_stats": ([C.POINTER(i32), C.POINTER(C.c_int64), C.POINTER(i32),
+                                        C.POINTER(C.c_float)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -197,5 +207,7 @@ def check(rc: int) -> int:
         msg = lib().lmb_last_error().decode(errors="replace")
         if rc == LMB_ERR_OVERFLOW:
             raise OverflowError_(rc, msg)
+        if rc == LMB_ERR_TIMEOUT:
+            raise TimeoutError_(rc, msg)
         raise LmbError(rc, msg)
     return rc

@@ -1,12 +1,16 @@
 """Autotuner of the compare pass launch shape.
 
-Sweeps kernel variant (block-barrier ring / warp-specialised), tile size,
-ring depth, consumer warps and grid size on the device for a DB of the given
-record size and batch width, checks that every shape returns the same
-survivors, and writes the fastest shape per (record words, batch bucket) to
-``tuning.json`` next to this file.  Engines load that table at creation.
+Sweeps kernel variant (block-barrier ring / warp-specialised / compact
+layout), tile size, ring depth, consumer warps and grid size on the device for
+a DB of the given record size and batch width, checks that every shape
+returns the same survivors, and writes the fastest shape per (record words,
+batch bucket) to ``tuning.json`` next to this file.  With ``--dense`` it
+sweeps the cell-mask pass (variant 4) on a DB of many spots per record and
+writes the ``_dense`` entries, the shape the automatic variant uses when it
+picks that pass.  Engines load the table at creation.
 
-    python -m lauematching_b200.autotune --n-orient 100000000 --batch 64
+    python -m lauematching_b200.autotune --n-orient 100000000 --batches 1,64 --write
+    python -m lauematching_b200.autotune --dense --n-orient 100000000 --batches 64 --write
 """
 from __future__ import annotations
 
@@ -39,16 +43,26 @@ def load_table() -> dict:
     return {}
 
 
-def lookup(R: int, k: int) -> dict | None:
-    """Best shape for records of R uint16 words and a pass of k images."""
+def lookup(R: int, k: int, dense: bool = False) -> dict | None:
+    """Best shape for records of R uint16 words and a pass of k images; with
+    ``dense``, the cell-mask pass's shape (variant 4), which the automatic
+    variant runs when the records that can pass hold many spots."""
     t = load_table().get("entries", {})
-    key = f"R{R}_K{batch_bucket(k)}"
+    suffix = f"_K{batch_bucket(k)}" + ("_dense" if dense else "")
+    key = f"R{R}{suffix}"
     if key in t:
         return t[key]["shape"]
     # nearest record size with the same batch bucket
     cands = [(abs(int(kk.split("_")[0][1:]) - R), v) for kk, v in t.items()
-             if kk.endswith(f"_K{batch_bucket(k)}")]
+             if kk.endswith(suffix)]
     return min(cands, key=lambda x: x[0])[1]["shape"] if cands else None
+
+
+def candidate_shapes_dense():
+    # the cell-mask pass: one block per SM; consumer warps and ring depth
+    # (0 = as deep as fits beside the mask and the hit lists)
+    for cons, st in itertools.product((4, 6, 8, 10, 12, 14, 16), (0, 2, 3, 4, 6)):
+        yield dict(variant=4, stages=st, consumers=cons)
 
 
 def candidate_shapes():
@@ -85,8 +99,15 @@ def main():
     ap.add_argument("--max-nr-spots", type=int, default=30)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--write", action="store_true", help="update tuning.json")
+    ap.add_argument("--dense", action="store_true",
+                    help="tune the cell-mask pass (variant 4) on a DB of many spots per "
+                         "record (the reference's tilted 34-ID-E detector); stored as the "
+                         "table's _dense entries")
     args = ap.parse_args()
-    txt = synth.params_text(max_nr_spots=args.max_nr_spots, min_nr_spots=5, min_intensity=200.0)
+    geo = dict(p=(0.028745, 0.002788, 0.513115),
+               r=(-1.20131258, -1.21399082, -1.21881158)) if args.dense else {}
+    txt = synth.params_text(max_nr_spots=args.max_nr_spots, min_nr_spots=5, min_intensity=200.0,
+                            **geo)
     p = P.parse_params_text(txt)
     hk = synth.hkls_cubic(8)
     e = Engine(p)
@@ -107,7 +128,7 @@ def main():
         slots = list(range(kb))
         ref = None
         results = []
-        for shape in candidate_shapes():
+        for shape in (candidate_shapes_dense() if args.dense else candidate_shapes()):
             e.set_tuning(**shape)
             try:
                 ms = time_shape(e, slots, p)
@@ -128,7 +149,7 @@ def main():
         shape.pop("last_variant", None)
         if shape["variant"] == 2:  # engines pick the layout per pass (automatic variant 3)
             shape["variant"] = 3
-        entries[f"R{R}_K{batch_bucket(kb)}"] = {
+        entries[f"R{R}_K{batch_bucket(kb)}" + ("_dense" if args.dense else "")] = {
             "shape": shape, "compare_ms": round(best[0], 4),
             "gbs": round(bytes_pass / (best[0] * 1e-3) / 1e9, 1), "n_orient": args.n_orient,
             "swept": len(results),

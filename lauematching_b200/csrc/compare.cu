@@ -608,6 +608,7 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], NC);
     }
+    if (a.test_consumer_wait_ns) mbar_init(&full[15], 1);  // nothing ever arrives (ST <= 15)
     fence_mbar_init();
   }
   __syncthreads();
@@ -656,7 +657,9 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
   uint32_t turn = 0;  // the consumer warp that takes the next chunk
   for (uint64_t i = 0; i < my_tiles; i++) {
     const int s = (int)(i % ST);
-    const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+    const bool ok = a.test_consumer_wait_ns
+                        ? mbar_wait_bounded(&full[15], 0, a.test_consumer_wait_ns)
+                        : mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
     if (!__all_sync(0xffffffffu, ok)) {
       if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
       return;
@@ -718,6 +721,192 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
     if (lane == 0) mbar_arrive(&empty[s]);
   }
   if (qn) flush();
+}
+
+// ----------------------------------------------------------------------------
+// Variant 4: the compact layout filtered by the batch's cell mask.
+//
+// With detector geometries that put ~15-20 spots of every orientation on the
+// detector, nearly every record can reach MinNrSpots and the pass is the
+// 8-byte occupancy gathers of all their spots (~1.5e9 per pass at 1e8
+// records), not the DB stream.  But the batch's frames are sparse: at K = 64
+// the union of their positive pixels covers ~12 % of the detector.  The cell
+// mask holds one bit per cell of 2^cm_shift consecutive pixels, set when a
+// pixel of the cell is positive in some slot of the pass; it is built per
+// pass (cellmask_kernel) and copied into each block's shared memory.  A spot
+// on an unmarked cell is zero in every slot, so
+//   * it adds nothing to any count or sum and is dropped from the record's
+//     spot list (the remaining spots keep record order, so the FP64 sums are
+//     those of the reference: zero pixels are skipped there too);
+//   * a record with fewer than MinNrSpots spots on marked cells cannot pass
+//     in any slot (LaueMatchingCPU.c:683) and is not gathered at all.
+// Consumer warps go through a chunk's spot array 32 spots at a time (one
+// conflict-free shared-memory read per lane), test each spot's cell, and
+// compact the hits into the warp's hit list in order; per window the hit
+// bits and the hits before it give every record its hit range with two
+// lookups.  The records that can still pass are counted from their hit
+// ranges with the per-record logic of the other variants.
+// ----------------------------------------------------------------------------
+__global__ void cellmask_kernel(const unsigned long long *__restrict__ occ, uint64_t npx,
+                                unsigned long long active, int shift, uint64_t nslots,
+                                uint32_t *__restrict__ mask) {
+  // thread per cell; nslots (32 x the mask words) and the grid stride are
+  // multiples of 32, so whole warps run every iteration together
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < nslots;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p0 = c << shift;
+    const uint64_t p1 = p0 + (1ull << shift) < npx ? p0 + (1ull << shift) : npx;
+    unsigned long long any = 0ull;
+    for (uint64_t p = p0; p < p1; p++) any |= occ[p];
+    const unsigned b = __ballot_sync(0xffffffffu, (any & active) != 0ull);
+    if ((threadIdx.x & 31) == 0) mask[c >> 5] = b;
+  }
+}
+
+int cellmask_launch(const unsigned long long *d_occ, uint64_t npx, unsigned long long active,
+                    int shift, uint32_t cm_bytes, uint32_t *d_mask, int num_sms, cudaStream_t st) {
+  const uint64_t nslots = (uint64_t)(cm_bytes / 4) * 32;
+  const unsigned blocks =
+      (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((nslots + 255) / 256, (uint64_t)num_sms * 8));
+  cellmask_kernel<<<blocks, 256, 0, st>>>(d_occ, npx, active, shift, nslots, d_mask);
+  LMB_CUDA(cudaGetLastError());
+  return LMB_OK;
+}
+
+template <int B>
+__global__ void __launch_bounds__(32 * 17, 1) compare_cell_kernel(const __grid_constant__ CmpArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int ST = a.stages;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *empty = full + 16;
+  uint32_t *cm = reinterpret_cast<uint32_t *>(smem + 256);
+  unsigned char *ring = smem + 256 + a.cm_bytes;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int NC = a.consumers;
+  const uint64_t G = gridDim.x;
+  const uint64_t my_tiles = (a.ntiles > blockIdx.x) ? (a.ntiles - 1 - blockIdx.x) / G + 1 : 0;
+  {  // the pass's cell mask into shared memory
+    const uint4 *src = reinterpret_cast<const uint4 *>(a.cellmask);
+    uint4 *dst = reinterpret_cast<uint4 *>(cm);
+    for (uint32_t i = threadIdx.x; i < a.cm_bytes / 16; i += blockDim.x) dst[i] = src[i];
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NC);
+    }
+    if (a.test_consumer_wait_ns) mbar_init(&full[15], 1);  // nothing ever arrives (ST <= 15)
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    if (lane != 0) return;
+    const uint64_t pol_db = l2_evict_first();
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < my_tiles; i++) {
+      const int s = (int)(i % ST);
+      if (i >= (uint64_t)ST &&
+          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+        atomicExch(a.err, DEV_TIMEOUT_TMA);
+        break;
+      }
+      const uint64_t t = blockIdx.x + i * G;
+      mbar_expect_tx(&full[s], a.tile_bytes);
+      bulk_g2s_hint(ring + (size_t)s * a.tile_bytes, a.cl + t * a.tile_bytes, a.tile_bytes,
+                    &full[s], pol_db);
+      issued = i + 1;
+    }
+    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
+      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    return;
+  }
+  const int cw = warp - 1;
+  if (cw >= NC) return;
+  const uint64_t pol_occ = l2_evict_last();
+  const uint32_t QS = (uint32_t)(a.qS < 1 ? 1 : a.qS);
+  uint32_t *hl = reinterpret_cast<uint32_t *>(ring + (size_t)ST * a.tile_bytes +
+                                              (size_t)cw * cell_warp_bytes(a.qS));
+  uint32_t *wm = hl + 32u * QS;  // per window: hit bits
+  uint32_t *cum = wm + QS;       // per window: hits before it
+  const unsigned lt = (1u << lane) - 1u;
+  const int need = a.full_gather ? 0 : a.min_spots;
+  const int sh = a.cm_shift;
+  uint32_t turn = 0;
+  for (uint64_t i = 0; i < my_tiles; i++) {
+    const int s = (int)(i % ST);
+    const bool ok = a.test_consumer_wait_ns
+                        ? mbar_wait_bounded(&full[15], 0, a.test_consumer_wait_ns)
+                        : mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
+      return;
+    }
+    const unsigned char *tb = ring + (size_t)s * a.tile_bytes;
+    const uint64_t first = *reinterpret_cast<const uint64_t *>(tb);
+    const uint32_t nch = *reinterpret_cast<const uint32_t *>(tb + 8);
+    const unsigned char *cmax = tb + 16;
+    const unsigned char *cnt = tb + clist_cnt_offset(nch);
+    const uint32_t *base = reinterpret_cast<const uint32_t *>(tb + clist_base_offset(nch));
+    const uint32_t *spots = reinterpret_cast<const uint32_t *>(tb + clist_spot_offset(nch));
+    for (uint32_t j0 = 0; j0 < nch; j0 += 32) {
+      unsigned m = __ballot_sync(0xffffffffu, j0 + lane < nch && cmax[j0 + lane] >= need);
+      while (m) {
+        const uint32_t ch = j0 + (uint32_t)(__ffs(m) - 1);
+        m &= m - 1;
+        const bool mine = turn == (uint32_t)cw;
+        turn = (turn + 1 == (uint32_t)NC) ? 0 : turn + 1;
+        if (!mine) continue;
+        const uint64_t oid = first + ch * 32 + lane;
+        const bool valid = oid < a.n;
+        const int c = valid ? cnt[ch * 32 + lane] : 0;
+        if (valid && c > a.qS) atomicExch(a.err, DEV_BAD_QUEUE);  // cannot come from this layout
+        int x = c;  // inclusive prefix sum of the counts over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        // the chunk's spots in windows of 32 (total <= 32 * qS: at most qS windows)
+        const uint32_t total = min((uint32_t)__shfl_sync(0xffffffffu, x, 31), 32u * QS);
+        const uint32_t *sp = spots + base[ch];
+        uint32_t hb = 0;
+        for (uint32_t w0 = 0; w0 < total; w0 += 32) {
+          const uint32_t k = w0 + lane;
+          uint32_t p = 0;
+          bool h = false;
+          if (k < total) {
+            p = sp[k];
+            const uint32_t q = p >> sh;
+            h = (cm[q >> 5] >> (q & 31u)) & 1u;
+          }
+          const unsigned hm = __ballot_sync(0xffffffffu, h);
+          if (h) hl[hb + __popc(hm & lt)] = p;
+          if (lane == 0) {
+            wm[w0 >> 5] = hm;
+            cum[w0 >> 5] = hb;
+          }
+          hb += (uint32_t)__popc(hm);
+        }
+        __syncwarp();
+        // this record's spots are [x - c, x) of the chunk; its hits, in order,
+        // are [h0, h1) of the hit list
+        auto hits_before = [&](uint32_t k) -> uint32_t {
+          if (k >= total) return hb;
+          const uint32_t w = k >> 5;
+          return cum[w] + (uint32_t)__popc(wm[w] & ((1u << (k & 31u)) - 1u));
+        };
+        const uint32_t xe = min((uint32_t)x, total), xs = min((uint32_t)(x - c), total);
+        const uint32_t h0 = hits_before(xs);
+        const int ub = (int)(hits_before(xe) - h0);
+        const bool cand = valid && c <= a.qS && ub >= need;
+        if (__any_sync(0xffffffffu, cand))
+          process<B, ListSpots, 1>(a, ListSpots{hl + h0}, cand ? ub : 0, oid, pol_occ, cand);
+        __syncwarp();
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -802,6 +991,15 @@ static int counter_bits(int S) {
 CompareTuning compare_config(int R, const CompareTuning &req) {
   CompareTuning c = req;
   const size_t rb = (size_t)R * 2;
+  if (c.variant == 4) {  // compact layout + cell mask: one block per SM
+    c.tile_sub = 0;
+    if (c.consumers <= 0) c.consumers = 12;
+    c.consumers = std::min(c.consumers, 16);
+    c.stages = c.stages > 0 ? std::max(2, std::min(c.stages, 16)) : 0;  // 0: as many as fit
+    c.blocks_per_sm = 1;
+    c.grid_mult = 1;
+    return c;
+  }
   if (c.variant == 2 || c.variant == 3) {  // compact layout: the tile shape comes with it
     c.tile_sub = 0;
     if (c.consumers <= 0) c.consumers = 16;
@@ -845,7 +1043,11 @@ static int launch_clist_bounded(const CmpArgs &a, unsigned grid, size_t smem, cu
 template <int B>
 static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, size_t smem,
                     int nblk, cudaStream_t st) {
-  if (c.variant == 2 && nblk >= 6) {
+  if (c.variant == 4) {
+    const int rc = ensure_smem((const void *)compare_cell_kernel<B>, (int)smem);
+    if (rc) return rc;
+    compare_cell_kernel<B><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
+  } else if (c.variant == 2 && nblk >= 6) {
     // six to eight 128-thread blocks per SM: registers bounded for that occupancy
     const int rc = nblk >= 8   ? launch_clist_bounded<B, 8>(a, grid, smem, st)
                    : nblk == 7 ? launch_clist_bounded<B, 7>(a, grid, smem, st)
@@ -872,8 +1074,25 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   LMB_REQUIRE((reinterpret_cast<uintptr_t>(a.db) & 15) == 0,
               "DB device pointer must be 16-byte aligned");
   CompareTuning c = compare_config(a.R, req);
+  a.test_consumer_wait_ns = (uint64_t)std::max(0, c.test_consumer_wait_us) * 1000ull;
+  LMB_REQUIRE(!a.test_consumer_wait_ns || c.variant == 2 || c.variant == 4,
+              "the test wait applies to the compact-layout passes only");
+  size_t fixed = 256;  // barriers
+  if (c.variant == 4) {
+    // the cell mask, and per consumer warp its hit list and window words; as
+    // many consumer warps as leave room for a two-stage ring
+    LMB_REQUIRE(a.cellmask && a.cm_bytes > 0 && a.cm_bytes % 128 == 0 &&
+                    a.cm_bytes <= kCellMaskBytes && (reinterpret_cast<uintptr_t>(a.cellmask) & 15) == 0,
+                "cell mask missing or malformed");
+    LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "cell pass hit lists of %d spots per record", a.qS);
+    while (c.consumers > 1 &&
+           256 + (size_t)a.cm_bytes + (size_t)c.consumers * cell_warp_bytes(a.qS) +
+                   2 * (size_t)a.tile_bytes > 227 * 1024)
+      c.consumers--;
+    fixed += a.cm_bytes + (size_t)c.consumers * cell_warp_bytes(a.qS);
+  }
   a.consumers = c.consumers;
-  if (c.variant == 2) {
+  if (c.variant == 2 || c.variant == 4) {
     // a.cl_tiles tiles of a.tile_bytes come from the compact layout; every
     // tile, the last included, is one bulk copy
     LMB_REQUIRE(a.cl && a.cl_tiles > 0 && a.tile_bytes > 0 && a.tile_bytes % 128 == 0,
@@ -884,9 +1103,11 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
     a.ntiles = a.cl_tiles;
     a.full_tiles = a.ntiles;
     LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "compact pass queue entry of %d spots", a.qS);
-    const size_t qbytes = (size_t)c.consumers * clist_queue_bytes(a.qS);
+    const size_t qbytes =
+        c.variant == 4 ? fixed - 256 : (size_t)c.consumers * clist_queue_bytes(a.qS);
     const size_t room = 227 * 1024 > 256 + qbytes ? 227 * 1024 - 256 - qbytes : 0;
-    const int fit = (int)std::min<size_t>(16, room / a.tile_bytes);
+    // barrier 15 is the test wait's when one is set
+    const int fit = (int)std::min<size_t>(a.test_consumer_wait_ns ? 15 : 16, room / a.tile_bytes);
     LMB_REQUIRE(fit >= 2, "compact tiles of %u bytes leave no room for a ring", a.tile_bytes);
     c.stages = c.stages > 0 ? std::min(c.stages, fit) : fit;
   } else {
@@ -900,6 +1121,7 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   if (a.ntiles == 0 || a.active == 0) return LMB_OK;
   size_t smem = 256 + (size_t)c.stages * a.tile_bytes;
   if (c.variant == 2) smem += (size_t)c.consumers * clist_queue_bytes(a.qS);
+  if (c.variant == 4) smem = fixed + (size_t)c.stages * a.tile_bytes;
   LMB_REQUIRE(smem <= 227 * 1024, "compare ring of %zu bytes exceeds shared memory", smem);
   const int mult = c.grid_mult > 0 ? c.grid_mult : 1;
   const unsigned grid = (unsigned)std::min<uint64_t>(

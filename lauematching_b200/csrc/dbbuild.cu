@@ -218,8 +218,15 @@ __device__ __forceinline__ double u01(uint64_t seed, uint64_t c) {
   return (double)(z >> 11) * (1.0 / 9007199254740992.0);
 }
 
+// Symmetry quaternions (w, x, y, z), normalised, of a fundamental-zone
+// reduction of the synthetic orientations (nsym = 0: none).
+struct SynthSym {
+  int nsym;
+  double q[24][4];
+};
+
 __global__ void synth_orient_kernel(uint64_t seed, uint64_t first, uint64_t n,
-                                    double *__restrict__ out) {
+                                    double *__restrict__ out, const SynthSym sym) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t id = first + i;
@@ -229,7 +236,34 @@ __global__ void synth_orient_kernel(uint64_t seed, uint64_t first, uint64_t n,
     double s2, c2, s3, c3;
     sincospi(2.0 * u2, &s2, &c2);
     sincospi(2.0 * u3, &s3, &c3);
-    const double x = a * s2, y = a * c2, z = b * s3, w = b * c3;
+    double x = a * s2, y = a * c2, z = b * s3, w = b * c3;
+    if (sym.nsym > 0) {
+      // of the equivalent rotations r (x) q keep the one with the largest
+      // |scalar part| (the first such), scalar part made non-negative and
+      // renormalised: the operator order and product of
+      // LaueMatchingHeaders.h:111-122,166-178, as synth.hexagonal_fundamental_zone
+      int best = 0;
+      double bw = -1.0;
+      for (int k = 0; k < sym.nsym; k++) {
+        const double *r = sym.q[k];
+        const double wk = fabs(r[0] * w - r[1] * x - r[2] * y - r[3] * z);
+        if (wk > bw) {
+          bw = wk;
+          best = k;
+        }
+      }
+      const double *r = sym.q[best];
+      double Q0 = r[0] * w - r[1] * x - r[2] * y - r[3] * z;
+      double Q1 = r[1] * w + r[0] * x + r[3] * y - r[2] * z;
+      double Q2 = r[2] * w + r[0] * y + r[1] * z - r[3] * x;
+      double Q3 = r[3] * w + r[0] * z + r[2] * x - r[1] * y;
+      const double sg = Q0 < 0 ? -1.0 : 1.0;
+      const double inv = sg / sqrt(Q0 * Q0 + Q1 * Q1 + Q2 * Q2 + Q3 * Q3);
+      w = Q0 * inv;
+      x = Q1 * inv;
+      y = Q2 * inv;
+      z = Q3 * inv;
+    }
     double *o = out + i * 9;
     o[0] = 1.0 - 2.0 * (y * y + z * z);
     o[1] = 2.0 * (x * y - z * w);
@@ -327,11 +361,27 @@ int dbbuild_launch(const double *d_om, uint64_t n, const int4 *d_hkl, int nh,
   return LMB_OK;
 }
 
+// The 12 operators of the hexagonal (622) group, LaueMatchingHeaders.h:111-122
+// (5-decimal values, normalised here).
+static const double kHexSym[12][4] = {
+    {1, 0, 0, 0},          {0.86603, 0, 0, 0.5},  {0.5, 0, 0, 0.86603},  {0, 0, 0, 1},
+    {0.5, 0, 0, -0.86603}, {0.86603, 0, 0, -0.5}, {0, 1, 0, 0},          {0, 0.86603, 0.5, 0},
+    {0, 0.5, 0.86603, 0},  {0, 0, 1, 0},          {0, -0.5, 0.86603, 0}, {0, -0.86603, 0.5, 0}};
+
 int synth_orient_launch(uint64_t seed, uint64_t first, uint64_t n, double *d_out,
-                        cudaStream_t st) {
+                        cudaStream_t st, uint32_t flags) {
   if (n == 0) return LMB_OK;
+  SynthSym sym{};
+  if (flags & LMB_BUILD_SYNTH_HEX_FZ) {
+    sym.nsym = 12;
+    for (int k = 0; k < 12; k++) {
+      const double *q = kHexSym[k];
+      const double nrm = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+      for (int j = 0; j < 4; j++) sym.q[k][j] = q[j] / nrm;
+    }
+  }
   const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148ull * 32);
-  synth_orient_kernel<<<(unsigned)blocks, 256, 0, st>>>(seed, first, n, d_out);
+  synth_orient_kernel<<<(unsigned)blocks, 256, 0, st>>>(seed, first, n, d_out, sym);
   LMB_CUDA(cudaGetLastError());
   return LMB_OK;
 }

@@ -81,6 +81,9 @@ struct lmb_engine {
   uint8_t *d_u8 = nullptr;
   double *d_f64 = nullptr;  // allocated on first keep_f64 load
   unsigned long long *d_occ = nullptr;
+  uint32_t *d_cellmask = nullptr;  // compare variant 4: the pass's cell mask
+  uint32_t cm_bytes = 0;
+  int cm_shift = 0;
   double *d_scale = nullptr;
   unsigned long long *d_max_bits = nullptr;
   void *d_stage = nullptr;  // one image in its wire dtype
@@ -105,7 +108,7 @@ struct lmb_engine {
   cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
   // automatic variant with the compact pass's tuned shape (2 stages, 3 consumer
   // warps, 8 blocks per SM)
-  CompareTuning tuning{3, 0, 2, 3, 1, 8, 0};
+  CompareTuning tuning{3, 0, 2, 3, 1, 8, 0, 0, 0, 0};
   int last_variant = -1;  // variant the latest pass ran
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
@@ -154,6 +157,7 @@ void free_engine(lmb_engine *e) {
   cudaFree(e->d_u8);
   cudaFree(e->d_f64);
   cudaFree(e->d_occ);
+  cudaFree(e->d_cellmask);
   cudaFree(e->d_scale);
   cudaFree(e->d_max_bits);
   cudaFree(e->d_stage);
@@ -489,6 +493,14 @@ double gathered_per_record(const lmb_engine *e, int min_spots) {
   return e->n ? g / (double)e->n : 0.0;
 }
 
+// The cell-mask pass needs its mask, a hit list per consumer warp and a
+// two-stage ring of the layout's tiles in one block's shared memory.
+bool cell_pass_fits(const lmb_engine *e) {
+  const size_t need = 256 + (size_t)e->cm_bytes + cell_warp_bytes(e->cl_qs > 0 ? e->cl_qs : e->S) +
+                      2 * (size_t)e->cl_stage;
+  return e->d_cellmask && need <= 227 * 1024;
+}
+
 int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   // timing events recorded inside a captured graph must be external to be
   // observable (and timed) after each replay
@@ -522,12 +534,22 @@ int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   a.pass_cnt = e->d_status + LMB_MAX_SLOTS;
   a.err = reinterpret_cast<int *>(e->d_status + 2 * LMB_MAX_SLOTS);
   a.full_gather = k.tuning.full_gather;
-  if (k.tuning.variant == 2) {
+  if (k.tuning.variant == 2 || k.tuning.variant == 4) {
     a.cl = e->d_cl;
     a.cl_tiles = e->cl_tiles;
     a.tile_bytes = e->cl_stage;
   }
+  if (k.tuning.variant == 4) {
+    a.cellmask = e->d_cellmask;
+    a.cm_bytes = e->cm_bytes;
+    a.cm_shift = e->cm_shift;
+  }
   if (k.min_spots <= e->S && !std::isnan(k.min_int)) {
+    if (k.tuning.variant == 4) {  // the cell mask of this pass's slots, then the pass
+      const int rc = cellmask_launch(e->d_occ, e->npx, k.mask, e->cm_shift, e->cm_bytes,
+                                     e->d_cellmask, e->num_sms, e->st);
+      if (rc) return rc;
+    }
     const int rc = compare_launch(a, k.tuning, e->num_sms, e->st);
     if (rc) return rc;
   }
@@ -622,6 +644,10 @@ int lmb_engine_create(int32_t device, const lmb_geometry *geo, uint64_t survivor
   TRY(cudaMemset(e->d_u8, 0, e->npx * LMB_MAX_SLOTS));
   TRY(cudaMalloc(&e->d_occ, e->npx * sizeof(unsigned long long)));
   TRY(cudaMemset(e->d_occ, 0, e->npx * sizeof(unsigned long long)));
+  e->cm_shift = cellmask_shift(e->npx);
+  e->cm_bytes = cellmask_bytes(e->npx);
+  TRY(cudaMalloc(&e->d_cellmask, e->cm_bytes));
+  TRY(cudaMemset(e->d_cellmask, 0, e->cm_bytes));
   TRY(cudaMalloc(&e->d_scale, LMB_MAX_SLOTS * sizeof(double)));
   TRY(cudaMemset(e->d_scale, 0, LMB_MAX_SLOTS * sizeof(double)));
   TRY(cudaMalloc(&e->d_max_bits, sizeof(unsigned long long)));
@@ -681,7 +707,7 @@ static int db_build_common(lmb_engine *e, const double *orients, uint64_t seed, 
   for (uint64_t off = 0; off < n && rc == LMB_OK; off += kChunk) {
     const uint64_t len = std::min(kChunk, n - off);
     if (synthetic) {
-      rc = synth_orient_launch(seed, off, len, d_om, e->st);
+      rc = synth_orient_launch(seed, off, len, d_om, e->st, flags);
     } else {
       rc = upload_chunked(e, d_om, orients + off * 9, len * 72, e->st);
     }
@@ -716,15 +742,28 @@ int lmb_db_build_synthetic(lmb_engine *e, uint64_t seed, uint64_t n, const int32
   return db_build_common(e, nullptr, seed, true, n, hkls, nh, orients_out, 0);
 }
 
+int lmb_db_build_synthetic_ex(lmb_engine *e, uint64_t seed, uint64_t n, const int32_t *hkls,
+                              int32_t nh, double *orients_out, uint32_t flags) {
+  LMB_REQUIRE((flags & ~(uint32_t)(LMB_BUILD_EXACT_FP64 | LMB_BUILD_SYNTH_HEX_FZ)) == 0,
+              "unknown build flags 0x%x", flags);
+  return db_build_common(e, nullptr, seed, true, n, hkls, nh, orients_out, flags);
+}
+
 int lmb_synth_orientations(lmb_engine *e, uint64_t seed, uint64_t first, uint64_t n,
                            double *out) {
+  return lmb_synth_orientations_ex(e, seed, first, n, out, 0);
+}
+
+int lmb_synth_orientations_ex(lmb_engine *e, uint64_t seed, uint64_t first, uint64_t n,
+                              double *out, uint32_t flags) {
   int rc = check_engine(e);
   if (rc) return rc;
   LMB_REQUIRE(out || n == 0, "null output");
+  LMB_REQUIRE((flags & ~(uint32_t)LMB_BUILD_SYNTH_HEX_FZ) == 0, "unknown flags 0x%x", flags);
   if (n == 0) return LMB_OK;
   double *d = nullptr;
   LMB_CUDA(cudaMalloc(&d, n * 72));
-  rc = synth_orient_launch(seed, first, n, d, e->st);
+  rc = synth_orient_launch(seed, first, n, d, e->st, flags);
   cudaError_t ce = cudaSuccess;
   if (rc == LMB_OK) ce = cudaMemcpyAsync(out, d, n * 72, cudaMemcpyDeviceToHost, e->st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
@@ -1036,20 +1075,27 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   LMB_REQUIRE(value_mode == LMB_VALUE_U8 || (slot_mask & ~e->f64_mask) == 0,
               "float64 pass needs images loaded with keep_f64");
   CompareTuning tun = e->tuning;
-  if (tun.variant == 2 || tun.variant == 3) {  // compact layout: derive it once per DB
+  if (tun.variant >= 2) {  // compact layout: derive it once per DB
     if (e->cl_state == 0) {
       rc = build_compact(e);
       if (rc) return rc;
     }
-    // variant 3 (automatic): the compact layout while the records that can
-    // pass are few enough, the reference records otherwise (below)
+    // variant 3 (automatic): the compact layout alone while the records that
+    // can pass hold few spots; beyond that, the compact layout filtered by
+    // the batch's cell mask (variant 4) when its hit lists fit a block, the
+    // reference records otherwise
     bool compact = e->cl_state == 1;
-    if (compact && tun.variant == 3)
-      compact = gathered_per_record(e, tun.full_gather ? 0 : min_nr_spots) <= kAutoGather;
-    if (compact)
-      tun.variant = 2;
-    else
-      tun = CompareTuning{1, 0, 0, 0, 0, 0, tun.full_gather};  // default warp-specialised shape
+    if (compact && tun.variant == 3) {
+      if (gathered_per_record(e, tun.full_gather ? 0 : min_nr_spots) <= kAutoGather)
+        tun.variant = 2;
+      else if (!tun.full_gather && min_nr_spots >= 1 && cell_pass_fits(e))
+        tun = CompareTuning{4, 0, tun.cell_stages, tun.cell_consumers, 1, 1, 0,
+                            tun.test_consumer_wait_us, 0, 0};  // the cell-mask pass's shape
+      else
+        compact = false;
+    }
+    if (!compact)  // warp-specialised over the reference records
+      tun = CompareTuning{1, 0, 0, 0, 0, 0, tun.full_gather, tun.test_consumer_wait_us, 0, 0};
   }
   e->last_variant = tun.variant;
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
@@ -1250,12 +1296,20 @@ int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms) {
 
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields) {
   LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
-  CompareTuning t{1, 0, 0, 0, 0, 0, 0};
-  int32_t *dst[7] = {&t.variant, &t.tile_sub, &t.stages, &t.consumers, &t.blocks_per_sm,
-                     &t.grid_mult, &t.full_gather};
-  for (int i = 0; i < n_fields && i < 7; i++) *dst[i] = fields[i];
+  CompareTuning t{1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int32_t *dst[10] = {&t.variant,     &t.tile_sub,  &t.stages,
+                      &t.consumers,   &t.blocks_per_sm, &t.grid_mult,
+                      &t.full_gather, &t.test_consumer_wait_us, &t.cell_consumers,
+                      &t.cell_stages};
+  for (int i = 0; i < n_fields && i < 10; i++) *dst[i] = fields[i];
+  LMB_REQUIRE(t.cell_consumers >= 0 && t.cell_consumers <= 16 && t.cell_stages >= 0 &&
+                  t.cell_stages <= 16,
+              "cell-mask pass shape (%d consumers, %d stages) out of range", t.cell_consumers,
+              t.cell_stages);
   LMB_REQUIRE(t.full_gather == 0 || t.full_gather == 1, "full_gather must be 0 or 1");
-  LMB_REQUIRE(t.variant >= 0 && t.variant <= 3, "unknown compare variant %d", t.variant);
+  LMB_REQUIRE(t.test_consumer_wait_us >= 0 && t.test_consumer_wait_us <= 1000000,
+              "test wait of %d us outside 0..1000000", t.test_consumer_wait_us);
+  LMB_REQUIRE(t.variant >= 0 && t.variant <= 4, "unknown compare variant %d", t.variant);
   e->tuning = t;
   return LMB_OK;
 }
@@ -1286,9 +1340,11 @@ int lmb_engine_set_sparse_uploads(lmb_engine *e, int32_t enable) {
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields) {
   LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
   const CompareTuning c = compare_config(e->R, e->tuning);
-  const int32_t src[8] = {c.variant, c.tile_sub, c.stages, c.consumers, c.blocks_per_sm,
-                          c.grid_mult, c.full_gather, e->last_variant};
-  for (int i = 0; i < n_fields && i < 8; i++) fields[i] = src[i];
+  const int32_t src[11] = {c.variant,        c.tile_sub,       c.stages,
+                           c.consumers,      c.blocks_per_sm,  c.grid_mult,
+                           c.full_gather,    e->last_variant,  c.test_consumer_wait_us,
+                           c.cell_consumers, c.cell_stages};
+  for (int i = 0; i < n_fields && i < 11; i++) fields[i] = src[i];
   return LMB_OK;
 }
 

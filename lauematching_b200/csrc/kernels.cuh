@@ -32,6 +32,16 @@ struct CmpArgs {
   // 0: a record with fewer spots than MinNrSpots (it cannot pass: its matched
   // count is at most its spot count) is not gathered; 1: every spot is
   int full_gather;
+  // variant 4: cell mask of the pass's slots, bit q = some pixel of
+  // [q << cm_shift, (q + 1) << cm_shift) is positive in an active slot;
+  // cm_bytes (a multiple of 128) of it are copied into each block's shared memory
+  const uint32_t *cellmask;
+  uint32_t cm_bytes;
+  int cm_shift;
+  // test only (compact-layout variants): > 0 makes every consumer warp wait
+  // this long on a shared-memory barrier nothing arrives at, instead of on its
+  // ring slot, so the pass gives up with a timeout (0 in every normal pass)
+  uint64_t test_consumer_wait_ns;
   // filled by compare_launch
   uint64_t full_tiles, ntiles;
   uint32_t tile_bytes;
@@ -43,13 +53,19 @@ struct CmpArgs {
 
 // Launch shape of the compare pass (autotuned; zero fields = defaults).
 struct CompareTuning {
-  int variant;        // 0 = block-barrier ring, 1 = warp-specialised, 2 = compact layout
+  int variant;        // 0 = block-barrier ring, 1 = warp-specialised, 2 = compact layout,
+                      // 3 = automatic, 4 = compact layout + the batch's cell mask
   int tile_sub;       // 32-orientation sub-tiles per tile
   int stages;         // ring depth
   int consumers;      // consumer warps (variant 1)
   int blocks_per_sm;  // resident blocks per SM (variant 0)
   int grid_mult;      // grid = SMs * blocks_per_sm * grid_mult
   int full_gather;    // 1: gather every spot even of records that cannot pass
+  int test_consumer_wait_us;  // test only: see CmpArgs::test_consumer_wait_ns
+  // shape of the cell-mask pass when the automatic variant picks it
+  // (0 = defaults): consumer warps, ring stages
+  int cell_consumers;
+  int cell_stages;
 };
 CompareTuning compare_config(int R, const CompareTuning &req);
 
@@ -67,7 +83,7 @@ struct OrderArgs {
 int dbbuild_launch(const double *d_om, uint64_t n, const int4 *d_hkl, int nh,
                    const lmb_geometry &geo, uint16_t *d_out, cudaStream_t st, bool exact_all);
 int synth_orient_launch(uint64_t seed, uint64_t first, uint64_t n, double *d_out,
-                        cudaStream_t st);
+                        cudaStream_t st, uint32_t flags = 0);
 int quantize_launch(const void *d_img, int dtype, size_t npx, unsigned long long *d_max_bits,
                     uint8_t *d_u8, double *d_f64_keep, unsigned long long *d_occ, int slot,
                     double *d_scale_slot, int num_sms, cudaStream_t st);
@@ -157,6 +173,32 @@ __host__ __device__ __forceinline__ uint32_t clist_queue_bytes(int S) {
 }
 int clist_chunk_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H,
                        uint32_t *d_chunk_spots, unsigned long long *d_hist, cudaStream_t st);
+
+// Cell mask of a pass (variant 4): at most kCellMaskBytes, so it fits a
+// block's shared memory beside the ring.  The shift is the smallest that
+// makes npx >> shift cells fit; cellmask_bytes is the buffer size used (a
+// multiple of 128, words past the last cell stay zero).
+constexpr uint32_t kCellMaskBytes = 128u * 1024u;
+__host__ __forceinline__ int cellmask_shift(uint64_t npx) {
+  int s = 0;
+  while (((npx + (1ull << s) - 1) >> s) > 8ull * kCellMaskBytes) s++;
+  return s;
+}
+__host__ __forceinline__ uint32_t cellmask_bytes(uint64_t npx) {
+  const int s = cellmask_shift(npx);
+  const uint64_t cells = (npx + (1ull << s) - 1) >> s;
+  const uint64_t words = (cells + 31) / 32;
+  return (uint32_t)(((words * 4 + 127) / 128) * 128);
+}
+// Per consumer warp of variant 4: the chunk's spots on marked cells (at most
+// 32 * qS pixel indices), then per 32-spot window its hit bits and the hits
+// before it.
+__host__ __device__ __forceinline__ uint32_t cell_warp_bytes(int qS) {
+  const uint32_t q = (uint32_t)(qS < 1 ? 1 : qS);
+  return ((32u * q + 2u * q) * 4u + 15u) / 16u * 16u;
+}
+int cellmask_launch(const unsigned long long *d_occ, uint64_t npx, unsigned long long active,
+                    int shift, uint32_t cm_bytes, uint32_t *d_mask, int num_sms, cudaStream_t st);
 int clist_fill_launch(const uint16_t *d_db, uint64_t n, int R, int S, int W, int H, uint32_t TB,
                       const uint32_t *d_ctile, const uint32_t *d_cpos, const uint32_t *d_cbase,
                       const uint32_t *d_tnch, unsigned char *d_cl, cudaStream_t st);

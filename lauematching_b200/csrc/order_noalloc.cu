@@ -21,6 +21,17 @@ static constexpr uint32_t kNoAllocSmemKeys = 8192;
 // name as a device address: it is the host-side shadow of the symbol).
 static __device__ __align__(256) unsigned long long g_order_scratch[kNoAllocMax];
 
+// Key order.  Packed keys (id << 24 | index) compare as integers while every
+// id is below 2^40; otherwise keys hold the index alone and compare by
+// (id, index) read from the input.  Keys past n sort last either way.
+__device__ __forceinline__ bool key_after(unsigned long long x, unsigned long long y,
+                                          const lmb_survivor *__restrict__ in, uint32_t n,
+                                          bool wide) {
+  if (!wide || x >= n || y >= n) return x > y;
+  const uint64_t ix = in[x].id, iy = in[y].id;
+  return ix != iy ? ix > iy : x > y;
+}
+
 __global__ void __launch_bounds__(1024) order_noalloc_kernel(const lmb_survivor *__restrict__ in,
                                                              uint32_t n,
                                                              lmb_survivor *__restrict__ out,
@@ -29,8 +40,11 @@ __global__ void __launch_bounds__(1024) order_noalloc_kernel(const lmb_survivor 
   uint32_t P = 1;
   while (P < n) P <<= 1;
   unsigned long long *keys = (P <= kNoAllocSmemKeys) ? sk : scratch;
-  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
-    keys[i] = (i < n) ? ((in[i].id << 24) | i) : ~0ull;  // every used key rewritten per call
+  int big = 0;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) big |= (in[i].id >> 40) != 0;
+  const bool wide = __syncthreads_or(big) != 0;
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)  // every used key rewritten per call
+    keys[i] = (i < n) ? (wide ? (unsigned long long)i : ((in[i].id << 24) | i)) : ~0ull;
   __syncthreads();
   for (uint32_t size = 2; size <= P; size <<= 1) {
     for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
@@ -39,7 +53,7 @@ __global__ void __launch_bounds__(1024) order_noalloc_kernel(const lmb_survivor 
         const uint32_t hi = lo + stride;
         const bool asc = (lo & size) == 0;
         const unsigned long long x = keys[lo], y = keys[hi];
-        if ((x > y) == asc) {
+        if (key_after(x, y, in, n, wide) == asc) {
           keys[lo] = y;
           keys[hi] = x;
         }
@@ -87,7 +101,8 @@ extern "C" int lmb_order_survivors_noalloc(const lmb_survivor *d_in, uint64_t n,
               (unsigned long long)n, kNoAllocMax);
   if (n == 0) return LMB_OK;
   LMB_REQUIRE(d_in && d_out, "null device pointer");
-  LMB_REQUIRE(d_in != d_out, "input and output must not alias");
+  // the final gather reads the input while it writes the output: no overlap
+  LMB_REQUIRE(d_out >= d_in + n || d_in >= d_out + n, "input and output must not overlap");
   int dev = 0;
   LMB_CUDA(cudaGetDevice(&dev));
   unsigned long long *scratch = nullptr;

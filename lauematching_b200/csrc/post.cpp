@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -581,6 +582,91 @@ int merge_clusters(int device, double band, const Sym &S, double max_angle,
 
 }  // namespace
 
+namespace {
+
+// Refinement handles of the post-stage, kept between calls: a handle on a
+// device holds device buffers, and creating and freeing those per image would
+// put cudaMalloc/cudaFree (and cudaFree's device-wide synchronisation) into
+// every frame of the streaming daemon's writer threads.  A call checks out an
+// idle handle made for the same device, geometry, parameters and HKL list (or
+// creates one) and returns it afterwards; concurrent calls each hold their
+// own.  At most kRefinePoolIdle idle handles are kept; the pool lives until
+// the process exits.
+constexpr size_t kRefinePoolIdle = 8;
+
+struct RefineKey {
+  int device = -1;
+  lmb_geometry geo{};
+  lmb_post_params pp{};
+  std::vector<int32_t> hkls;
+  bool operator==(const RefineKey &o) const {
+    return device == o.device && memcmp(&geo, &o.geo, sizeof(geo)) == 0 &&
+           memcmp(&pp, &o.pp, sizeof(pp)) == 0 && hkls == o.hkls;
+  }
+};
+
+struct RefinePool {
+  std::mutex mu;
+  std::vector<std::pair<RefineKey, lmb_refine *>> idle;
+};
+
+RefinePool &refine_pool() {
+  static RefinePool *pool = new RefinePool();  // never destroyed: no CUDA calls at exit
+  return *pool;
+}
+
+int refine_checkout(int device, const lmb_geometry *geo, const lmb_post_params *pp,
+                    const int32_t *hkls, int32_t nh, RefineKey *key, lmb_refine **out) {
+  key->device = device;
+  memcpy(&key->geo, geo, sizeof(lmb_geometry));
+  memcpy(&key->pp, pp, sizeof(lmb_post_params));
+  key->hkls.assign(hkls, hkls + 3 * (size_t)nh);
+  {
+    RefinePool &pool = refine_pool();
+    std::lock_guard<std::mutex> lk(pool.mu);
+    for (size_t i = 0; i < pool.idle.size(); i++)
+      if (pool.idle[i].first == *key) {
+        *out = pool.idle[i].second;
+        pool.idle.erase(pool.idle.begin() + (ptrdiff_t)i);
+        return LMB_OK;
+      }
+  }
+  return lmb_refine_create(device, geo, pp, hkls, nh, out);
+}
+
+void refine_return(RefineKey &&key, lmb_refine *rf, bool reusable) {
+  if (!rf) return;
+  if (reusable) {
+    RefinePool &pool = refine_pool();
+    std::lock_guard<std::mutex> lk(pool.mu);
+    if (pool.idle.size() < kRefinePoolIdle) {
+      pool.idle.emplace_back(std::move(key), rf);
+      return;
+    }
+  }
+  lmb_refine_destroy(rf);
+}
+
+// What the calling thread's last lmb_post_process refined, and where.
+struct PostRefineStats {
+  int32_t device = -2;  // -2: no refinement; -1: host threads; else the device
+  int64_t points = 0;
+  int32_t rounds = 0;
+  float kernel_ms = 0.0f;
+};
+thread_local PostRefineStats t_post_refine;
+
+}  // namespace
+
+extern "C" int lmb_post_last_refine_stats(int32_t *device, int64_t *points, int32_t *rounds,
+                                          float *kernel_ms) {
+  if (device) *device = t_post_refine.device;
+  if (points) *points = t_post_refine.points;
+  if (rounds) *rounds = t_post_refine.rounds;
+  if (kernel_ms) *kernel_ms = t_post_refine.kernel_ms;
+  return LMB_OK;
+}
+
 extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *pp,
                                 const double *orients, uint64_t n_orients, const uint64_t *ids,
                                 const double *scores, int64_t n_results, const float *image,
@@ -647,12 +733,14 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
   // way); optimizer 0 (below): evaluate once, as the reference built without
   // NLopt does
   std::vector<double> nm_x, nm_ov;
+  t_post_refine = PostRefineStats{};
   if (pp->optimizer == 1 && nsol > 0) {
     lmb_refine *rf = nullptr;
     const int rdev = (pp->merge_on_device > 0 && nsol >= kDeviceRefineMin)
                          ? pp->merge_on_device - 1
                          : -1;
-    int rc = lmb_refine_create(rdev, geo, pp, hkls, nh, &rf);
+    RefineKey key;
+    int rc = refine_checkout(rdev, geo, pp, hkls, nh, &key, &rf);
     std::vector<double> om((size_t)nsol * 9);
     std::vector<int32_t> im((size_t)nsol, 0);
     for (int it = 0; it < nsol; it++)
@@ -666,7 +754,12 @@ extern "C" int lmb_post_process(const lmb_geometry *geo, const lmb_post_params *
       nm_ov.resize((size_t)nsol);
       rc = lmb_refine_fit(rf, 1, kFitMaxEval, 0.0, nm_x.data(), nm_ov.data(), nullptr);
     }
-    lmb_refine_destroy(rf);
+    if (!rc) {
+      t_post_refine.device = rdev;
+      rc = lmb_refine_last_stats(rf, &t_post_refine.points, &t_post_refine.rounds,
+                                 &t_post_refine.kernel_ms);
+    }
+    refine_return(std::move(key), rf, rc == LMB_OK);
     if (rc) return rc;
   }
   std::vector<GrainOut> go(nsol);

@@ -106,12 +106,24 @@ class Engine:
     TUNING_FIELDS = ("variant", "tile_sub", "stages", "consumers", "blocks_per_sm", "grid_mult",
                      "full_gather")
 
-    def set_tuning(self, **kw) -> None:
-        vals = (C.c_int32 * 7)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS])
+    def set_tuning(self, test_consumer_wait_us: int = 0, cell_consumers: int = 0,
+                   cell_stages: int = 0, **kw) -> None:
+        """Pin the compare pass's launch shape (TUNING_FIELDS; variant 3 =
+        automatic when not given; cell_consumers / cell_stages shape the
+        cell-mask pass when the automatic variant picks it).
+        test_consumer_wait_us is for tests only: the pass gives up after that
+        wait and reports a timeout."""
+        check(lib().lmb_engine_set_tuning(
+            self._h, self._tuning_vals(kw, test_consumer_wait_us, cell_consumers, cell_stages),
+            10))
+        self._pinned_shape = True
+
+    def _tuning_vals(self, kw, test_wait=0, cell_consumers=0, cell_stages=0):
+        vals = (C.c_int32 * 10)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS],
+                                int(test_wait), int(cell_consumers), int(cell_stages))
         if "variant" not in kw:
             vals[0] = 3
-        check(lib().lmb_engine_set_tuning(self._h, vals, 7))
-        self._pinned_shape = True
+        return vals
 
     def set_sparse_uploads(self, enable: bool) -> None:
         check(lib().lmb_engine_set_sparse_uploads(self._h, int(bool(enable))))
@@ -152,17 +164,28 @@ class Engine:
         self.n_orient = om.shape[0]
 
     def build_db_synthetic(self, seed: int, n: int, hkls: np.ndarray,
-                           return_orients: bool = False):
+                           return_orients: bool = False, hex_fz: bool = False):
+        """DB of n device-generated uniform rotations (seeded); ``hex_fz``
+        reduces them to the hexagonal fundamental zone first."""
         hk = np.ascontiguousarray(hkls, dtype=np.int32).reshape(-1, 3)
         out = np.empty((n, 9), np.float64) if return_orients else None
-        check(lib().lmb_db_build_synthetic(self._h, int(seed), int(n), hk.ctypes.data,
-                                           hk.shape[0], out.ctypes.data if out is not None else None))
+        flags = _lib.LMB_BUILD_SYNTH_HEX_FZ if hex_fz else 0
+        check(lib().lmb_db_build_synthetic_ex(self._h, int(seed), int(n), hk.ctypes.data,
+                                              hk.shape[0],
+                                              out.ctypes.data if out is not None else None, flags))
         self.n_orient = n
+        self._synth_flags = flags
         return out
 
-    def synth_orientations(self, seed: int, first: int, n: int) -> np.ndarray:
+    def synth_orientations(self, seed: int, first: int, n: int,
+                           hex_fz: bool | None = None) -> np.ndarray:
+        """Matrices of the synthetic generator (those of the last synthetic
+        build unless ``hex_fz`` says otherwise)."""
+        flags = getattr(self, "_synth_flags", 0) if hex_fz is None else \
+            (_lib.LMB_BUILD_SYNTH_HEX_FZ if hex_fz else 0)
         out = np.empty((n, 9), np.float64)
-        check(lib().lmb_synth_orientations(self._h, int(seed), int(first), int(n), out.ctypes.data))
+        check(lib().lmb_synth_orientations_ex(self._h, int(seed), int(first), int(n),
+                                              out.ctypes.data, flags))
         return out
 
     def download_db(self, first: int = 0, count: int | None = None) -> np.ndarray:
@@ -225,9 +248,11 @@ class Engine:
         b = batch_bucket(k)
         if b != self._shape_bucket:
             shape = lookup(self.R, b)
+            dense = lookup(self.R, b, dense=True) or {}
             if shape:
-                vals = (C.c_int32 * 7)(*[int(shape.get(f, 0)) for f in self.TUNING_FIELDS])
-                check(lib().lmb_engine_set_tuning(self._h, vals, 7))
+                check(lib().lmb_engine_set_tuning(
+                    self._h, self._tuning_vals(shape, 0, dense.get("consumers", 0),
+                                               dense.get("stages", 0)), 10))
             self._shape_bucket = b
 
     def match(self, slots, min_nr_spots: int, min_intensity: float, value_mode: int = 0) -> None:

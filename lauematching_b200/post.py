@@ -88,6 +88,16 @@ def post_process(params: LaueParams, geometry, orients: np.ndarray, ids: np.ndar
     return sol, spt, n_unique
 
 
+def last_refine_stats() -> dict:
+    """What this thread's last post_process refined: ``device`` -2 (nothing),
+    -1 (host threads) or the device ordinal; points, rounds and the
+    objective kernel's time."""
+    d, pts, rnd, km = C.c_int32(0), C.c_int64(0), C.c_int32(0), C.c_float(0)
+    check(lib().lmb_post_last_refine_stats(C.byref(d), C.byref(pts), C.byref(rnd), C.byref(km)))
+    return {"device": d.value, "points": pts.value, "rounds": rnd.value,
+            "kernel_ms": float(km.value)}
+
+
 def collected_matches(survivors, n_pass: int):
     """(ids, scores) as the reference hands them to the merge: survivors in
     ascending ID, followed by one (0, 0.0) entry for each orientation that

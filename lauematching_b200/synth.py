@@ -50,9 +50,13 @@ def uniform_u01(seed: int, counters: np.ndarray) -> np.ndarray:
     return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
-def shoemake_orientations(n: int, seed: int, start: int = 0) -> np.ndarray:
-    """(n, 9) float64 row-major rotation matrices for IDs start..start+n-1."""
-    ids = np.arange(start, start + n, dtype=np.uint64)
+def shoemake_orientations(n: int, seed: int, start: int = 0, ids=None) -> np.ndarray:
+    """(n, 9) float64 row-major rotation matrices for IDs start..start+n-1 (or
+    for the given ``ids``).  The device generator draws the same uniforms; its
+    sines and cosines may differ from numpy's in the last bit."""
+    ids = np.arange(start, start + n, dtype=np.uint64) if ids is None else \
+        np.asarray(ids, dtype=np.uint64)
+    n = ids.shape[0]
     u1 = uniform_u01(seed, ids * np.uint64(3) + np.uint64(0))
     u2 = uniform_u01(seed, ids * np.uint64(3) + np.uint64(1))
     u3 = uniform_u01(seed, ids * np.uint64(3) + np.uint64(2))

@@ -136,12 +136,13 @@ def test_input_dtypes_f32_u8_match_f64():
         assert np.array_equal(r[0][0], r[k][0]) and r[0][1] == r[k][1]
 
 
-@pytest.mark.parametrize("variant,full_gather", [(1, 0), (1, 1), (2, 0), (2, 1)])
+@pytest.mark.parametrize("variant,full_gather", [(1, 0), (1, 1), (2, 0), (2, 1), (4, 0), (4, 1)])
 def test_edge_records_partial_tiles_and_thresholds(variant, full_gather):
     """Counts above S (clamped), pixels off the detector (skipped), DB sizes
     that are not a multiple of the tile, MinNrSpots <= 0 and > S; in the
-    reference layout (variant 1) and the compact one (variant 2), with and
-    without skipping records that have fewer spots than MinNrSpots."""
+    reference layout (variant 1), the compact one (variant 2) and the compact
+    one filtered by the cell mask (variant 4), with and without skipping
+    records that have fewer spots than MinNrSpots."""
     rng = np.random.default_rng(1)
     txt = synth.params_text(nr_px=(300, 200), max_nr_spots=7, min_nr_spots=2,
                             min_intensity=3.0)
@@ -164,15 +165,17 @@ def test_edge_records_partial_tiles_and_thresholds(variant, full_gather):
                 ref = O.compare(rec, 7, img, 300, 200, ms, mi)
                 assert npass == ref.n_pass, (n, ms, mi)
                 assert_same_survivors(got, ref)
-            if variant == 2 and n:
+            if variant in (2, 4) and n:
                 assert e.layout_info()["compact"] == 1
+                assert e.get_tuning()["last_variant"] == variant
 
 
 @pytest.mark.parametrize("name", golden_names())
 def test_automatic_variant_follows_the_spots_that_can_pass(name):
     """The default (automatic) variant runs the compact layout while the
-    records that can pass hold at most 3 spots per DB record, the reference
-    records otherwise; both give the oracle's survivors."""
+    records that can pass hold at most 3 spots per DB record, the compact
+    layout filtered by the frames' cell mask otherwise; both give the
+    oracle's survivors."""
     c = golden_case(name)
     p = c.params
     cnt = np.minimum(c.records[:, 0], p.max_nr_spots).astype(np.int64)  # all on the detector
@@ -186,14 +189,16 @@ def test_automatic_variant_follows_the_spots_that_can_pass(name):
         got, npass = e.results(1)
         used = e.get_tuning()
     assert used["variant"] == 3
-    assert used["last_variant"] == (2 if gathered <= 3.0 else 1), gathered
+    assert used["last_variant"] == (2 if gathered <= 3.0 else 4), gathered
     assert npass == ref.n_pass
     assert_same_survivors(got, ref)
 
 
-def test_many_spots_per_record_keep_the_reference_layout():
+@pytest.mark.parametrize("variant", [2, 3, 4])
+def test_many_spots_per_record_keep_the_reference_layout(variant):
     """MaxNrLaueSpots above 255 (uint8 counts cannot hold it): a pass asked for
-    the compact layout runs over the reference records and matches the oracle."""
+    the compact layout (alone, automatic or with the cell mask) runs over the
+    reference records and matches the oracle."""
     rng = np.random.default_rng(3)
     S = 300
     txt = synth.params_text(nr_px=(256, 256), max_nr_spots=S, min_nr_spots=20,
@@ -207,12 +212,13 @@ def test_many_spots_per_record_keep_the_reference_layout():
     img = np.where(rng.random(256 * 256) < 0.2, rng.integers(1, 256, 256 * 256), 0).astype(np.float64)
     ref = O.compare(rec, S, img, 256, 256, p.min_nr_spots, p.min_intensity)
     with engine_for(p) as e:
-        e.set_tuning(variant=2)
+        e.set_tuning(variant=variant)
         e.upload_db(rec)
         e.load_image(0, img)
         e.match([0], p.min_nr_spots, p.min_intensity)
         got, npass = e.results(0)
         assert e.layout_info()["compact"] == -1
+        assert e.get_tuning()["last_variant"] == 1
     assert npass == ref.n_pass
     assert_same_survivors(got, ref)
 
@@ -236,6 +242,77 @@ def test_compact_layout_matches_oracle(name, mode):
     assert info["compact"] == 1 and 0 < info["bytes"]
     assert npass == ref.n_pass
     assert_same_survivors(got, ref)
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("mode", [0, 1])
+def test_cell_mask_pass_matches_oracle(name, mode):
+    """Variant 4 (compact layout filtered by the cell mask of the pass's
+    frames) on the reference's golden cases.  A frame in a slot outside the
+    pass, positive everywhere, must not widen or change anything: the mask is
+    built from the pass's slots."""
+    c = golden_case(name)
+    p = c.params
+    ref = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                    p.min_nr_spots, p.min_intensity, mode=mode)
+    ref2 = O.compare(c.records, p.max_nr_spots, c.image * 0.5, p.nr_px_x, p.nr_px_y,
+                     p.min_nr_spots, p.min_intensity, mode=mode)
+    with engine_for(p) as e:
+        e.set_tuning(variant=4)
+        e.upload_db(c.records)
+        e.load_image(5, c.image, keep_f64=(mode == 1))
+        e.load_image(6, c.image * 0.5, keep_f64=(mode == 1))
+        e.load_image(9, np.full(p.nr_px_x * p.nr_px_y, 7.0), keep_f64=(mode == 1))
+        for _ in range(2):  # eager pass, then the graph replay
+            e.match([5, 6], p.min_nr_spots, p.min_intensity, value_mode=mode)
+            got, npass = e.results(5)
+            got2, npass2 = e.results(6)
+            assert e.get_tuning()["last_variant"] == 4
+            assert npass == ref.n_pass and npass2 == ref2.n_pass
+            assert_same_survivors(got, ref)
+            assert_same_survivors(got2, ref2)
+
+
+@pytest.mark.parametrize("nr_px", [(1100, 1001), (2048, 2048), (1024, 1024)])
+def test_cell_mask_cells_and_detector_sizes(nr_px):
+    """Cell masks of 2^shift-pixel cells (shift 0 for 1024^2, 1 with a
+    partial last cell for 1100x1001, 2 for 2048^2) on dense random records
+    and frames of a few percent positive pixels: the oracle's survivors, for
+    MinNrSpots from 1 to above the records' spot counts."""
+    rng = np.random.default_rng(11)
+    W, H = nr_px
+    S = 30
+    txt = synth.params_text(nr_px=(W, H), max_nr_spots=S, min_nr_spots=3, min_intensity=5.0)
+    p = P.parse_params_text(txt)
+    n = 40000
+    rec = np.zeros((n, 1 + 2 * S), np.uint16)
+    rec[:, 0] = rng.integers(8, 25, n)
+    rec[:, 1::2] = rng.integers(0, W, (n, S))
+    rec[:, 2::2] = rng.integers(0, H, (n, S))
+    # frames: positive pixels around the spots of a few records (so records
+    # match) plus scattered singles, the last pixel of the detector included
+    imgs = []
+    for k in range(3):
+        img = np.zeros(W * H)
+        img[rng.integers(0, W * H, W * H // 40)] = rng.integers(1, 256, W * H // 40)
+        for r in rng.integers(0, n, 30):
+            c = int(rec[r, 0])
+            img[rec[r, 2:2 + 2 * c:2].astype(np.int64) * W + rec[r, 1:1 + 2 * c:2]] = 200.0
+        img[-1] = 99.0
+        imgs.append(img)
+    with engine_for(p) as e:
+        e.set_tuning(variant=4)
+        e.upload_db(rec)
+        for k in range(3):
+            e.load_image(k, imgs[k])
+        for ms in (1, 3, 6, 24, 30):
+            e.match([0, 1, 2], ms, 5.0)
+            assert e.get_tuning()["last_variant"] == 4
+            for k in range(3):
+                got, npass = e.results(k)
+                ref = O.compare(rec, S, imgs[k], W, H, ms, 5.0)
+                assert npass == ref.n_pass, (ms, k)
+                assert_same_survivors(got, ref)
 
 
 @pytest.mark.parametrize("nb", [7, 8])
@@ -283,6 +360,15 @@ def test_compact_layout_batched_equals_reference_layout():
             e.set_tuning(variant=2, **shape)
             e.match(range(12), p.min_nr_spots, p.min_intensity)
             got = e.results_batch(range(12))
+            for k in range(12):
+                assert got[k][1] == ref[k][1] and np.array_equal(got[k][0], ref[k][0])
+        # the cell-mask pass (variant 4) under several shapes
+        for shape in ({}, {"consumers": 4}, {"consumers": 16, "stages": 2}, {"stages": 3},
+                      {"full_gather": 1}, {"consumers": 1}):
+            e.set_tuning(variant=4, **shape)
+            e.match(range(12), p.min_nr_spots, p.min_intensity)
+            got = e.results_batch(range(12))
+            assert e.get_tuning()["last_variant"] == 4
             for k in range(12):
                 assert got[k][1] == ref[k][1] and np.array_equal(got[k][0], ref[k][0])
         assert e.layout_info()["compact"] == 1
@@ -513,3 +599,61 @@ def test_errors_are_reported_not_silent():
             e.match([3], 5, 1.0)  # slot 3 holds no image
         with pytest.raises(LmbError):
             e.load_image(64, c.image)
+
+
+def test_hexagonal_fundamental_zone_db_build():
+    """Synthetic DB restricted to the hexagonal fundamental zone: each device
+    rotation is the host reduction (synth.hexagonal_fundamental_zone) of the
+    plain generator's rotation with the same ID, to rounding; it is one of
+    the 12 equivalents of that rotation; and the records built from the zone
+    rotations equal the oracle's forward simulation of them, byte for byte
+    (hexagonal SG 194, 7790 HKLs)."""
+    txt = synth.params_text(lattice=(0.295, 0.295, 0.468, 90, 90, 120), space_group=194,
+                            max_nr_spots=30, min_nr_spots=5)
+    p = P.parse_params_text(txt)
+    hk = synth.hkls_hexagonal(10)
+    n = 20000
+    with engine_for(p) as e:
+        om_fz = e.build_db_synthetic(seed=3, n=n, hkls=hk, return_orients=True, hex_fz=True)
+        rec = e.download_db()
+        assert np.array_equal(e.synth_orientations(3, 0, n), om_fz)
+        plain = e.synth_orientations(3, 0, n, hex_fz=False)
+    host = synth.hexagonal_fundamental_zone(plain)
+    assert np.max(np.abs(host - om_fz)) < 1e-12
+    # an equivalent rotation: R_fz = R_plain . S for a symmetry operator S
+    m_fz, m_pl = om_fz.reshape(-1, 3, 3), plain.reshape(-1, 3, 3)
+    rel = np.einsum("nji,njk->nik", m_pl, m_fz)  # R_plain^T R_fz
+    tr = np.clip((np.trace(rel, axis1=1, axis2=2) - 1) / 2, -1, 1)
+    ang = np.degrees(np.arccos(tr))
+    assert np.all(np.min(np.abs(ang[:, None] - np.array([0, 60, 120, 180])[None]), 1) < 1e-3)
+    assert np.array_equal(rec, O.forward(p, om_fz, hk))
+
+
+@pytest.mark.parametrize("variant", [2, 4])
+def test_a_consumer_wait_that_runs_out_reports_a_timeout(variant):
+    """The compare pass's waits are bounded.  A test wait (1 ms on a barrier
+    nothing arrives at) makes the consumers give up; the producer's own wait
+    for a free ring slot then runs out after its full bound and it waits for
+    its own copies before returning.  The pass reports LMB_ERR_TIMEOUT (and
+    keeps reporting it: the device error word is sticky), and the device
+    stays usable: a new engine on it matches the oracle."""
+    from lauematching_b200._lib import TimeoutError_
+    c = golden_case("tilted_fcc")
+    p = c.params
+    ref = O.compare(c.records, p.max_nr_spots, c.image, p.nr_px_x, p.nr_px_y,
+                    p.min_nr_spots, p.min_intensity)
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        e.load_image(0, c.image)
+        e.set_tuning(variant=variant, test_consumer_wait_us=1000)
+        e.match([0], p.min_nr_spots, p.min_intensity)
+        with pytest.raises(TimeoutError_):
+            e.results(0)
+        assert e.get_tuning()["last_variant"] == variant
+    with engine_for(p) as e:
+        e.upload_db(c.records)
+        e.load_image(0, c.image)
+        e.match([0], p.min_nr_spots, p.min_intensity)
+        got, npass = e.results(0)
+    assert npass == ref.n_pass
+    assert_same_survivors(got, ref)

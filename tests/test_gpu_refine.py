@@ -137,7 +137,17 @@ def test_post_stage_refines_many_grains_on_the_device_with_the_host_text():
     img = frames[0].ravel()
     host = post.post_process(p, geo, om_c, ids, sc, img, c.hkls, num_threads=8,
                              optimizer="nelder-mead")
+    st_host = post.last_refine_stats()
     dev = post.post_process(p, geo, om_c, ids, sc, img, c.hkls, num_threads=8,
                             optimizer="nelder-mead", merge_device=0)
+    st_dev = post.last_refine_stats()
     assert host[2] >= 2048
     assert dev == host
+    # the device path ran on the merge device, the host one on host threads
+    assert st_host["device"] == -1 and st_host["kernel_ms"] == 0.0
+    assert st_dev["device"] == 0 and st_dev["rounds"] > 0 and st_dev["kernel_ms"] > 0.0
+    assert st_dev["points"] == st_host["points"] > 0
+    # a second image reuses the post-stage's refinement handle: same text
+    dev2 = post.post_process(p, geo, om_c, ids, sc, img, c.hkls, num_threads=8,
+                             optimizer="nelder-mead", merge_device=0)
+    assert dev2 == host and post.last_refine_stats()["device"] == 0

@@ -217,3 +217,34 @@ def test_stream_raw_frames_preprocessed_on_the_device(tmp_path):
         n_lines += len(es)
     assert 30 + len(raws) - 1 not in sol
     assert n_lines > 0
+
+
+@pytest.mark.parametrize("name", ["tilted_fcc", "tilted_dense", "tilted_hex"])
+def test_stream_lines_are_the_reference_binarys_lines_with_the_image_number(name, tmp_path):
+    """With MinGoodSpots equal to MinNrSpots (the batch executables gate the
+    written grains by MinNrSpots, LaueMatchingCPU.c:809; the daemon by
+    MinGoodSpots, LaueMatchingGPUStream.cu:1173), the daemon's lines for a
+    golden frame sent in the reference's message are the reference binary's
+    own solutions/spots lines for that frame (tests/golden, written by
+    LaueMatchingCPU) with the image number as the first column
+    (LaueMatchingHeaders.h:1070-1071,1132-1133,888-899)."""
+    c = golden_case(name)
+    txt = "".join(ln for ln in c.params_text.splitlines(keepends=True)
+                  if not ln.startswith("ForwardFile"))
+    p = P.parse_params_text(txt + f"MinGoodSpots {c.params.min_nr_spots}\n", binary="stream")
+    ports = _ports()
+    srv = _server([p], c.orients, c.hkls, tmp_path, 64, ports)
+    try:
+        time.sleep(0.3)
+        _send(ports[0], [(7, c.image.astype(np.float32)), (9, c.image.astype(np.float32))])
+        _wait_done(srv, 2)
+    finally:
+        srv.stop()
+    sol = _lines_by_image(str(tmp_path / "solutions.txt"))
+    spt = _lines_by_image(str(tmp_path / "spots.txt"))
+    want_sol = c.cmp_solutions.splitlines()[1:]
+    want_spt = c.cmp_spots.splitlines()[1:]
+    assert want_sol and want_spt
+    for num in (7, 9):
+        assert sol[num] == [f"{num}\t{ln}" for ln in want_sol]
+        assert spt[num] == [f"{num}\t{ln}" for ln in want_spt]

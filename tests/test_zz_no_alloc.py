@@ -53,6 +53,11 @@ def _order_on_device(unsorted):
     return d_out.cpu().numpy().view(SURVIVOR_DTYPE)
 
 
+def _expected_order(lst):
+    """Ascending id, ties by position in the unsorted list."""
+    return lst[np.lexsort((np.arange(lst.shape[0]), lst["id"]))]
+
+
 def test_noalloc_order_equals_engine_order_twice():
     ref = _engine_survivors()
     assert ref.shape[0] > 8192  # large enough for the scratch array
@@ -74,3 +79,35 @@ def test_noalloc_order_small_list_and_limits():
     assert rc == LMB_ERR_INVALID
     assert b"LMB_NOALLOC_ORDER_MAX" in lib().lmb_last_error()
     assert lib().lmb_order_survivors_noalloc(None, 0, None, None) == 0
+
+
+def test_noalloc_order_of_ids_beyond_40_bits():
+    """Ids of 2^40 and above (which a packed id << 24 key cannot hold) and
+    repeated ids are still ordered by (id, position), in shared memory and
+    in the scratch array."""
+    base = _engine_survivors()
+    rng = np.random.default_rng(8)
+    for n in (2500, 20000):
+        lst = base[rng.permutation(base.shape[0])[:n]].copy()
+        lst["id"][::3] += np.uint64(1) << np.uint64(41)
+        lst["id"][1::7] = lst["id"][0]
+        for _ in range(2):
+            got = _order_on_device(lst)
+            assert np.array_equal(got.view(np.uint8), _expected_order(lst).view(np.uint8))
+
+
+def test_noalloc_order_rejects_overlapping_buffers():
+    """The output may not overlap the input at all (the last step reads the
+    input while writing the output): equal, partly overlapping either way."""
+    import torch
+    n = 100
+    buf = torch.zeros(3 * n * SURVIVOR_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    b = buf.data_ptr()
+    sz = SURVIVOR_DTYPE.itemsize
+    for d_in, d_out in ((b, b), (b, b + 10 * sz), (b + 10 * sz, b), (b, b + (n - 1) * sz)):
+        rc = lib().lmb_order_survivors_noalloc(C.c_void_p(d_in), n, C.c_void_p(d_out), None)
+        assert rc == LMB_ERR_INVALID
+        assert b"overlap" in lib().lmb_last_error()
+    # adjacent ranges are fine
+    check(lib().lmb_order_survivors_noalloc(C.c_void_p(b), n, C.c_void_p(b + n * sz), None))
+    torch.cuda.synchronize()
