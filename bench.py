@@ -192,89 +192,157 @@ def dbbuild_parity_sample(e, p, hkls, seed, n_orient, per_block=20000, blocks=5)
     return {"sampled_orientations": total, "records_differing": mism}
 
 
-def survivor_parity(e, p, img_u8, n_sample=2_000_000):
-    """This run's survivors of one bench image against the oracle on the DB's
-    first n_sample records: ids, spot counts, uint8 sums and the FP64
-    intensity sums and scores bit for bit.  Returns (summary, our survivors
-    over the whole DB) -- the reference's own count is checked in
-    cpu_baseline."""
+def _same_fields(sub, want):
+    return (np.array_equal(sub["id"], want.ids.astype(np.uint64))
+            and np.array_equal(sub["n_spots"], want.n_spots)
+            and np.array_equal(sub["sum_u8"], want.sum_u8)
+            and np.array_equal(sub["tot_int"].view(np.uint64), want.tot_int.view(np.uint64))
+            and np.array_equal(sub["score"].view(np.uint64), want.score.view(np.uint64)))
+
+
+def survivor_parity(e, p, img_u8, n_sample=None, chunk=4_000_000, sink=None):
+    """This run's survivors of one bench image against the oracle over the
+    DB's first n_sample records (all of them by default), chunk by chunk:
+    ids, spot counts, uint8 sums and the FP64 intensity sums and scores bit
+    for bit.  ``sink(first, records)`` also receives every chunk of records
+    (to write the reference's input files from the same pass).  Returns
+    (summary, our survivors over the whole DB, n_pass)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     e.load_image(0, img_u8, want_scale=False)
     e.match([0], p.min_nr_spots, p.min_intensity)
     ours, npass = e.results(0)
-    n_sample = min(n_sample, e.n_orient)
-    want = O.compare(e.download_db(0, n_sample), p.max_nr_spots, img_u8.astype(np.float64),
-                     p.nr_px_x, p.nr_px_y, p.min_nr_spots, p.min_intensity,
-                     nthreads=os.cpu_count() or 1)
-    sub = ours[ours["id"] < n_sample]
-    same = (np.array_equal(sub["id"], want.ids.astype(np.uint64))
-            and np.array_equal(sub["n_spots"], want.n_spots)
-            and np.array_equal(sub["sum_u8"], want.sum_u8)
-            and np.array_equal(sub["tot_int"].view(np.uint64), want.tot_int.view(np.uint64))
-            and np.array_equal(sub["score"].view(np.uint64), want.score.view(np.uint64)))
-    return {"records": n_sample, "survivors": int(sub.shape[0]),
-            "oracle_survivors": int(want.ids.shape[0]), "identical": bool(same)}, ours
+    n_sample = min(n_sample or e.n_orient, e.n_orient)
+    img = img_u8.astype(np.float64)
+    same, n_want, n_got, t_or = True, 0, 0, 0.0
+    for first in range(0, n_sample, chunk):
+        cnt = min(chunk, n_sample - first)
+        rec = e.download_db(first, cnt)
+        if sink is not None:
+            sink(first, rec)
+        t0 = time.perf_counter()
+        want = O.compare(rec, p.max_nr_spots, img, p.nr_px_x, p.nr_px_y, p.min_nr_spots,
+                         p.min_intensity, nthreads=os.cpu_count() or 1)
+        t_or += time.perf_counter() - t0
+        want.ids = want.ids.astype(np.uint64) + np.uint64(first)
+        sub = ours[(ours["id"] >= first) & (ours["id"] < first + cnt)]
+        same = same and _same_fields(sub, want)
+        n_want += int(want.ids.shape[0])
+        n_got += int(sub.shape[0])
+    return {"records": n_sample, "survivors": n_got, "oracle_survivors": n_want,
+            "identical": bool(same and n_got == n_want), "oracle_seconds": round(t_or, 2),
+            "oracle_threads": os.cpu_count() or 1}, ours, npass
 
 
-def cpu_baseline(e, p, txt, hkls, img_u8, seed, n_sample, runs=3, ours=None):
-    """The reference LaueMatchingCPU (or the oracle port) on a bounded sample;
-    with ``ours`` (this run's survivors of the same image over the whole DB),
-    the reference's "Initial solutions" count on the sample is compared with
-    ours over the same records."""
+def full_db_parity_and_cpu_baseline(e, p, txt, hkls, img_u8, seed, cpu=True, parity=True):
+    """One bench image over the whole device DB, three ways:
+
+    * our survivors against the oracle on every record (survivor_parity);
+    * the reference's own LaueMatchingCPU (DoFwd 0, all host cores) on the
+      same DB written as its ForwardFile (the device build is byte-identical
+      to the reference's cache) and the orientations as its orientation
+      file: its compare stage, unscaled, is the CPU baseline;
+    * its "Initial solutions" count and its solutions.txt / spots.txt
+      against this library's post-stage on our survivors, byte for byte.
+
+    Needs the DB files on the host (194 B per orientation, /dev/shm when it
+    has room so the reference memory-maps them); a host too small for the
+    whole DB gets the largest prefix that fits, and the records field says
+    so."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from lauematching_b200 import formats
-    n_sample = min(n_sample, e.n_orient)
-    cores = os.cpu_count() or 1
-    rec = e.download_db(0, n_sample)
-    img = img_u8.astype(np.float64)
-    if O.have_ref():
-        base = scratch_dir(n_sample * (REC_BYTES_PER_ORIENT + 72))
-        wd = tempfile.mkdtemp(prefix="lmb_cpu_", dir=base)
-        fwd = os.path.join(wd, "fwd.bin")
-        rec.tofile(fwd)
-        om = e.synth_orientations(seed, 0, n_sample)
-        pp = os.path.join(wd, "params.txt")
+    from lauematching_b200 import formats, post
+    n = e.n_orient
+    per = REC_BYTES_PER_ORIENT + 72
+    base = scratch_dir(n * per)
+    if base is None:
+        import psutil
+        n = int(min(n, psutil.virtual_memory().available * 0.4 // per))
+    have_ref = cpu and O.have_ref() and n > 0
+    wd = tempfile.mkdtemp(prefix="lmb_full_", dir=base)
+    fwd, op = os.path.join(wd, "fwd.bin"), os.path.join(wd, "orients.bin")
+    files = {}
+    if have_ref:
+        files = {"fwd": open(fwd, "wb"), "om": open(op, "wb")}
+
+    def sink(first, rec):
+        if files:
+            rec.tofile(files["fwd"])
+            e.synth_orientations(seed, first, rec.shape[0]).tofile(files["om"])
+    out = {}
+    try:
+        t0 = time.perf_counter()
+        par, ours, npass = survivor_parity(e, p, img_u8, n_sample=n, sink=sink)
+        if parity:
+            out["survivor_parity"] = par
+        for f in files.values():
+            f.close()
+        t_write = time.perf_counter() - t0
+        if not have_ref:
+            return out
+        hp, ip, pp = (os.path.join(wd, x) for x in ("hkls.csv", "image.bin", "params.txt"))
+        formats.write_hkls(hp, hkls)
+        img = img_u8.astype(np.float64)
+        formats.write_image_bin(ip, img)
         with open(pp, "w") as f:
             f.write(txt + f"ForwardFile {fwd}\nDoFwd 0\n")
-        op = os.path.join(wd, "orients.bin")
-        formats.write_orientations(op, om)
-        hp = os.path.join(wd, "hkls.csv")
-        formats.write_hkls(hp, hkls)
-        ip = os.path.join(wd, "image.bin")
-        formats.write_image_bin(ip, img)
-        times, walls = [], []
-        for _ in range(runs):
-            r = O.run_reference(pp, op, hp, ip, ncpus=cores)
-            if r.returncode != 0 or r.compare_seconds is None:
-                raise RuntimeError("reference run failed: " + r.stdout[-500:] + r.stderr[-500:])
-            times.append(r.compare_seconds)
-            walls.append(r.wall_seconds)
-        t = statistics.median(times)
-        ref_initial = r.initial_solutions
+        cores = os.cpu_count() or 1
+        r = O.run_reference(pp, op, hp, ip, ncpus=cores)
+        if r.returncode != 0 or r.compare_seconds is None:
+            raise RuntimeError("reference run failed: " + r.stdout[-500:] + r.stderr[-500:])
+        sub = ours[ours["id"] < n]
+        ids, sc = post.collected_matches(sub, sub.shape[0] if n < e.n_orient else npass)
+        om = np.memmap(op, dtype=np.float64, mode="r").reshape(-1, 9)
+        sol, spt, _ = post.post_process(p, e.geometry, om, ids, sc, img.astype(np.float32),
+                                        hkls, num_threads=cores, merge_device=e.device)
+        del om
+        same_sol = r.solutions == post.SOLUTIONS_HEADER + sol
+        same_spt = r.spots == post.SPOTS_HEADER + spt
+        out["cpu_baseline"] = {
+            "value": 1.0 / r.compare_seconds * (n / 1e8), "unit": UNIT, "cores": cores,
+            "kind": "reference",
+            "sample": f"LaueMatchingCPU (reference source, gcc -O3 -fopenmp, NLopt stand-in) "
+                      f"DoFwd 0, one bench image against {n:,} records (the device-built DB "
+                      f"written as its ForwardFile{' in /dev/shm' if base else ''}): compare "
+                      f"stage {r.compare_seconds:.3f} s"
+                      + ("" if n == e.n_orient else f", scaled x{1e8 / n:g} to 1e8")
+                      + f"; whole process {r.wall_seconds:.2f} s"}
+        out["reference_full_db"] = {
+            "records": n, "initial_solutions": {"reference": r.initial_solutions,
+                                                "ours": int(sub.shape[0]),
+                                                "identical": r.initial_solutions == sub.shape[0]},
+            "unique_orientations": r.unique,
+            "solutions_txt_identical": bool(same_sol), "spots_txt_identical": bool(same_spt),
+            "files_written_s": round(t_write, 1)}
+        # the reference's plain single-image GPU executable (LaueMatchingGPU.cu,
+        # sm_100a build) on the same files: one process, the DB streamed to the
+        # device in <= 4 GB chunks, its one-thread-per-orientation kernel
+        if O.have_ref_gpu():
+            env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+            rg = O.run_reference_gpu(pp, op, hp, ip, ncpus=cores, env=env)
+            if rg.returncode == 0 and rg.chunks:
+                k_s = sum(k for _, k in rg.chunks)
+                out["reference_gpu"] = {
+                    "binary": "oracle/_ref/LaueMatchingGPU (reference source, nvcc -O3 -w "
+                              "-rdc=true sm_100a, NLopt stand-in)",
+                    "records": n, "kernel_s_per_image": round(k_s, 5),
+                    "kernel_images_per_s": round(1.0 / k_s, 2) if k_s > 0 else None,
+                    "kernel_time_resolution_s": 0.001,
+                    "match_stage_s_per_image": rg.match_seconds,
+                    "match_stage_images_per_s": round(1.0 / rg.match_seconds, 3)
+                    if rg.match_seconds else None,
+                    "forward_read_s": rg.read_seconds, "chunks_h2d_kernel_s": rg.chunks,
+                    "process_wall_s": round(rg.wall_seconds, 2),
+                    "nr_matches": rg.n_matches, "n_pass_ours": int(npass)}
+            else:
+                out["reference_gpu"] = {"failed": (rg.stderr or rg.stdout)[-300:]}
+        return out
+    finally:
+        for f in files.values():
+            f.close()
         for fn in os.listdir(wd):
             os.remove(os.path.join(wd, fn))
         os.rmdir(wd)
-        per_image = t * (1e8 / n_sample)
-        res = {"value": 1.0 / per_image, "unit": UNIT, "cores": cores, "kind": "reference",
-               "sample": f"LaueMatchingCPU DoFwd 0 compare stage on {n_sample} of the DB's "
-                         f"records (1 image), median of {runs} runs = {t:.4f} s, scaled x"
-                         f"{1e8 / n_sample:g} to the 1e8-orientation DB; whole-process wall "
-                         f"{statistics.median(walls):.2f} s per run"}
-        if ours is not None:
-            mine = int((ours["id"] < n_sample).sum())
-            res["initial_solutions"] = {"reference": ref_initial, "ours": mine,
-                                        "identical": ref_initial == mine}
-        return res
-    t0 = time.perf_counter()
-    for _ in range(runs):
-        O.compare(rec, p.max_nr_spots, img, p.nr_px_x, p.nr_px_y, p.min_nr_spots,
-                  p.min_intensity, nthreads=cores)
-    t = (time.perf_counter() - t0) / runs
-    per_image = t * (1e8 / n_sample)
-    return {"value": 1.0 / per_image, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"oracle compare on {n_sample} records x {runs} runs, scaled to 1e8"}
 
 
 # DRAM bytes (read + write) per orientation of one compare launch, from ncu
@@ -328,6 +396,365 @@ def merge_timing(space_group, max_angle, device, n_base=800, per=12, seed=5):
 # refinement objective sees realistic valid-HKL lists.
 TILTED_P = (0.028745, 0.002788, 0.513115)
 TILTED_R = (-1.20131258, -1.21399082, -1.21881158)
+
+
+def pass_stats(e, slots, p, n):
+    """n passes back to back on the engine stream: mean compare-kernel time
+    (per-pass events, synchronised) and the per-pass time of an unsynchronised
+    stream of passes (CUDA events around the whole stream)."""
+    import torch
+    stream = torch.cuda.ExternalStream(e.stream)
+    cmp = []
+    for _ in range(max(3, n // 4)):
+        e.match(slots, p.min_nr_spots, p.min_intensity)
+        cmp.append(e.last_pass_ms()[0])
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(n):
+        e.match(slots, p.min_nr_spots, p.min_intensity)
+    b.record(stream)
+    b.synchronize()
+    return statistics.mean(cmp), a.elapsed_time(b) / n
+
+
+def survivor_lists(e, slots):
+    return {k: e.results(k) for k in slots}
+
+
+def same_survivors(x, y):
+    for k in x:
+        (a, na), (b, nb) = x[k], y[k]
+        if na != nb or a.shape != b.shape:
+            return False
+        for f in ("id", "n_spots", "sum_u8"):
+            if not np.array_equal(a[f], b[f]):
+                return False
+        for f in ("tot_int", "score"):
+            if not np.array_equal(a[f].view(np.uint64), b[f].view(np.uint64)):
+                return False
+    return True
+
+
+def gather_counts(rec, p, imgs, mask_shift):
+    """Per DB record of a sample: spots, spots of the records that can pass
+    (>= MinNrSpots on-detector spots), and the gathers left after the cell
+    mask of the batch (cells of 2^shift consecutive pixels holding a positive
+    pixel of any frame) -- the counts the compare kernels act on."""
+    W, H = p.nr_px_x, p.nr_px_y
+    S = p.max_nr_spots
+    cnt = np.minimum(rec[:, 0].astype(np.int64), S)
+    xs = rec[:, 1::2].astype(np.int64)
+    ys = rec[:, 2::2].astype(np.int64)
+    on = (np.arange(S)[None, :] < cnt[:, None]) & (xs < W) & (ys < H)
+    pix = np.where(on, ys * W + xs, 0)
+    c_on = on.sum(1)
+    pos = np.zeros(W * H, bool)
+    for im in imgs:
+        pos |= np.asarray(im).ravel() > 0
+    cells = np.zeros(((W * H) >> mask_shift) + 1, bool)
+    cells[np.nonzero(pos)[0] >> mask_shift] = True
+    hit = cells[pix >> mask_shift] & on
+    ub = hit.sum(1)
+    need = max(1, p.min_nr_spots)
+    n = rec.shape[0]
+    return {"spots_per_record": round(float(c_on.mean()), 3),
+            "passable_records": round(float((c_on >= need).mean()), 4),
+            "gathers_per_record_unfiltered": round(float(c_on[c_on >= need].sum()) / n, 3),
+            "union_pixel_density": round(float(pos.mean()), 4),
+            "cell_mask_shift": int(mask_shift),
+            "cell_density": round(float(cells[:-1].mean()), 4),
+            "records_past_cell_mask": round(float((ub >= need).mean()), 4),
+            "gathers_per_record_cell_mask": round(float(hit[ub >= need].sum()) / n, 3),
+            "sample_records": int(n)}
+
+
+def tilted_leg(args, dev, K=64, n=None):
+    """The batched pass at the reference's own detector geometry (APS 34-ID-E,
+    simulation/params_sim.txt: tilted 2048^2 detector at ~0.51 m, fcc Ni-like
+    a=3.52 A, 1240 HKLs, 5-30 keV, MaxNrLaueSpots 30, MinNrSpots 5): ~15
+    on-detector spots per record instead of ~1.25, so nearly every record can
+    pass and the image gathers, not the DB stream, decide the pass.  Every
+    variant's survivors are compared; the automatic one is the headline."""
+    from lauematching_b200 import params as P, synth
+    from lauematching_b200.engine import Engine
+    n = n or args.n_orient
+    txt = synth.params_text(p=TILTED_P, r=TILTED_R, max_nr_spots=30, min_nr_spots=5,
+                            min_intensity=args.min_intensity)
+    p = P.parse_params_text(txt)
+    hk = synth.hkls_cubic(8)
+    e = Engine(p, device=dev)
+    try:
+        t0 = time.perf_counter()
+        e.build_db_synthetic(seed=args.seed, n=n, hkls=hk)
+        t_build = time.perf_counter() - t0
+        imgs, rec = make_images(e, p, K, seed=2000)
+        for k in range(K):
+            e.load_image(k, imgs[k], want_scale=False)
+        slots = list(range(K))
+        nsteps = max(5, min(args.steps, 40))
+        out = {"workload": f"{K} uint8 2048x2048 frames (U{{1..20}} fcc grains each) vs a "
+                           f"{n:,}-orientation DB, tilted 34-ID-E detector",
+               "n_orient": n, "batch": K, "min_nr_spots": p.min_nr_spots,
+               "min_intensity": p.min_intensity, "dbbuild_s": round(t_build, 3)}
+        runs = {}
+        ref_surv = None
+        for name, tun in (("auto", None), ("reference_layout", dict(variant=1)),
+                          ("compact_no_mask", dict(variant=2, stages=2, consumers=3,
+                                                   grid_mult=8))):
+            if tun is None:
+                e._pinned_shape = False
+                e._shape_bucket = None
+            else:
+                e.set_tuning(**tun)
+            pass_stats(e, slots, p, 3)
+            cmp_ms, step_ms = pass_stats(e, slots, p, nsteps)
+            sv = survivor_lists(e, slots)
+            if ref_surv is None:
+                ref_surv = sv
+            runs[name] = {"compare_ms": round(cmp_ms, 4), "step_ms": round(step_ms, 4),
+                          "images_per_s": round(K / (step_ms * 1e-3), 1),
+                          "variant": e.get_tuning()["last_variant"],
+                          "identical_to_auto": same_survivors(sv, ref_surv)}
+        lay = e.layout_info()
+        surv = [int(ref_surv[k][0].shape[0]) for k in slots]
+        out["runs"] = runs
+        # the survivor volume downstream of the pass: ordering kernel,
+        # download of the 64 lists, host post-stage (merge on the device from
+        # 1024 candidates, evaluate-once refinement, text) per image
+        e._pinned_shape = False
+        e._shape_bucket = None
+        e.match(slots, p.min_nr_spots, p.min_intensity)
+        order_ms = e.last_pass_ms()[1]
+        t0 = time.perf_counter()
+        res = e.results_batch(slots)
+        t_dl = time.perf_counter() - t0
+        nb = sum(r.nbytes for r, _ in res.values())
+        from lauematching_b200 import post
+        # rows filled for the survivors only (the host generator: the same
+        # rotations as the device's to the last bit or so; this part is timed,
+        # not compared)
+        om_sparse = np.zeros((n, 9))
+        post_ms, uniq = [], []
+        for k in slots[:8]:
+            sv, npass = res[k]
+            u = np.unique(sv["id"]).astype(np.int64)
+            om_sparse[u] = synth.shoemake_orientations(0, args.seed, ids=u)
+            ids, sc = post.collected_matches(sv, npass)
+            t0 = time.perf_counter()
+            _, _, nu = post.post_process(p, e.geometry, om_sparse, ids, sc,
+                                         imgs[k].astype(np.float32), hk,
+                                         num_threads=os.cpu_count() or 1, merge_device=dev)
+            post_ms.append((time.perf_counter() - t0) * 1e3)
+            uniq.append(nu)
+        del om_sparse
+        out["downstream"] = {"order_kernel_ms": round(order_ms, 4),
+                             "results_download_ms": round(t_dl * 1e3, 3),
+                             "results_bytes": int(nb),
+                             "post_stage_ms_per_image_median": round(statistics.median(post_ms), 2),
+                             "post_stage_images": len(post_ms),
+                             "unique_grains_per_image": uniq,
+                             "host_threads": os.cpu_count()}
+        out["survivors_per_image"] = {"min": min(surv), "max": max(surv),
+                                      "mean": statistics.mean(surv)}
+        shift = 0
+        while ((p.nr_px_x * p.nr_px_y) >> shift) > 8 * 131072:
+            shift += 1
+        out["gathers"] = gather_counts(rec, p, imgs, shift)
+        out["compact_layout"] = lay
+        # roofline of the automatic pass: on the reference records (the D6
+        # headline bytes) and on the layout it streams
+        peak, peak_src = hbm_peak()
+        auto = runs["auto"]
+        t = auto["compare_ms"] * 1e-3
+        ref_bytes = n * REC_BYTES_PER_ORIENT + K * p.nr_px_x * p.nr_px_y
+        streamed = (lay["bytes"] + p.nr_px_x * p.nr_px_y * 8) if auto["variant"] in (2, 4) \
+            else ref_bytes
+        out["roofline"] = {"bound": "hbm", "peak": peak, "peak_source": peak_src, "unit": "GB/s",
+                           "reference_layout_bytes": ref_bytes,
+                           "reference_layout_gbs": round(ref_bytes / t / 1e9, 1),
+                           "reference_layout_frac": round(ref_bytes / t / 1e9 / peak, 4),
+                           "streamed_bytes": streamed,
+                           "achieved": round(streamed / t / 1e9, 1),
+                           "frac": round(streamed / t / 1e9 / peak, 4)}
+        if not args.no_parity:
+            out["survivor_parity"] = survivor_parity(e, p, imgs[0])[0]
+    finally:
+        e.close()
+    return out
+
+
+def dbbuild_leg(args, dev):
+    """The device DB build alone: n device-generated orientations (seed 1)
+    forward-simulated with the 1240 fcc HKLs, on the bench's beam-normal
+    detector and on the tilted 34-ID-E detector.  The first build of an
+    engine includes the DB allocation (cudaMalloc of n x 122 B) and the
+    kernels' first launch; the repeated builds run into the allocated DB.
+    Times are synchronised wall time around the whole build call."""
+    import torch
+    from lauematching_b200 import params as P, synth
+    from lauematching_b200.engine import Engine
+    n = args.n_orient
+    hk = synth.hkls_cubic(8)
+    out = {"n_orient": n, "hkls": int(len(hk))}
+    for name, geo in (("beam_normal", {}), ("tilted", dict(p=TILTED_P, r=TILTED_R))):
+        p = P.parse_params_text(synth.params_text(max_nr_spots=30, **geo))
+        with Engine(p, device=dev) as e:
+            ts = []
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                e.build_db_synthetic(seed=args.seed, n=n, hkls=hk)
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+        out[name] = {"first_build_s": round(ts[0], 3), "warm_build_s": round(min(ts[1:]), 3),
+                     "warm_orientations_per_s": round(n / min(ts[1:]), 1),
+                     "warm_hkl_evals_per_s": round(n * len(hk) / min(ts[1:]), 1)}
+    return out
+
+
+HEX_LATTICE = (0.295, 0.295, 0.468, 90.0, 90.0, 120.0)
+
+
+def hex_leg(args, dev, K=32, grains=5, top=50, n=None):
+    """Lower symmetry plus refinement: hexagonal a=2.95 A, c=4.68 A (SG 194),
+    the 7790 HKLs with |h|,|k|,|l| <= 10, a DB of 1e8 rotations restricted to
+    the hexagonal fundamental zone, built on the device (timed: the DB
+    build's hardest HKL count); 32 frames of 5 grains each, every frame
+    simulated with c/a scaled by 1+U(-1 %, +1 %); one batched pass; the top
+    50 candidates of every frame by score go to the c/a refinement
+    (tol_c_over_a 0.02, FitOrientation's box, LaueMatchingHeaders.h:664,714,
+    738) with this library's Nelder-Mead, objective on the device and, for
+    comparison, on host threads."""
+    from lauematching_b200 import params as P, synth
+    from lauematching_b200.engine import Engine
+    from lauematching_b200.refine import Refiner
+    n = n or args.n_orient
+    seed = 3
+
+    def text(lat, tol=0.0):
+        return synth.params_text(lattice=lat, space_group=194, max_nr_spots=30, min_nr_spots=5,
+                                 min_intensity=args.min_intensity, tol_c_over_a=tol)
+    p = P.parse_params_text(text(HEX_LATTICE))
+    pr = P.parse_params_text(text(HEX_LATTICE, 0.02))
+    hk = synth.hkls_hexagonal(10)
+    W, H = p.nr_px_x, p.nr_px_y
+    e = Engine(p, device=dev)
+    try:
+        t0 = time.perf_counter()
+        e.build_db_synthetic(seed=seed, n=n, hkls=hk, hex_fz=True)
+        t_build = time.perf_counter() - t0
+        scan = min(2_000_000, n)
+        rec = e.download_db(0, scan)
+        om_scan = e.synth_orientations(seed, 0, scan)
+        rng = np.random.default_rng(3000)
+        frames, ca_true, true_ids = [], [], []
+        for _ in range(K):
+            ca = 1.0 + rng.uniform(-0.01, 0.01)
+            g = synth.pick_grains(rec, grains, p.min_nr_spots, rng)
+            lat = (HEX_LATTICE[0], HEX_LATTICE[1], HEX_LATTICE[2] * ca) + HEX_LATTICE[3:]
+            with Engine(P.parse_params_text(text(lat)), device=dev, survivor_capacity=1024) as eg:
+                eg.build_db(om_scan[g], hk)
+                grec = eg.download_db()
+            frames.append(synth.render_image(grec, W, H, rng).astype(np.uint8))
+            ca_true.append(ca)
+            true_ids.append(g)
+        del om_scan
+        for k in range(K):
+            e.load_image(k, frames[k], want_scale=False)
+        slots = list(range(K))
+        nsteps = max(5, min(args.steps, 40))
+        pass_stats(e, slots, p, 3)
+        cmp_ms, step_ms = pass_stats(e, slots, p, nsteps)
+        res = {k: e.results(k) for k in slots}
+        surv = [int(res[k][0].shape[0]) for k in slots]
+        out = {"workload": f"{K} uint8 {W}x{H} frames of {grains} hexagonal grains (c/a x "
+                           f"(1+U(-1%,+1%)) per frame) vs a {n:,}-orientation hexagonal "
+                           f"fundamental-zone DB, SG 194, {len(hk)} HKLs",
+               "n_orient": n, "batch": K, "hkls": int(len(hk)),
+               "dbbuild": {"seconds": round(t_build, 3),
+                           "orientations_per_s": round(n / t_build, 1),
+                           "hkl_evals_per_s": round(n * len(hk) / t_build, 1)},
+               "pass": {"compare_ms": round(cmp_ms, 4), "step_ms": round(step_ms, 4),
+                        "images_per_s": round(K / (step_ms * 1e-3), 1),
+                        "variant": e.get_tuning()["last_variant"]},
+               "survivors_per_image": {"min": min(surv), "max": max(surv),
+                                       "mean": statistics.mean(surv)}}
+        # the top candidates of every frame into the c/a refinement
+        cand, img_of, ca_of = [], [], []
+        for k in slots:
+            sv = res[k][0]
+            order = np.argsort(-sv["score"], kind="stable")[:top]
+            cand += [int(i) for i in sv["id"][order]]
+            img_of += [k] * len(order)
+            ca_of += [ca_true[k]] * len(order)
+        om_c = np.concatenate([e.synth_orientations(seed, i, 1) for i in cand]) if cand \
+            else np.zeros((0, 9))
+        fl = [f.astype(np.float32).reshape(H, W) for f in frames]
+        fits = {}
+        for name, d in (("device", dev), ("host", None)):
+            with Refiner(pr, e.geometry, hk, device=d) as r:
+                r.set_images(fl)
+                nv = r.set_grains(om_c, np.array(img_of, np.int32))
+                x0, _, _ = r.start()
+                r.fit("nelder-mead", 200)  # warm
+                t0 = time.perf_counter()
+                x, ov, ev = r.fit("nelder-mead", 200)
+                dt = time.perf_counter() - t0
+                st = r.last_stats()
+                fits[name] = (x, ov, ev)
+                out.setdefault("refine", {})[name] = {
+                    "fit_ms": round(dt * 1e3, 2), "grains": int(len(cand)),
+                    "evaluations": st["points"], "rounds": st["rounds"],
+                    "objective_kernel_ms": round(st["kernel_ms"], 3)}
+        x, ov, _ = fits["device"]
+        ref = out["refine"]
+        ref["identical_device_host"] = all(np.array_equal(a, b) for a, b in
+                                           zip(fits["device"], fits["host"]))
+        ref["valid_hkls_per_grain"] = round(float(nv.mean()), 1) if len(nv) else 0.0
+        if len(cand):
+            ca0 = P.parse_params_text(text(HEX_LATTICE)).lattice
+            ca_orig = ca0[2] / ca0[0]
+            truth = np.array(ca_of)
+            # candidates that are one of their frame's true grains
+            hit = np.array([c in set(true_ids[k].tolist()) for c, k in zip(cand, img_of)])
+            err0 = np.abs(1.0 - truth)
+            err1 = np.abs(x[:, 3] / ca_orig - truth)
+            ref["c_over_a_rel_error_median"] = {
+                "before": float(np.median(err0)), "after_all": float(np.median(err1)),
+                "after_true_grains": float(np.median(err1[hit])) if hit.any() else None,
+                "true_grain_candidates": int(hit.sum())}
+        if not args.no_parity:
+            out["survivor_parity"] = survivor_parity(e, p, frames[0])[0]
+            out["dbbuild"]["parity"] = dbbuild_parity_sample(e, p, hk, seed, n, per_block=10000,
+                                                             blocks=2)
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import ref_objective as RO
+            if RO.available() and len(cand):
+                ro = RO.RefObjective(pr, e.geometry, hk)
+                m = min(64, len(cand))
+                with Refiner(pr, e.geometry, hk, device=dev) as r:
+                    r.set_images(fl)
+                    r.set_grains(om_c[:m], np.array(img_of[:m], np.int32))
+                    x0, _, _ = r.start()
+                    pts = np.concatenate([x0, x[:m]])
+                    gi = np.concatenate([np.arange(m), np.arange(m)])
+                    val = r.evaluate(gi, pts)
+                want = [ro.problem(pts[j], fl[img_of[gi[j]]], ro.prefilter(x0[gi[j]][:3]))
+                        for j in range(len(gi))]
+                out["refine"]["objective_vs_reference"] = {
+                    "points": int(len(gi)),
+                    "identical": bool(np.array_equal(val, np.array(want)))}
+    finally:
+        e.close()
+    return out
+
+
+def hbm_peak():
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        return float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
 
 
 def refine_scene(device, n_frames, per_frame, seed=17, min_spots=8):
@@ -767,6 +1194,73 @@ def run_ours(args, rank, world):
         if i >= args.warmup:
             platency.append((time.perf_counter() - ts) * 1e3)
 
+    # ---- end to end from the reference's own input types ----------------------
+    # float32 wire frames (LaueMatchingGPUStream.cu:1201-1205) and float64 .bin
+    # frames (LaueMatchingGPU.cu:704-715), page-locked, quantised on the way in:
+    # the same pipelined two-half loop as above, the host scan and the uint8
+    # quantisation inside the timed region
+    e2e_types = {}
+    for name, dt in (("float32_wire_frames", np.float32), ("float64_bin_frames", np.float64)):
+        tp = []
+        for k in range(K // 2 * 2 or 1):
+            pb = PinnedBuffer((p.nr_px_x * p.nr_px_y,), dt)
+            pb.array[:] = imgs[k % K]
+            tp.append(pb)
+        hv = [slots[: K // 2], slots[K // 2:]] if K >= 2 else [slots, slots]
+        nx = [0]
+
+        def load_t(h):
+            e.load_images(hv[h], [tp[(nx[0] + i) % len(tp)].array for i in range(len(hv[h]))])
+            nx[0] += len(hv[h])
+
+        def loop(npasses):
+            load_t(0)
+            e.match(hv[0], p.min_nr_spots, p.min_intensity)
+            for i in range(npasses):
+                h = i % 2
+                if i + 1 < npasses:
+                    load_t(1 - h)
+                    e.match(hv[1 - h], p.min_nr_spots, p.min_intensity)
+                e.results_batch(hv[h])
+        loop(2 * args.warmup)
+        m0 = e.bytes_moved()
+        t0 = time.perf_counter()
+        loop(2 * args.steps)
+        dt_s = time.perf_counter() - t0
+        m1 = e.bytes_moved()
+        e2e_types[name] = {"value": round(world * len(hv[0]) * 2 * args.steps / dt_s, 2),
+                           "unit": UNIT, "h2d_bytes_per_step": (m1[0] - m0[0]) // args.steps,
+                           "d2h_bytes_per_step": (m1[1] - m0[1]) // args.steps,
+                           "frame_bytes": int(p.nr_px_x * p.nr_px_y * np.dtype(dt).itemsize)}
+        for pb in tp:
+            pb.free()
+    # survivors of the float frames equal those of the uint8 frames they hold
+    for k in range(K):
+        e.load_image(k, imgs[k], want_scale=False)
+    e.match(slots, p.min_nr_spots, p.min_intensity)
+    ref_lists = {k: e.results(k) for k in slots}
+    f32 = [imgs[k].astype(np.float32) for k in range(K)]
+    e.load_images(slots, f32)
+    e.match(slots, p.min_nr_spots, p.min_intensity)
+    e2e_types["float_frames_same_survivors"] = same_survivors(
+        {k: e.results(k) for k in slots}, ref_lists)
+
+    # ---- K sweep: images/s of the resident batched pass, K = 1 .. 64 ----------
+    k_sweep = []
+    for kk in (1, 2, 4, 8, 16, 32, 64):
+        if kk > K:
+            break
+        for k in range(kk):
+            e.load_image(k, imgs[k], want_scale=False)
+        sl = list(range(kk))
+        timed_stream(args.warmup, sl)
+        nk = max(10, min(args.steps, 200))
+        _, tk = timed_stream(nk, sl)
+        k_sweep.append({"K": kk, "images_per_s": round(kk * nk / (tk * 1e-3), 1),
+                        "ms_per_pass": round(tk / nk, 4)})
+    for k in range(K):
+        e.load_image(k, imgs[k], want_scale=False)
+
     # ---- the same batched pass gathering every spot ----------------------------
     # (records with fewer spots than MinNrSpots are otherwise not gathered:
     # they cannot pass; the survivors are identical either way)
@@ -836,19 +1330,24 @@ def run_ours(args, rank, world):
                    "l2": "inputs larger than L2 (12.2 GB DB streamed every pass)",
                    "parallelism": f"replicas x{world} (images split, DB replicated)"},
         "roofline": roof,
-        "e2e": {"value": round(e2e_ips, 2), "unit": UNIT,
-                "h2d_bytes_per_step": h2d_step,
-                "h2d_dense_frame_bytes_per_step": K * p.nr_px_x * p.nr_px_y,
-                "d2h_bytes_per_step": d2h[0],
-                "path": "public Engine API from pinned uint8 frames: per step 64 frames in two "
-                        "passes of 32, the upload of one half overlapping the pass of the other "
-                        "and its pass queued before the other's results are read (load_images "
-                        "of 32 frames, match, results_batch of the previous 32, twice)",
-                "sequential": round(seq_ips, 2),
-                # host wall time per call, median: load_images (host scan + copy
-                # enqueue), match (enqueue), results_batch (wait for the pass + copy)
-                "breakdown_ms_p50": {k: round(1e3 * float(np.median(v)), 3)
-                                     for k, v in phase.items() if v}},
+        "e2e": dict(e2e_types["float32_wire_frames"],
+                    path="public Engine API from page-locked float32 frames (the daemon's wire "
+                         "frames, LaueMatchingGPUStream.cu:1201-1205), host scan and uint8 "
+                         "quantisation inside the timed region: per step 64 frames in two "
+                         "passes of 32, the upload of one half overlapping the pass of the other "
+                         "and its pass queued before the other's results are read (load_images "
+                         "of 32 frames, match, results_batch of the previous 32, twice)"),
+        "e2e_uint8_frames": {
+            "value": round(e2e_ips, 2), "unit": UNIT,
+            "h2d_bytes_per_step": h2d_step,
+            "h2d_dense_frame_bytes_per_step": K * p.nr_px_x * p.nr_px_y,
+            "d2h_bytes_per_step": d2h[0],
+            "path": "the same loop from page-locked uint8 frames (already quantised)",
+            "sequential": round(seq_ips, 2),
+            # host wall time per call, median: load_images (host scan + copy
+            # enqueue), match (enqueue), results_batch (wait for the pass + copy)
+            "breakdown_ms_p50": {k: round(1e3 * float(np.median(v)), 3)
+                                 for k, v in phase.items() if v}},
         # per timed pass: status reset, compare, ordering (one graph replay)
         "gpu_launches": 3 * args.steps,
         "clocks": clk,
@@ -862,6 +1361,8 @@ def run_ours(args, rank, world):
                   "e2e": round(1e3 / statistics.mean(platency), 2),
                   "compare_ms": round(statistics.mean(pcmp), 4)},
         "batched_over_plain": round(value / world / plain_ips, 2),
+        "e2e_input_types": e2e_types,
+        "k_sweep": k_sweep,
         "full_gather": full_gather,
         "merge": merge,
         "refine": refine,
@@ -872,12 +1373,18 @@ def run_ours(args, rank, world):
     }
     if rank == 0 and world == 1 and not args.no_parity:
         out["dbbuild"]["parity"] = dbbuild_parity_sample(e, p, hkls, args.seed, N)
-    ours0 = None
-    if rank == 0 and world == 1 and not args.no_parity:
-        out["survivor_parity"], ours0 = survivor_parity(e, p, imgs[0])
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(e, p, txt, hkls, imgs[0], args.seed, args.cpu_sample,
-                                           ours=ours0)
+    if rank == 0 and world == 1 and not (args.no_parity and args.no_cpu_baseline):
+        out.update(full_db_parity_and_cpu_baseline(e, p, txt, hkls, imgs[0], args.seed,
+                                                   cpu=not args.no_cpu_baseline,
+                                                   parity=not args.no_parity))
+    # the other configurations' legs (one GPU, rank 0 only)
+    legs = [x for x in args.legs.split(",") if x] if rank == 0 and world == 1 else []
+    if "tilted" in legs:
+        out["tilted"] = tilted_leg(args, dev, K=K)
+    if "hex" in legs:
+        out["hex"] = hex_leg(args, dev)
+    if "serve" in legs:
+        out["serving"] = serve_leg(args, e)
     for pb in pins:
         pb.free()
     e.close()
@@ -933,41 +1440,66 @@ def run_reference(args, rank, world):
     for _ in range(max(1, min(args.batch, 8))):
         g = synth.pick_grains(rec, int(rng.integers(1, 21)), p.min_nr_spots, rng)
         imgs.append(synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng))
+    # the full-size DB: the reference-built sample repeated up to 1e8 records
+    # (cache and orientation file alike), in /dev/shm when it has room so the
+    # reference memory-maps both; every timed run compares against all of it
+    tiles = max(1, args.n_orient // n_s)
+    per = REC_BYTES_PER_ORIENT + 72
+    big = scratch_dir(tiles * n_s * per)
+    if big is None:
+        import psutil
+        tiles = max(1, min(tiles, int(psutil.virtual_memory().available * 0.4 // (n_s * per))))
+    n = tiles * n_s
+    wd_f = tempfile.mkdtemp(prefix="lmb_ref_full_", dir=big)
+    fwd_f, op_f = os.path.join(wd_f, "fwd.bin"), os.path.join(wd_f, "orients.bin")
+    rec_bytes = rec.tobytes()
+    om_bytes = open(op, "rb").read()
+    with open(fwd_f, "wb") as ff, open(op_f, "wb") as fo:
+        for _ in range(tiles):
+            ff.write(rec_bytes)
+            fo.write(om_bytes)
+    del rec_bytes, om_bytes
     with open(pp, "w") as f:
-        f.write(txt + f"ForwardFile {fwd}\nDoFwd 0\n")
-    times, walls = [], []
+        f.write(txt + f"ForwardFile {fwd_f}\nDoFwd 0\n")
+    times, walls, inits = [], [], []
     for i in range(args.warmup + args.steps):
         formats.write_image_bin(ip, imgs[i % len(imgs)])
-        r = O.run_reference(pp, op, hp, ip, ncpus=cores)
+        r = O.run_reference(pp, op_f, hp, ip, ncpus=cores)
         if r.returncode != 0 or r.compare_seconds is None:
-            print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
+            print(json.dumps({"impl": "reference", "unavailable": "reference run failed: "
+                              + (r.stderr or r.stdout)[-200:].replace("\n", " ")}))
             return
         if i >= args.warmup:
             times.append(r.compare_seconds)
             walls.append(r.wall_seconds)
-    for d in (wd, wd_o):
+            inits.append(r.initial_solutions)
+    for d in (wd, wd_o, wd_f):
         for fn in os.listdir(d):
             os.remove(os.path.join(d, fn))
         os.rmdir(d)
-    scale = 1e8 / n_s
+    scale = 1e8 / n
     per_img = statistics.mean(times) * scale
     value = 1.0 / per_img
-    sample = (f"LaueMatchingCPU (reference source, gcc -O3 -fopenmp, NLopt stand-in) DoFwd 0 "
-              f"compare stage on a {n_s}-orientation sample of the workload, 1 image per run, "
-              f"mean of {args.steps} runs = {statistics.mean(times):.4f} s, scaled x{scale:g} "
-              f"to the 1e8-orientation DB; whole-process wall {statistics.mean(walls):.2f} s per "
-              f"run; sample DB built by the reference (DoFwd 1) in {rb.compare_seconds:.2f} s")
+    sample = (f"LaueMatchingCPU (reference source, gcc -O3 -fopenmp, NLopt stand-in) DoFwd 0, "
+              f"one image per run against {n:,} records (a {n_s:,}-orientation DB built by the "
+              f"reference itself, DoFwd 1 in {rb.compare_seconds:.2f} s, repeated x{tiles}"
+              f"{' in /dev/shm' if big else ''}): compare stage mean of {args.steps} runs = "
+              f"{statistics.mean(times):.4f} s"
+              + ("" if n == 100_000_000 else f", scaled x{scale:g} to 1e8")
+              + f"; whole process {statistics.mean(walls):.2f} s per run")
     out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(per_img * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-           "config": {"workload": f"plain single-image compare vs a 100,000,000-orientation DB "
-                                  f"(sampled: {n_s})", "n_orient": 100_000_000,
-                      "max_nr_spots": 30, "hkls": int(len(hkls))},
+           "config": {"workload": f"plain single-image compare vs a {n:,}-record DB "
+                                  f"(reference-built {n_s:,}-orientation DB x{tiles})",
+                      "n_orient": n, "max_nr_spots": 30, "hkls": int(len(hkls))},
            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores,
                             "kind": "reference", "sample": sample},
            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0},
+           "process_wall_s_per_step": round(statistics.mean(walls), 3),
+           "initial_solutions_per_image": inits,
            "dbbuild_reference": {"orientations_per_s": round(n_s / rb.compare_seconds, 1),
                                  "sample": n_s}}
     print(json.dumps(out), flush=True)
@@ -1082,9 +1614,12 @@ def run_reference_gpu(args, rank, world):
 # ---------------------------------------------------------------------------
 # serving: Poisson arrivals of mixed 1024^2 / 2048^2 frames through the daemon
 # ---------------------------------------------------------------------------
-def _serve_client(port, wire, keys, n_total, rate, nsend):
-    """Poisson arrivals of frames on nsend connections (the extended header:
-    b"LMB2", image number, width, height, dtype uint8)."""
+def _serve_client(port, wire, keys, n_total, rate, nsend, plain, sent):
+    """Poisson arrivals of frames on nsend connections.  plain: the
+    reference's message (2-byte host-endian image number + the float32 frame
+    of the daemon's detector); else the extended header (b"LMB2", image
+    number, width, height, dtype 1 = uint8).  sent[i] = time.monotonic() just
+    before image i+1 is sent."""
     import socket
     import struct
     import threading as th
@@ -1098,10 +1633,14 @@ def _serve_client(port, wire, keys, n_total, rate, nsend):
             dt = t - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
-            key = keys[int(r2.integers(0, 2))]
+            key = keys[int(r2.integers(0, len(keys)))]
             fr = wire[key][int(r2.integers(0, len(wire[key])))]
-            s.sendall(struct.pack("<4sHHHBB", b"LMB2", (i % 65535) + 1, key[0], key[1], 1, 0))
-            s.sendall(fr)
+            num = (i % 65535) + 1
+            sent[i] = time.monotonic()
+            if plain:
+                s.sendall(num.to_bytes(2, sys.byteorder) + fr)
+            else:
+                s.sendall(struct.pack("<4sHHHBB", b"LMB2", num, key[0], key[1], 1, 0) + fr)
         s.close()
     ts = [th.Thread(target=sender, args=(j,)) for j in range(nsend)]
     for t in ts:
@@ -1110,66 +1649,170 @@ def _serve_client(port, wire, keys, n_total, rate, nsend):
         t.join()
 
 
-def run_serve(args):
-    from lauematching_b200 import synth, params as P
+def _serve_run(port, wire, keys, n_total, rate, plain, done_at, nsend=4, wait_s=120.0):
+    """One Poisson run from a client process; latency per image = the moment
+    its results were written (done_at: image number -> time.monotonic()) minus
+    the moment its message started to go out."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    sent = ctx.Array("d", n_total, lock=False)
+    client = ctx.Process(target=_serve_client,
+                         args=(port, wire, keys, n_total, rate, nsend, plain, sent))
+    client.start()
+    client.join()
+    deadline = time.monotonic() + wait_s
+    while len(done_at) < n_total and time.monotonic() < deadline:
+        time.sleep(0.02)
+    done = dict(done_at)
+    lat = [done[(i % 65535) + 1] - sent[i] for i in range(n_total) if (i % 65535) + 1 in done]
+    first = min(sent[:n_total])
+    last = max(done.values()) if done else first
+    lat_ms = np.array(lat) * 1e3 if lat else np.zeros(1)
+    return {"offered_rate": rate, "sent": n_total, "served": len(lat),
+            "throughput": round(len(lat) / max(last - first, 1e-9), 1),
+            "p50_ms": round(float(np.percentile(lat_ms, 50)), 2),
+            "p99_ms": round(float(np.percentile(lat_ms, 99)), 2)}
+
+
+def serve_leg(args, e2=None):
+    """Serving under Poisson arrivals against device-resident 1e8 DBs.
+
+    * mixed: half 1024^2, half 2048^2 uint8 frames (1-30 fcc grains) on the
+      extended port of this library's daemon (one DB per detector size), in
+      its batched form (continuous batching, up to 64 images per pass) and
+      one image per pass;
+    * vs_reference: 2048^2 float32 frames in the reference's own message
+      (2-byte image number + float32 frame) to this library's daemon and to
+      the reference's LaueMatchingGPUStream (built for sm_100a from its
+      sources; its DB, the device-built one byte-identical to its cache, read
+      from its ForwardFile): the plain one-pass-per-image serving baseline.
+    Latency = results written minus message start, per image."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from lauematching_b200 import formats, synth, params as P
     from lauematching_b200.engine import Engine
     from lauematching_b200.stream import StreamServer
-    txt2, p2 = workload_params(args.min_intensity)
+    txt2, _ = workload_params(args.min_intensity)
     p2 = P.parse_params_text(txt2 + "MinGoodSpots 5\n", binary="stream")
     txt1 = txt2.replace("NrPxX 2048", "NrPxX 1024").replace("NrPxY 2048", "NrPxY 1024")
     txt1 = txt1.replace("PxX 0.0002", "PxX 0.0004").replace("PxY 0.0002", "PxY 0.0004")
     p1 = P.parse_params_text(txt1 + "MinGoodSpots 5\n", binary="stream")
     hkls = synth.hkls_cubic(8)
     N = args.n_orient
-    e2 = Engine(p2)
-    om = e2.build_db_synthetic(args.seed, N, hkls, return_orients=True)
+    own2 = e2 is None
+    if own2:
+        e2 = Engine(p2)
+        e2.build_db_synthetic(args.seed, N, hkls)
+    om = np.empty((N, 9), np.float64)
+    for s0 in range(0, N, 4_000_000):
+        c = min(4_000_000, N - s0)
+        om[s0:s0 + c] = e2.synth_orientations(args.seed, s0, c)
     e1 = Engine(p1)
     e1.build_db_synthetic(args.seed, N, hkls)
     rng = np.random.default_rng(11)
-    pool = {}
+    pool, pool_f32 = {}, []
     for e, p in ((e2, p2), (e1, p1)):
         rec = e.download_db(0, min(2_000_000, N))
         frames = []
         for _ in range(16):
             g = synth.pick_grains(rec, int(rng.integers(1, 31)), p.min_nr_spots, rng)
-            frames.append(synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng).astype(np.uint8))
-        pool[(p.nr_px_x, p.nr_px_y)] = frames
-    keys = list(pool)
-    wire = {k: [f.tobytes() for f in v] for k, v in pool.items()}
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    results = []
+            frames.append(synth.render_image(rec[g], p.nr_px_x, p.nr_px_y, rng))
+        pool[(p.nr_px_x, p.nr_px_y)] = [f.astype(np.uint8).tobytes() for f in frames]
+        if e is e2:
+            pool_f32 = [f.astype(np.float32).tobytes() for f in frames]
+    key2 = (p2.nr_px_x, p2.nr_px_y)
+    out = {"n_orient": N, "mixed": [], "vs_reference": {"ours": [], "reference": []}}
     port0 = 45000 + (os.getpid() % 200) * 10
-    for mode, mb in (("batched", 64), ("plain", 1)):
-        for rate in [float(r) for r in args.serve_rates.split(",")]:
+    secs = args.serve_seconds
+
+    def ours(mode_batch, rates, keys, wire, plain):
+        nonlocal port0
+        res = []
+        for rate in rates:
             port0 += 2
-            srv = StreamServer([p2, p1], om, hkls, ncpus=os.cpu_count() or 1, max_batch=mb,
-                               result_dir=tempfile.mkdtemp(prefix="lmb_serve_"), port=port0,
-                               ext_port=port0 + 1, host="127.0.0.1", log=lambda *a: None,
-                               engines=[e2, e1], max_queue=256).start()
+            srv = StreamServer([p2, p1], om, hkls, ncpus=os.cpu_count() or 1,
+                               max_batch=mode_batch, result_dir=tempfile.mkdtemp(prefix="lmb_sv_"),
+                               port=port0, ext_port=port0 + 1, host="127.0.0.1",
+                               log=lambda *a: None, engines=[e2, e1], max_queue=256).start()
             time.sleep(0.3)
-            n_total = int(min(args.serve_images, max(50, rate * args.serve_seconds)))
-            # the clients run in a process of their own, as the detector-side
-            # image server does, so they do not share the daemon's interpreter
-            client = ctx.Process(target=_serve_client,
-                                 args=(port0 + 1, wire, keys, n_total, rate, 4))
-            t0 = time.perf_counter()
-            client.start()
-            client.join()
-            deadline = time.time() + 300
-            while srv.images_done < n_total and time.time() < deadline:
-                time.sleep(0.02)
-            wall = time.perf_counter() - t0
+            n_total = int(min(args.serve_images, max(50, rate * secs)))
+            r = _serve_run(port0 if plain else port0 + 1, wire, keys, n_total, rate, plain,
+                           srv.done_at)
             st = srv.stop(close_engines=False)
-            st.update({"mode": mode, "offered_rate": rate, "sent": n_total,
-                       "throughput": round(srv.images_done / wall, 1)})
-            results.append(st)
-            log(json.dumps(st))
+            r.update({"passes": st["passes"], "mean_batch": round(st["mean_batch"], 2)})
+            res.append(r)
+            log(json.dumps(r))
+        return res
+
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    keys = list(pool)
+    for mode, mb in (("batched", 64), ("one_image_per_pass", 1)):
+        for r in ours(mb, rates, keys, pool, plain=False):
+            r["mode"] = mode
+            out["mixed"].append(r)
+    # same float32 2048^2 frames in the reference's message, both daemons
+    ref_rates = [float(r) for r in args.serve_ref_rates.split(",")]
+    wire32 = {key2: pool_f32}
+    out["vs_reference"]["ours"] = ours(64, ref_rates, [key2], wire32, plain=True)
+    if O.have_ref_stream():
+        per = REC_BYTES_PER_ORIENT + 72
+        base = scratch_dir(N * per)
+        wd = tempfile.mkdtemp(prefix="lmb_refstream_", dir=base)
+        fwd, op = os.path.join(wd, "fwd.bin"), os.path.join(wd, "orients.bin")
+        try:
+            with open(fwd, "wb") as ff:
+                for s0 in range(0, N, 4_000_000):
+                    e2.download_db(s0, min(4_000_000, N - s0)).tofile(ff)
+            om.tofile(op)
+            hp, pp = os.path.join(wd, "hkls.csv"), os.path.join(wd, "params.txt")
+            formats.write_hkls(hp, hkls)
+            with open(pp, "w") as f:
+                f.write(txt2 + f"ForwardFile {fwd}\nDoFwd 0\nResultDir results_ref\n"
+                              f"MinGoodSpots 5\n")
+            cores = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            rs = O.RefStream(pp, op, hp, cores, cwd=wd)
+            if not rs.wait_ready():
+                out["vs_reference"]["reference"] = {
+                    "unavailable": "the reference daemon did not start: "
+                                   + "".join(rs.lines[-5:])[-300:]}
+                rs.stop()
+            else:
+                t_ready = time.perf_counter() - t0
+                for rate in ref_rates:
+                    rs.done.clear()
+                    n_total = int(min(args.serve_images, max(50, rate * secs)))
+                    r = _serve_run(60517, wire32, [key2], n_total, rate, True, rs.done)
+                    out["vs_reference"]["reference"].append(r)
+                    log(json.dumps(dict(r, daemon="reference")))
+                rc = rs.stop()
+                out["vs_reference"]["reference_daemon"] = {
+                    "binary": "oracle/_ref/LaueMatchingGPUStream (reference source, nvcc -O3 "
+                              "-rdc=true sm_100a, NLopt stand-in)",
+                    "startup_s": round(t_ready, 1), "exit_code": rc, "cores": cores}
+        finally:
+            for fn in ("fwd.bin", "orients.bin", "hkls.csv", "params.txt"):
+                if os.path.exists(os.path.join(wd, fn)):
+                    os.remove(os.path.join(wd, fn))
+            import shutil
+            shutil.rmtree(wd, ignore_errors=True)
+    else:
+        out["vs_reference"]["reference"] = {"unavailable": "oracle/_ref/LaueMatchingGPUStream "
+                                                           "was not built"}
+    sat = lambda lst: max((r["throughput"] for r in lst), default=0.0) \
+        if isinstance(lst, list) else 0.0  # noqa: E731
+    out["vs_reference"]["saturation_images_per_s"] = {
+        "ours": sat(out["vs_reference"]["ours"]), "reference": sat(out["vs_reference"]["reference"])}
     e1.close()
-    e2.close()
-    print(json.dumps({"metric": "serving: p50/p99 image latency under Poisson arrivals, "
-                                "mixed 1024^2/2048^2 uint8 frames, 100M-orientation DB each",
-                      "n_orient": N, "serving": results}), flush=True)
+    if own2:
+        e2.close()
+    return out
+
+
+def run_serve(args):
+    print(json.dumps({"metric": "serving: images/s and p50/p99 image latency under Poisson "
+                                "arrivals, 1e8-orientation DB per detector size",
+                      "serving": serve_leg(args)}), flush=True)
 
 
 def main():
@@ -1186,8 +1829,6 @@ def main():
                     help="pin the compare variant (default: the autotuned shape)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--min-intensity", type=float, default=200.0)
-    ap.add_argument("--cpu-sample", type=int, default=10_000_000,
-                    help="orientations in the CPU-baseline sample of our arm")
     ap.add_argument("--ref-sample", type=int, default=2_000_000,
                     help="orientations per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1197,8 +1838,18 @@ def main():
     ap.add_argument("--refine", action="store_true",
                     help="only the batched refinement leg (device against host threads)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (Poisson arrivals)")
-    ap.add_argument("--serve-rates", type=str, default="50,200,500,1000,2000")
-    ap.add_argument("--serve-seconds", type=float, default=4.0)
+    ap.add_argument("--legs", type=str, default="tilted,hex,serve",
+                    help="legs of the other configurations run after the headline one "
+                         "(comma list of tilted, hex, serve; empty for none)")
+    ap.add_argument("--leg", choices=["tilted", "hex", "dbbuild"], default=None,
+                    help="only one leg of the bench: tilted = the batched pass at the "
+                         "reference's tilted 34-ID-E detector (~15 spots per record); "
+                         "hex = hexagonal fundamental-zone DB, 32 frames with c/a "
+                         "perturbed, top-50 candidates into the c/a refinement; "
+                         "dbbuild = the device DB build alone (cold and warm)")
+    ap.add_argument("--serve-rates", type=str, default="10,100,500,2000")
+    ap.add_argument("--serve-ref-rates", type=str, default="50,200,500,1000")
+    ap.add_argument("--serve-seconds", type=float, default=2.5)
     ap.add_argument("--serve-images", type=int, default=4000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -1210,6 +1861,12 @@ def main():
         run_reference_gpu(args, rank, world)
     elif args.serve:
         run_serve(args)
+    elif args.leg == "tilted":
+        print(json.dumps(tilted_leg(args, 0, K=args.batch)), flush=True)
+    elif args.leg == "hex":
+        print(json.dumps(hex_leg(args, 0)), flush=True)
+    elif args.leg == "dbbuild":
+        print(json.dumps(dbbuild_leg(args, 0)), flush=True)
     elif args.refine:
         print(json.dumps(refine_timing(0, cpu=not args.no_cpu_baseline)), flush=True)
     elif args.preprocess:
