@@ -1637,10 +1637,12 @@ def _serve_client(port, wire, keys, n_total, rate, nsend, plain, sent):
             fr = wire[key][int(r2.integers(0, len(wire[key])))]
             num = (i % 65535) + 1
             sent[i] = time.monotonic()
+            # header and frame as two sends (no 16 MiB concatenation per message)
             if plain:
-                s.sendall(num.to_bytes(2, sys.byteorder) + fr)
+                s.sendall(num.to_bytes(2, sys.byteorder))
             else:
-                s.sendall(struct.pack("<4sHHHBB", b"LMB2", num, key[0], key[1], 1, 0) + fr)
+                s.sendall(struct.pack("<4sHHHBB", b"LMB2", num, key[0], key[1], 1, 0))
+            s.sendall(fr)
         s.close()
     ts = [th.Thread(target=sender, args=(j,)) for j in range(nsend)]
     for t in ts:

@@ -107,9 +107,12 @@ void *lmb_engine_stream(lmb_engine *e);
  * compact layout cannot be built --, 4 the compact layout filtered by the
  * cell mask of the pass's frames), tile_sub (32-orientation sub-tiles per
  * tile), stages, consumer warps, blocks per SM, grid multiplier,
- * full_gather, test_consumer_wait_us, cell_consumers, cell_stages}; 0 =
- * default.  cell_consumers and cell_stages shape variant 4 when the
- * automatic variant picks it (the autotuner's dense-DB entry).  full_gather = 1
+ * full_gather, test_consumer_wait_us, cell_consumers, cell_stages,
+ * cell_queue}; 0 = default.  cell_consumers, cell_stages and cell_queue (1:
+ * the records that can still pass are queued and counted 32 at a time; 0:
+ * counted chunk by chunk) shape variant 4 when the automatic variant picks it
+ * (the autotuner's dense-DB entry); a pinned variant 4 takes cell_queue from
+ * this field too.  full_gather = 1
  * gathers every spot even of records with fewer spots than MinNrSpots (which
  * cannot pass; by default they are skipped; results are identical either
  * way), for measuring the full gather cost.  test_consumer_wait_us (tests
@@ -121,7 +124,7 @@ void *lmb_engine_stream(lmb_engine *e);
  * (the reference launches <<<ceil(n/1024),1024>>>, LaueMatchingGPU.cu:739-743). */
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields);
 /* get: fields 0-6 as set, 7: the variant the latest pass ran, 8: the test
- * wait, 9-10: the cell-mask pass's shape for the automatic variant. */
+ * wait, 9-11: the cell-mask pass's shape for the automatic variant. */
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields);
 
 /* The compact device layout variant 2 streams: derived from the resident

@@ -59,10 +59,11 @@ def lookup(R: int, k: int, dense: bool = False) -> dict | None:
 
 
 def candidate_shapes_dense():
-    # the cell-mask pass: one block per SM; consumer warps and ring depth
-    # (0 = as deep as fits beside the mask and the hit lists)
-    for cons, st in itertools.product((4, 6, 8, 10, 12, 14, 16), (0, 2, 3, 4, 6)):
-        yield dict(variant=4, stages=st, consumers=cons)
+    # the cell-mask pass: one block per SM; consumer warps (at most 12), ring
+    # depth (0 = as deep as fits beside the mask and the hit lists), and
+    # whether the records that can pass are queued or counted in place
+    for q, cons, st in itertools.product((0, 1), (4, 6, 8, 10, 12), (0, 2, 3, 4, 6)):
+        yield dict(variant=4, stages=st, consumers=cons, cell_queue=q)
 
 
 def candidate_shapes():
@@ -139,7 +140,7 @@ def main():
             if ref is None:
                 ref = got
             same = all(np.array_equal(a, b) for a, b in zip(ref, got))
-            used = e.get_tuning()
+            used = dict(e.get_tuning(), cell_queue=shape.get("cell_queue", 0))
             results.append((ms, used, same))
             print(f"K={kb} {used} {ms:.4f} ms identical={same}", file=sys.stderr)
         ok = [r for r in results if r[2]]

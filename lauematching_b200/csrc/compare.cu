@@ -774,7 +774,7 @@ int cellmask_launch(const unsigned long long *d_occ, uint64_t npx, unsigned long
 }
 
 template <int B>
-__global__ void __launch_bounds__(32 * 17, 1) compare_cell_kernel(const __grid_constant__ CmpArgs a) {
+__global__ void __launch_bounds__(32 * 13, 1) compare_cell_kernel(const __grid_constant__ CmpArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int ST = a.stages;
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
@@ -824,10 +824,26 @@ __global__ void __launch_bounds__(32 * 17, 1) compare_cell_kernel(const __grid_c
   if (cw >= NC) return;
   const uint64_t pol_occ = l2_evict_last();
   const uint32_t QS = (uint32_t)(a.qS < 1 ? 1 : a.qS);
-  uint32_t *hl = reinterpret_cast<uint32_t *>(ring + (size_t)ST * a.tile_bytes +
-                                              (size_t)cw * cell_warp_bytes(a.qS));
+  unsigned char *wb = ring + (size_t)ST * a.tile_bytes +
+                      (size_t)cw * cell_warp_bytes(a.qS, a.cell_queue);
+  uint32_t *hl = reinterpret_cast<uint32_t *>(wb);
   uint32_t *wm = hl + 32u * QS;  // per window: hit bits
   uint32_t *cum = wm + QS;       // per window: hits before it
+  // the candidate queue (cell_queue): id, count, marked spots at an odd stride
+  const uint32_t SP = clist_queue_stride(a.qS);
+  unsigned char *qb = wb + cell_warp_bytes(a.qS);
+  uint64_t *q_oid = reinterpret_cast<uint64_t *>(qb);
+  uint32_t *q_c = reinterpret_cast<uint32_t *>(qb + 256);
+  uint32_t *q_sp = reinterpret_cast<uint32_t *>(qb + 384);
+  int qn = 0;
+  auto flush = [&]() {
+    __syncwarp();
+    const bool v = lane < qn;
+    process<B, ListSpots, 1>(a, ListSpots{q_sp + lane * SP}, v ? (int)q_c[lane] : 0,
+                             v ? q_oid[lane] : 0, pol_occ, v);
+    __syncwarp();
+    qn = 0;
+  };
   const unsigned lt = (1u << lane) - 1u;
   const int need = a.full_gather ? 0 : a.min_spots;
   const int sh = a.cm_shift;
@@ -899,14 +915,33 @@ __global__ void __launch_bounds__(32 * 17, 1) compare_cell_kernel(const __grid_c
         const uint32_t h0 = hits_before(xs);
         const int ub = (int)(hits_before(xe) - h0);
         const bool cand = valid && c <= a.qS && ub >= need;
-        if (__any_sync(0xffffffffu, cand))
+        if (a.cell_queue) {
+          // into the queue (marked spots only, in order), emptied when full
+          unsigned qm = __ballot_sync(0xffffffffu, cand);
+          while (qm) {
+            unsigned rest = qm;
+            for (int r = 32 - qn; r > 0 && rest; r--) rest &= rest - 1;
+            const unsigned take = qm & ~rest;
+            if ((take >> lane) & 1u) {
+              const int pos = qn + __popc(take & ((1u << lane) - 1u));
+              q_oid[pos] = oid;
+              q_c[pos] = (uint32_t)ub;
+              for (int k = 0; k < ub; k++) q_sp[pos * SP + k] = hl[h0 + k];
+            }
+            qn += __popc(take);
+            qm = rest;
+            if (qn == 32) flush();
+          }
+        } else if (__any_sync(0xffffffffu, cand)) {
           process<B, ListSpots, 1>(a, ListSpots{hl + h0}, cand ? ub : 0, oid, pol_occ, cand);
+        }
         __syncwarp();
       }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
+  if (qn) flush();
 }
 
 // ----------------------------------------------------------------------------
@@ -994,7 +1029,7 @@ CompareTuning compare_config(int R, const CompareTuning &req) {
   if (c.variant == 4) {  // compact layout + cell mask: one block per SM
     c.tile_sub = 0;
     if (c.consumers <= 0) c.consumers = 12;
-    c.consumers = std::min(c.consumers, 16);
+    c.consumers = std::min(c.consumers, 12);  // 13 warps: __launch_bounds__ of the kernel
     c.stages = c.stages > 0 ? std::max(2, std::min(c.stages, 16)) : 0;  // 0: as many as fit
     c.blocks_per_sm = 1;
     c.grid_mult = 1;
@@ -1085,11 +1120,13 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
                     a.cm_bytes <= kCellMaskBytes && (reinterpret_cast<uintptr_t>(a.cellmask) & 15) == 0,
                 "cell mask missing or malformed");
     LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "cell pass hit lists of %d spots per record", a.qS);
+    a.cell_queue = c.cell_queue ? 1 : 0;
+    const size_t per_warp = cell_warp_bytes(a.qS, a.cell_queue);
     while (c.consumers > 1 &&
-           256 + (size_t)a.cm_bytes + (size_t)c.consumers * cell_warp_bytes(a.qS) +
-                   2 * (size_t)a.tile_bytes > 227 * 1024)
+           256 + (size_t)a.cm_bytes + (size_t)c.consumers * per_warp + 2 * (size_t)a.tile_bytes >
+               227 * 1024)
       c.consumers--;
-    fixed += a.cm_bytes + (size_t)c.consumers * cell_warp_bytes(a.qS);
+    fixed += a.cm_bytes + (size_t)c.consumers * per_warp;
   }
   a.consumers = c.consumers;
   if (c.variant == 2 || c.variant == 4) {

@@ -108,7 +108,7 @@ struct lmb_engine {
   cudaEvent_t ev_released[LMB_MAX_SLOTS] = {};
   // automatic variant with the compact pass's tuned shape (2 stages, 3 consumer
   // warps, 8 blocks per SM)
-  CompareTuning tuning{3, 0, 2, 3, 1, 8, 0, 0, 0, 0};
+  CompareTuning tuning{3, 0, 2, 3, 1, 8, 0, 0, 0, 0, 0};
   int last_variant = -1;  // variant the latest pass ran
   std::vector<PassGraph> graphs;  // captured passes, most recent last
   bool use_graphs = true;
@@ -496,7 +496,8 @@ double gathered_per_record(const lmb_engine *e, int min_spots) {
 // The cell-mask pass needs its mask, a hit list per consumer warp and a
 // two-stage ring of the layout's tiles in one block's shared memory.
 bool cell_pass_fits(const lmb_engine *e) {
-  const size_t need = 256 + (size_t)e->cm_bytes + cell_warp_bytes(e->cl_qs > 0 ? e->cl_qs : e->S) +
+  const size_t need = 256 + (size_t)e->cm_bytes +
+                      cell_warp_bytes(e->cl_qs > 0 ? e->cl_qs : e->S, e->tuning.cell_queue) +
                       2 * (size_t)e->cl_stage;
   return e->d_cellmask && need <= 227 * 1024;
 }
@@ -1090,12 +1091,12 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
         tun.variant = 2;
       else if (!tun.full_gather && min_nr_spots >= 1 && cell_pass_fits(e))
         tun = CompareTuning{4, 0, tun.cell_stages, tun.cell_consumers, 1, 1, 0,
-                            tun.test_consumer_wait_us, 0, 0};  // the cell-mask pass's shape
+                            tun.test_consumer_wait_us, 0, 0, tun.cell_queue};  // cell-mask pass
       else
         compact = false;
     }
     if (!compact)  // warp-specialised over the reference records
-      tun = CompareTuning{1, 0, 0, 0, 0, 0, tun.full_gather, tun.test_consumer_wait_us, 0, 0};
+      tun = CompareTuning{1, 0, 0, 0, 0, 0, tun.full_gather, tun.test_consumer_wait_us, 0, 0, 0};
   }
   e->last_variant = tun.variant;
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
@@ -1296,12 +1297,13 @@ int lmb_last_pass_ms(lmb_engine *e, float *compare_ms, float *order_ms) {
 
 int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields) {
   LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
-  CompareTuning t{1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  int32_t *dst[10] = {&t.variant,     &t.tile_sub,  &t.stages,
+  CompareTuning t{1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int32_t *dst[11] = {&t.variant,     &t.tile_sub,      &t.stages,
                       &t.consumers,   &t.blocks_per_sm, &t.grid_mult,
                       &t.full_gather, &t.test_consumer_wait_us, &t.cell_consumers,
-                      &t.cell_stages};
-  for (int i = 0; i < n_fields && i < 10; i++) *dst[i] = fields[i];
+                      &t.cell_stages, &t.cell_queue};
+  for (int i = 0; i < n_fields && i < 11; i++) *dst[i] = fields[i];
+  LMB_REQUIRE(t.cell_queue == 0 || t.cell_queue == 1, "cell_queue must be 0 or 1");
   LMB_REQUIRE(t.cell_consumers >= 0 && t.cell_consumers <= 16 && t.cell_stages >= 0 &&
                   t.cell_stages <= 16,
               "cell-mask pass shape (%d consumers, %d stages) out of range", t.cell_consumers,
@@ -1340,11 +1342,11 @@ int lmb_engine_set_sparse_uploads(lmb_engine *e, int32_t enable) {
 int lmb_engine_get_tuning(lmb_engine *e, int32_t *fields, int32_t n_fields) {
   LMB_REQUIRE(e && (fields || n_fields == 0), "null argument");
   const CompareTuning c = compare_config(e->R, e->tuning);
-  const int32_t src[11] = {c.variant,        c.tile_sub,       c.stages,
+  const int32_t src[12] = {c.variant,        c.tile_sub,       c.stages,
                            c.consumers,      c.blocks_per_sm,  c.grid_mult,
                            c.full_gather,    e->last_variant,  c.test_consumer_wait_us,
-                           c.cell_consumers, c.cell_stages};
-  for (int i = 0; i < n_fields && i < 11; i++) fields[i] = src[i];
+                           c.cell_consumers, c.cell_stages,    c.cell_queue};
+  for (int i = 0; i < n_fields && i < 12; i++) fields[i] = src[i];
   return LMB_OK;
 }
 

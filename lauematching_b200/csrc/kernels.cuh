@@ -42,6 +42,10 @@ struct CmpArgs {
   // this long on a shared-memory barrier nothing arrives at, instead of on its
   // ring slot, so the pass gives up with a timeout (0 in every normal pass)
   uint64_t test_consumer_wait_ns;
+  // variant 4: 1 = records that can still pass are copied (their marked
+  // spots) into a per-warp queue and counted 32 at a time; 0 = counted in
+  // place, chunk by chunk
+  int cell_queue;
   // filled by compare_launch
   uint64_t full_tiles, ntiles;
   uint32_t tile_bytes;
@@ -66,6 +70,7 @@ struct CompareTuning {
   // (0 = defaults): consumer warps, ring stages
   int cell_consumers;
   int cell_stages;
+  int cell_queue;  // variant 4: see CmpArgs::cell_queue
 };
 CompareTuning compare_config(int R, const CompareTuning &req);
 
@@ -196,6 +201,10 @@ __host__ __forceinline__ uint32_t cellmask_bytes(uint64_t npx) {
 __host__ __device__ __forceinline__ uint32_t cell_warp_bytes(int qS) {
   const uint32_t q = (uint32_t)(qS < 1 ? 1 : qS);
   return ((32u * q + 2u * q) * 4u + 15u) / 16u * 16u;
+}
+// ... plus, with the candidate queue, a record queue like the compact pass's
+__host__ __device__ __forceinline__ uint32_t cell_warp_bytes(int qS, int queue) {
+  return cell_warp_bytes(qS) + (queue ? clist_queue_bytes(qS) : 0u);
 }
 int cellmask_launch(const unsigned long long *d_occ, uint64_t npx, unsigned long long active,
                     int shift, uint32_t cm_bytes, uint32_t *d_mask, int num_sms, cudaStream_t st);

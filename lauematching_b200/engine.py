@@ -107,20 +107,21 @@ class Engine:
                      "full_gather")
 
     def set_tuning(self, test_consumer_wait_us: int = 0, cell_consumers: int = 0,
-                   cell_stages: int = 0, **kw) -> None:
+                   cell_stages: int = 0, cell_queue: int = 0, **kw) -> None:
         """Pin the compare pass's launch shape (TUNING_FIELDS; variant 3 =
         automatic when not given; cell_consumers / cell_stages shape the
         cell-mask pass when the automatic variant picks it).
         test_consumer_wait_us is for tests only: the pass gives up after that
         wait and reports a timeout."""
         check(lib().lmb_engine_set_tuning(
-            self._h, self._tuning_vals(kw, test_consumer_wait_us, cell_consumers, cell_stages),
-            10))
+            self._h, self._tuning_vals(kw, test_consumer_wait_us, cell_consumers, cell_stages,
+                                       cell_queue), 11))
         self._pinned_shape = True
 
-    def _tuning_vals(self, kw, test_wait=0, cell_consumers=0, cell_stages=0):
-        vals = (C.c_int32 * 10)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS],
-                                int(test_wait), int(cell_consumers), int(cell_stages))
+    def _tuning_vals(self, kw, test_wait=0, cell_consumers=0, cell_stages=0, cell_queue=0):
+        vals = (C.c_int32 * 11)(*[int(kw.get(f, 0)) for f in self.TUNING_FIELDS],
+                                int(test_wait), int(cell_consumers), int(cell_stages),
+                                int(cell_queue))
         if "variant" not in kw:
             vals[0] = 3
         return vals
@@ -252,7 +253,8 @@ class Engine:
             if shape:
                 check(lib().lmb_engine_set_tuning(
                     self._h, self._tuning_vals(shape, 0, dense.get("consumers", 0),
-                                               dense.get("stages", 0)), 10))
+                                               dense.get("stages", 0),
+                                               dense.get("cell_queue", 0)), 11))
             self._shape_bucket = b
 
     def match(self, slots, min_nr_spots: int, min_intensity: float, value_mode: int = 0) -> None:

@@ -136,8 +136,9 @@ def test_input_dtypes_f32_u8_match_f64():
         assert np.array_equal(r[0][0], r[k][0]) and r[0][1] == r[k][1]
 
 
-@pytest.mark.parametrize("variant,full_gather", [(1, 0), (1, 1), (2, 0), (2, 1), (4, 0), (4, 1)])
-def test_edge_records_partial_tiles_and_thresholds(variant, full_gather):
+@pytest.mark.parametrize("variant,full_gather,queue", [(1, 0, 0), (1, 1, 0), (2, 0, 0), (2, 1, 0),
+                                                      (4, 0, 0), (4, 1, 0), (4, 0, 1), (4, 1, 1)])
+def test_edge_records_partial_tiles_and_thresholds(variant, full_gather, queue):
     """Counts above S (clamped), pixels off the detector (skipped), DB sizes
     that are not a multiple of the tile, MinNrSpots <= 0 and > S; in the
     reference layout (variant 1), the compact one (variant 2) and the compact
@@ -156,7 +157,7 @@ def test_edge_records_partial_tiles_and_thresholds(variant, full_gather):
         img = np.where(rng.random(300 * 200) < 0.3, rng.integers(1, 256, 300 * 200), 0)
         img = img.astype(np.float64) * 0.77
         with engine_for(p) as e:
-            e.set_tuning(variant=variant, full_gather=full_gather)
+            e.set_tuning(variant=variant, full_gather=full_gather, cell_queue=queue)
             e.upload_db(rec)
             e.load_image(0, img)
             for ms, mi in ((2, 3.0), (0, 0.0), (-3, -1.0), (8, 0.0), (1, 1e9)):
@@ -246,7 +247,8 @@ def test_compact_layout_matches_oracle(name, mode):
 
 @pytest.mark.parametrize("name", golden_names())
 @pytest.mark.parametrize("mode", [0, 1])
-def test_cell_mask_pass_matches_oracle(name, mode):
+@pytest.mark.parametrize("queue", [0, 1])
+def test_cell_mask_pass_matches_oracle(name, mode, queue):
     """Variant 4 (compact layout filtered by the cell mask of the pass's
     frames) on the reference's golden cases.  A frame in a slot outside the
     pass, positive everywhere, must not widen or change anything: the mask is
@@ -258,7 +260,7 @@ def test_cell_mask_pass_matches_oracle(name, mode):
     ref2 = O.compare(c.records, p.max_nr_spots, c.image * 0.5, p.nr_px_x, p.nr_px_y,
                      p.min_nr_spots, p.min_intensity, mode=mode)
     with engine_for(p) as e:
-        e.set_tuning(variant=4)
+        e.set_tuning(variant=4, cell_queue=queue)
         e.upload_db(c.records)
         e.load_image(5, c.image, keep_f64=(mode == 1))
         e.load_image(6, c.image * 0.5, keep_f64=(mode == 1))
@@ -301,18 +303,19 @@ def test_cell_mask_cells_and_detector_sizes(nr_px):
         img[-1] = 99.0
         imgs.append(img)
     with engine_for(p) as e:
-        e.set_tuning(variant=4)
         e.upload_db(rec)
         for k in range(3):
             e.load_image(k, imgs[k])
-        for ms in (1, 3, 6, 24, 30):
-            e.match([0, 1, 2], ms, 5.0)
-            assert e.get_tuning()["last_variant"] == 4
-            for k in range(3):
-                got, npass = e.results(k)
-                ref = O.compare(rec, S, imgs[k], W, H, ms, 5.0)
-                assert npass == ref.n_pass, (ms, k)
-                assert_same_survivors(got, ref)
+        for queue in (0, 1):
+            e.set_tuning(variant=4, cell_queue=queue)
+            for ms in (1, 3, 6, 24, 30):
+                e.match([0, 1, 2], ms, 5.0)
+                assert e.get_tuning()["last_variant"] == 4
+                for k in range(3):
+                    got, npass = e.results(k)
+                    ref = O.compare(rec, S, imgs[k], W, H, ms, 5.0)
+                    assert npass == ref.n_pass, (ms, k, queue)
+                    assert_same_survivors(got, ref)
 
 
 @pytest.mark.parametrize("nb", [7, 8])
@@ -363,8 +366,9 @@ def test_compact_layout_batched_equals_reference_layout():
             for k in range(12):
                 assert got[k][1] == ref[k][1] and np.array_equal(got[k][0], ref[k][0])
         # the cell-mask pass (variant 4) under several shapes
-        for shape in ({}, {"consumers": 4}, {"consumers": 16, "stages": 2}, {"stages": 3},
-                      {"full_gather": 1}, {"consumers": 1}):
+        for shape in ({}, {"consumers": 4}, {"consumers": 12, "stages": 2}, {"stages": 3},
+                      {"full_gather": 1}, {"consumers": 1}, {"cell_queue": 1},
+                      {"cell_queue": 1, "consumers": 11}, {"cell_queue": 1, "full_gather": 1}):
             e.set_tuning(variant=4, **shape)
             e.match(range(12), p.min_nr_spots, p.min_intensity)
             got = e.results_batch(range(12))
