@@ -501,7 +501,9 @@ def tilted_leg(args, dev, K=64, n=None):
         ref_surv = None
         for name, tun in (("auto", None), ("reference_layout", dict(variant=1)),
                           ("compact_no_mask", dict(variant=2, stages=2, consumers=3,
-                                                   grid_mult=8))):
+                                                   grid_mult=8)),
+                          ("cell_mask_in_place", dict(variant=4)),
+                          ("cell_mask_queued", dict(variant=4, cell_queue=1))):
             if tun is None:
                 e._pinned_shape = False
                 e._shape_bucket = None
