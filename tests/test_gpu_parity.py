@@ -623,7 +623,9 @@ def test_hexagonal_fundamental_zone_db_build():
         assert np.array_equal(e.synth_orientations(3, 0, n), om_fz)
         plain = e.synth_orientations(3, 0, n, hex_fz=False)
     host = synth.hexagonal_fundamental_zone(plain)
-    assert np.max(np.abs(host - om_fz)) < 1e-12
+    # the host reduction recovers the quaternion from the matrix (square roots
+    # of small diagonal sums) and loses a few ulps more than the device's path
+    assert np.max(np.abs(host - om_fz)) < 1e-10
     # an equivalent rotation: R_fz = R_plain . S for a symmetry operator S
     m_fz, m_pl = om_fz.reshape(-1, 3, 3), plain.reshape(-1, 3, 3)
     rel = np.einsum("nji,njk->nik", m_pl, m_fz)  # R_plain^T R_fz
