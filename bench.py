@@ -513,7 +513,8 @@ def tilted_leg(args, dev, K=64, n=None):
                           ("compact_no_mask", dict(variant=2, stages=2, consumers=3,
                                                    grid_mult=8)),
                           ("cell_mask_in_place", dict(variant=4)),
-                          ("cell_mask_queued", dict(variant=4, cell_queue=1))):
+                          ("cell_mask_queued", dict(variant=4, cell_queue=1)),
+                          ("cell_filter_then_count", dict(variant=5))):
             if tun is None:
                 e._pinned_shape = False
                 e._shape_bucket = None
@@ -580,7 +581,7 @@ def tilted_leg(args, dev, K=64, n=None):
         auto = runs["auto"]
         t = auto["compare_ms"] * 1e-3
         ref_bytes = n * REC_BYTES_PER_ORIENT + K * p.nr_px_x * p.nr_px_y
-        streamed = (lay["bytes"] + p.nr_px_x * p.nr_px_y * 8) if auto["variant"] in (2, 4) \
+        streamed = (lay["bytes"] + p.nr_px_x * p.nr_px_y * 8) if auto["variant"] in (2, 4, 5) \
             else ref_bytes
         out["roofline"] = {"bound": "hbm", "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                            "reference_layout_bytes": ref_bytes,

@@ -132,6 +132,12 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst_smem, const void *src_gm
       : "memory");
 }
 
+// Prefetch `bytes` (multiple of 16, 16-byte aligned) of global memory into L2.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src_gmem, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src_gmem), "r"(bytes)
+               : "memory");
+}
+
 // 1-D bulk copy global -> shared of `bytes` (multiple of 16, both addresses
 // 16-byte aligned), completing on `bar` via complete_tx.
 __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes,

@@ -945,6 +945,230 @@ __global__ void __launch_bounds__(32 * 13, 1) compare_cell_kernel(const __grid_c
 }
 
 // ----------------------------------------------------------------------------
+// Variant 5: the cell-mask filter and the counting of its candidates as two
+// kernels.
+//
+// In one kernel (variant 4) the per-record counting logic rides along with
+// the spot filter: its registers and branches weigh on every chunk, and the
+// chunks of a tile are dealt out across all consumer warps, so each warp
+// walks every chunk of every tile.  Here the filter kernel only streams and
+// filters: one ring stage per consumer warp, the warp takes whole tiles (the
+// producer prefetches the warp's next tile into L2 while the warp works),
+// tests each spot's cell 64 spots at a time, and appends the records that can
+// still pass (at least MinNrSpots spots on marked cells) with their marked
+// pixels, in record order, to its block's region of a candidate buffer.  The
+// counting kernel then runs the per-record logic of the other variants on
+// full warps of candidates.  Survivors and pass counts are those of the other
+// variants (the candidate set and each candidate's nonzero spots are the
+// same; order is restored by the ordering kernel).
+// ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_constant__ CmpArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int ST = a.stages;  // == consumer warps: stage w belongs to consumer warp w
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *empty = full + 16;
+  uint32_t *ctr = reinterpret_cast<uint32_t *>(smem + 256);  // entries, pixels, warps done
+  uint32_t *cm = reinterpret_cast<uint32_t *>(smem + 384);
+  unsigned char *ring = smem + 384 + a.cm_bytes;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int NC = a.consumers;
+  const uint64_t G = gridDim.x;
+  const uint64_t my_tiles = (a.ntiles > blockIdx.x) ? (a.ntiles - 1 - blockIdx.x) / G + 1 : 0;
+  {  // the pass's cell mask into shared memory
+    const uint4 *src = reinterpret_cast<const uint4 *>(a.cellmask);
+    uint4 *dst = reinterpret_cast<uint4 *>(cm);
+    for (uint32_t i = threadIdx.x; i < a.cm_bytes / 16; i += blockDim.x) dst[i] = src[i];
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    ctr[0] = ctr[1] = ctr[2] = 0u;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    if (lane != 0) return;
+    const uint64_t pol_db = l2_evict_first();
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < my_tiles; i++) {
+      const int s = (int)(i % ST);
+      if (i >= (uint64_t)ST &&
+          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+        atomicExch(a.err, DEV_TIMEOUT_TMA);
+        break;
+      }
+      const uint64_t t = blockIdx.x + i * G;
+      mbar_expect_tx(&full[s], a.tile_bytes);
+      bulk_g2s_hint(ring + (size_t)s * a.tile_bytes, a.cl + t * a.tile_bytes, a.tile_bytes,
+                    &full[s], pol_db);
+      // the same warp's next tile, into L2 while this one is worked on
+      if (i + ST < my_tiles) bulk_prefetch_l2(a.cl + (t + ST * G) * a.tile_bytes, a.tile_bytes);
+      issued = i + 1;
+    }
+    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
+      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    return;
+  }
+  const int cw = warp - 1;
+  if (cw >= NC) return;
+  const uint32_t QS = (uint32_t)(a.qS < 1 ? 1 : a.qS);
+  uint32_t *wm = reinterpret_cast<uint32_t *>(ring + (size_t)ST * a.tile_bytes +
+                                              (size_t)cw * filter_warp_bytes(a.qS));
+  const unsigned lt = (1u << lane) - 1u;
+  const int need = a.full_gather ? 0 : a.min_spots;
+  const int sh = a.cm_shift;
+  const uint64_t e_base = a.cq_ebase[blockIdx.x], e_cap = a.cq_ebase[blockIdx.x + 1] - e_base;
+  const uint64_t p_base = a.cq_pbase[blockIdx.x], p_cap = a.cq_pbase[blockIdx.x + 1] - p_base;
+  CandEntry *E = a.cq_e + e_base;
+  uint32_t *P = a.cq_pix + p_base;
+  const int s = cw;  // this warp's ring stage
+  for (uint64_t i = (uint64_t)cw; i < my_tiles; i += (uint64_t)NC) {
+    const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
+      break;
+    }
+    const unsigned char *tb = ring + (size_t)s * a.tile_bytes;
+    const uint64_t first = *reinterpret_cast<const uint64_t *>(tb);
+    const uint32_t nch = *reinterpret_cast<const uint32_t *>(tb + 8);
+    const unsigned char *cmax = tb + 16;
+    const unsigned char *cnt = tb + clist_cnt_offset(nch);
+    const uint32_t *base = reinterpret_cast<const uint32_t *>(tb + clist_base_offset(nch));
+    const uint32_t *spots = reinterpret_cast<const uint32_t *>(tb + clist_spot_offset(nch));
+    for (uint32_t j0 = 0; j0 < nch; j0 += 32) {
+      unsigned m = __ballot_sync(0xffffffffu, j0 + lane < nch && cmax[j0 + lane] >= need);
+      while (m) {
+        const uint32_t ch = j0 + (uint32_t)(__ffs(m) - 1);
+        m &= m - 1;
+        const uint64_t oid = first + ch * 32 + lane;
+        const bool valid = oid < a.n;
+        const int c = valid ? cnt[ch * 32 + lane] : 0;
+        if (valid && c > a.qS) atomicExch(a.err, DEV_BAD_QUEUE);  // cannot come from this layout
+        int x = c;  // inclusive prefix sum of the counts over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        const uint32_t total = min((uint32_t)__shfl_sync(0xffffffffu, x, 31), 32u * QS);
+        const uint32_t *sp = spots + base[ch];
+        // hit bits of the chunk's spots, two 32-spot windows per step
+        for (uint32_t w0 = 0; w0 < total; w0 += 64) {
+          const uint32_t k0 = w0 + lane, k1 = w0 + 32 + lane;
+          bool h0 = false, h1 = false;
+          if (k0 < total) {
+            const uint32_t q = sp[k0] >> sh;
+            h0 = (cm[q >> 5] >> (q & 31u)) & 1u;
+          }
+          if (k1 < total) {
+            const uint32_t q = sp[k1] >> sh;
+            h1 = (cm[q >> 5] >> (q & 31u)) & 1u;
+          }
+          const unsigned b0 = __ballot_sync(0xffffffffu, h0);
+          const unsigned b1 = __ballot_sync(0xffffffffu, h1);
+          if (lane == 0) {
+            wm[w0 >> 5] = b0;
+            if (w0 + 32 < total) wm[(w0 >> 5) + 1] = b1;
+          }
+        }
+        __syncwarp();
+        // this record's spots are [xs, xe) of the chunk: its marked ones
+        const uint32_t xe = min((uint32_t)x, total), xs = min((uint32_t)(x - c), total);
+        int ub = 0;
+        for (uint32_t w = xs >> 5; xe > xs && w <= (xe - 1) >> 5; w++) {
+          unsigned mw = wm[w];
+          const int lo = (int)xs - (int)(w << 5), hi = (int)xe - (int)(w << 5);
+          if (lo > 0) mw &= ~0u << lo;
+          if (hi < 32) mw &= (1u << hi) - 1u;
+          ub += __popc(mw);
+        }
+        const bool cand = valid && c <= a.qS && ub >= need;
+        const unsigned cmk = __ballot_sync(0xffffffffu, cand);
+        if (cmk) {
+          // the warp's places in the block's region: one reservation per chunk
+          const int mine = cand ? ub : 0;
+          int px = mine;  // inclusive prefix of the candidates' marked spots
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, px, o);
+            if (lane >= o) px += y;
+          }
+          uint32_t e0 = 0, p0 = 0;
+          if (lane == 31) {
+            e0 = atomicAdd(&ctr[0], (uint32_t)__popc(cmk));
+            p0 = atomicAdd(&ctr[1], (uint32_t)px);
+          }
+          e0 = __shfl_sync(0xffffffffu, e0, 31);
+          p0 = __shfl_sync(0xffffffffu, p0, 31);
+          if (cand) {
+            const uint64_t e = (uint64_t)e0 + (uint64_t)__popc(cmk & lt);
+            const uint64_t off = (uint64_t)p0 + (uint64_t)(px - mine);
+            if (e < e_cap && off + (uint64_t)ub <= p_cap) {
+              CandEntry ce;
+              ce.oid = oid;
+              ce.off = (uint32_t)off;
+              ce.n = (uint32_t)ub;
+              E[e] = ce;
+              uint32_t k = 0;  // its marked pixels in record order
+              for (uint32_t w = xs >> 5; w <= (xe - 1) >> 5; w++) {
+                unsigned mw = wm[w];
+                const int lo = (int)xs - (int)(w << 5), hi = (int)xe - (int)(w << 5);
+                if (lo > 0) mw &= ~0u << lo;
+                if (hi < 32) mw &= (1u << hi) - 1u;
+                while (mw) {
+                  const int b = __ffs(mw) - 1;
+                  mw &= mw - 1;
+                  P[off + k++] = sp[(w << 5) + (uint32_t)b];
+                }
+              }
+            } else {
+              atomicExch(a.err, DEV_BAD_QUEUE);  // regions hold every record: cannot happen
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  // the last consumer warp to finish publishes the block's counts
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence_block();
+    if (atomicAdd(&ctr[2], 1u) == (uint32_t)NC - 1) {
+      a.cq_count[2 * blockIdx.x] = atomicAdd(&ctr[0], 0u);
+      a.cq_count[2 * blockIdx.x + 1] = atomicAdd(&ctr[1], 0u);
+    }
+  }
+}
+
+// The filter's candidates, 32 per warp: the per-record logic of the other
+// variants over each candidate's marked pixels.  blockIdx.y = the filter
+// block whose region is read.
+template <int B>
+__global__ void __launch_bounds__(256) cell_count_kernel(const __grid_constant__ CmpArgs a) {
+  const uint32_t b = blockIdx.y;
+  const uint64_t cap = a.cq_ebase[b + 1] - a.cq_ebase[b];
+  const uint64_t n = min((uint64_t)a.cq_count[2 * b], cap);
+  const CandEntry *E = a.cq_e + a.cq_ebase[b];
+  const uint32_t *P = a.cq_pix + a.cq_pbase[b];
+  const int lane = threadIdx.x & 31;
+  const uint64_t wpb = blockDim.x >> 5;
+  const uint64_t nw = gridDim.x * wpb;
+  const uint64_t pol_occ = l2_evict_last();
+  for (uint64_t g = (blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; g < n; g += nw * 32) {
+    const uint64_t e = g + lane;
+    const bool v = e < n;
+    CandEntry ce{0ull, 0u, 0u};
+    if (v) ce = E[e];
+    process<B, ListSpots, 1>(a, ListSpots{P + ce.off}, v ? (int)ce.n : 0, ce.oid, pol_occ, v);
+  }
+}
+
+// ----------------------------------------------------------------------------
 // Ordering: per slot, sort survivors by ID (keys id<<24 | index), bitonic.
 // ----------------------------------------------------------------------------
 
@@ -1026,6 +1250,15 @@ static int counter_bits(int S) {
 CompareTuning compare_config(int R, const CompareTuning &req) {
   CompareTuning c = req;
   const size_t rb = (size_t)R * 2;
+  if (c.variant == 5) {  // cell-mask filter + counting kernel: one filter block per SM
+    c.tile_sub = 0;
+    if (c.consumers <= 0) c.consumers = 12;
+    c.consumers = std::min(c.consumers, 12);  // 13 warps: __launch_bounds__ of the kernel
+    c.stages = c.consumers;                   // one ring stage per consumer warp
+    c.blocks_per_sm = 1;
+    c.grid_mult = 1;
+    return c;
+  }
   if (c.variant == 4) {  // compact layout + cell mask: one block per SM
     c.tile_sub = 0;
     if (c.consumers <= 0) c.consumers = 12;
@@ -1078,7 +1311,14 @@ static int launch_clist_bounded(const CmpArgs &a, unsigned grid, size_t smem, cu
 template <int B>
 static int launch_b(const CmpArgs &a, const CompareTuning &c, unsigned grid, size_t smem,
                     int nblk, cudaStream_t st) {
-  if (c.variant == 4) {
+  if (c.variant == 5) {
+    int rc = ensure_smem((const void *)cell_filter_kernel, (int)smem);
+    if (rc) return rc;
+    cell_filter_kernel<<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
+    LMB_CUDA(cudaGetLastError());
+    // the counting kernel: four 256-thread blocks per filter block's region
+    cell_count_kernel<B><<<dim3(4, grid), 256, 0, st>>>(a);
+  } else if (c.variant == 4) {
     const int rc = ensure_smem((const void *)compare_cell_kernel<B>, (int)smem);
     if (rc) return rc;
     compare_cell_kernel<B><<<grid, 32 * (1 + c.consumers), smem, st>>>(a);
@@ -1111,8 +1351,25 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   CompareTuning c = compare_config(a.R, req);
   a.test_consumer_wait_ns = (uint64_t)std::max(0, c.test_consumer_wait_us) * 1000ull;
   LMB_REQUIRE(!a.test_consumer_wait_ns || c.variant == 2 || c.variant == 4,
-              "the test wait applies to the compact-layout passes only");
+              "the test wait applies to variants 2 and 4");
   size_t fixed = 256;  // barriers
+  if (c.variant == 5) {
+    // barriers and block counters, the cell mask, and per consumer warp one
+    // ring stage (set below) and its window words
+    LMB_REQUIRE(a.cellmask && a.cm_bytes > 0 && a.cm_bytes % 128 == 0 &&
+                    a.cm_bytes <= kCellMaskBytes && (reinterpret_cast<uintptr_t>(a.cellmask) & 15) == 0,
+                "cell mask missing or malformed");
+    LMB_REQUIRE(a.cq_e && a.cq_pix && a.cq_ebase && a.cq_pbase && a.cq_count,
+                "candidate buffer missing");
+    LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "filter windows for %d spots per record", a.qS);
+    LMB_REQUIRE(!c.test_consumer_wait_us, "the test wait applies to variants 2 and 4");
+    while (c.consumers > 1 &&
+           384 + (size_t)a.cm_bytes +
+                   (size_t)c.consumers * (a.tile_bytes + filter_warp_bytes(a.qS)) > 227 * 1024)
+      c.consumers--;
+    c.stages = c.consumers;
+    fixed = 384 + a.cm_bytes + (size_t)c.consumers * filter_warp_bytes(a.qS);
+  }
   if (c.variant == 4) {
     // the cell mask, and per consumer warp its hit list and window words; as
     // many consumer warps as leave room for a two-stage ring
@@ -1129,7 +1386,7 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
     fixed += a.cm_bytes + (size_t)c.consumers * per_warp;
   }
   a.consumers = c.consumers;
-  if (c.variant == 2 || c.variant == 4) {
+  if (c.variant == 2 || c.variant == 4 || c.variant == 5) {
     // a.cl_tiles tiles of a.tile_bytes come from the compact layout; every
     // tile, the last included, is one bulk copy
     LMB_REQUIRE(a.cl && a.cl_tiles > 0 && a.tile_bytes > 0 && a.tile_bytes % 128 == 0,
@@ -1141,12 +1398,17 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
     a.full_tiles = a.ntiles;
     LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "compact pass queue entry of %d spots", a.qS);
     const size_t qbytes =
-        c.variant == 4 ? fixed - 256 : (size_t)c.consumers * clist_queue_bytes(a.qS);
+        c.variant >= 4 ? fixed - 256 : (size_t)c.consumers * clist_queue_bytes(a.qS);
     const size_t room = 227 * 1024 > 256 + qbytes ? 227 * 1024 - 256 - qbytes : 0;
     // barrier 15 is the test wait's when one is set
     const int fit = (int)std::min<size_t>(a.test_consumer_wait_ns ? 15 : 16, room / a.tile_bytes);
-    LMB_REQUIRE(fit >= 2, "compact tiles of %u bytes leave no room for a ring", a.tile_bytes);
-    c.stages = c.stages > 0 ? std::min(c.stages, fit) : fit;
+    if (c.variant == 5) {  // one stage per consumer warp, sized above
+      LMB_REQUIRE(c.stages >= 1 && c.stages <= fit && c.stages <= 16,
+                  "compact tiles of %u bytes leave no room for the filter's stages", a.tile_bytes);
+    } else {
+      LMB_REQUIRE(fit >= 2, "compact tiles of %u bytes leave no room for a ring", a.tile_bytes);
+      c.stages = c.stages > 0 ? std::min(c.stages, fit) : fit;
+    }
   } else {
     a.tile_sub = c.tile_sub;
     a.tile = (uint32_t)c.tile_sub * 32;
@@ -1158,11 +1420,13 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
   if (a.ntiles == 0 || a.active == 0) return LMB_OK;
   size_t smem = 256 + (size_t)c.stages * a.tile_bytes;
   if (c.variant == 2) smem += (size_t)c.consumers * clist_queue_bytes(a.qS);
-  if (c.variant == 4) smem = fixed + (size_t)c.stages * a.tile_bytes;
+  if (c.variant >= 4) smem = fixed + (size_t)c.stages * a.tile_bytes;
   LMB_REQUIRE(smem <= 227 * 1024, "compare ring of %zu bytes exceeds shared memory", smem);
   const int mult = c.grid_mult > 0 ? c.grid_mult : 1;
   const unsigned grid = (unsigned)std::min<uint64_t>(
       a.ntiles, (uint64_t)num_sms * c.blocks_per_sm * (uint64_t)mult);
+  LMB_REQUIRE(c.variant != 5 || grid == a.cq_blocks,
+              "candidate regions laid out for %u filter blocks, grid of %u", a.cq_blocks, grid);
   const int B = counter_bits(a.S);
   // six to eight 128-thread compact-pass blocks per SM (the tuned shapes) get
   // a kernel whose registers are bounded for that occupancy

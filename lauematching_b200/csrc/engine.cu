@@ -77,6 +77,17 @@ struct lmb_engine {
   int cl_state = 0;  // 0 not built, 1 built, -1 this DB cannot use it
   unsigned long long cl_hist[256] = {};  // records per on-detector spot count
   int cl_qs = 0;  // largest on-detector spot count of a record (sizes the pass's queues)
+  // per tile of the compact layout: its chunks and its spots (sizes the
+  // variant-5 candidate regions: at most every record and spot of a tile)
+  std::vector<uint32_t> cl_tile_nch;
+  std::vector<uint64_t> cl_tile_spots;
+  // variant 5: candidate buffer, per filter block a region of entries and one
+  // of pixels (bases [G+1] each, in one allocation), counts written per block
+  CandEntry *d_cq_e = nullptr;
+  uint32_t *d_cq_pix = nullptr;
+  uint64_t *d_cq_base = nullptr;
+  uint32_t *d_cq_count = nullptr;
+  uint32_t cq_blocks = 0;
   // image slots
   uint8_t *d_u8 = nullptr;
   double *d_f64 = nullptr;  // allocated on first keep_f64 load
@@ -138,6 +149,56 @@ struct lmb_engine {
 
 namespace {
 
+void free_candidates(lmb_engine *e) {
+  cudaFree(e->d_cq_e);
+  cudaFree(e->d_cq_pix);
+  cudaFree(e->d_cq_base);
+  cudaFree(e->d_cq_count);
+  e->d_cq_e = nullptr;
+  e->d_cq_pix = nullptr;
+  e->d_cq_base = nullptr;
+  e->d_cq_count = nullptr;
+  e->cq_blocks = 0;
+}
+
+// The variant-5 candidate buffer for a filter grid of G blocks (block b takes
+// tiles b, b + G, ...): per block room for every record and every spot of its
+// tiles, so the filter cannot run out of room whatever the frames.  Made
+// before the first such pass (never inside a captured pass).
+int ensure_candidates(lmb_engine *e, uint32_t G) {
+  if (e->d_cq_e && e->cq_blocks == G) return LMB_OK;
+  free_candidates(e);
+  std::vector<uint64_t> base(2 * ((size_t)G + 1), 0);
+  uint64_t *eb = base.data(), *pb = base.data() + G + 1;
+  for (uint64_t t = 0; t < e->cl_tiles; t++) {
+    const uint64_t b = t % G;
+    eb[b + 1] += 32ull * e->cl_tile_nch[t];
+    pb[b + 1] += e->cl_tile_spots[t];
+  }
+  for (uint32_t b = 0; b < G; b++) {
+    eb[b + 1] += eb[b];
+    pb[b + 1] += pb[b];
+  }
+  LMB_REQUIRE(pb[G] < (1ull << 40), "candidate pixel buffer too large");
+  for (uint32_t b = 0; b < G; b++)
+    LMB_REQUIRE(pb[b + 1] - pb[b] < (1ull << 32), "candidate region of block %u too large", b);
+  cudaError_t ce = cudaMalloc(&e->d_cq_e, std::max<uint64_t>(eb[G], 1) * sizeof(CandEntry));
+  if (ce == cudaSuccess)
+    ce = cudaMalloc(&e->d_cq_pix, std::max<uint64_t>(pb[G], 1) * sizeof(uint32_t));
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_cq_base, base.size() * sizeof(uint64_t));
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_cq_count, 2ull * G * sizeof(uint32_t));
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(e->d_cq_base, base.data(), base.size() * sizeof(uint64_t),
+                    cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemset(e->d_cq_count, 0, 2ull * G * sizeof(uint32_t));
+  if (ce != cudaSuccess) {
+    free_candidates(e);
+    return cuda_fail(ce, "variant-5 candidate buffer", __FILE__, __LINE__);
+  }
+  e->cq_blocks = G;
+  return LMB_OK;
+}
+
 int check_engine(lmb_engine *e) {
   if (!e) {
     set_error("null engine");
@@ -154,6 +215,10 @@ void free_engine(lmb_engine *e) {
   if (e->ld) cudaStreamSynchronize(e->ld);
   cudaFree(e->d_db);
   cudaFree(e->d_cl);
+  cudaFree(e->d_cq_e);
+  cudaFree(e->d_cq_pix);
+  cudaFree(e->d_cq_base);
+  cudaFree(e->d_cq_count);
   cudaFree(e->d_u8);
   cudaFree(e->d_f64);
   cudaFree(e->d_occ);
@@ -255,6 +320,7 @@ int alloc_db(lmb_engine *e, uint64_t n) {
   e->cl_state = 0;
   e->cl_bytes = 0;
   e->cl_qs = 0;
+  free_candidates(e);
   const size_t bytes = (size_t)n * e->R * 2;
   const size_t alloc = ((bytes + 255) / 256) * 256 + 256;
   LMB_CUDA(cudaMalloc(&e->d_db, alloc));
@@ -474,6 +540,9 @@ int build_compact(lmb_engine *e) {
   e->cl_stage = (uint32_t)TB;
   e->cl_bytes = total;
   e->cl_state = 1;
+  e->cl_tile_nch = tnch;
+  e->cl_tile_spots.assign(nt, 0);
+  for (uint64_t c = 0; c < nch; c++) e->cl_tile_spots[ctile[c]] += cs[c];
   return LMB_OK;
 }
 
@@ -485,6 +554,8 @@ int build_compact(lmb_engine *e) {
 // on average, and up to 1.4x slower beyond (dense records, where the
 // reference records' stream is no longer the cost).
 constexpr double kAutoGather = 3.0;
+// the cell-mask pass the automatic variant runs beyond that
+constexpr int kAutoCellVariant = 5;
 
 double gathered_per_record(const lmb_engine *e, int min_spots) {
   const int m = std::max(0, min_spots);
@@ -535,18 +606,26 @@ int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   a.pass_cnt = e->d_status + LMB_MAX_SLOTS;
   a.err = reinterpret_cast<int *>(e->d_status + 2 * LMB_MAX_SLOTS);
   a.full_gather = k.tuning.full_gather;
-  if (k.tuning.variant == 2 || k.tuning.variant == 4) {
+  if (k.tuning.variant == 2 || k.tuning.variant >= 4) {
     a.cl = e->d_cl;
     a.cl_tiles = e->cl_tiles;
     a.tile_bytes = e->cl_stage;
   }
-  if (k.tuning.variant == 4) {
+  if (k.tuning.variant >= 4) {
     a.cellmask = e->d_cellmask;
     a.cm_bytes = e->cm_bytes;
     a.cm_shift = e->cm_shift;
   }
+  if (k.tuning.variant == 5) {
+    a.cq_e = e->d_cq_e;
+    a.cq_pix = e->d_cq_pix;
+    a.cq_ebase = e->d_cq_base;
+    a.cq_pbase = e->d_cq_base + e->cq_blocks + 1;
+    a.cq_count = e->d_cq_count;
+    a.cq_blocks = e->cq_blocks;
+  }
   if (k.min_spots <= e->S && !std::isnan(k.min_int)) {
-    if (k.tuning.variant == 4) {  // the cell mask of this pass's slots, then the pass
+    if (k.tuning.variant >= 4) {  // the cell mask of this pass's slots, then the pass
       const int rc = cellmask_launch(e->d_occ, e->npx, k.mask, e->cm_shift, e->cm_bytes,
                                      e->d_cellmask, e->num_sms, e->st);
       if (rc) return rc;
@@ -1090,13 +1169,18 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
       if (gathered_per_record(e, tun.full_gather ? 0 : min_nr_spots) <= kAutoGather)
         tun.variant = 2;
       else if (!tun.full_gather && min_nr_spots >= 1 && cell_pass_fits(e))
-        tun = CompareTuning{4, 0, tun.cell_stages, tun.cell_consumers, 1, 1, 0,
+        tun = CompareTuning{kAutoCellVariant, 0, tun.cell_stages, tun.cell_consumers, 1, 1, 0,
                             tun.test_consumer_wait_us, 0, 0, tun.cell_queue};  // cell-mask pass
       else
         compact = false;
     }
     if (!compact)  // warp-specialised over the reference records
       tun = CompareTuning{1, 0, 0, 0, 0, 0, tun.full_gather, tun.test_consumer_wait_us, 0, 0, 0};
+  }
+  if (tun.variant == 5) {  // its candidate regions, for the filter grid it will launch
+    const uint32_t G = (uint32_t)std::min<uint64_t>(e->cl_tiles, (uint64_t)e->num_sms);
+    rc = ensure_candidates(e, std::max<uint32_t>(G, 1));
+    if (rc) return rc;
   }
   e->last_variant = tun.variant;
   for (int k = 0; k < LMB_MAX_SLOTS; k++)
@@ -1311,7 +1395,7 @@ int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields
   LMB_REQUIRE(t.full_gather == 0 || t.full_gather == 1, "full_gather must be 0 or 1");
   LMB_REQUIRE(t.test_consumer_wait_us >= 0 && t.test_consumer_wait_us <= 1000000,
               "test wait of %d us outside 0..1000000", t.test_consumer_wait_us);
-  LMB_REQUIRE(t.variant >= 0 && t.variant <= 4, "unknown compare variant %d", t.variant);
+  LMB_REQUIRE(t.variant >= 0 && t.variant <= 5, "unknown compare variant %d", t.variant);
   e->tuning = t;
   return LMB_OK;
 }

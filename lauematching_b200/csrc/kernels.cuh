@@ -6,6 +6,15 @@
 
 namespace lmb {
 
+// A record the cell filter kept: its id and its marked pixels (n of them at
+// offset off of its block's pixel region).
+struct CandEntry {
+  unsigned long long oid;
+  uint32_t off;
+  uint32_t n;
+};
+static_assert(sizeof(CandEntry) == 16, "candidate entry layout");
+
 // One batched DB pass (compare.cu).
 struct CmpArgs {
   const uint16_t *db;  // n records of R uint16, 16-byte aligned
@@ -46,6 +55,17 @@ struct CmpArgs {
   // spots) into a per-warp queue and counted 32 at a time; 0 = counted in
   // place, chunk by chunk
   int cell_queue;
+  // variant 5: records that can still pass after the cell mask, appended by
+  // the filter kernel to its block's region (entries at cq_e + cq_ebase[b],
+  // their marked pixels at cq_pix + cq_pbase[b]); cq_count[2b], [2b + 1] =
+  // entries and pixels the block wrote; the regions hold every record and
+  // spot of the block's tiles, so they cannot overflow
+  struct CandEntry *cq_e;
+  uint32_t *cq_pix;
+  const uint64_t *cq_ebase;
+  const uint64_t *cq_pbase;
+  uint32_t *cq_count;
+  uint32_t cq_blocks;  // the filter grid the regions were laid out for
   // filled by compare_launch
   uint64_t full_tiles, ntiles;
   uint32_t tile_bytes;
@@ -58,7 +78,8 @@ struct CmpArgs {
 // Launch shape of the compare pass (autotuned; zero fields = defaults).
 struct CompareTuning {
   int variant;        // 0 = block-barrier ring, 1 = warp-specialised, 2 = compact layout,
-                      // 3 = automatic, 4 = compact layout + the batch's cell mask
+                      // 3 = automatic, 4 = compact layout + the batch's cell mask,
+                      // 5 = cell-mask filter kernel + candidate counting kernel
   int tile_sub;       // 32-orientation sub-tiles per tile
   int stages;         // ring depth
   int consumers;      // consumer warps (variant 1)
@@ -205,6 +226,12 @@ __host__ __device__ __forceinline__ uint32_t cell_warp_bytes(int qS) {
 // ... plus, with the candidate queue, a record queue like the compact pass's
 __host__ __device__ __forceinline__ uint32_t cell_warp_bytes(int qS, int queue) {
   return cell_warp_bytes(qS) + (queue ? clist_queue_bytes(qS) : 0u);
+}
+// Variant 5's filter kernel: per consumer warp the hit bits of up to qS
+// 32-spot windows.
+__host__ __device__ __forceinline__ uint32_t filter_warp_bytes(int qS) {
+  const uint32_t q = (uint32_t)(qS < 1 ? 1 : qS);
+  return (4u * q + 15u) / 16u * 16u;
 }
 int cellmask_launch(const unsigned long long *d_occ, uint64_t npx, unsigned long long active,
                     int shift, uint32_t cm_bytes, uint32_t *d_mask, int num_sms, cudaStream_t st);

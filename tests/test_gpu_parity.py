@@ -137,7 +137,8 @@ def test_input_dtypes_f32_u8_match_f64():
 
 
 @pytest.mark.parametrize("variant,full_gather,queue", [(1, 0, 0), (1, 1, 0), (2, 0, 0), (2, 1, 0),
-                                                      (4, 0, 0), (4, 1, 0), (4, 0, 1), (4, 1, 1)])
+                                                      (4, 0, 0), (4, 1, 0), (4, 0, 1), (4, 1, 1),
+                                                      (5, 0, 0), (5, 1, 0)])
 def test_edge_records_partial_tiles_and_thresholds(variant, full_gather, queue):
     """Counts above S (clamped), pixels off the detector (skipped), DB sizes
     that are not a multiple of the tile, MinNrSpots <= 0 and > S; in the
@@ -166,7 +167,7 @@ def test_edge_records_partial_tiles_and_thresholds(variant, full_gather, queue):
                 ref = O.compare(rec, 7, img, 300, 200, ms, mi)
                 assert npass == ref.n_pass, (n, ms, mi)
                 assert_same_survivors(got, ref)
-            if variant in (2, 4) and n:
+            if variant in (2, 4, 5) and n:
                 assert e.layout_info()["compact"] == 1
                 assert e.get_tuning()["last_variant"] == variant
 
@@ -190,12 +191,12 @@ def test_automatic_variant_follows_the_spots_that_can_pass(name):
         got, npass = e.results(1)
         used = e.get_tuning()
     assert used["variant"] == 3
-    assert used["last_variant"] == (2 if gathered <= 3.0 else 4), gathered
+    assert used["last_variant"] == (2 if gathered <= 3.0 else 5), gathered
     assert npass == ref.n_pass
     assert_same_survivors(got, ref)
 
 
-@pytest.mark.parametrize("variant", [2, 3, 4])
+@pytest.mark.parametrize("variant", [2, 3, 4, 5])
 def test_many_spots_per_record_keep_the_reference_layout(variant):
     """MaxNrLaueSpots above 255 (uint8 counts cannot hold it): a pass asked for
     the compact layout (alone, automatic or with the cell mask) runs over the
@@ -247,8 +248,8 @@ def test_compact_layout_matches_oracle(name, mode):
 
 @pytest.mark.parametrize("name", golden_names())
 @pytest.mark.parametrize("mode", [0, 1])
-@pytest.mark.parametrize("queue", [0, 1])
-def test_cell_mask_pass_matches_oracle(name, mode, queue):
+@pytest.mark.parametrize("variant,queue", [(4, 0), (4, 1), (5, 0)])
+def test_cell_mask_pass_matches_oracle(name, mode, variant, queue):
     """Variant 4 (compact layout filtered by the cell mask of the pass's
     frames) on the reference's golden cases.  A frame in a slot outside the
     pass, positive everywhere, must not widen or change anything: the mask is
@@ -260,7 +261,7 @@ def test_cell_mask_pass_matches_oracle(name, mode, queue):
     ref2 = O.compare(c.records, p.max_nr_spots, c.image * 0.5, p.nr_px_x, p.nr_px_y,
                      p.min_nr_spots, p.min_intensity, mode=mode)
     with engine_for(p) as e:
-        e.set_tuning(variant=4, cell_queue=queue)
+        e.set_tuning(variant=variant, cell_queue=queue)
         e.upload_db(c.records)
         e.load_image(5, c.image, keep_f64=(mode == 1))
         e.load_image(6, c.image * 0.5, keep_f64=(mode == 1))
@@ -269,7 +270,7 @@ def test_cell_mask_pass_matches_oracle(name, mode, queue):
             e.match([5, 6], p.min_nr_spots, p.min_intensity, value_mode=mode)
             got, npass = e.results(5)
             got2, npass2 = e.results(6)
-            assert e.get_tuning()["last_variant"] == 4
+            assert e.get_tuning()["last_variant"] == variant
             assert npass == ref.n_pass and npass2 == ref2.n_pass
             assert_same_survivors(got, ref)
             assert_same_survivors(got2, ref2)
@@ -306,11 +307,11 @@ def test_cell_mask_cells_and_detector_sizes(nr_px):
         e.upload_db(rec)
         for k in range(3):
             e.load_image(k, imgs[k])
-        for queue in (0, 1):
-            e.set_tuning(variant=4, cell_queue=queue)
+        for variant, queue in ((4, 0), (4, 1), (5, 0)):
+            e.set_tuning(variant=variant, cell_queue=queue)
             for ms in (1, 3, 6, 24, 30):
                 e.match([0, 1, 2], ms, 5.0)
-                assert e.get_tuning()["last_variant"] == 4
+                assert e.get_tuning()["last_variant"] == variant
                 for k in range(3):
                     got, npass = e.results(k)
                     ref = O.compare(rec, S, imgs[k], W, H, ms, 5.0)
@@ -375,6 +376,15 @@ def test_compact_layout_batched_equals_reference_layout():
             assert e.get_tuning()["last_variant"] == 4
             for k in range(12):
                 assert got[k][1] == ref[k][1] and np.array_equal(got[k][0], ref[k][0])
+        # the two-kernel cell-mask pass (variant 5): filter then count
+        for shape in ({}, {"consumers": 4}, {"consumers": 1}, {"full_gather": 1}):
+            for _ in range(2):  # eager, then graph replay (candidate buffer reused)
+                e.set_tuning(variant=5, **shape)
+                e.match(range(12), p.min_nr_spots, p.min_intensity)
+                got = e.results_batch(range(12))
+                assert e.get_tuning()["last_variant"] == 5
+                for k in range(12):
+                    assert got[k][1] == ref[k][1] and np.array_equal(got[k][0], ref[k][0])
         assert e.layout_info()["compact"] == 1
 
 
