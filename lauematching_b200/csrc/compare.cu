@@ -1111,8 +1111,8 @@ __global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_co
               ce.off = (uint32_t)off;
               ce.n = (uint32_t)ub;
               E[e] = ce;
-              uint32_t k = 0;  // its marked pixels in record order
-              for (uint32_t w = xs >> 5; w <= (xe - 1) >> 5; w++) {
+              uint32_t k = 0;  // its marked pixels in record order (none when xe == xs)
+              for (uint32_t w = xs >> 5; xe > xs && w <= (xe - 1) >> 5; w++) {
                 unsigned mw = wm[w];
                 const int lo = (int)xs - (int)(w << 5), hi = (int)xe - (int)(w << 5);
                 if (lo > 0) mw &= ~0u << lo;
