@@ -962,9 +962,12 @@ __global__ void __launch_bounds__(32 * 13, 1) compare_cell_kernel(const __grid_c
 // variants (the candidate set and each candidate's nonzero spots are the
 // same; order is restored by the ordering kernel).
 // ----------------------------------------------------------------------------
-__global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_constant__ CmpArgs a) {
+__global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_constant__ CmpArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const int ST = a.stages;  // == consumer warps: stage w belongs to consumer warp w
+  // consumers / stages warps share a ring stage (its tiles), splitting each
+  // tile's chunks between them
+  const int ST = a.stages;
+  const int CPT = a.consumers / a.stages;
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
   uint64_t *empty = full + 16;
   uint32_t *ctr = reinterpret_cast<uint32_t *>(smem + 256);  // entries, pixels, warps done
@@ -982,7 +985,7 @@ __global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_co
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; s++) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+      mbar_init(&empty[s], CPT);
     }
     ctr[0] = ctr[1] = ctr[2] = 0u;
     fence_mbar_init();
@@ -1003,7 +1006,7 @@ __global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_co
       mbar_expect_tx(&full[s], a.tile_bytes);
       bulk_g2s_hint(ring + (size_t)s * a.tile_bytes, a.cl + t * a.tile_bytes, a.tile_bytes,
                     &full[s], pol_db);
-      // the same warp's next tile, into L2 while this one is worked on
+      // the stage's next tile, into L2 while this one is worked on
       if (i + ST < my_tiles) bulk_prefetch_l2(a.cl + (t + ST * G) * a.tile_bytes, a.tile_bytes);
       issued = i + 1;
     }
@@ -1023,8 +1026,8 @@ __global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_co
   const uint64_t p_base = a.cq_pbase[blockIdx.x], p_cap = a.cq_pbase[blockIdx.x + 1] - p_base;
   CandEntry *E = a.cq_e + e_base;
   uint32_t *P = a.cq_pix + p_base;
-  const int s = cw;  // this warp's ring stage
-  for (uint64_t i = (uint64_t)cw; i < my_tiles; i += (uint64_t)NC) {
+  const int s = cw / CPT, sub = cw % CPT;  // this warp's ring stage, its share of the chunks
+  for (uint64_t i = (uint64_t)s; i < my_tiles; i += (uint64_t)ST) {
     const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
     if (!__all_sync(0xffffffffu, ok)) {
       if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
@@ -1037,11 +1040,15 @@ __global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_co
     const unsigned char *cnt = tb + clist_cnt_offset(nch);
     const uint32_t *base = reinterpret_cast<const uint32_t *>(tb + clist_base_offset(nch));
     const uint32_t *spots = reinterpret_cast<const uint32_t *>(tb + clist_spot_offset(nch));
+    uint32_t turn = 0;  // the k-th chunk that can pass goes to sub-warp k mod CPT
     for (uint32_t j0 = 0; j0 < nch; j0 += 32) {
       unsigned m = __ballot_sync(0xffffffffu, j0 + lane < nch && cmax[j0 + lane] >= need);
       while (m) {
         const uint32_t ch = j0 + (uint32_t)(__ffs(m) - 1);
         m &= m - 1;
+        const bool take = turn == (uint32_t)sub;
+        turn = (turn + 1 == (uint32_t)CPT) ? 0 : turn + 1;
+        if (!take) continue;
         const uint64_t oid = first + ch * 32 + lane;
         const bool valid = oid < a.n;
         const int c = valid ? cnt[ch * 32 + lane] : 0;
@@ -1054,23 +1061,25 @@ __global__ void __launch_bounds__(32 * 13, 1) cell_filter_kernel(const __grid_co
         }
         const uint32_t total = min((uint32_t)__shfl_sync(0xffffffffu, x, 31), 32u * QS);
         const uint32_t *sp = spots + base[ch];
-        // hit bits of the chunk's spots, two 32-spot windows per step
-        for (uint32_t w0 = 0; w0 < total; w0 += 64) {
-          const uint32_t k0 = w0 + lane, k1 = w0 + 32 + lane;
-          bool h0 = false, h1 = false;
-          if (k0 < total) {
-            const uint32_t q = sp[k0] >> sh;
-            h0 = (cm[q >> 5] >> (q & 31u)) & 1u;
+        // hit bits of the chunk's spots, four 32-spot windows per step
+        for (uint32_t w0 = 0; w0 < total; w0 += 128) {
+          bool h[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const uint32_t k = w0 + 32u * (uint32_t)u + (uint32_t)lane;
+            h[u] = false;
+            if (k < total) {
+              const uint32_t q = sp[k] >> sh;
+              h[u] = (cm[q >> 5] >> (q & 31u)) & 1u;
+            }
           }
-          if (k1 < total) {
-            const uint32_t q = sp[k1] >> sh;
-            h1 = (cm[q >> 5] >> (q & 31u)) & 1u;
-          }
-          const unsigned b0 = __ballot_sync(0xffffffffu, h0);
-          const unsigned b1 = __ballot_sync(0xffffffffu, h1);
+          unsigned bw[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) bw[u] = __ballot_sync(0xffffffffu, h[u]);
           if (lane == 0) {
-            wm[w0 >> 5] = b0;
-            if (w0 + 32 < total) wm[(w0 >> 5) + 1] = b1;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+              if (w0 + 32u * (uint32_t)u < total) wm[(w0 >> 5) + (uint32_t)u] = bw[u];
           }
         }
         __syncwarp();
@@ -1252,9 +1261,15 @@ CompareTuning compare_config(int R, const CompareTuning &req) {
   const size_t rb = (size_t)R * 2;
   if (c.variant == 5) {  // cell-mask filter + counting kernel: one filter block per SM
     c.tile_sub = 0;
-    if (c.consumers <= 0) c.consumers = 12;
-    c.consumers = std::min(c.consumers, 12);  // 13 warps: __launch_bounds__ of the kernel
-    c.stages = c.consumers;                   // one ring stage per consumer warp
+    // stages (tiles in flight) and consumer warps, a multiple of them: the
+    // warps of a stage split its tiles' chunks; 25 warps at most
+    // (__launch_bounds__ of the kernel)
+    if (c.stages <= 0) c.stages = 12;
+    c.stages = std::max(1, std::min(c.stages, 16));
+    if (c.consumers <= 0) c.consumers = 2 * c.stages;
+    int cpt = std::max(1, c.consumers / c.stages);
+    while (cpt > 1 && c.stages * cpt > 24) cpt--;
+    c.consumers = c.stages * cpt;
     c.blocks_per_sm = 1;
     c.grid_mult = 1;
     return c;
@@ -1363,11 +1378,13 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
                 "candidate buffer missing");
     LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "filter windows for %d spots per record", a.qS);
     LMB_REQUIRE(!c.test_consumer_wait_us, "the test wait applies to variants 2 and 4");
-    while (c.consumers > 1 &&
-           384 + (size_t)a.cm_bytes +
-                   (size_t)c.consumers * (a.tile_bytes + filter_warp_bytes(a.qS)) > 227 * 1024)
-      c.consumers--;
-    c.stages = c.consumers;
+    // fewer stages (keeping the warps per stage) until the ring fits
+    const int cpt = c.consumers / c.stages;
+    while (c.stages > 1 && 384 + (size_t)a.cm_bytes + (size_t)c.stages * a.tile_bytes +
+                                   (size_t)c.stages * cpt * filter_warp_bytes(a.qS) >
+                               227 * 1024)
+      c.stages--;
+    c.consumers = c.stages * cpt;
     fixed = 384 + a.cm_bytes + (size_t)c.consumers * filter_warp_bytes(a.qS);
   }
   if (c.variant == 4) {

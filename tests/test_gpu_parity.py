@@ -377,7 +377,9 @@ def test_compact_layout_batched_equals_reference_layout():
             for k in range(12):
                 assert got[k][1] == ref[k][1] and np.array_equal(got[k][0], ref[k][0])
         # the two-kernel cell-mask pass (variant 5): filter then count
-        for shape in ({}, {"consumers": 4}, {"consumers": 1}, {"full_gather": 1}):
+        for shape in ({}, {"stages": 6, "consumers": 24}, {"stages": 8, "consumers": 8},
+                      {"stages": 3, "consumers": 6}, {"stages": 1, "consumers": 1},
+                      {"full_gather": 1}):
             for _ in range(2):  # eager, then graph replay (candidate buffer reused)
                 e.set_tuning(variant=5, **shape)
                 e.match(range(12), p.min_nr_spots, p.min_intensity)
