@@ -109,7 +109,7 @@ class ClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.002)
+            time.sleep(0.0001)  # the timed region can be a few ms long
 
     def _run_smi(self):
         proc = subprocess.Popen(
@@ -1747,21 +1747,31 @@ def serve_leg(args, e2=None):
             pool_f32 = [f.astype(np.float32).tobytes() for f in frames]
     key2 = (p2.nr_px_x, p2.nr_px_y)
     out = {"n_orient": N, "mixed": [], "vs_reference": {"ours": [], "reference": []}}
-    port0 = 45000 + (os.getpid() % 200) * 10
     secs = args.serve_seconds
 
+    def free_ports():
+        """Two ports the kernel just handed out as free (fixed numbers can
+        collide with the ephemeral ports of earlier connections)."""
+        import socket
+        socks = [socket.socket() for _ in range(2)]
+        for sk in socks:
+            sk.bind(("127.0.0.1", 0))
+        ports = [sk.getsockname()[1] for sk in socks]
+        for sk in socks:
+            sk.close()
+        return ports
+
     def ours(mode_batch, rates, keys, wire, plain):
-        nonlocal port0
         res = []
         for rate in rates:
-            port0 += 2
+            port0, port1 = free_ports()
             srv = StreamServer([p2, p1], om, hkls, ncpus=os.cpu_count() or 1,
                                max_batch=mode_batch, result_dir=tempfile.mkdtemp(prefix="lmb_sv_"),
-                               port=port0, ext_port=port0 + 1, host="127.0.0.1",
+                               port=port0, ext_port=port1, host="127.0.0.1",
                                log=lambda *a: None, engines=[e2, e1], max_queue=256).start()
             time.sleep(0.3)
             n_total = int(min(args.serve_images, max(50, rate * secs)))
-            r = _serve_run(port0 if plain else port0 + 1, wire, keys, n_total, rate, plain,
+            r = _serve_run(port0 if plain else port1, wire, keys, n_total, rate, plain,
                            srv.done_at)
             st = srv.stop(close_engines=False)
             r.update({"passes": st["passes"], "mean_batch": round(st["mean_batch"], 2)})
