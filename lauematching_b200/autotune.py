@@ -59,11 +59,15 @@ def lookup(R: int, k: int, dense: bool = False) -> dict | None:
 
 
 def candidate_shapes_dense():
-    # the cell-mask pass: one block per SM; consumer warps (at most 12), ring
-    # depth (0 = as deep as fits beside the mask and the hit lists), and
-    # whether the records that can pass are queued or counted in place
-    for q, cons, st in itertools.product((0, 1), (4, 6, 8, 10, 12), (0, 2, 3, 4, 6)):
-        yield dict(variant=4, stages=st, consumers=cons, cell_queue=q)
+    # the two-kernel cell-mask pass (what the automatic variant runs on dense
+    # DBs): ring stages (tiles in flight per SM) and consumer warps, a
+    # multiple of the stages (warps per stage split its tiles' chunks), 24 at
+    # most; then a few shapes of the one-kernel pass for comparison
+    for st, cpt in itertools.product((4, 6, 8, 10, 12, 16), (1, 2, 3, 4)):
+        if st * cpt <= 24:
+            yield dict(variant=5, stages=st, consumers=st * cpt)
+    for q, cons in itertools.product((0, 1), (8, 12)):
+        yield dict(variant=4, consumers=cons, cell_queue=q)
 
 
 def candidate_shapes():
@@ -144,7 +148,9 @@ def main():
             results.append((ms, used, same))
             print(f"K={kb} {used} {ms:.4f} ms identical={same}", file=sys.stderr)
         ok = [r for r in results if r[2]]
-        best = min(ok, key=lambda r: r[0])
+        # the dense entry shapes the pass the automatic variant runs there (5)
+        best = min([r for r in ok if not args.dense or r[1]["variant"] == 5] or ok,
+                   key=lambda r: r[0])
         bytes_pass = args.n_orient * R * 2 + kb * p.nr_px_x * p.nr_px_y
         shape = dict(best[1])
         shape.pop("last_variant", None)
