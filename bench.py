@@ -1761,7 +1761,7 @@ def serve_leg(args, e2=None):
             sk.close()
         return ports
 
-    def ours(mode_batch, rates, keys, wire, plain):
+    def ours(mode_batch, rates, keys, wire, plain, nsend=4):
         res = []
         for rate in rates:
             port0, port1 = free_ports()
@@ -1772,7 +1772,7 @@ def serve_leg(args, e2=None):
             time.sleep(0.3)
             n_total = int(min(args.serve_images, max(50, rate * secs)))
             r = _serve_run(port0 if plain else port1, wire, keys, n_total, rate, plain,
-                           srv.done_at)
+                           srv.done_at, nsend=nsend)
             st = srv.stop(close_engines=False)
             r.update({"passes": st["passes"], "mean_batch": round(st["mean_batch"], 2)})
             res.append(r)
@@ -1788,7 +1788,8 @@ def serve_leg(args, e2=None):
     # same float32 2048^2 frames in the reference's message, both daemons
     ref_rates = [float(r) for r in args.serve_ref_rates.split(",")]
     wire32 = {key2: pool_f32}
-    out["vs_reference"]["ours"] = ours(64, ref_rates, [key2], wire32, plain=True)
+    # 16 MiB frames: eight sending connections, so the client is not the limit
+    out["vs_reference"]["ours"] = ours(64, ref_rates, [key2], wire32, plain=True, nsend=8)
     if O.have_ref_stream():
         per = REC_BYTES_PER_ORIENT + 72
         base = scratch_dir(N * per)
@@ -1816,8 +1817,9 @@ def serve_leg(args, e2=None):
                 t_ready = time.perf_counter() - t0
                 for rate in ref_rates:
                     rs.done.clear()
-                    n_total = int(min(args.serve_images, max(50, rate * secs)))
-                    r = _serve_run(60517, wire32, [key2], n_total, rate, True, rs.done)
+                    # its saturated rate is ~150 images/s: at most 1500 frames per rate
+                    n_total = int(min(args.serve_images, 1500, max(50, rate * secs)))
+                    r = _serve_run(60517, wire32, [key2], n_total, rate, True, rs.done, nsend=8)
                     out["vs_reference"]["reference"].append(r)
                     log(json.dumps(dict(r, daemon="reference")))
                 rc = rs.stop()
@@ -1883,7 +1885,7 @@ def main():
                          "perturbed, top-50 candidates into the c/a refinement; "
                          "dbbuild = the device DB build alone (cold and warm)")
     ap.add_argument("--serve-rates", type=str, default="10,100,500,2000")
-    ap.add_argument("--serve-ref-rates", type=str, default="50,200,500,1000")
+    ap.add_argument("--serve-ref-rates", type=str, default="50,200,1000,2000")
     ap.add_argument("--serve-seconds", type=float, default=2.5)
     ap.add_argument("--serve-images", type=int, default=4000)
     args = ap.parse_args()
