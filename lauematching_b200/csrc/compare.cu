@@ -1023,7 +1023,9 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
   const int need = a.full_gather ? 0 : a.min_spots;
   const int sh = a.cm_shift;
   const uint64_t e_base = a.cq_ebase[blockIdx.x], e_cap = a.cq_ebase[blockIdx.x + 1] - e_base;
+  const uint64_t p_base = a.cq_pbase[blockIdx.x], p_cap = a.cq_pbase[blockIdx.x + 1] - p_base;
   CandEntry *E = a.cq_e + e_base;
+  uint32_t *P = a.cq_pix + p_base;
   const int s = cw / CPT, sub = cw % CPT;  // this warp's ring stage, its share of the chunks
   for (uint64_t i = (uint64_t)s; i < my_tiles; i += (uint64_t)ST) {
     const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
@@ -1038,9 +1040,6 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
     const unsigned char *cnt = tb + clist_cnt_offset(nch);
     const uint32_t *base = reinterpret_cast<const uint32_t *>(tb + clist_base_offset(nch));
     const uint32_t *spots = reinterpret_cast<const uint32_t *>(tb + clist_spot_offset(nch));
-    // word offset of this tile's spot array in the layout (candidates point there)
-    const uint64_t tile_words =
-        ((blockIdx.x + i * G) * (uint64_t)a.tile_bytes + clist_spot_offset(nch)) / 4;
     uint32_t turn = 0;  // the k-th chunk that can pass goes to sub-warp k mod CPT
     for (uint32_t j0 = 0; j0 < nch; j0 += 32) {
       unsigned m = __ballot_sync(0xffffffffu, j0 + lane < nch && cmax[j0 + lane] >= need);
@@ -1098,19 +1097,43 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
         const unsigned cmk = __ballot_sync(0xffffffffu, cand);
         if (cmk) {
           // the warp's places in the block's region: one reservation per chunk
-          uint32_t e0 = 0;
-          if (lane == 0) e0 = atomicAdd(&ctr[0], (uint32_t)__popc(cmk));
-          e0 = __shfl_sync(0xffffffffu, e0, 0);
+          const int mine = cand ? ub : 0;
+          int px = mine;  // inclusive prefix of the candidates' marked spots
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, px, o);
+            if (lane >= o) px += y;
+          }
+          uint32_t e0 = 0, p0 = 0;
+          if (lane == 31) {
+            e0 = atomicAdd(&ctr[0], (uint32_t)__popc(cmk));
+            p0 = atomicAdd(&ctr[1], (uint32_t)px);
+          }
+          e0 = __shfl_sync(0xffffffffu, e0, 31);
+          p0 = __shfl_sync(0xffffffffu, p0, 31);
           if (cand) {
             const uint64_t e = (uint64_t)e0 + (uint64_t)__popc(cmk & lt);
-            if (e < e_cap) {
+            const uint64_t off = (uint64_t)p0 + (uint64_t)(px - mine);
+            if (e < e_cap && off + (uint64_t)ub <= p_cap) {
               CandEntry ce;
               ce.oid = oid;
-              ce.where = ((unsigned long long)c << 56) |
-                         (tile_words + base[ch] + (uint64_t)(x - c));
+              ce.off = (uint32_t)off;
+              ce.n = (uint32_t)ub;
               E[e] = ce;
+              uint32_t k = 0;  // its marked pixels in record order (none when xe == xs)
+              for (uint32_t w = xs >> 5; xe > xs && w <= (xe - 1) >> 5; w++) {
+                unsigned mw = wm[w];
+                const int lo = (int)xs - (int)(w << 5), hi = (int)xe - (int)(w << 5);
+                if (lo > 0) mw &= ~0u << lo;
+                if (hi < 32) mw &= (1u << hi) - 1u;
+                while (mw) {
+                  const int b = __ffs(mw) - 1;
+                  mw &= mw - 1;
+                  P[off + k++] = sp[(w << 5) + (uint32_t)b];
+                }
+              }
             } else {
-              atomicExch(a.err, DEV_BAD_QUEUE);  // a region holds every record: cannot happen
+              atomicExch(a.err, DEV_BAD_QUEUE);  // regions hold every record: cannot happen
             }
           }
         }
@@ -1124,35 +1147,23 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
   __syncwarp();
   if (lane == 0) {
     __threadfence_block();
-    if (atomicAdd(&ctr[2], 1u) == (uint32_t)NC - 1) a.cq_count[blockIdx.x] = atomicAdd(&ctr[0], 0u);
+    if (atomicAdd(&ctr[2], 1u) == (uint32_t)NC - 1) {
+      a.cq_count[2 * blockIdx.x] = atomicAdd(&ctr[0], 0u);
+      a.cq_count[2 * blockIdx.x + 1] = atomicAdd(&ctr[1], 0u);
+    }
   }
 }
 
-// A candidate's spots read back from the compact layout in global memory; a
-// spot on an unmarked cell (zero in every slot of the pass) is skipped like a
-// pixel off the detector, so it is neither gathered nor summed.
-struct MaskedSpots {
-  const uint32_t *sp;
-  const uint32_t *cm;
-  int sh;
-  __device__ __forceinline__ bool pixel(const CmpArgs &, int s, size_t &p) const {
-    const uint32_t v = __ldg(sp + s);
-    p = v;
-    const uint32_t q = v >> sh;
-    return (__ldg(cm + (q >> 5)) >> (q & 31u)) & 1u;
-  }
-};
-
 // The filter's candidates, 32 per warp: the per-record logic of the other
-// variants over each candidate's spots.  blockIdx.y = the filter block whose
-// region is read.
+// variants over each candidate's marked pixels.  blockIdx.y = the filter
+// block whose region is read.
 template <int B>
 __global__ void __launch_bounds__(256) cell_count_kernel(const __grid_constant__ CmpArgs a) {
   const uint32_t b = blockIdx.y;
   const uint64_t cap = a.cq_ebase[b + 1] - a.cq_ebase[b];
-  const uint64_t n = min((uint64_t)a.cq_count[b], cap);
+  const uint64_t n = min((uint64_t)a.cq_count[2 * b], cap);
   const CandEntry *E = a.cq_e + a.cq_ebase[b];
-  const uint32_t *L = reinterpret_cast<const uint32_t *>(a.cl);
+  const uint32_t *P = a.cq_pix + a.cq_pbase[b];
   const int lane = threadIdx.x & 31;
   const uint64_t wpb = blockDim.x >> 5;
   const uint64_t nw = gridDim.x * wpb;
@@ -1160,12 +1171,9 @@ __global__ void __launch_bounds__(256) cell_count_kernel(const __grid_constant__
   for (uint64_t g = (blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; g < n; g += nw * 32) {
     const uint64_t e = g + lane;
     const bool v = e < n;
-    CandEntry ce{0ull, 0ull};
+    CandEntry ce{0ull, 0u, 0u};
     if (v) ce = E[e];
-    const int c = (int)(ce.where >> 56);
-    const uint64_t off = ce.where & ((1ull << 56) - 1ull);
-    process<B, MaskedSpots, 1>(a, MaskedSpots{L + off, a.cellmask, a.cm_shift}, v ? c : 0,
-                               ce.oid, pol_occ, v);
+    process<B, ListSpots, 1>(a, ListSpots{P + ce.off}, v ? (int)ce.n : 0, ce.oid, pol_occ, v);
   }
 }
 
@@ -1366,7 +1374,8 @@ int compare_launch(CmpArgs a, const CompareTuning &req, int num_sms, cudaStream_
     LMB_REQUIRE(a.cellmask && a.cm_bytes > 0 && a.cm_bytes % 128 == 0 &&
                     a.cm_bytes <= kCellMaskBytes && (reinterpret_cast<uintptr_t>(a.cellmask) & 15) == 0,
                 "cell mask missing or malformed");
-    LMB_REQUIRE(a.cq_e && a.cq_ebase && a.cq_count, "candidate buffer missing");
+    LMB_REQUIRE(a.cq_e && a.cq_pix && a.cq_ebase && a.cq_pbase && a.cq_count,
+                "candidate buffer missing");
     LMB_REQUIRE(a.qS >= 1 && a.qS <= a.S, "filter windows for %d spots per record", a.qS);
     LMB_REQUIRE(!c.test_consumer_wait_us, "the test wait applies to variants 2 and 4");
     // fewer stages (keeping the warps per stage) until the ring fits

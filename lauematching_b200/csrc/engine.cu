@@ -77,12 +77,14 @@ struct lmb_engine {
   int cl_state = 0;  // 0 not built, 1 built, -1 this DB cannot use it
   unsigned long long cl_hist[256] = {};  // records per on-detector spot count
   int cl_qs = 0;  // largest on-detector spot count of a record (sizes the pass's queues)
-  // per tile of the compact layout: its chunks (sizes the variant-5
-  // candidate regions: at most every record of a tile)
+  // per tile of the compact layout: its chunks and its spots (sizes the
+  // variant-5 candidate regions: at most every record and spot of a tile)
   std::vector<uint32_t> cl_tile_nch;
-  // variant 5: candidate buffer, per filter block a region of entries (bases
-  // [G+1]), counts written per block
+  std::vector<uint64_t> cl_tile_spots;
+  // variant 5: candidate buffer, per filter block a region of entries and one
+  // of pixels (bases [G+1] each, in one allocation), counts written per block
   CandEntry *d_cq_e = nullptr;
+  uint32_t *d_cq_pix = nullptr;
   uint64_t *d_cq_base = nullptr;
   uint32_t *d_cq_count = nullptr;
   uint32_t cq_blocks = 0;
@@ -149,30 +151,46 @@ namespace {
 
 void free_candidates(lmb_engine *e) {
   cudaFree(e->d_cq_e);
+  cudaFree(e->d_cq_pix);
   cudaFree(e->d_cq_base);
   cudaFree(e->d_cq_count);
   e->d_cq_e = nullptr;
+  e->d_cq_pix = nullptr;
   e->d_cq_base = nullptr;
   e->d_cq_count = nullptr;
   e->cq_blocks = 0;
 }
 
 // The variant-5 candidate buffer for a filter grid of G blocks (block b takes
-// tiles b, b + G, ...): per block room for an entry for every record of its
+// tiles b, b + G, ...): per block room for every record and every spot of its
 // tiles, so the filter cannot run out of room whatever the frames.  Made
 // before the first such pass (never inside a captured pass).
 int ensure_candidates(lmb_engine *e, uint32_t G) {
   if (e->d_cq_e && e->cq_blocks == G) return LMB_OK;
   free_candidates(e);
-  std::vector<uint64_t> eb((size_t)G + 1, 0);
-  for (uint64_t t = 0; t < e->cl_tiles; t++) eb[t % G + 1] += 32ull * e->cl_tile_nch[t];
-  for (uint32_t b = 0; b < G; b++) eb[b + 1] += eb[b];
+  std::vector<uint64_t> base(2 * ((size_t)G + 1), 0);
+  uint64_t *eb = base.data(), *pb = base.data() + G + 1;
+  for (uint64_t t = 0; t < e->cl_tiles; t++) {
+    const uint64_t b = t % G;
+    eb[b + 1] += 32ull * e->cl_tile_nch[t];
+    pb[b + 1] += e->cl_tile_spots[t];
+  }
+  for (uint32_t b = 0; b < G; b++) {
+    eb[b + 1] += eb[b];
+    pb[b + 1] += pb[b];
+  }
+  LMB_REQUIRE(pb[G] < (1ull << 40), "candidate pixel buffer too large");
+  for (uint32_t b = 0; b < G; b++)
+    LMB_REQUIRE(pb[b + 1] - pb[b] < (1ull << 32), "candidate region of block %u too large", b);
   cudaError_t ce = cudaMalloc(&e->d_cq_e, std::max<uint64_t>(eb[G], 1) * sizeof(CandEntry));
-  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_cq_base, eb.size() * sizeof(uint64_t));
-  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_cq_count, (size_t)G * sizeof(uint32_t));
   if (ce == cudaSuccess)
-    ce = cudaMemcpy(e->d_cq_base, eb.data(), eb.size() * sizeof(uint64_t), cudaMemcpyHostToDevice);
-  if (ce == cudaSuccess) ce = cudaMemset(e->d_cq_count, 0, (size_t)G * sizeof(uint32_t));
+    ce = cudaMalloc(&e->d_cq_pix, std::max<uint64_t>(pb[G], 1) * sizeof(uint32_t));
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_cq_base, base.size() * sizeof(uint64_t));
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_cq_count, 2ull * G * sizeof(uint32_t));
+  if (ce == cudaSuccess)
+    ce = cudaMemcpy(e->d_cq_base, base.data(), base.size() * sizeof(uint64_t),
+                    cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemset(e->d_cq_count, 0, 2ull * G * sizeof(uint32_t));
   if (ce != cudaSuccess) {
     free_candidates(e);
     return cuda_fail(ce, "variant-5 candidate buffer", __FILE__, __LINE__);
@@ -198,6 +216,7 @@ void free_engine(lmb_engine *e) {
   cudaFree(e->d_db);
   cudaFree(e->d_cl);
   cudaFree(e->d_cq_e);
+  cudaFree(e->d_cq_pix);
   cudaFree(e->d_cq_base);
   cudaFree(e->d_cq_count);
   cudaFree(e->d_u8);
@@ -522,6 +541,8 @@ int build_compact(lmb_engine *e) {
   e->cl_bytes = total;
   e->cl_state = 1;
   e->cl_tile_nch = tnch;
+  e->cl_tile_spots.assign(nt, 0);
+  for (uint64_t c = 0; c < nch; c++) e->cl_tile_spots[ctile[c]] += cs[c];
   return LMB_OK;
 }
 
@@ -597,7 +618,9 @@ int enqueue_pass(lmb_engine *e, const PassKey &k, bool capturing) {
   }
   if (k.tuning.variant == 5) {
     a.cq_e = e->d_cq_e;
+    a.cq_pix = e->d_cq_pix;
     a.cq_ebase = e->d_cq_base;
+    a.cq_pbase = e->d_cq_base + e->cq_blocks + 1;
     a.cq_count = e->d_cq_count;
     a.cq_blocks = e->cq_blocks;
   }
@@ -1365,7 +1388,7 @@ int lmb_engine_set_tuning(lmb_engine *e, const int32_t *fields, int32_t n_fields
                       &t.cell_stages, &t.cell_queue};
   for (int i = 0; i < n_fields && i < 11; i++) *dst[i] = fields[i];
   LMB_REQUIRE(t.cell_queue == 0 || t.cell_queue == 1, "cell_queue must be 0 or 1");
-  LMB_REQUIRE(t.cell_consumers >= 0 && t.cell_consumers <= 16 && t.cell_stages >= 0 &&
+  LMB_REQUIRE(t.cell_consumers >= 0 && t.cell_consumers <= 24 && t.cell_stages >= 0 &&
                   t.cell_stages <= 16,
               "cell-mask pass shape (%d consumers, %d stages) out of range", t.cell_consumers,
               t.cell_stages);

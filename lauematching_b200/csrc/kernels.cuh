@@ -6,12 +6,12 @@
 
 namespace lmb {
 
-// A record the cell filter kept: its id, and where its spots lie in the
-// compact layout: bits 0-55 the 32-bit word offset of its first spot from the
-// layout's start, bits 56-63 its spot count (at most 255).
+// A record the cell filter kept: its id and its marked pixels (n of them at
+// offset off of its block's pixel region).
 struct CandEntry {
   unsigned long long oid;
-  unsigned long long where;
+  uint32_t off;
+  uint32_t n;
 };
 static_assert(sizeof(CandEntry) == 16, "candidate entry layout");
 
@@ -56,11 +56,14 @@ struct CmpArgs {
   // place, chunk by chunk
   int cell_queue;
   // variant 5: records that can still pass after the cell mask, appended by
-  // the filter kernel to its block's region (entries at cq_e + cq_ebase[b]);
-  // cq_count[b] = entries the block wrote; a region holds every record of
-  // the block's tiles, so it cannot overflow
+  // the filter kernel to its block's region (entries at cq_e + cq_ebase[b],
+  // their marked pixels at cq_pix + cq_pbase[b]); cq_count[2b], [2b + 1] =
+  // entries and pixels the block wrote; the regions hold every record and
+  // spot of the block's tiles, so they cannot overflow
   struct CandEntry *cq_e;
+  uint32_t *cq_pix;
   const uint64_t *cq_ebase;
+  const uint64_t *cq_pbase;
   uint32_t *cq_count;
   uint32_t cq_blocks;  // the filter grid the regions were laid out for
   // filled by compare_launch
