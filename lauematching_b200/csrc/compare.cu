@@ -1096,24 +1096,20 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
         const bool cand = valid && c <= a.qS && ub >= need;
         const unsigned cmk = __ballot_sync(0xffffffffu, cand);
         if (cmk) {
-          // the warp's places in the block's region: one reservation per chunk
-          const int mine = cand ? ub : 0;
-          int px = mine;  // inclusive prefix of the candidates' marked spots
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, px, o);
-            if (lane >= o) px += y;
-          }
+          // the warp's places in the block's region, one reservation per
+          // chunk: an entry per candidate, and pixel room for all the chunk's
+          // spots, so a candidate's pixels go where its spots sit in the chunk
+          // (its count prefix; the room a region holds covers every spot)
           uint32_t e0 = 0, p0 = 0;
-          if (lane == 31) {
+          if (lane == 0) {
             e0 = atomicAdd(&ctr[0], (uint32_t)__popc(cmk));
-            p0 = atomicAdd(&ctr[1], (uint32_t)px);
+            p0 = atomicAdd(&ctr[1], total);
           }
-          e0 = __shfl_sync(0xffffffffu, e0, 31);
-          p0 = __shfl_sync(0xffffffffu, p0, 31);
+          e0 = __shfl_sync(0xffffffffu, e0, 0);
+          p0 = __shfl_sync(0xffffffffu, p0, 0);
           if (cand) {
             const uint64_t e = (uint64_t)e0 + (uint64_t)__popc(cmk & lt);
-            const uint64_t off = (uint64_t)p0 + (uint64_t)(px - mine);
+            const uint64_t off = (uint64_t)p0 + (uint64_t)xs;
             if (e < e_cap && off + (uint64_t)ub <= p_cap) {
               CandEntry ce;
               ce.oid = oid;
