@@ -29,6 +29,7 @@ import argparse
 import json
 import os
 import statistics
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -1642,10 +1643,30 @@ def _serve_client(port, wire, keys, n_total, rate, nsend, plain, sent):
     reference's message (2-byte host-endian image number + the float32 frame
     of the daemon's detector); else the extended header (b"LMB2", image
     number, width, height, dtype 1 = uint8).  sent[i] = time.monotonic() just
-    before image i+1 is sent."""
+    before image i+1 is sent.
+
+    Each distinct frame is written once to a file in shared memory and sent
+    with sendfile (no copy through this process), so the load generator's
+    own copies do not cap the rate the daemons are offered."""
     import socket
     import struct
     import threading as th
+
+    tmp = tempfile.mkdtemp(prefix="lmb_client_",
+                           dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    fds = {}
+    for key, frs in wire.items():
+        for q, fr in enumerate(frs):
+            fn = os.path.join(tmp, f"{key[0]}x{key[1]}_{q}.bin")
+            with open(fn, "wb") as fh:
+                fh.write(fr)
+            fds[(key, q)] = (os.open(fn, os.O_RDONLY), len(fr))
+
+    def send_frame(s, key, q):
+        fd, size = fds[(key, q)]
+        off = 0
+        while off < size:
+            off += os.sendfile(s.fileno(), fd, off, size - off)
 
     def sender(j):
         r2 = np.random.default_rng(100 + j)
@@ -1657,7 +1678,7 @@ def _serve_client(port, wire, keys, n_total, rate, nsend, plain, sent):
             if dt > 0:
                 time.sleep(dt)
             key = keys[int(r2.integers(0, len(keys)))]
-            fr = wire[key][int(r2.integers(0, len(wire[key])))]
+            q = int(r2.integers(0, len(wire[key])))
             num = (i % 65535) + 1
             sent[i] = time.monotonic()
             # header and frame as two sends (no 16 MiB concatenation per message)
@@ -1665,13 +1686,18 @@ def _serve_client(port, wire, keys, n_total, rate, nsend, plain, sent):
                 s.sendall(num.to_bytes(2, sys.byteorder))
             else:
                 s.sendall(struct.pack("<4sHHHBB", b"LMB2", num, key[0], key[1], 1, 0))
-            s.sendall(fr)
+            send_frame(s, key, q)
         s.close()
-    ts = [th.Thread(target=sender, args=(j,)) for j in range(nsend)]
-    for t in ts:
-        t.start()
-    for t in ts:
-        t.join()
+    try:
+        ts = [th.Thread(target=sender, args=(j,)) for j in range(nsend)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+    finally:
+        for fd, _ in fds.values():
+            os.close(fd)
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def _serve_run(port, wire, keys, n_total, rate, plain, done_at, nsend=4, wait_s=120.0):
@@ -1716,7 +1742,7 @@ def serve_leg(args, e2=None):
     import oracle as O
     from lauematching_b200 import formats, synth, params as P
     from lauematching_b200.engine import Engine
-    from lauematching_b200.stream import StreamServer
+    from lauematching_b200.stream import PINNED_BYTES, FramePool, StreamServer
     txt2, _ = workload_params(args.min_intensity)
     p2 = P.parse_params_text(txt2 + "MinGoodSpots 5\n", binary="stream")
     txt1 = txt2.replace("NrPxX 2048", "NrPxX 1024").replace("NrPxY 2048", "NrPxY 1024")
@@ -1768,7 +1794,8 @@ def serve_leg(args, e2=None):
             srv = StreamServer([p2, p1], om, hkls, ncpus=os.cpu_count() or 1,
                                max_batch=mode_batch, result_dir=tempfile.mkdtemp(prefix="lmb_sv_"),
                                port=port0, ext_port=port1, host="127.0.0.1",
-                               log=lambda *a: None, engines=[e2, e1], max_queue=256).start()
+                               log=lambda *a: None, engines=[e2, e1], max_queue=256,
+                               frame_pool=frames).start()
             time.sleep(0.3)
             n_total = int(min(args.serve_images, max(50, rate * secs)))
             r = _serve_run(port0 if plain else port1, wire, keys, n_total, rate, plain,
@@ -1779,6 +1806,10 @@ def serve_leg(args, e2=None):
             log(json.dumps(r))
         return res
 
+    # receive buffers kept across the daemon runs (page-locked up to the
+    # daemon's budget: those frames go to the device over the copy engine)
+    frames = FramePool(PINNED_BYTES)
+    out["receive_buffers"] = {"page_locked_bytes": PINNED_BYTES, "dense_share": 1.0}
     rates = [float(r) for r in args.serve_rates.split(",")]
     keys = list(pool)
     for mode, mb in (("batched", 64), ("one_image_per_pass", 1)):
@@ -1840,6 +1871,7 @@ def serve_leg(args, e2=None):
         if isinstance(lst, list) else 0.0  # noqa: E731
     out["vs_reference"]["saturation_images_per_s"] = {
         "ours": sat(out["vs_reference"]["ours"]), "reference": sat(out["vs_reference"]["reference"])}
+    frames.close()
     e1.close()
     if own2:
         e2.close()

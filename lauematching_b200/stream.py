@@ -62,6 +62,7 @@ MAX_CONNECTIONS = 10
 MAX_QUEUE = 32
 EXT_MAGIC = b"LMB2"
 RCVBUF = 32 << 20
+PINNED_BYTES = 2 << 30  # page-locked receive buffers (the rest are ordinary memory)
 EXT_HEADER = struct.Struct("<4sHHHBB")
 _SURV_DTYPE = np.dtype([("id", "<u8"), ("n_spots", "<i4"), ("sum_u8", "<i4"),
                         ("tot_int", "<f8"), ("score", "<f8")])
@@ -101,22 +102,76 @@ class FramePool:
     """Receive buffers reused across messages, per (pixel count, dtype): a
     fresh 16 MiB array per frame costs its page faults on every message.  A
     buffer goes back to the pool when its image is finished (or dropped);
-    arrays the pool did not make are ignored on return."""
+    arrays the pool did not make are ignored on return.
 
-    def __init__(self):
+    Up to ``pinned_bytes`` of the float32 buffers (the reference's wire
+    frames, 16 MiB at 2048^2) are page-locked: the engine sends such frames to
+    the device over the copy engine (its dense share) instead of scanning them
+    on host threads, which leaves the host's cores to the socket receives.
+    uint8 frames stay in ordinary memory: their host scan is cheap and sends
+    only the positive pixels.  Buffers beyond the budget are ordinary memory."""
+
+    def __init__(self, pinned_bytes=0, pin_dtypes=(np.float32,)):
+        self._pin_dtypes = {np.dtype(d).str for d in pin_dtypes}
         self._lock = threading.Lock()
         self._free: dict = collections.defaultdict(list)
         self._mine: set = set()
+        self._pinned_left = int(pinned_bytes)
+        self._keep: list = []  # the page-locked allocations, alive as long as the pool
+        self._made: dict = {}  # buffers made per (pixel count, dtype)
+
+    def _alloc(self, n, dtype):
+        nb = int(n) * np.dtype(dtype).itemsize
+        with self._lock:
+            pin = np.dtype(dtype).str in self._pin_dtypes and nb <= self._pinned_left
+            if pin:
+                self._pinned_left -= nb
+        if pin:
+            from .engine import PinnedBuffer
+            try:
+                pb = PinnedBuffer((int(n),), dtype)
+            except Exception:  # no page-locked memory to be had: ordinary buffer
+                with self._lock:
+                    self._pinned_left += nb
+            else:
+                with self._lock:
+                    self._keep.append(pb)
+                return pb.array
+        return np.empty(int(n), dtype)
+
+    def prefill(self, n, dtype, count):
+        """Make up to ``count`` buffers of n pixels of dtype ahead of the
+        first frames (page-locking costs milliseconds per buffer)."""
+        k = (int(n), np.dtype(dtype).str)
+        with self._lock:
+            have = self._made.get(k, 0)
+        for _ in range(max(0, int(count) - have)):
+            a = self._alloc(n, dtype)
+            with self._lock:
+                self._mine.add(id(a))
+                self._made[k] = self._made.get(k, 0) + 1
+                self._free[k].append(a)
 
     def get(self, n, dtype):
         k = (int(n), np.dtype(dtype).str)
         with self._lock:
             if self._free[k]:
                 return self._free[k].pop()
-        a = np.empty(int(n), dtype)
+        a = self._alloc(n, dtype)
         with self._lock:
             self._mine.add(id(a))
+            self._made[k] = self._made.get(k, 0) + 1
         return a
+
+    def close(self):
+        """Free the page-locked buffers (after the last frame is finished)."""
+        with self._lock:
+            keep, self._keep = self._keep, []
+            self._free.clear()
+            self._mine.clear()
+            self._made.clear()
+        for pb in keep:
+            pb.free()
 
     def put(self, a):
         if a is None:
@@ -152,7 +207,8 @@ class StreamServer:
     def __init__(self, params_list, orients, hkls, ncpus=1, max_batch=64, device=0,
                  result_dir=None, port=PORT, ext_port=EXT_PORT, host="0.0.0.0",
                  log=print, max_queue=MAX_QUEUE, engines=None, preprocess_cfgs=None,
-                 free_bytes=None):
+                 free_bytes=None, pinned_bytes=PINNED_BYTES, dense_share=1.0,
+                 frame_pool=None):
         from . import _lib, formats
         from .engine import Engine
         self.log = log
@@ -201,7 +257,14 @@ class StreamServer:
         for g in self.geoms.values():
             g.free = list(range(self.max_batch))[::-1]
         self.queue: queue.Queue = queue.Queue(maxsize=max_queue)
-        self.frames = FramePool()
+        # receive buffers: page-locked up to pinned_bytes; that share of them
+        # goes to the device over the copy engine (dense_share of the
+        # engines), the others through the host scan
+        # (frame_pool: a caller's pool, kept across servers; the caller closes it)
+        self._own_frames = frame_pool is None
+        self.frames = FramePool(pinned_bytes) if frame_pool is None else frame_pool
+        for g in self.geoms.values():
+            g.engine.set_dense_share(dense_share)
         self._backlog = collections.deque()
         self.done_q: queue.Queue = queue.Queue()
         self.running = False
@@ -449,6 +512,11 @@ class StreamServer:
 
     # ---- lifecycle --------------------------------------------------------------
     def start(self, listen=True):
+        # receive buffers of the primary detector's float32 wire frames made
+        # before the first message: as many as can wait in the queue and in
+        # two passes' slots (the page-locked budget caps it)
+        W, H = int(self.primary.nr_px_x), int(self.primary.nr_px_y)
+        self.frames.prefill(W * H, np.float32, self.queue.maxsize + 2 * self.max_batch)
         self.running = True
         if listen:
             self._accept_threads = [
@@ -490,6 +558,10 @@ class StreamServer:
         for g in self.geoms.values():
             if g.pool is not None:
                 g.pool.close()
+        if self._gpu.is_alive() or any(t.is_alive() for t in self._wr):
+            self.log("stop: images still in flight; receive buffers kept")
+        elif self._own_frames:
+            self.frames.close()
         if close_engines:
             for g in self.geoms.values():
                 g.engine.close()

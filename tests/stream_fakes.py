@@ -25,6 +25,9 @@ class FakeEngine:
         self.passes = []   # slots of every pass
         self.inflight = 0
 
+    def set_dense_share(self, share):
+        self.dense_share = share
+
     def load_images(self, slots, frames):
         with self.lock:
             self.frames += [np.array(f, copy=True) for f in frames]
@@ -54,4 +57,5 @@ def make_server(tmp_dir, port, ext_port, engine, nr_px=(64, 64), max_batch=4, ma
     return StreamServer([p], np.zeros((1, 9)), np.zeros((1, 3), np.int32), ncpus=1,
                         max_batch=max_batch, result_dir=str(tmp_dir), port=port,
                         ext_port=ext_port, host="127.0.0.1", log=lambda *a: None,
-                        engines=[engine], max_queue=max_queue, free_bytes=1 << 34)
+                        engines=[engine], max_queue=max_queue, free_bytes=1 << 34,
+                        pinned_bytes=0)
