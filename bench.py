@@ -1917,7 +1917,7 @@ def main():
                          "perturbed, top-50 candidates into the c/a refinement; "
                          "dbbuild = the device DB build alone (cold and warm)")
     ap.add_argument("--serve-rates", type=str, default="10,100,500,2000")
-    ap.add_argument("--serve-ref-rates", type=str, default="50,200,1000,2000")
+    ap.add_argument("--serve-ref-rates", type=str, default="50,200,1000,4000")
     ap.add_argument("--serve-seconds", type=float, default=2.5)
     ap.add_argument("--serve-images", type=int, default=4000)
     args = ap.parse_args()
