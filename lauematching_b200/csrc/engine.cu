@@ -442,13 +442,40 @@ int try_sparse(lmb_engine *e, const T *px, int slot, int dtype, bool *sparse) {
   return LMB_OK;
 }
 
+// Automatic variant.  Each spot the pass gathers costs the same in both
+// layouts; what the compact layout saves is the stream of the records'
+// padding.  Measured on B200 at 1e8 records (two detector geometries, K=64),
+// the compact pass is as fast or faster while the records that can pass
+// (at least min_spots on-detector spots) hold up to ~3 spots per DB record
+// on average, and up to 1.4x slower beyond (dense records, where the
+// reference records' stream is no longer the cost).
+constexpr double kAutoGather = 3.0;
+// the cell-mask pass the automatic variant runs beyond that
+constexpr int kAutoCellVariant = 5;
+
+double gathered_per_record(const lmb_engine *e, int min_spots) {
+  const int m = std::max(0, min_spots);
+  double g = 0;
+  for (int c = m; c < 256; c++) g += (double)c * (double)e->cl_hist[c];
+  return e->n ? g / (double)e->n : 0.0;
+}
+
+// Tile size of the compact layout of a dense DB (one whose passes run the
+// cell-mask filter): a dozen ring stages of it fit beside the 128 KiB cell
+// mask, and a tile holds an even number of chunks at ~15 spots per record,
+// so the two warps of a stage split it evenly (measured on B200 at 1e8
+// records, K = 64: 3.72 ms per pass against 4.1-5.4 ms with 4-10 KiB tiles
+// at the same warp count, 3.70 ms with 12 KiB tiles and three warps per stage).
+constexpr uint64_t kCellTileBytes = 8192;
+
 // One pass: status reset, compare, ordering, status copy-back, on e->st.
 // Derive the compact layout of the resident DB (see clist.cu): spots per
 // 32-record chunk on the device; on the host, the tile size (about 64 chunks
 // of the DB's average size, 4-24 KiB, at least the largest chunk) and a
 // greedy packing of consecutive chunks into tiles; then the tiles on the
-// device.
-int build_compact(lmb_engine *e) {
+// device.  min_spots: MinNrSpots of the pass that asks for the layout; a DB
+// dense at that threshold gets the cell-mask filter's tile size.
+int build_compact(lmb_engine *e, int min_spots) {
   e->cl_state = -1;
   if (e->S > 255 || e->n == 0) return LMB_OK;  // counts are uint8
   const uint64_t n = e->n, nch = (n + 31) / 32;
@@ -481,7 +508,11 @@ int build_compact(lmb_engine *e) {
   auto round128 = [](uint64_t b) { return ((b + 127) / 128) * 128; };
   const uint64_t avg_chunk = 36 + (4 * total_spots + nch - 1) / nch;
   uint64_t TB = std::min<uint64_t>(24 * 1024, std::max<uint64_t>(4096, round128(64 * avg_chunk)));
-  {
+  if (gathered_per_record(e, min_spots) > kAutoGather) {
+    // the automatic variant will run the cell-mask filter over it: its tile
+    // size, whatever the tuning of this pass
+    TB = kCellTileBytes;
+  } else {
     // room for the pass shape's blocks (three consumer warps, a two-stage
     // ring; six per SM, or up to eight when the tuning asks for more) on an
     // SM, when the largest chunk allows it
@@ -546,23 +577,6 @@ int build_compact(lmb_engine *e) {
   return LMB_OK;
 }
 
-// Automatic variant.  Each spot the pass gathers costs the same in both
-// layouts; what the compact layout saves is the stream of the records'
-// padding.  Measured on B200 at 1e8 records (two detector geometries, K=64),
-// the compact pass is as fast or faster while the records that can pass
-// (at least min_spots on-detector spots) hold up to ~3 spots per DB record
-// on average, and up to 1.4x slower beyond (dense records, where the
-// reference records' stream is no longer the cost).
-constexpr double kAutoGather = 3.0;
-// the cell-mask pass the automatic variant runs beyond that
-constexpr int kAutoCellVariant = 5;
-
-double gathered_per_record(const lmb_engine *e, int min_spots) {
-  const int m = std::max(0, min_spots);
-  double g = 0;
-  for (int c = m; c < 256; c++) g += (double)c * (double)e->cl_hist[c];
-  return e->n ? g / (double)e->n : 0.0;
-}
 
 // The cell-mask pass needs its mask, a hit list per consumer warp and a
 // two-stage ring of the layout's tiles in one block's shared memory.
@@ -1157,7 +1171,7 @@ int lmb_match(lmb_engine *e, uint64_t slot_mask, int32_t min_nr_spots, double mi
   CompareTuning tun = e->tuning;
   if (tun.variant >= 2) {  // compact layout: derive it once per DB
     if (e->cl_state == 0) {
-      rc = build_compact(e);
+      rc = build_compact(e, min_nr_spots);
       if (rc) return rc;
     }
     // variant 3 (automatic): the compact layout alone while the records that
