@@ -598,6 +598,78 @@ def tilted_leg(args, dev, K=64, n=None):
     return out
 
 
+def volume_leg(args, e, rec, dev, K=16, min_ints=(50.0, 30.0), post_images=4):
+    """Survivor volume downstream of the pass (the MinIntensity that gives
+    1e3-1e4 survivors per image).  Frames of the bench geometry with the
+    Poisson background kept (no threshold: every pixel is positive, so every
+    record with >= MinNrSpots on-detector spots reaches the intensity test),
+    K of them in one pass over the resident 1e8 DB; per MinIntensity: the
+    pass (compare and ordering kernels), the download of the K sorted lists,
+    the host post-stage of a few images (merge on the device from 1024
+    candidates, evaluate-once refinement, text), and one frame's survivors
+    against the oracle over all records."""
+    from lauematching_b200 import post, synth
+    rng = np.random.default_rng(77)
+    frames = []
+    for _ in range(K):
+        g = synth.pick_grains(rec, int(rng.integers(1, 21)), 5, rng)
+        frames.append(synth.render_image(rec[g], e.params.nr_px_x, e.params.nr_px_y, rng,
+                                         threshold=None).astype(np.uint8))
+    hk = synth.hkls_cubic(8)
+    slots = list(range(K))
+    out = {"workload": f"{K} uint8 2048x2048 frames with the Poisson(5) background kept "
+                       f"(U{{1..20}} fcc grains each) vs the {e.n_orient:,}-orientation DB, "
+                       "MinNrSpots 5", "runs": []}
+    for mi in min_ints:
+        _, p = workload_params(mi)
+        for k in slots:
+            e.load_image(k, frames[k], want_scale=False)
+        for _ in range(3):
+            e.match(slots, p.min_nr_spots, p.min_intensity)
+            e.results_batch(slots)
+        cmp_ms, order_ms, step_ms, dl_ms = [], [], [], []
+        for _ in range(max(3, min(args.steps, 10))):
+            t0 = time.perf_counter()
+            e.match(slots, p.min_nr_spots, p.min_intensity)
+            res = e.results_batch(slots)
+            step_ms.append((time.perf_counter() - t0) * 1e3)
+            c, o = e.last_pass_ms()[:2]
+            cmp_ms.append(c)
+            order_ms.append(o)
+        t0 = time.perf_counter()
+        res = e.results_batch(slots)
+        dl_ms.append((time.perf_counter() - t0) * 1e3)
+        surv = [int(res[k][0].shape[0]) for k in slots]
+        om_sparse = np.zeros((e.n_orient, 9))
+        post_ms, uniq = [], []
+        for k in slots[:post_images]:
+            sv, npass = res[k]
+            u = np.unique(sv["id"]).astype(np.int64)
+            om_sparse[u] = synth.shoemake_orientations(0, args.seed, ids=u)
+            ids, sc = post.collected_matches(sv, npass)
+            t0 = time.perf_counter()
+            _, _, nu = post.post_process(p, e.geometry, om_sparse, ids, sc,
+                                         frames[k].astype(np.float32), hk,
+                                         num_threads=os.cpu_count() or 1, merge_device=dev)
+            post_ms.append((time.perf_counter() - t0) * 1e3)
+            uniq.append(int(nu))
+        del om_sparse
+        run = {"min_intensity": mi,
+               "survivors_per_image": {"min": min(surv), "max": max(surv),
+                                       "mean": round(statistics.mean(surv), 1)},
+               "compare_ms": round(statistics.median(cmp_ms), 4),
+               "order_kernel_ms": round(statistics.median(order_ms), 4),
+               "match_and_download_ms": round(statistics.median(step_ms), 3),
+               "results_download_ms": round(dl_ms[0], 3),
+               "results_bytes": int(sum(r.nbytes for r, _ in res.values())),
+               "post_stage_ms_per_image": [round(x, 1) for x in post_ms],
+               "unique_grains_per_image": uniq}
+        if not args.no_parity:
+            run["survivor_parity"] = survivor_parity(e, p, frames[0])[0]
+        out["runs"].append(run)
+    return out
+
+
 def dbbuild_leg(args, dev):
     """The device DB build alone: n device-generated orientations (seed 1)
     forward-simulated with the 1240 fcc HKLs, on the bench's beam-normal
@@ -1407,6 +1479,8 @@ def run_ours(args, rank, world):
         out["tilted"] = guarded("tilted", lambda: tilted_leg(args, dev, K=K))
     if "hex" in legs:
         out["hex"] = guarded("hex", lambda: hex_leg(args, dev))
+    if "volume" in legs:
+        out["survivor_volume"] = guarded("volume", lambda: volume_leg(args, e, rec_head, dev))
     if "serve" in legs:
         out["serving"] = guarded("serve", lambda: serve_leg(args, e))
     for pb in pins:
@@ -1907,9 +1981,9 @@ def main():
     ap.add_argument("--refine", action="store_true",
                     help="only the batched refinement leg (device against host threads)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (Poisson arrivals)")
-    ap.add_argument("--legs", type=str, default="tilted,hex,serve",
+    ap.add_argument("--legs", type=str, default="tilted,hex,volume,serve",
                     help="legs of the other configurations run after the headline one "
-                         "(comma list of tilted, hex, serve; empty for none)")
+                         "(comma list of tilted, hex, volume, serve; empty for none)")
     ap.add_argument("--leg", choices=["tilted", "hex", "dbbuild"], default=None,
                     help="only one leg of the bench: tilted = the batched pass at the "
                          "reference's tilted 34-ID-E detector (~15 spots per record); "

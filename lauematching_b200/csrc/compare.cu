@@ -1198,6 +1198,53 @@ __device__ __forceinline__ void bitonic(unsigned long long *keys, uint32_t P) {
   }
 }
 
+// One compare-exchange step of the bitonic network over the pairs (lo, lo +
+// stride) of keys[0, m), m a power of two; `base` is keys[0]'s index in the
+// whole sequence, which decides each pair's direction for this `size`.
+__device__ __forceinline__ void bitonic_step(unsigned long long *keys, uint32_t m, uint32_t base,
+                                             uint32_t size, uint32_t stride) {
+  for (uint32_t i = threadIdx.x; i < (m >> 1); i += blockDim.x) {
+    const uint32_t lo = 2 * i - (i & (stride - 1));
+    const uint32_t hi = lo + stride;
+    const bool asc = ((base + lo) & size) == 0;
+    const unsigned long long x = keys[lo], y = keys[hi];
+    if ((x > y) == asc) {
+      keys[lo] = y;
+      keys[hi] = x;
+    }
+  }
+  __syncthreads();
+}
+
+// The bitonic network of bitonic() over P > kSmemSortMax keys in global
+// memory (P a power of two), with every stage whose pairs lie within one
+// tile of kSmemSortMax keys run on that tile in shared memory: the tiles are
+// sorted there first (sizes up to the tile), and each larger size runs its
+// strides of a tile or more over global memory and then the smaller strides
+// tile by tile.  Same comparisons as bitonic(), so the same order; global
+// passes per size log2(size / tile) instead of log2(size).
+__device__ void bitonic_tiled(unsigned long long *g, uint32_t P, unsigned long long *sk) {
+  constexpr uint32_t T = kSmemSortMax;
+  for (uint32_t t0 = 0; t0 < P; t0 += T) {
+    for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) sk[i] = g[t0 + i];
+    __syncthreads();
+    for (uint32_t size = 2; size <= T; size <<= 1)
+      for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) bitonic_step(sk, T, t0, size, stride);
+    for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) g[t0 + i] = sk[i];
+    __syncthreads();
+  }
+  for (uint32_t size = 2 * T; size <= P; size <<= 1) {
+    for (uint32_t stride = size >> 1; stride >= T; stride >>= 1) bitonic_step(g, P, 0, size, stride);
+    for (uint32_t t0 = 0; t0 < P; t0 += T) {
+      for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) sk[i] = g[t0 + i];
+      __syncthreads();
+      for (uint32_t stride = T >> 1; stride > 0; stride >>= 1) bitonic_step(sk, T, t0, size, stride);
+      for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) g[t0 + i] = sk[i];
+      __syncthreads();
+    }
+  }
+}
+
 __global__ void __launch_bounds__(1024) order_kernel(OrderArgs a) {
   extern __shared__ __align__(16) unsigned long long sk[];  // kSmemSortMax keys
   const int k = a.slots[blockIdx.x];
@@ -1210,7 +1257,10 @@ __global__ void __launch_bounds__(1024) order_kernel(OrderArgs a) {
   for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
     keys[i] = (i < n) ? ((src[i].id << 24) | i) : ~0ull;
   __syncthreads();
-  bitonic(keys, P);
+  if (P <= kSmemSortMax)
+    bitonic(keys, P);
+  else
+    bitonic_tiled(keys, P, sk);
   lmb_survivor *dst = a.out + (size_t)k * a.cap;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[keys[i] & 0xFFFFFFull];
 }

@@ -390,6 +390,36 @@ def test_compact_layout_batched_equals_reference_layout():
         assert e.layout_info()["compact"] == 1
 
 
+@pytest.mark.parametrize("n_rec", [30000, 150000])
+def test_long_survivor_lists_are_ordered_like_the_oracle(n_rec):
+    """Lists far longer than the ordering kernel's shared-memory tile (8192
+    keys): ~21k and ~100k survivors in one slot, so the tile-wise network
+    runs two and four size levels beyond the tile; ids ascending as the
+    reference collects them (LaueMatchingCPU.c:781-788)."""
+    txt = synth.params_text(nr_px=(256, 256), max_nr_spots=7, min_nr_spots=1,
+                            min_intensity=1.0)
+    p = P.parse_params_text(txt)
+    rng = np.random.default_rng(n_rec)
+    rec = np.zeros((n_rec, 15), np.uint16)
+    rec[:, 0] = rng.integers(0, 8, n_rec)
+    rec[:, 1::2] = rng.integers(0, 256, (n_rec, 7))
+    rec[:, 2::2] = rng.integers(0, 256, (n_rec, 7))
+    img = np.where(rng.random(256 * 256) < 0.4, rng.integers(1, 256, 256 * 256), 0)
+    img = img.astype(np.float64)
+    ref = O.compare(rec, p.max_nr_spots, img, p.nr_px_x, p.nr_px_y, p.min_nr_spots,
+                    p.min_intensity)
+    assert ref.ids.shape[0] > 2 * 8192
+    with engine_for(p) as e:
+        e.upload_db(rec)
+        for slot in (0, 37):
+            e.load_image(slot, img)
+        e.match([0, 37], p.min_nr_spots, p.min_intensity)
+        for slot in (0, 37):
+            got, npass = e.results(slot)
+            assert npass == ref.n_pass
+            assert_same_survivors(got, ref)
+
+
 def test_survivor_overflow_is_reported():
     c = golden_case("tilted_dense")
     p = c.params
