@@ -249,6 +249,17 @@ int batch_sparse_load_launch(const SparseFrameDesc *d_desc, int nframes, uint32_
 
 
 static constexpr uint64_t kWaitNs = 2000000000ull;  // bounded TMA waits: 2 s
+
+// Stage and round of consecutive tiles of a ring of ST stages (tile i sits in
+// stage i % ST of round i / ST), advanced by step <= ST tiles without a 64-bit
+// division per tile.
+__device__ __forceinline__ void ring_next(int &st, uint32_t &rd, int ST, int step = 1) {
+  st += step;
+  if (st >= ST) {
+    st -= ST;
+    rd++;
+  }
+}
 static constexpr int kGather = 8;                    // spots gathered per group
 static constexpr int kSumGroup = 4;                  // pixel values loaded per group
 static constexpr int kDirect = 16;  // compact pass: a chunk with this many passable records is
@@ -616,10 +627,11 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
     if (lane != 0) return;
     const uint64_t pol_db = l2_evict_first();
     uint64_t issued = 0;
-    for (uint64_t i = 0; i < my_tiles; i++) {
-      const int s = (int)(i % ST);
-      if (i >= (uint64_t)ST &&
-          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+    int ps = 0;
+    uint32_t pr = 0;
+    for (uint64_t i = 0; i < my_tiles; i++, ring_next(ps, pr, ST)) {
+      const int s = ps;
+      if (pr > 0 && !mbar_wait_bounded(&empty[s], (pr - 1) & 1u, kWaitNs)) {
         atomicExch(a.err, DEV_TIMEOUT_TMA);
         break;
       }
@@ -629,8 +641,13 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
                     &full[s], pol_db);
       issued = i + 1;
     }
-    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
-      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    {
+      const uint64_t j0 = issued > (uint64_t)ST ? issued - ST : 0;
+      int ds = (int)(j0 % ST);
+      uint32_t dr = (uint32_t)(j0 / ST);
+      for (uint64_t j = j0; j < issued; j++, ring_next(ds, dr, ST))
+        mbar_wait_bounded(&full[ds], dr & 1u, kWaitNs);
+    }
     return;
   }
   const int cw = warp - 1;
@@ -655,11 +672,13 @@ __global__ void __launch_bounds__(MINB > 1 ? 128 : 576, MINB)
     qn = 0;
   };
   uint32_t turn = 0;  // the consumer warp that takes the next chunk
-  for (uint64_t i = 0; i < my_tiles; i++) {
-    const int s = (int)(i % ST);
+  int cs = 0;
+  uint32_t cr = 0;
+  for (uint64_t i = 0; i < my_tiles; i++, ring_next(cs, cr, ST)) {
+    const int s = cs;
     const bool ok = a.test_consumer_wait_ns
                         ? mbar_wait_bounded(&full[15], 0, a.test_consumer_wait_ns)
-                        : mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+                        : mbar_wait_bounded(&full[s], cr & 1u, kWaitNs);
     if (!__all_sync(0xffffffffu, ok)) {
       if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
       return;
@@ -995,10 +1014,11 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
     if (lane != 0) return;
     const uint64_t pol_db = l2_evict_first();
     uint64_t issued = 0;
-    for (uint64_t i = 0; i < my_tiles; i++) {
-      const int s = (int)(i % ST);
-      if (i >= (uint64_t)ST &&
-          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+    int ps = 0;
+    uint32_t pr = 0;
+    for (uint64_t i = 0; i < my_tiles; i++, ring_next(ps, pr, ST)) {
+      const int s = ps;
+      if (pr > 0 && !mbar_wait_bounded(&empty[s], (pr - 1) & 1u, kWaitNs)) {
         atomicExch(a.err, DEV_TIMEOUT_TMA);
         break;
       }
@@ -1010,8 +1030,13 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
       if (i + ST < my_tiles) bulk_prefetch_l2(a.cl + (t + ST * G) * a.tile_bytes, a.tile_bytes);
       issued = i + 1;
     }
-    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
-      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    {
+      const uint64_t j0 = issued > (uint64_t)ST ? issued - ST : 0;
+      int ds = (int)(j0 % ST);
+      uint32_t dr = (uint32_t)(j0 / ST);
+      for (uint64_t j = j0; j < issued; j++, ring_next(ds, dr, ST))
+        mbar_wait_bounded(&full[ds], dr & 1u, kWaitNs);
+    }
     return;
   }
   const int cw = warp - 1;
@@ -1027,8 +1052,9 @@ __global__ void __launch_bounds__(32 * 25, 1) cell_filter_kernel(const __grid_co
   CandEntry *E = a.cq_e + e_base;
   uint32_t *P = a.cq_pix + p_base;
   const int s = cw / CPT, sub = cw % CPT;  // this warp's ring stage, its share of the chunks
-  for (uint64_t i = (uint64_t)s; i < my_tiles; i += (uint64_t)ST) {
-    const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+  uint32_t rd = 0;  // round of tile i (i / ST)
+  for (uint64_t i = (uint64_t)s; i < my_tiles; i += (uint64_t)ST, rd++) {
+    const bool ok = mbar_wait_bounded(&full[s], rd & 1u, kWaitNs);
     if (!__all_sync(0xffffffffu, ok)) {
       if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
       break;
