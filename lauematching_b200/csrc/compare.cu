@@ -545,10 +545,11 @@ __global__ void __launch_bounds__(576, 1) compare_ws_kernel(const __grid_constan
     if (lane != 0) return;
     const uint64_t pol_db = l2_evict_first();
     uint64_t issued = 0;
-    for (uint64_t i = 0; i < my_full; i++) {
-      const int s = (int)(i % ST);
-      if (i >= (uint64_t)ST &&
-          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+    int ps = 0;
+    uint32_t pr = 0;
+    for (uint64_t i = 0; i < my_full; i++, ring_next(ps, pr, ST)) {
+      const int s = ps;
+      if (pr > 0 && !mbar_wait_bounded(&empty[s], (pr - 1) & 1u, kWaitNs)) {
         atomicExch(a.err, DEV_TIMEOUT_TMA);
         break;
       }
@@ -560,20 +561,27 @@ __global__ void __launch_bounds__(576, 1) compare_ws_kernel(const __grid_constan
       issued = i + 1;
     }
     // stay until the last copies have landed (bounded)
-    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
-      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    {
+      const uint64_t j0 = issued > (uint64_t)ST ? issued - ST : 0;
+      int ds = (int)(j0 % ST);
+      uint32_t dr = (uint32_t)(j0 / ST);
+      for (uint64_t j = j0; j < issued; j++, ring_next(ds, dr, ST))
+        mbar_wait_bounded(&full[ds], dr & 1u, kWaitNs);
+    }
     return;
   }
   const int cw = warp - 1;
   const int g = cw / TS, sub = cw % TS;
   if (g >= NG) return;
   const uint64_t pol_occ = l2_evict_last();
-  for (uint64_t i = g; i < my_tiles; i += NG) {
+  int cs = g;  // stage and round of tile i (g < NG <= ST; stages are a multiple of NG)
+  uint32_t cr = 0;
+  for (uint64_t i = g; i < my_tiles; i += NG, ring_next(cs, cr, ST, NG)) {
     const uint64_t tile = blockIdx.x + i * G;
     const uint64_t oid = tile * a.tile + (uint64_t)sub * 32 + lane;
     if (i < my_full) {
-      const int s = (int)(i % ST);
-      const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+      const int s = cs;
+      const bool ok = mbar_wait_bounded(&full[s], cr & 1u, kWaitNs);
       if (!__all_sync(0xffffffffu, ok)) {
         if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
         return;
@@ -822,10 +830,11 @@ __global__ void __launch_bounds__(32 * 13, 1) compare_cell_kernel(const __grid_c
     if (lane != 0) return;
     const uint64_t pol_db = l2_evict_first();
     uint64_t issued = 0;
-    for (uint64_t i = 0; i < my_tiles; i++) {
-      const int s = (int)(i % ST);
-      if (i >= (uint64_t)ST &&
-          !mbar_wait_bounded(&empty[s], (uint32_t)(((i / ST) - 1) & 1), kWaitNs)) {
+    int ps = 0;
+    uint32_t pr = 0;
+    for (uint64_t i = 0; i < my_tiles; i++, ring_next(ps, pr, ST)) {
+      const int s = ps;
+      if (pr > 0 && !mbar_wait_bounded(&empty[s], (pr - 1) & 1u, kWaitNs)) {
         atomicExch(a.err, DEV_TIMEOUT_TMA);
         break;
       }
@@ -835,8 +844,13 @@ __global__ void __launch_bounds__(32 * 13, 1) compare_cell_kernel(const __grid_c
                     &full[s], pol_db);
       issued = i + 1;
     }
-    for (uint64_t j = issued > (uint64_t)ST ? issued - ST : 0; j < issued; j++)
-      mbar_wait_bounded(&full[j % ST], (uint32_t)((j / ST) & 1), kWaitNs);
+    {
+      const uint64_t j0 = issued > (uint64_t)ST ? issued - ST : 0;
+      int ds = (int)(j0 % ST);
+      uint32_t dr = (uint32_t)(j0 / ST);
+      for (uint64_t j = j0; j < issued; j++, ring_next(ds, dr, ST))
+        mbar_wait_bounded(&full[ds], dr & 1u, kWaitNs);
+    }
     return;
   }
   const int cw = warp - 1;
@@ -867,11 +881,13 @@ __global__ void __launch_bounds__(32 * 13, 1) compare_cell_kernel(const __grid_c
   const int need = a.full_gather ? 0 : a.min_spots;
   const int sh = a.cm_shift;
   uint32_t turn = 0;
-  for (uint64_t i = 0; i < my_tiles; i++) {
-    const int s = (int)(i % ST);
+  int cs = 0;
+  uint32_t cr = 0;
+  for (uint64_t i = 0; i < my_tiles; i++, ring_next(cs, cr, ST)) {
+    const int s = cs;
     const bool ok = a.test_consumer_wait_ns
                         ? mbar_wait_bounded(&full[15], 0, a.test_consumer_wait_ns)
-                        : mbar_wait_bounded(&full[s], (uint32_t)((i / ST) & 1), kWaitNs);
+                        : mbar_wait_bounded(&full[s], cr & 1u, kWaitNs);
     if (!__all_sync(0xffffffffu, ok)) {
       if (lane == 0) atomicExch(a.err, DEV_TIMEOUT_TMA);
       return;
