@@ -128,13 +128,17 @@ __global__ void dbbuild_kernel(const double *__restrict__ om, uint64_t n,
   float4 *sh_hklf = reinterpret_cast<float4 *>(smem + kHklChunk * sizeof(int4));
   uint32_t *sh_list = reinterpret_cast<uint32_t *>(smem + kHklChunk * 2 * sizeof(int4));
   int *sh_cnt = reinterpret_cast<int *>(sh_list + (size_t)g.S * TB);
+  // per warp, the pairs that passed the screen and wait for FP64: lane << 16 | HKL
+  uint32_t *q = reinterpret_cast<uint32_t *>(sh_cnt + TB) + (threadIdx.x >> 5) * (2 * 32);
 
   const int t = threadIdx.x;
+  const int lane = t & 31;
+  const unsigned lt = (1u << lane) - 1u;
   const uint64_t base = (uint64_t)blockIdx.x * TB;
   const uint64_t oid = base + t;
   const bool valid = oid < n;
 
-  double T[9];
+  double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   float Tf[9];
   if (valid) {
     double m[9];
@@ -153,6 +157,34 @@ __global__ void dbbuild_kernel(const double *__restrict__ om, uint64_t n,
   }
   int cnt = 0;
   bool done = !valid || g.S <= 0;
+  // The FP64 evaluations of the first m queued pairs (m <= 32), one per lane
+  // with the owner's matrix, then their outcomes in queue order: each owner
+  // takes its own in HKL order (dedup, append, stop at S) exactly as it
+  // would have evaluating them one by one.
+  auto evaluate = [&](int m) {
+    const uint32_t ent = lane < m ? q[lane] : 0u;
+    const int o = lane < m ? (int)(ent >> 16) : lane;
+    double To[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) To[j] = __shfl_sync(0xffffffffu, T[j], o);
+    int ix = 0, iy = 0;
+    const bool ok = lane < m && exact_spot(To, sh_hkl[ent & 0xFFFFu], g, ix, iy);
+    const uint32_t key = (uint32_t)(ix & 0xFFFF) | ((uint32_t)(iy & 0xFFFF) << 16);
+    const unsigned okm = __ballot_sync(0xffffffffu, ok);
+    for (int e = 0; e < m; e++) {
+      const int oe = __shfl_sync(0xffffffffu, o, e);
+      const uint32_t ke = __shfl_sync(0xffffffffu, key, e);
+      if (lane == oe && ((okm >> e) & 1u) && !done) {
+        bool dup = false;
+        for (int s = 0; s < cnt; s++) dup |= (sh_list[(size_t)s * TB + t] == ke);
+        if (!dup) {
+          sh_list[(size_t)cnt * TB + t] = ke;
+          done = (++cnt == g.S);
+        }
+      }
+    }
+    __syncwarp();
+  };
   for (int c0 = 0; c0 < nh; c0 += kHklChunk) {
     const int cn = min(kHklChunk, nh - c0);
     __syncthreads();
@@ -162,24 +194,34 @@ __global__ void dbbuild_kernel(const double *__restrict__ om, uint64_t n,
       sh_hklf[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
     }
     __syncthreads();
-    // Warp-uniform loop: no break/continue, so lanes that took the (rare)
-    // FP64 path reconverge with the others at the end of every HKL.
+    // Warp-uniform loop over the chunk: every lane screens its orientation
+    // against HKL i in FP32; the pairs that pass join the warp's queue in
+    // HKL order, and every 32 of them are evaluated in FP64 on all lanes at
+    // once (a lane that has reached S spots queues nothing more; pairs it
+    // queued before its last spot are evaluated and dropped).
+    int qn = 0;
     for (int i = 0; i < cn; i++) {
       bool go = !done;
       if (!kExactAll && go) go = screen(Tf, sh_hklf[i], g);
-      if (go) {
-        int ix = 0, iy = 0;
-        if (exact_spot(T, sh_hkl[i], g, ix, iy)) {
-          const uint32_t key = (uint32_t)(ix & 0xFFFF) | ((uint32_t)(iy & 0xFFFF) << 16);
-          bool dup = false;
-          for (int s = 0; s < cnt; s++) dup |= (sh_list[(size_t)s * TB + t] == key);
-          if (!dup) {
-            sh_list[(size_t)cnt * TB + t] = key;
-            done = (++cnt == g.S);
-          }
+      const unsigned bm = __ballot_sync(0xffffffffu, go);
+      if (bm) {
+        if (go) q[qn + __popc(bm & lt)] = ((uint32_t)lane << 16) | (uint32_t)i;
+        qn += __popc(bm);
+        if (qn >= 32) {
+          __syncwarp();
+          evaluate(32);
+          const int rest = qn - 32;  // < 32: move the tail to the front
+          const uint32_t v = lane < rest ? q[32 + lane] : 0u;
+          __syncwarp();
+          if (lane < rest) q[lane] = v;
+          __syncwarp();
+          qn = rest;
         }
       }
+    }
+    if (qn) {  // the chunk's last pairs, before its HKLs leave shared memory
       __syncwarp();
+      evaluate(qn);
     }
     if (__syncthreads_and(done)) break;
   }
@@ -333,7 +375,8 @@ static int build_block(int S) {
 
 size_t dbbuild_smem_bytes(int S) {
   const int tb = build_block(S);
-  return kHklChunk * 2 * sizeof(int4) + (size_t)S * tb * 4 + (size_t)tb * 4;
+  // HKL chunk (int and float copies), pixel lists, counts, per-warp queues of 64
+  return kHklChunk * 2 * sizeof(int4) + (size_t)S * tb * 4 + (size_t)tb * 4 + (size_t)tb * 8;
 }
 
 int dbbuild_launch(const double *d_om, uint64_t n, const int4 *d_hkl, int nh,
