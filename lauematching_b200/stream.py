@@ -202,7 +202,13 @@ def _recv_exact(sock, buf, running):
 
 
 class StreamServer:
-    """The daemon, usable in-process (tests, benchmarks) or from the CLI."""
+    """The daemon, usable in-process (tests, benchmarks) or from the CLI.
+
+    pinned_bytes: page-locked budget of the receive buffers (float32 frames);
+    dense_share: the share of page-locked frames each engine sends over the
+    copy engine (set on the engines, including engines passed in, for as long
+    as they live); frame_pool: a FramePool kept across servers (its owner
+    closes it), else the server makes and frees its own."""
 
     def __init__(self, params_list, orients, hkls, ncpus=1, max_batch=64, device=0,
                  result_dir=None, port=PORT, ext_port=EXT_PORT, host="0.0.0.0",
